@@ -1,0 +1,341 @@
+"""Throughput benchmark of the Monte Carlo update engine on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl engine|reference]
+
+Workload (default): 2D Ising ferromagnet, periodic square lattice L = 16384
+(2.68e8 int8 spins), J = 1 (reference sign J = -1), h = 0, beta_c =
+0.44068679, random initial state; one step = one elementary MC step of
+`--nmetro` checkerboard Metropolis sweeps (no clusters).  Metric:
+Metropolis spin-updates per ns, whole job.  With N GPUs (torchrun) every
+rank runs its own replica (replica id = rank): weak scaling, no collective on
+the data path; the timed region is bracketed by barriers and the slowest
+rank's time counts.
+
+Keys beyond the base contract:
+  e2e          the same metric through the C-ABI call a user makes
+               (mqv_emcs with a host observable buffer), the initial state
+               uploaded from pinned host memory inside the timed region;
+  e2e_host_state  the drop-in-on-host-data variant: every step uploads the
+               whole state from pinned host memory and reads it back;
+  roofline     the fused sweep kernel against measured HBM bandwidth;
+  cpu_baseline the reference's own Metropolis templates (random-site order,
+               RNGCache<mt19937_64>) on one host core, bounded sample;
+  clocks       SM clocks and throttle reasons sampled (NVML) during timing.
+
+`--impl reference` times the reference CPU path instead: one replica per host
+thread (the reference's thread farm), rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "Metropolis spin-updates/ns + Wolff spins/ns on 1 B200; batched vs plain"
+UNIT = "spin-updates/ns"
+BETA_C = 0.44068679
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=50)
+    p.add_argument("--warmup", type=int, default=5)
+    p.add_argument("--impl", choices=["engine", "reference"], default="engine")
+    p.add_argument("--L", type=int, default=16384)
+    p.add_argument("--nmetro", type=int, default=20, help="sweeps per step (one EMCS)")
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+# ---------------------------------------------------------------------------
+# clocks (NVML reads only)
+
+class ClockSampler:
+    REASONS = {
+        0x1: "gpu_idle", 0x2: "applications_clocks_setting", 0x4: "sw_power_cap", 0x8: "hw_slowdown",
+        0x10: "sync_boost", 0x20: "sw_thermal_slowdown", 0x40: "hw_thermal_slowdown",
+        0x80: "hw_power_brake_slowdown", 0x100: "display_clock_setting",
+    }
+
+    def __init__(self, index: int, period: float = 0.01):
+        self.index = index
+        self.period = period
+        self.samples = []
+        self.reasons = set()
+        self._stop = threading.Event()
+        self.ok = False
+        self.max_mhz = None
+        try:
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(index)
+            self.max_mhz = pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM)
+            self.ok = True
+        except Exception:
+            self.ok = False
+
+    def _run(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+                r = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for bit, name in self.REASONS.items():
+                    if r & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            time.sleep(self.period)
+
+    def __enter__(self):
+        if self.ok:
+            self.t = threading.Thread(target=self._run, daemon=True)
+            self.t.start()
+        return self
+
+    def __exit__(self, *exc):
+        if self.ok:
+            self._stop.set()
+            self.t.join()
+
+    def summary(self):
+        if not self.ok:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvml unavailable"], "samples": 0}
+        reasons = sorted(self.reasons - {"gpu_idle"})
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None,
+                "sm_max_mhz": self.max_mhz, "reasons": reasons, "samples": len(self.samples)}
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            d = json.load(fh)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profiled_traffic(kernel: str):
+    """DRAM bytes per launch from the committed ncu summary, if any."""
+    path = os.path.join(ROOT, "profiles", "traffic.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh).get(kernel)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# reference arm
+
+def run_reference(args, ws, rank):
+    if rank != 0:
+        return 0
+    from oracle.build import build_ref
+    from oracle.oracle import RefHarness
+    if build_ref() is None and not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmarqov_ref.so")):
+        print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
+        return 0
+    ref = RefHarness()
+    L = args.L
+    n = L * L
+    cores = os.cpu_count() or 1
+    try:
+        import psutil
+        avail = psutil.virtual_memory().available
+        cores = max(1, min(cores, int(0.5 * avail // (n + (1 << 20)))))
+    except Exception:
+        pass
+    nup = max(1, n // 256)  # random-site updates per replica per step
+    farm = ref.farm(L, BETA_C, cores, seed=2024)
+    for _ in range(args.warmup):
+        farm.step(nup)
+    t = 0.0
+    for _ in range(args.steps):
+        t += farm.step(nup)
+    farm.close()
+    value = cores * nup * args.steps / (t * 1e9)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "int8",
+        "data": "synthetic",
+        "config": {"workload": f"2D Ising L={L} Metropolis (reference random-site order)", "L": L,
+                   "beta": BETA_C, "replicas": cores, "updates_per_replica_per_step": nup},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
+                         "sample": f"{cores} replicas x {nup} random-site updates per step on L={L}, "
+                                   f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# engine arm
+
+def cpu_baseline(L):
+    from oracle.oracle import RefHarness
+    ref = RefHarness()
+    n = L * L
+    nup = n // 2
+    farm = ref.farm(L, BETA_C, 1, seed=77)
+    t = farm.step(nup)
+    farm.close()
+    return {"value": nup / (t * 1e9), "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{nup} random-site updates (half a sweep) of one L={L} replica, "
+                      f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>, {t:.1f} s"}
+
+
+def run_engine(args, ws, rank, local):
+    import torch
+    import torch.distributed as dist
+
+    import marqov_b200 as M
+    from marqov_b200 import _lib
+
+    torch.cuda.set_device(local)
+    if ws > 1:
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+
+    def barrier():
+        if ws > 1:
+            dist.barrier()
+
+    def max_over_ranks(x: float) -> float:
+        if ws == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    L = args.L
+    n = L * L
+    cfg = M.Config(seed=20240601, repid=rank, ncluster=0, nmetro=args.nmetro, device=local)
+    core = M.makeCore(M.RegularHypercubic(L, 2), cfg, M.Ising(-1.0), BETA_C)
+    stream = torch.cuda.Stream()
+    core.set_stream(stream.cuda_stream)
+
+    # initial configuration on the host, uploaded from pinned memory
+    rng = np.random.default_rng(1000 + rank)
+    host = torch.from_numpy(np.where(rng.random(n) > 0.5, 1, -1).astype(np.int8)).pin_memory()
+    core.state = host.numpy()
+
+    lib = _lib.load()
+    h = core.handle
+    for _ in range(args.warmup):
+        _lib.check(lib.mqv_metropolis(h, args.nmetro))
+    torch.cuda.synchronize()
+
+    # ---- device-timed region: K steps of nmetro fused sweeps
+    l0 = core.launches
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with ClockSampler(local) as clk:
+        barrier()
+        torch.cuda.synchronize()
+        ev0.record(stream)
+        for _ in range(args.steps):
+            _lib.check(lib.mqv_metropolis(h, args.nmetro))
+        ev1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = core.launches - l0
+    ms = ev0.elapsed_time(ev1)
+    ms_max = max_over_ranks(ms)
+    updates = n * args.nmetro * args.steps
+    value = ws * updates / (ms_max * 1e6)
+
+    # ---- end to end through the public call, host buffers
+    obs = torch.zeros(4, dtype=torch.float64).pin_memory()
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    core.state = host.numpy()
+    for _ in range(args.steps):
+        _lib.check(lib.mqv_emcs(h, 1, 0, args.nmetro, obs.data_ptr(), None))
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    e2e = {"value": ws * updates / (e2e_s * 1e9), "unit": UNIT,
+           "h2d_bytes_per_step": n // args.steps, "d2h_bytes_per_step": 32,
+           "note": "initial state uploaded once from pinned host memory inside the timed region "
+                   "(bytes amortised over the steps); each step is one mqv_emcs call returning the "
+                   "step's observables (32 B) to a pinned host buffer"}
+
+    # ---- drop-in on host data: whole state both ways every step
+    back = torch.empty(n, dtype=torch.int8).pin_memory()
+    ksteps = max(1, min(args.steps, 10))
+    barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(ksteps):
+        _lib.check(lib.mqv_set_state(h, host.data_ptr(), n))
+        _lib.check(lib.mqv_metropolis(h, args.nmetro))
+        _lib.check(lib.mqv_get_state(h, back.data_ptr(), n))
+    hs_s = max_over_ranks(time.perf_counter() - t0)
+    e2e_host = {"value": ws * n * args.nmetro * ksteps / (hs_s * 1e9), "unit": UNIT,
+                "h2d_bytes_per_step": n, "d2h_bytes_per_step": n, "steps": ksteps}
+
+    core.close()
+    peak, peak_kind = measured_peaks()
+    per_launch_s = ms * 1e-3 / (args.steps * args.nmetro)
+    alg_bytes = 2 * n  # one int8 read + one int8 write per site update
+    achieved = alg_bytes / per_launch_s / 1e9
+    tr = profiled_traffic("ising2d_fused")
+    roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+            "traffic": None if tr is None else tr.get("bytes_per_launch"),
+            "kernel": "ising2d_fused<256,32>", "peak_source": f"{peak_kind} hbm_gbs",
+            "algorithmic_bytes_per_launch": alg_bytes}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms_max / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "int8", "data": "synthetic",
+        "config": {"workload": f"2D Ising L={L} Metropolis checkerboard sweeps", "L": L, "beta": BETA_C,
+                   "sweeps_per_step": args.nmetro, "parallelism": f"replicas ({ws} x 1 per GPU)",
+                   "l2": "inputs larger than L2: two 268 MB int8 state buffers (ping-pong)"},
+        "e2e": e2e, "e2e_host_state": e2e_host, "roofline": roof, "gpu_launches": launches,
+        "clocks": clk.summary(),
+    }
+    if rank == 0 and ws == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline(L)
+        except Exception as exc:  # the baseline is informative; keep the GPU line
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                                    "sample": f"unavailable: {exc}"}
+    if rank == 0:
+        print(json.dumps(line))
+    if ws > 1:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    ws, rank, local = dist_env()
+    if args.impl == "reference":
+        return run_reference(args, ws, rank)
+    return run_engine(args, ws, rank, local)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,189 @@
+/*
+ * marqov_b200 -- C ABI of the B200 Monte Carlo update engine.
+ *
+ * The engine runs MARQOV's elementary Monte Carlo step -- Wolff embedded
+ * clusters followed by Metropolis sweeps -- on one GPU, with the state resident
+ * in device memory.  Hosts that speak MARQOV's plugin API (Hamiltonian terms,
+ * lattice neighbours, Metropolis / Wolff / Embedder specialisations) lower
+ * their model and lattice into the plain descriptors below; every entry point
+ * takes plain pointers and sizes and returns an int32 status.
+ *
+ * Reference interfaces replaced (file:line in the MARQOV source tree):
+ *   mqv_create        MARQOV::makeCore            src/libmarqov/core.h:1223-1246
+ *                     (Core constructor           src/libmarqov/core.h:469-530)
+ *   mqv_init_state    Core::init / initstatespace src/libmarqov/core.h:829-834,
+ *                                                 src/hamiltonian/Ising.h:99-107
+ *   mqv_metropolis    the Metropolis sweeps of    src/libmarqov/emcs.h:91-106
+ *                     Metropolis<H,L>::move       src/libmarqov/metropolis.h:88-126
+ *   mqv_wolff         the cluster loop of         src/libmarqov/emcs.h:77-89
+ *                     Wolff<H,L>::move            src/libmarqov/wolff.h:72-126
+ *   mqv_emcs          EMCS<H,L>::move + measure   src/libmarqov/emcs.h:69-109,
+ *                                                 src/libmarqov/core.h:1001-1028
+ *   mqv_measure       Energy / Magnetization      src/hamiltonian/util/observables.h:47-65,331-352
+ *   mqv_get_state /   the state space and its     src/libmarqov/core.h:249-342
+ *   mqv_set_state     checkpoint dump             src/libmarqov/core.h:543-607
+ *   mqv_last_error    exit(-1)/throw paths        src/libmarqov/metropolishelpers.h:297-302,
+ *                                                 src/libmarqov/core.h:336-340
+ *
+ * Conventions: status 0 is success; no exception crosses the ABI; the library
+ * owns device memory and the caller owns the host buffers it passes; a handle
+ * is bound to one CUDA stream and is not thread safe, while distinct handles
+ * may be used from distinct host threads (one MARQOV Core per thread).
+ */
+#ifndef MARQOV_B200_H
+#define MARQOV_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#if defined(__GNUC__)
+#define MQV_API __attribute__((visibility("default")))
+#else
+#define MQV_API
+#endif
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef int32_t mqv_status;
+
+enum {
+    MQV_OK = 0,
+    MQV_ERR_INVALID_ARG = 1,      /* bad argument or size */
+    MQV_ERR_UNSUPPORTED_TERM = 2, /* model / term shape the engine does not lower */
+    MQV_ERR_BAD_DESCRIPTOR = 3,   /* inconsistent lattice or model descriptor */
+    MQV_ERR_CUDA = 4,             /* CUDA runtime error (message in mqv_last_error) */
+    MQV_ERR_TIMEOUT = 5,          /* a bounded device wait gave up */
+    MQV_ERR_CHECKSUM = 6,         /* checkpoint / state checksum mismatch */
+    MQV_ERR_NO_DEVICE = 7,        /* no usable CUDA device */
+    MQV_ERR_OUT_OF_MEMORY = 8,    /* device allocation failed */
+    MQV_ERR_STATE = 9             /* call out of order (e.g. run before init) */
+};
+
+/* Model kinds: the reference Hamiltonians the engine lowers. */
+enum {
+    MQV_MODEL_ISING = 1,        /* Ising<int>: int8 +-1, flip proposal, Wolff<Ising<int>> (exact -expm1) */
+    MQV_MODEL_ISING_EMBED = 2,  /* Ising<int8_t>: generic Wolff + default Embedder */
+    MQV_MODEL_POTTS = 3,        /* Potts<Q>: int8 0..Q-1, flex delta term k */
+    MQV_MODEL_BLUME_CAPEL = 4,  /* BlumeCapel: int8 -1/0/+1, Spin1 proposal, onsite h = D */
+    MQV_MODEL_EA = 5,           /* EdwardsAndersonIsing: Ising with lattice bonds */
+    MQV_MODEL_HEISENBERG = 6,   /* Heisenberg: float 3-vectors */
+    MQV_MODEL_PHI4 = 7,         /* scalar phi^4: float, onsite h = mass/beta, h2 = lambda/beta */
+    MQV_MODEL_XXZ = 8           /* XXZ: float 3-vectors, z coupling weighted by delta */
+};
+
+/* Metropolis proposal (Initializer<H>::newsv). */
+enum {
+    MQV_PROPOSAL_DEFAULT = 0,   /* the model's reference initializer */
+    MQV_PROPOSAL_SMALL_CAP = 1  /* O(3): uniform in the cap cos(angle) >= cap around the old spin */
+};
+
+typedef struct mqv_model_desc {
+    int32_t kind;      /* MQV_MODEL_* */
+    int32_t q;         /* Potts states (2..64) */
+    int32_t proposal;  /* MQV_PROPOSAL_* */
+    int32_t reserved;
+    double J;          /* interaction coefficient, reference sign: dE = J dot(s_new - s_old, sum_nbrs) */
+    double h;          /* first onsite coefficient */
+    double h2;         /* second onsite coefficient */
+    double k;          /* flex (multisite) coefficient */
+    double delta;      /* XXZ anisotropy */
+    double cap;        /* proposal width: small-cap cos(half-angle), or phi^4 shift amplitude */
+} mqv_model_desc;
+
+/* Lattice kinds. */
+enum {
+    MQV_LATTICE_HYPERCUBIC = 1, /* FixedDimRegularHypercubic<d>: periodic, even len, stencil path */
+    MQV_LATTICE_CSR = 2         /* any lattice with nbrs(): CSR neighbours (+ optional bnds) */
+};
+
+typedef struct mqv_lattice_desc {
+    int32_t kind;              /* MQV_LATTICE_* */
+    int32_t dim;               /* hypercubic dimension (1..4) */
+    int32_t len;               /* hypercubic side length */
+    int32_t n;                 /* CSR: number of sites */
+    const int32_t* row_ptr;    /* CSR: n+1 offsets (host memory, copied) */
+    const int32_t* col_idx;    /* CSR: neighbour ids in nbrs(0,i) order (host, copied) */
+    const int8_t* bonds;       /* optional per-entry bond weights (bnds), symmetric */
+    const int32_t* colours;    /* optional proper colouring; NULL = greedy colouring */
+} mqv_lattice_desc;
+
+/* Run flags. */
+enum {
+    MQV_FLAG_PER_COLOUR = 1  /* always use one launch per colour class (no fused two-colour tiles) */
+};
+
+typedef struct mqv_run_params {
+    double beta;       /* inverse temperature */
+    uint64_t seed;     /* Philox key */
+    uint32_t replica;  /* replica id (24 bits), part of every counter */
+    int32_t device;    /* CUDA device ordinal */
+    uint32_t flags;    /* MQV_FLAG_* */
+    uint32_t reserved;
+} mqv_run_params;
+
+/* Per-measurement observables (FP64): energy per site, |m|, m^2, m^4. */
+typedef struct mqv_obs {
+    double e, m, m2, m4;
+} mqv_obs;
+
+typedef struct mqv_sim mqv_sim;
+
+MQV_API const char* mqv_version(void);
+/* Number of CUDA devices visible to the engine (0 on a machine without GPUs). */
+MQV_API mqv_status mqv_device_count(int32_t* count);
+/* Copies the calling thread's last error message (NUL-terminated). */
+MQV_API mqv_status mqv_last_error(char* buf, size_t len);
+
+MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_desc* lattice,
+                              const mqv_run_params* params, mqv_sim** out);
+MQV_API mqv_status mqv_destroy(mqv_sim* sim);
+
+/* Bind the handle to a caller stream (cudaStream_t passed as void*). */
+MQV_API mqv_status mqv_set_stream(mqv_sim* sim, void* stream);
+MQV_API mqv_status mqv_get_stream(mqv_sim* sim, void** stream);
+MQV_API mqv_status mqv_set_beta(mqv_sim* sim, double beta);
+MQV_API mqv_status mqv_set_model(mqv_sim* sim, const mqv_model_desc* model);
+
+/* Random initial state from the INIT stream (reference initstatespace rules). */
+MQV_API mqv_status mqv_init_state(mqv_sim* sim);
+/* Host copy of the state in the reference layout: site-major, symd
+ * components per site; int8 for integer models, float32 otherwise. */
+MQV_API mqv_status mqv_get_state(mqv_sim* sim, void* host, size_t bytes);
+MQV_API mqv_status mqv_set_state(mqv_sim* sim, const void* host, size_t bytes);
+/* Device pointer of the current state (valid until the next engine call). */
+MQV_API mqv_status mqv_state_device_ptr(mqv_sim* sim, void** dev, size_t* bytes);
+MQV_API mqv_status mqv_state_bytes(mqv_sim* sim, size_t* bytes);
+
+/* Sweep / cluster counters: together with (seed, replica) they are the whole
+ * random-number state, so checkpoint = state + counters. */
+MQV_API mqv_status mqv_get_counters(mqv_sim* sim, uint64_t* sweep, uint64_t* cluster);
+MQV_API mqv_status mqv_set_counters(mqv_sim* sim, uint64_t sweep, uint64_t cluster);
+
+/* nsweeps colour-ordered Metropolis sweeps (asynchronous on the handle's stream). */
+MQV_API mqv_status mqv_metropolis(mqv_sim* sim, int32_t nsweeps);
+/* nclusters Wolff clusters; sizes (host, may be NULL) receives each size
+ * (synchronises when sizes != NULL). */
+MQV_API mqv_status mqv_wolff(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
+/* n_emcs elementary MC steps (ncluster clusters then nmetro sweeps each),
+ * measuring after every step.  obs (host, may be NULL) receives n_emcs
+ * records; mean_cluster (host, may be NULL) receives n_emcs mean sizes. */
+MQV_API mqv_status mqv_emcs(mqv_sim* sim, int32_t n_emcs, int32_t ncluster, int32_t nmetro,
+                            mqv_obs* obs, double* mean_cluster);
+/* Observables of the current state. */
+MQV_API mqv_status mqv_measure(mqv_sim* sim, mqv_obs* out);
+MQV_API mqv_status mqv_synchronize(mqv_sim* sim);
+/* Number of engine kernel launches issued by this handle so far. */
+MQV_API mqv_status mqv_launch_count(mqv_sim* sim, uint64_t* count);
+
+/* Self test: Philox blocks for n counters (c0 = i, other words given) computed
+ * on the device by the engine and by cuRAND's Philox4_32_10; out_engine and
+ * out_curand receive 4n words each (host). */
+MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3,
+                                       int32_t n, uint32_t* out_engine, uint32_t* out_curand);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* MARQOV_B200_H */

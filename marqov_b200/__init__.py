@@ -1,0 +1,21 @@
+"""marqov_b200 -- MARQOV's Monte Carlo update hot path on NVIDIA B200 (sm_100a).
+
+Metropolis colour sweeps and Wolff embedded clusters run as CUDA kernels
+behind a C ABI (include/marqov_b200.h, libmarqov_b200.so in this package);
+this package is the host side that mirrors MARQOV's Hamiltonian / lattice /
+Core interface.  Importing it loads the engine library; there is no CPU path.
+"""
+from . import _lib
+from ._lib import MarqovError
+from .core import Config, Core, makeCore
+from .hamiltonians import (BlumeCapel, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising, Phi4, Potts,
+                           XXZAntiferro)
+from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
+                       RegularRandomBond, read_graph_csv)
+
+_lib.load()
+
+__all__ = ["Config", "Core", "makeCore", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
+           "Potts", "BlumeCapel", "Heisenberg", "XXZAntiferro", "Phi4", "CSRLattice",
+           "FixedDimRegularHypercubic", "RegularHypercubic", "RegularRandomBond", "RandomGeometricGraph2D",
+           "read_graph_csv"]

@@ -1,0 +1,219 @@
+"""GPU simulation core mirroring ``MARQOV::Core`` (src/libmarqov/core.h:372-1167).
+
+``makeCore(lattice, config, ham, beta)`` plays the part of
+``makeCore<L,H>(std::tuple<L&, Config, std::tuple<beta, HArgs...>>)``
+(core.h:1223-1246); ``Core`` exposes ``init``, ``wrmploop``, ``gameloop`` and
+``elementaryMCstep`` (core.h:829-834, 1001-1050; emcs.h:111-119) over one
+engine handle.  The state lives on the GPU; observables come back per EMCS.
+"""
+from __future__ import annotations
+
+import ctypes as C
+from dataclasses import dataclass, field
+
+import numpy as np
+
+from . import _lib as L
+from .hamiltonians import Hamiltonian
+from .lattices import Lattice
+
+
+@dataclass
+class Config:
+    """``MARQOV::Config`` (core.h:74-192): method parameters."""
+    outpath: str = ""
+    id: int = 0
+    repid: int = 0
+    seed: int = 0
+    nsteps: int = 250
+    warmupsteps: int = 100
+    gameloopsteps: int = 200
+    ncluster: int = 20
+    nmetro: int = 10
+    device: int = 0
+    # force one launch per colour class (no fused two-colour tiles)
+    per_colour: bool = False
+
+    def setid(self, i):
+        self.id = i
+        return self
+
+    def setrepid(self, r):
+        self.repid = r
+        return self
+
+    def setseed(self, s):
+        self.seed = s
+        return self
+
+    def setwarmupsteps(self, w):
+        self.warmupsteps = w
+        return self
+
+    def setgameloopsteps(self, g):
+        self.gameloopsteps = g
+        return self
+
+    def setncluster(self, n):
+        self.ncluster = n
+        return self
+
+    def setnmetro(self, n):
+        self.nmetro = n
+        return self
+
+
+@dataclass
+class TimeSeries:
+    e: list = field(default_factory=list)
+    m: list = field(default_factory=list)
+    m2: list = field(default_factory=list)
+    m4: list = field(default_factory=list)
+    clustersize: list = field(default_factory=list)
+
+    def arrays(self):
+        return {k: np.asarray(v) for k, v in vars(self).items()}
+
+
+class Core:
+    def __init__(self, lattice: Lattice, config: Config, ham: Hamiltonian, beta: float):
+        lib = L.load()
+        self.lattice = lattice
+        self.config = config
+        self.ham = ham
+        self.beta = float(beta)
+        self._lib = lib
+        self._h = C.c_void_p()
+        md = ham.desc(self.beta)
+        ld = lattice.desc()
+        rp = L.RunParams(beta=self.beta, seed=int(config.seed) & (2 ** 64 - 1),
+                         replica=int(config.repid), device=int(config.device),
+                         flags=L.FLAG_PER_COLOUR if config.per_colour else 0)
+        L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
+        self.n = int(lattice.size())
+        self.symd = ham.SymD
+        self.dtype = ham.dtype
+        self.obs = TimeSeries()
+        self.step = 0
+
+    # -- lifecycle
+    def close(self):
+        if self._h:
+            self._lib.mqv_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self) -> C.c_void_p:
+        return self._h
+
+    # -- reference Core API
+    def init(self):
+        """Random initial state (Core::init -> initstatespace)."""
+        L.check(self._lib.mqv_init_state(self._h))
+
+    def elementaryMCstep(self) -> float:
+        """One EMCS (emcs.h:69-109); returns the mean cluster size."""
+        mc = np.zeros(1, np.float64)
+        L.check(self._lib.mqv_emcs(self._h, 1, self.config.ncluster, self.config.nmetro, None,
+                                   mc.ctypes.data))
+        return float(mc[0])
+
+    def wrmploop(self):
+        """warmupsteps EMCS without measurements (core.h:1034-1050)."""
+        n = 10 * (self.config.warmupsteps // 10)
+        self.emcs(n, measure=False)
+
+    def gameloop(self):
+        """gameloopsteps EMCS, measuring after each (core.h:1001-1028)."""
+        n = 10 * (self.config.gameloopsteps // 10)
+        obs, mc = self.emcs(n, measure=True)
+        self.obs.e.extend(obs[:, 0].tolist())
+        self.obs.m.extend(obs[:, 1].tolist())
+        self.obs.m2.extend(obs[:, 2].tolist())
+        self.obs.m4.extend(obs[:, 3].tolist())
+        self.obs.clustersize.extend(mc.tolist())
+        return obs
+
+    # -- engine calls
+    def emcs(self, n: int, ncluster: int | None = None, nmetro: int | None = None, measure: bool = True):
+        nc = self.config.ncluster if ncluster is None else ncluster
+        nm = self.config.nmetro if nmetro is None else nmetro
+        obs = np.zeros((n, 4), np.float64) if measure else None
+        mc = np.zeros(n, np.float64) if measure else None
+        L.check(self._lib.mqv_emcs(self._h, n, nc, nm, None if obs is None else obs.ctypes.data,
+                                   None if mc is None else mc.ctypes.data))
+        self.step += n
+        return obs, mc
+
+    def metropolis(self, nsweeps: int):
+        L.check(self._lib.mqv_metropolis(self._h, int(nsweeps)))
+
+    def wolff(self, nclusters: int) -> np.ndarray:
+        sizes = np.zeros(nclusters, np.int32)
+        L.check(self._lib.mqv_wolff(self._h, int(nclusters), sizes.ctypes.data))
+        return sizes
+
+    def measure(self) -> tuple[float, float, float, float]:
+        o = L.Obs()
+        L.check(self._lib.mqv_measure(self._h, C.byref(o)))
+        return o.e, o.m, o.m2, o.m4
+
+    def synchronize(self):
+        L.check(self._lib.mqv_synchronize(self._h))
+
+    def set_beta(self, beta: float):
+        self.beta = float(beta)
+        L.check(self._lib.mqv_set_beta(self._h, self.beta))
+
+    def set_stream(self, stream_ptr: int):
+        L.check(self._lib.mqv_set_stream(self._h, C.c_void_p(stream_ptr)))
+
+    @property
+    def state(self) -> np.ndarray:
+        out = np.empty(self.n * self.symd, self.dtype)
+        L.check(self._lib.mqv_get_state(self._h, out.ctypes.data, out.nbytes))
+        return out
+
+    @state.setter
+    def state(self, value):
+        v = np.ascontiguousarray(value, self.dtype).reshape(-1)
+        L.check(self._lib.mqv_set_state(self._h, v.ctypes.data, v.nbytes))
+
+    def state_device_ptr(self) -> tuple[int, int]:
+        p = C.c_void_p()
+        nb = C.c_size_t()
+        L.check(self._lib.mqv_state_device_ptr(self._h, C.byref(p), C.byref(nb)))
+        return int(p.value or 0), int(nb.value)
+
+    @property
+    def counters(self) -> tuple[int, int]:
+        a, b = C.c_uint64(), C.c_uint64()
+        L.check(self._lib.mqv_get_counters(self._h, C.byref(a), C.byref(b)))
+        return int(a.value), int(b.value)
+
+    @counters.setter
+    def counters(self, v):
+        L.check(self._lib.mqv_set_counters(self._h, int(v[0]), int(v[1])))
+
+    @property
+    def launches(self) -> int:
+        c = C.c_uint64()
+        L.check(self._lib.mqv_launch_count(self._h, C.byref(c)))
+        return int(c.value)
+
+
+def makeCore(lattice: Lattice, config: Config, ham: Hamiltonian, beta: float) -> Core:
+    """``MARQOV::makeCore`` (core.h:1223-1246)."""
+    return Core(lattice, config, ham, beta)

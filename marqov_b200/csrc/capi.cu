@@ -1,0 +1,695 @@
+// C ABI of the marqov_b200 engine: handle lifecycle, descriptor lowering and
+// validation, the EMCS driver and state transfer.  No exception crosses the
+// ABI; every entry point returns an mqv_status and leaves a message for
+// mqv_last_error on failure.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "engine.h"
+
+namespace mqv {
+
+static thread_local std::string g_err;
+void set_error(const std::string& msg) { g_err = msg; }
+
+// launchers implemented in the kernel files
+cudaError_t launch_init_int8(Sim* s);
+cudaError_t launch_metropolis_int8(Sim* s, int slot);
+cudaError_t launch_measure_int8(Sim* s, int slot);
+cudaError_t launch_finalize_int8(Sim* s, int nslots, double* d_out);
+cudaError_t launch_wolff_int8(Sim* s, int slot);
+cudaError_t launch_init_f32(Sim* s);
+cudaError_t launch_metropolis_f32(Sim* s, int slot);
+cudaError_t launch_measure_f32(Sim* s, int slot);
+cudaError_t launch_finalize_f32(Sim* s, int nslots, double* d_out);
+cudaError_t launch_wolff_f32(Sim* s, int slot);
+
+// Smallest u53 rejected by update_accepted<pref>(dE, beta, .), 2^53 when all
+// are accepted: the rule accepts exactly the words with u53 below a cut.
+unsigned long long accept_cut(int pref, double dE, double beta)
+{
+    if (dE <= 0) return 1ull << 53;
+    if (!update_accepted(pref, dE, beta, 0)) return 0;
+    unsigned long long lo = 1, hi = 1ull << 53;
+    while (lo < hi) {
+        const unsigned long long mid = lo + (hi - lo) / 2;
+        if (update_accepted(pref, dE, beta, mid << 11)) lo = mid + 1;
+        else hi = mid;
+    }
+    return lo;
+}
+
+static bool is_f32_kind(int k) { return k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ; }
+
+static void compute_thresholds(Sim* s)
+{
+    if (!s->fused_ising2d) return;
+    for (int mc = 0; mc < 2; ++mc)
+        for (int M = 0; M <= 4; ++M) {
+            const int sg = 1 - 2 * mc, sum = 4 - 2 * M;
+            const double dE = s->md.J * (double)((-2 * sg) * sum);
+            s->thr2d[mc * 5 + M] = accept_cut(1, dE, s->md.beta);
+        }
+}
+
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev)
+    {
+        cudaGetDevice(&prev);
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard()
+    {
+        int now = -1;
+        cudaGetDevice(&now);
+        if (prev >= 0 && now != prev) cudaSetDevice(prev);
+    }
+};
+
+#define MQV_CK(expr)                                                                         \
+    do {                                                                                     \
+        cudaError_t e_ = (expr);                                                             \
+        if (e_ != cudaSuccess) {                                                             \
+            set_error(std::string("CUDA error: ") + cudaGetErrorString(e_) + " at " #expr); \
+            return e_ == cudaErrorMemoryAllocation ? MQV_ERR_OUT_OF_MEMORY : MQV_ERR_CUDA;   \
+        }                                                                                    \
+    } while (0)
+
+static mqv_status fail(mqv_status st, const std::string& msg)
+{
+    set_error(msg);
+    return st;
+}
+
+static void free_sim(Sim* s)
+{
+    if (!s) return;
+    DeviceGuard g(s->device);
+    if (s->stream) cudaStreamSynchronize(s->stream);
+    for (void* p : {s->state[0], s->state[1], (void*)s->d_rp, (void*)s->d_ci, (void*)s->d_bonds, (void*)s->d_order,
+                    (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize})
+        if (p) cudaFree(p);
+    if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
+    delete s;
+}
+
+static mqv_status ensure_slots(Sim* s, int nslots)
+{
+    if (nslots <= s->nslots) return MQV_OK;
+    if (s->d_acc) cudaFree(s->d_acc);
+    if (s->d_obs) cudaFree(s->d_obs);
+    s->d_acc = nullptr;
+    s->d_obs = nullptr;
+    s->nslots = 0;
+    MQV_CK(cudaMalloc(&s->d_acc, sizeof(long long) * kAccStride * (size_t)nslots));
+    MQV_CK(cudaMalloc(&s->d_obs, sizeof(double) * 4 * (size_t)nslots));
+    s->nslots = nslots;
+    return MQV_OK;
+}
+
+static mqv_status ensure_cslots(Sim* s, int n)
+{
+    if (n <= s->nslots_c) return MQV_OK;
+    if (s->d_csize) cudaFree(s->d_csize);
+    s->d_csize = nullptr;
+    s->nslots_c = 0;
+    MQV_CK(cudaMalloc(&s->d_csize, sizeof(int32_t) * (size_t)n));
+    s->nslots_c = n;
+    return MQV_OK;
+}
+
+static mqv_status ensure_wolff(Sim* s)
+{
+    if (s->d_queue) return MQV_OK;
+    MQV_CK(cudaMalloc(&s->d_queue, sizeof(int32_t) * (size_t)s->n));
+    const size_t words = (size_t)((s->n + 31) / 32);
+    MQV_CK(cudaMalloc(&s->d_visited, sizeof(uint32_t) * words));
+    MQV_CK(cudaMemsetAsync(s->d_visited, 0, sizeof(uint32_t) * words, s->stream));
+    return MQV_OK;
+}
+
+// ---- lattice lowering -----------------------------------------------------------
+
+static mqv_status lower_csr(Sim* s, const mqv_lattice_desc* L)
+{
+    const int64_t n = L->n;
+    if (n < 2 || n >= (int64_t)1 << 31) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: n out of range");
+    if (!L->row_ptr || !L->col_idx) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: row_ptr/col_idx missing");
+    const int32_t* rp = L->row_ptr;
+    const int32_t* ci = L->col_idx;
+    if (rp[0] != 0) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: row_ptr[0] != 0");
+    int maxdeg = 0;
+    for (int64_t i = 0; i < n; ++i) {
+        if (rp[i + 1] < rp[i]) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: row_ptr not monotone");
+        maxdeg = std::max(maxdeg, rp[i + 1] - rp[i]);
+    }
+    const int64_t nnz = rp[n];
+    // neighbour ids in range, no self bonds, symmetric adjacency with equal bond weights
+    std::vector<std::pair<int64_t, int64_t>> e;
+    e.reserve((size_t)nnz);
+    for (int64_t i = 0; i < n; ++i)
+        for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+            const int64_t j = ci[p];
+            if (j < 0 || j >= n) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: neighbour id out of range");
+            if (j == i) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: self bond at site " + std::to_string(i));
+            e.emplace_back(i, j);
+        }
+    {
+        std::vector<std::pair<int64_t, int64_t>> a = e, b;
+        b.reserve(a.size());
+        for (auto& x : a) b.emplace_back(x.second, x.first);
+        std::sort(a.begin(), a.end());
+        std::sort(b.begin(), b.end());
+        if (a != b) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: adjacency is not symmetric");
+        if (std::adjacent_find(a.begin(), a.end()) != a.end())
+            return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: repeated bond");
+    }
+    if (L->bonds) {
+        // bnds must be symmetric: the weight of (i,j) equals that of (j,i)
+        std::vector<std::vector<std::pair<int32_t, int8_t>>> w((size_t)n);
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t p = rp[i]; p < rp[i + 1]; ++p) w[i].emplace_back(ci[p], L->bonds[p]);
+        for (auto& v : w) std::sort(v.begin(), v.end());
+        for (int64_t i = 0; i < n; ++i)
+            for (auto& pr : w[i]) {
+                auto& o = w[pr.first];
+                auto it = std::lower_bound(o.begin(), o.end(), std::make_pair((int32_t)i, (int8_t)-128));
+                if (it == o.end() || it->first != i || it->second != pr.second)
+                    return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: bond weights are not symmetric");
+            }
+    }
+    // colours: given (validated) or greedy in site order
+    std::vector<int32_t> col((size_t)n, -1);
+    int ncol = 0;
+    if (L->colours) {
+        for (int64_t i = 0; i < n; ++i) {
+            if (L->colours[i] < 0 || L->colours[i] > 4096)
+                return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: colour out of range");
+            col[i] = L->colours[i];
+            ncol = std::max(ncol, col[i] + 1);
+        }
+        for (int64_t i = 0; i < n; ++i)
+            for (int32_t p = rp[i]; p < rp[i + 1]; ++p)
+                if (col[ci[p]] == col[i]) return fail(MQV_ERR_BAD_DESCRIPTOR, "CSR lattice: colouring is not proper");
+    } else {
+        std::vector<int64_t> mark((size_t)maxdeg + 2, -1);
+        for (int64_t i = 0; i < n; ++i) {
+            for (int32_t p = rp[i]; p < rp[i + 1]; ++p) {
+                const int c = col[ci[p]];
+                if (c >= 0 && c <= maxdeg) mark[c] = i;
+            }
+            int c = 0;
+            while (mark[c] == i) ++c;
+            col[i] = c;
+            ncol = std::max(ncol, c + 1);
+        }
+    }
+    std::vector<int32_t> order((size_t)n);
+    s->colour_ptr.assign((size_t)ncol + 1, 0);
+    for (int64_t i = 0; i < n; ++i) s->colour_ptr[col[i] + 1]++;
+    for (int c = 0; c < ncol; ++c) s->colour_ptr[c + 1] += s->colour_ptr[c];
+    {
+        std::vector<int32_t> fill(s->colour_ptr.begin(), s->colour_ptr.end() - 1);
+        for (int64_t i = 0; i < n; ++i) order[fill[col[i]]++] = (int32_t)i;
+    }
+    MQV_CK(cudaMalloc(&s->d_rp, sizeof(int32_t) * (size_t)(n + 1)));
+    MQV_CK(cudaMalloc(&s->d_ci, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
+    MQV_CK(cudaMalloc(&s->d_order, sizeof(int32_t) * (size_t)n));
+    MQV_CK(cudaMemcpy(s->d_rp, rp, sizeof(int32_t) * (size_t)(n + 1), cudaMemcpyHostToDevice));
+    if (nnz) MQV_CK(cudaMemcpy(s->d_ci, ci, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice));
+    MQV_CK(cudaMemcpy(s->d_order, order.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice));
+    if (L->bonds) {
+        MQV_CK(cudaMalloc(&s->d_bonds, (size_t)std::max<int64_t>(nnz, 1)));
+        if (nnz) MQV_CK(cudaMemcpy(s->d_bonds, L->bonds, (size_t)nnz, cudaMemcpyHostToDevice));
+    }
+    s->n = n;
+    s->max_degree = maxdeg;
+    s->csr = CSRDev{n, s->d_rp, s->d_ci, s->d_bonds};
+    return MQV_OK;
+}
+
+static mqv_status lower_model(Sim* s, const mqv_model_desc* m, bool has_bonds)
+{
+    if (m->kind < MQV_MODEL_ISING || m->kind > MQV_MODEL_XXZ)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "unsupported model kind " + std::to_string(m->kind));
+    if (m->kind == MQV_MODEL_POTTS && (m->q < 2 || m->q > 64))
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "Potts q must be in [2, 64]");
+    if (m->kind == MQV_MODEL_EA && !has_bonds)
+        return fail(MQV_ERR_BAD_DESCRIPTOR, "EdwardsAndersonIsing needs a lattice with bonds");
+    if (has_bonds && !(m->kind == MQV_MODEL_EA || m->kind == MQV_MODEL_ISING || m->kind == MQV_MODEL_ISING_EMBED))
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "lattice bonds are supported for Ising-type models only");
+    if (m->proposal == MQV_PROPOSAL_SMALL_CAP &&
+        !(m->kind == MQV_MODEL_HEISENBERG || m->kind == MQV_MODEL_XXZ))
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "small-cap proposals need an O(3) model");
+    if (m->proposal == MQV_PROPOSAL_SMALL_CAP && !(m->cap >= -1.0 && m->cap < 1.0))
+        return fail(MQV_ERR_INVALID_ARG, "small-cap proposal: cap must be cos(half-angle) in [-1, 1)");
+    for (double v : {m->J, m->h, m->h2, m->k, m->delta, m->cap})
+        if (!std::isfinite(v)) return fail(MQV_ERR_INVALID_ARG, "model coefficients must be finite");
+    s->model = *m;
+    s->md.kind = m->kind;
+    s->md.q = m->q;
+    s->md.proposal = m->proposal;
+    s->md.J = m->J;
+    s->md.h = m->h;
+    s->md.h2 = m->h2;
+    s->md.k = m->k;
+    s->md.delta = m->delta;
+    s->md.cap = m->cap;
+    s->is_f32 = is_f32_kind(m->kind);
+    s->symd = (m->kind == MQV_MODEL_HEISENBERG || m->kind == MQV_MODEL_XXZ) ? 3 : 1;
+    s->md.symd = s->symd;
+    return MQV_OK;
+}
+
+static mqv_status launch_measure(Sim* s, int slot)
+{
+    MQV_CK(s->is_f32 ? launch_measure_f32(s, slot) : launch_measure_int8(s, slot));
+    return MQV_OK;
+}
+static mqv_status launch_finalize(Sim* s, int nslots)
+{
+    MQV_CK(s->is_f32 ? launch_finalize_f32(s, nslots, s->d_obs) : launch_finalize_int8(s, nslots, s->d_obs));
+    return MQV_OK;
+}
+static mqv_status launch_sweep(Sim* s, int slot)
+{
+    MQV_CK(s->is_f32 ? launch_metropolis_f32(s, slot) : launch_metropolis_int8(s, slot));
+    return MQV_OK;
+}
+static mqv_status launch_cluster(Sim* s, int slot)
+{
+    mqv_status st = ensure_wolff(s);
+    if (st) return st;
+    MQV_CK(s->is_f32 ? launch_wolff_f32(s, slot) : launch_wolff_int8(s, slot));
+    return MQV_OK;
+}
+
+static mqv_status check_wolff_supported(Sim* s)
+{
+    if (s->md.kind == MQV_MODEL_ISING_EMBED && s->md.J > 0)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "embedded Wolff clusters need a ferromagnetic J < 0");
+    if (s->md.kind == MQV_MODEL_BLUME_CAPEL || s->md.kind == MQV_MODEL_EA)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "no Wolff embedding for this model");
+    if (s->is_f32 && s->md.J > 0)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "embedded Wolff clusters need a ferromagnetic J < 0");
+    if (s->is_f32 && s->md.kind == MQV_MODEL_XXZ)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "no Wolff embedding for XXZ");
+    return MQV_OK;
+}
+
+}  // namespace mqv
+
+using namespace mqv;
+
+#define MQV_GUARD(sim)                                                      \
+    if (!(sim)) return fail(MQV_ERR_INVALID_ARG, "null handle");            \
+    DeviceGuard guard_((sim)->device)
+
+extern "C" {
+
+MQV_API const char* mqv_version(void) { return "marqov_b200 0.1 (sm_100a)"; }
+
+MQV_API mqv_status mqv_device_count(int32_t* count)
+{
+    if (!count) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess) {
+        cudaGetLastError();
+        n = 0;
+    }
+    *count = n;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_last_error(char* buf, size_t len)
+{
+    if (!buf || len == 0) return MQV_ERR_INVALID_ARG;
+    std::snprintf(buf, len, "%s", g_err.c_str());
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_desc* lattice,
+                              const mqv_run_params* params, mqv_sim** out)
+{
+    if (!model || !lattice || !params || !out) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MQV_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (params->device < 0 || params->device >= ndev) return fail(MQV_ERR_INVALID_ARG, "device ordinal out of range");
+    if (!(params->beta >= 0) || !std::isfinite(params->beta)) return fail(MQV_ERR_INVALID_ARG, "beta must be finite and >= 0");
+    if (params->replica > 0xFFFFFFu) return fail(MQV_ERR_INVALID_ARG, "replica id must fit in 24 bits");
+    Sim* s = new (std::nothrow) Sim();
+    if (!s) return fail(MQV_ERR_OUT_OF_MEMORY, "host allocation failed");
+    s->device = params->device;
+    DeviceGuard g(s->device);
+    auto bail = [&](mqv_status st) {
+        free_sim(s);
+        return st;
+    };
+    mqv_status st = lower_model(s, model, lattice->bonds != nullptr);
+    if (st) return bail(st);
+    s->md.beta = params->beta;
+    s->seed = params->seed;
+    s->replica = params->replica;
+    if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("cudaStreamCreate failed");
+        return bail(MQV_ERR_CUDA);
+    }
+    s->own_stream = true;
+    if (lattice->kind == MQV_LATTICE_HYPERCUBIC) {
+        if (lattice->dim < 1 || lattice->dim > 4) return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "hypercubic dim must be 1..4"));
+        if (lattice->len < 4 || (lattice->len & 1))
+            return bail(fail(MQV_ERR_BAD_DESCRIPTOR,
+                             "hypercubic checkerboard needs an even side >= 4 (use a CSR lattice otherwise)"));
+        if (lattice->bonds) return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "bonds need a CSR lattice"));
+        int64_t n = 1;
+        for (int j = 0; j < lattice->dim; ++j) {
+            s->sten.pows[j] = n;
+            n *= lattice->len;
+            if (n >= (int64_t)1 << 31) return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "lattice too large (>= 2^31 sites)"));
+        }
+        s->lat_kind = MQV_LATTICE_HYPERCUBIC;
+        s->dim = lattice->dim;
+        s->len = lattice->len;
+        s->n = n;
+        s->sten.dim = lattice->dim;
+        s->sten.len = lattice->len;
+        s->sten.n = n;
+        s->max_degree = 2 * lattice->dim;
+        s->colour_ptr = {0, (int32_t)(n / 2), (int32_t)n};
+    } else if (lattice->kind == MQV_LATTICE_CSR) {
+        s->lat_kind = MQV_LATTICE_CSR;
+        st = lower_csr(s, lattice);
+        if (st) return bail(st);
+    } else {
+        return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "unknown lattice kind"));
+    }
+    s->fused_ising2d = !(params->flags & MQV_FLAG_PER_COLOUR) && !s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC && s->dim == 2 && (s->len % 16) == 0 &&
+                       (s->md.kind == MQV_MODEL_ISING || s->md.kind == MQV_MODEL_ISING_EMBED);
+    compute_thresholds(s);
+    s->state_bytes = (size_t)s->n * (s->is_f32 ? sizeof(float) * s->symd : 1);
+    if (cudaMalloc(&s->state[0], s->state_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of the state failed");
+        return bail(MQV_ERR_OUT_OF_MEMORY);
+    }
+    if (s->fused_ising2d && cudaMalloc(&s->state[1], s->state_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of the second state buffer failed");
+        return bail(MQV_ERR_OUT_OF_MEMORY);
+    }
+    st = ensure_slots(s, 64);
+    if (st) return bail(st);
+    st = ensure_cslots(s, 256);
+    if (st) return bail(st);
+    *out = reinterpret_cast<mqv_sim*>(s);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_destroy(mqv_sim* h)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s) return MQV_OK;
+    free_sim(s);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_stream(mqv_sim* h, void* stream)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    if (s->own_stream) cudaStreamDestroy(s->stream);
+    s->stream = (cudaStream_t)stream;
+    s->own_stream = false;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_get_stream(mqv_sim* h, void** stream)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !stream) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *stream = (void*)s->stream;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_beta(mqv_sim* h, double beta)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (!(beta >= 0) || !std::isfinite(beta)) return fail(MQV_ERR_INVALID_ARG, "beta must be finite and >= 0");
+    s->md.beta = beta;
+    compute_thresholds(s);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_model(mqv_sim* h, const mqv_model_desc* m)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (!m) return fail(MQV_ERR_INVALID_ARG, "null model");
+    if (m->kind != s->model.kind) return fail(MQV_ERR_INVALID_ARG, "mqv_set_model cannot change the model kind");
+    const double beta = s->md.beta;
+    mqv_status st = lower_model(s, m, s->d_bonds != nullptr);
+    if (st) return st;
+    s->md.beta = beta;
+    compute_thresholds(s);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_init_state(mqv_sim* h)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    MQV_CK(s->is_f32 ? launch_init_f32(s) : launch_init_int8(s));
+    s->initialised = true;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_state_bytes(mqv_sim* h, size_t* bytes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !bytes) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *bytes = s->state_bytes;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_get_state(mqv_sim* h, void* host, size_t bytes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (!host || bytes != s->state_bytes)
+        return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
+    MQV_CK(cudaMemcpyAsync(host, s->state[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (!host || bytes != s->state_bytes)
+        return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
+    if (!s->is_f32) {
+        // integer states must be legal values of the model (branch-free scan)
+        const int8_t* v = (const int8_t*)host;
+        const int kind = s->md.kind, q = s->md.q;
+        int bad = 0;
+        if (kind == MQV_MODEL_POTTS)
+            for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] < 0) | (v[i] >= q);
+        else if (kind == MQV_MODEL_BLUME_CAPEL)
+            for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] < -1) | (v[i] > 1);
+        else
+            for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] * v[i]) != 1;
+        if (bad) return fail(MQV_ERR_INVALID_ARG, "illegal spin value in the state");
+    }
+    MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    s->initialised = true;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_state_device_ptr(mqv_sim* h, void** dev, size_t* bytes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !dev) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *dev = s->state[s->cur];
+    if (bytes) *bytes = s->state_bytes;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_get_counters(mqv_sim* h, uint64_t* sweep, uint64_t* cluster)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (sweep) *sweep = s->sweep;
+    if (cluster) *cluster = s->cluster;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_counters(mqv_sim* h, uint64_t sweep, uint64_t cluster)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    s->sweep = sweep;
+    s->cluster = cluster;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_metropolis(mqv_sim* h, int32_t nsweeps)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (nsweeps < 0) return fail(MQV_ERR_INVALID_ARG, "nsweeps < 0");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    for (int t = 0; t < nsweeps; ++t) {
+        mqv_status st = launch_sweep(s, -1);
+        if (st) return st;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_wolff(mqv_sim* h, int32_t nclusters, int32_t* sizes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (nclusters < 0) return fail(MQV_ERR_INVALID_ARG, "nclusters < 0");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    mqv_status st = check_wolff_supported(s);
+    if (st) return st;
+    int done = 0;
+    while (done < nclusters) {
+        const int chunk = std::min(nclusters - done, 65536);
+        st = ensure_cslots(s, chunk);
+        if (st) return st;
+        for (int c = 0; c < chunk; ++c) {
+            st = launch_cluster(s, c);
+            if (st) return st;
+        }
+        if (sizes) {
+            MQV_CK(cudaMemcpyAsync(sizes + done, s->d_csize, sizeof(int32_t) * chunk, cudaMemcpyDeviceToHost, s->stream));
+            MQV_CK(cudaStreamSynchronize(s->stream));
+        }
+        done += chunk;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_t nmetro, mqv_obs* obs,
+                            double* mean_cluster)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    if (ncluster > 0) {
+        mqv_status st = check_wolff_supported(s);
+        if (st) return st;
+    }
+    const int CH = 1024;
+    std::vector<int32_t> csz;
+    int done = 0;
+    while (done < n_emcs) {
+        const int ch = std::min(n_emcs - done, CH);
+        mqv_status st = ensure_slots(s, ch);
+        if (st) return st;
+        if (ncluster > 0) {
+            st = ensure_cslots(s, ch * ncluster);
+            if (st) return st;
+        }
+        MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch, s->stream));
+        for (int e = 0; e < ch; ++e) {
+            for (int c = 0; c < ncluster; ++c) {
+                st = launch_cluster(s, e * ncluster + c);
+                if (st) return st;
+            }
+            for (int j = 0; j < nmetro; ++j) {
+                st = launch_sweep(s, j == nmetro - 1 ? e : -1);
+                if (st) return st;
+            }
+            if (nmetro == 0) {
+                st = launch_measure(s, e);
+                if (st) return st;
+            }
+        }
+        st = launch_finalize(s, ch);
+        if (st) return st;
+        if (obs) MQV_CK(cudaMemcpyAsync(obs + done, s->d_obs, sizeof(double) * 4 * ch, cudaMemcpyDeviceToHost, s->stream));
+        if (mean_cluster && ncluster > 0) {
+            csz.resize((size_t)ch * ncluster);
+            MQV_CK(cudaMemcpyAsync(csz.data(), s->d_csize, sizeof(int32_t) * csz.size(), cudaMemcpyDeviceToHost, s->stream));
+        }
+        if (obs || mean_cluster) MQV_CK(cudaStreamSynchronize(s->stream));
+        if (mean_cluster) {
+            for (int e = 0; e < ch; ++e) {
+                double a = 0;
+                for (int c = 0; c < ncluster; ++c) a += (double)csz[(size_t)e * ncluster + c];
+                mean_cluster[done + e] = ncluster > 0 ? a / ncluster : 0.0;
+            }
+        }
+        done += ch;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_measure(mqv_sim* h, mqv_obs* out)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (!out) return fail(MQV_ERR_INVALID_ARG, "null output");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride, s->stream));
+    mqv_status st = launch_measure(s, 0);
+    if (st) return st;
+    st = launch_finalize(s, 1);
+    if (st) return st;
+    MQV_CK(cudaMemcpyAsync(out, s->d_obs, sizeof(double) * 4, cudaMemcpyDeviceToHost, s->stream));
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_synchronize(mqv_sim* h)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_launch_count(mqv_sim* h, uint64_t* count)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !count) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *count = s->launches;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3, int32_t n,
+                                       uint32_t* out_engine, uint32_t* out_curand)
+{
+    if (n <= 0 || !out_engine || !out_curand) return fail(MQV_ERR_INVALID_ARG, "bad arguments");
+    uint32_t *de = nullptr, *dc = nullptr;
+    MQV_CK(cudaMalloc(&de, sizeof(uint32_t) * 4 * (size_t)n));
+    MQV_CK(cudaMalloc(&dc, sizeof(uint32_t) * 4 * (size_t)n));
+    cudaError_t e = launch_selftest_philox(seed, c1, c2, c3, n, de, dc, 0);
+    if (e == cudaSuccess) e = cudaMemcpy(out_engine, de, sizeof(uint32_t) * 4 * (size_t)n, cudaMemcpyDeviceToHost);
+    if (e == cudaSuccess) e = cudaMemcpy(out_curand, dc, sizeof(uint32_t) * 4 * (size_t)n, cudaMemcpyDeviceToHost);
+    cudaFree(de);
+    cudaFree(dc);
+    MQV_CK(e);
+    return MQV_OK;
+}
+
+}  // extern "C"

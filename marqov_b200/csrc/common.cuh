@@ -1,0 +1,163 @@
+// Shared device/host pieces of the MARQOV update engine for sm_100a.
+//
+// * Philox4x32-10 counter-based generator keyed by (seed, replica) and counted
+//   by (site, sweep, block, stream): the random word a site update consumes
+//   does not depend on which thread or tile performs it.
+// * The reference acceptance rule update_accepted<pref>
+//   (src/libmarqov/metropolishelpers.h:109-142) in FP64 with every operation
+//   rounded separately (no contraction), so host and device agree bit for bit.
+#pragma once
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#define MQV_HD __host__ __device__ __forceinline__
+
+namespace mqv {
+
+// Stream tags, counter word 3 bits 24..31 (replica id in bits 0..23).
+enum Stream : uint32_t { kMetro = 1, kInit = 2, kWolffSeed = 3, kWolffBond = 4 };
+
+struct Key {
+    uint32_t k0, k1;
+};
+
+MQV_HD Key make_key(uint64_t seed) { return Key{(uint32_t)seed, (uint32_t)(seed >> 32)}; }
+
+MQV_HD uint32_t tag(uint32_t stream, uint32_t replica) { return (stream << 24) | (replica & 0xFFFFFFu); }
+
+MQV_HD void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
+{
+#ifdef __CUDA_ARCH__
+    hi = __umulhi(a, b);
+    lo = a * b;
+#else
+    uint64_t p = (uint64_t)a * b;
+    hi = (uint32_t)(p >> 32);
+    lo = (uint32_t)p;
+#endif
+}
+
+// Philox4x32-10 (Salmon et al., SC'11): 10 rounds, multipliers 0xD2511F53 /
+// 0xCD9E8D57, Weyl key increments 0x9E3779B9 / 0xBB67AE85.
+MQV_HD uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, Key k)
+{
+    uint32_t k0 = k.k0, k1 = k.k1;
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        if (r) {
+            k0 += 0x9E3779B9u;
+            k1 += 0xBB67AE85u;
+        }
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo(0xD2511F53u, c0, hi0, lo0);
+        mulhilo(0xCD9E8D57u, c2, hi1, lo1);
+        uint32_t n0 = hi1 ^ c1 ^ k0;
+        uint32_t n2 = hi0 ^ c3 ^ k1;
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+MQV_HD uint64_t lo64(uint4 v) { return (uint64_t)v.x | ((uint64_t)v.y << 32); }
+MQV_HD uint64_t hi64(uint4 v) { return (uint64_t)v.z | ((uint64_t)v.w << 32); }
+
+// real() of RNGCache: (word >> 11) * 2^-53 (src/libmarqov/rngcache.h:202-206).
+MQV_HD double real01(uint64_t w) { return (double)(w >> 11) * 0x1.0p-53; }
+
+// Sequential words of one (stream, c0, c1) substream: word k sits in block
+// c2 = k/2, half k%2.  Blocks are computed on demand.
+struct SubStream {
+    Key key;
+    uint32_t c0, c1, c3;
+    uint32_t k;
+    uint4 blk;
+    MQV_HD SubStream(Key key_, uint32_t c0_, uint32_t c1_, uint32_t c3_)
+        : key(key_), c0(c0_), c1(c1_), c3(c3_), k(0), blk(make_uint4(0, 0, 0, 0)) {}
+    MQV_HD uint64_t next()
+    {
+        if ((k & 1u) == 0) blk = philox(c0, c1, k >> 1, c3, key);
+        uint64_t w = (k & 1u) ? hi64(blk) : lo64(blk);
+        ++k;
+        return w;
+    }
+    MQV_HD double real() { return real01(next()); }
+};
+
+// ---- acceptance rule -------------------------------------------------------
+
+#ifdef __CUDA_ARCH__
+#define MQV_DMUL(a, b) __dmul_rn((a), (b))
+#define MQV_DADD(a, b) __dadd_rn((a), (b))
+#define MQV_DSUB(a, b) __dsub_rn((a), (b))
+#else
+#define MQV_DMUL(a, b) ((a) * (b))
+#define MQV_DADD(a, b) ((a) + (b))
+#define MQV_DSUB(a, b) ((a) - (b))
+#endif
+
+// 2^x on [-1, 0]: the reference's sixth-order polynomial, Horner order
+// (src/libmarqov/metropolishelpers.h:39-48).
+MQV_HD double exp2app6(double x)
+{
+    double u = 1.0944614513161076e-4;
+    u = MQV_DADD(MQV_DMUL(u, x), 1.2758920456516547e-3);
+    u = MQV_DADD(MQV_DMUL(u, x), 9.5802562122641916e-3);
+    u = MQV_DADD(MQV_DMUL(u, x), 5.5491137793956362e-2);
+    u = MQV_DADD(MQV_DMUL(u, x), 2.4022437948159954e-1);
+    u = MQV_DADD(MQV_DMUL(u, x), 6.9314704935511511e-1);
+    return MQV_DADD(MQV_DMUL(u, x), 9.9999999867786389e-1);
+}
+
+// cvttsd2si: truncation toward zero, INT64_MIN for NaN / out of range
+// (src/libmarqov/metropolishelpers.h:59-70).
+MQV_HD int64_t trunc_i64(double f)
+{
+    if (!(f > -9223372036854775808.0 && f < 9223372036854775808.0)) return INT64_MIN;
+    return (int64_t)f;
+}
+
+MQV_HD int64_t bits_of(double d)
+{
+#ifdef __CUDA_ARCH__
+    return __double_as_longlong(d);
+#else
+    int64_t i;
+    __builtin_memcpy(&i, &d, 8);
+    return i;
+#endif
+}
+MQV_HD double double_of(int64_t i)
+{
+#ifdef __CUDA_ARCH__
+    return __longlong_as_double(i);
+#else
+    double d;
+    __builtin_memcpy(&d, &i, 8);
+    return d;
+#endif
+}
+
+// update_accepted<pref>(dE, beta, rng) with the word the reference would
+// draw: accept when dE <= 0; otherwise compare the binary exponent of
+// u = real(word) with trunc(pref log2(e) (-beta dE)) and, on a tie, the
+// mantissa in [0.5, 1) with exp2app6 of the fractional part.
+MQV_HD bool update_accepted(int pref, double dE, double beta, uint64_t word)
+{
+    if (dE <= 0) return true;
+    const double plog2e = (double)pref * 1.4426950408889634074;
+    double rngnum = real01(word);
+    double action = MQV_DMUL(-beta, dE);
+    double action2 = MQV_DMUL(plog2e, action);
+    int64_t i64 = bits_of(rngnum);
+    int64_t t = trunc_i64(action2);
+    int64_t e = (i64 >> 52) - 1022;
+    if (e != t) return e < t;
+    i64 = (i64 & ~(int64_t)0xFFF0000000000000LL) | 0x3FE0000000000000LL;
+    double remainder = MQV_DSUB(action2, trunc(action2));
+    return double_of(i64) < exp2app6(remainder);
+}
+
+}  // namespace mqv

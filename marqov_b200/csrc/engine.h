@@ -1,0 +1,111 @@
+// Internal declarations of the marqov_b200 engine (not part of the ABI).
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+#include <vector>
+
+#include "../../include/marqov_b200.h"
+#include "common.cuh"
+
+namespace mqv {
+
+// Observable accumulators of one measurement slot (int64, exact for integer
+// models; float models keep FP64 sums in the double view of the same slot).
+constexpr int kAccStride = 72;
+enum AccIdx { kAccEne = 0, kAccMag = 1, kAccSq = 2, kAccQ4 = 3, kAccMagY = 4, kAccMagZ = 5, kAccPotts = 8 };
+
+// Model parameters as the kernels see them.
+struct ModelDev {
+    int kind;
+    int q;
+    int proposal;
+    int symd;
+    double J, h, h2, k, delta, cap;
+    double beta;
+};
+
+// Periodic hypercubic stencil: neighbour order +x,-x,+y,-y,... of
+// FixedDimRegularHypercubic::nbrs (src/lattice/regular_hypercubic.h:31-66).
+struct StencilDev {
+    int dim;
+    int len;
+    int64_t n;
+    int64_t pows[4];
+    MQV_HD int degree(int64_t) const { return 2 * dim; }
+    MQV_HD int64_t nbr(int64_t i, int slot) const
+    {
+        const int j = slot >> 1;
+        const int64_t p = pows[j];
+        const int64_t x = (i / p) % len;
+        if ((slot & 1) == 0) return x == len - 1 ? i - (int64_t)(len - 1) * p : i + p;
+        return x == 0 ? i + (int64_t)(len - 1) * p : i - p;
+    }
+    MQV_HD int bond(int64_t, int) const { return 1; }
+};
+
+struct CSRDev {
+    int64_t n;
+    const int32_t* rp;
+    const int32_t* ci;
+    const int8_t* bonds;
+    MQV_HD int degree(int64_t i) const { return rp[i + 1] - rp[i]; }
+    MQV_HD int64_t nbr(int64_t i, int slot) const { return ci[rp[i] + slot]; }
+    MQV_HD int bond(int64_t i, int slot) const { return bonds ? bonds[rp[i] + slot] : 1; }
+};
+
+struct Sim;
+// Smallest u53 rejected by update_accepted<pref>(dE, beta, .) (2^53: all accepted).
+unsigned long long accept_cut(int pref, double dE, double beta);
+cudaError_t launch_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3, int n,
+                                   uint32_t* d_eng, uint32_t* d_cur, cudaStream_t st);
+
+struct Sim {
+    mqv_model_desc model{};
+    ModelDev md{};
+    int lat_kind = 0;
+    int dim = 0, len = 0;
+    int64_t n = 0;
+    int symd = 1;
+    bool is_f32 = false;
+    size_t state_bytes = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    // state: two buffers; stencil sweeps ping-pong between them
+    void* state[2] = {nullptr, nullptr};
+    int cur = 0;
+    bool initialised = false;
+    // lattice
+    StencilDev sten{};
+    CSRDev csr{};
+    int32_t* d_rp = nullptr;
+    int32_t* d_ci = nullptr;
+    int8_t* d_bonds = nullptr;
+    int max_degree = 0;
+    std::vector<int32_t> colour_ptr;  // host
+    int32_t* d_order = nullptr;       // sites grouped by colour
+    // random numbers
+    uint64_t seed = 0;
+    uint32_t replica = 0;
+    uint64_t sweep = 0;
+    uint64_t cluster = 0;
+    // fused 2D Ising path: accept thresholds over (minus-self, minus-neighbour count)
+    bool fused_ising2d = false;
+    uint64_t thr2d[10] = {};
+    // measurement
+    int nslots = 0;
+    long long* d_acc = nullptr;  // nslots * kAccStride
+    double* d_obs = nullptr;     // nslots * 4
+    // Wolff scratch
+    uint32_t* d_visited = nullptr;  // n bits
+    int32_t* d_queue = nullptr;     // n entries
+    int32_t* d_csize = nullptr;     // cluster sizes, nslots_c entries
+    int nslots_c = 0;
+    uint64_t launches = 0;
+};
+
+void set_error(const std::string& msg);
+
+}  // namespace mqv

@@ -1,0 +1,220 @@
+"""Lattices in MARQOV's form, lowered to engine lattice descriptors.
+
+* ``RegularHypercubic(len, dim)`` / ``FixedDimRegularHypercubic(dim, len)``:
+  periodic hypercubic lattices (src/lattice/regular_hypercubic.h:15-143); the
+  engine runs them on its stencil path (checkerboard colours, even ``len``).
+* ``CSRLattice``: any lattice given by its neighbour lists in ``nbrs(0, i)``
+  order (the reference lattice concept), with optional symmetric bonds
+  (``bnds``) and an optional proper colouring (else the engine colours
+  greedily).  ``from_nbrs`` lowers any object with ``size()`` / ``nbrs()`` /
+  optional ``bnds()``, the way a reference lattice plugs in.
+* Builders for the synthetic workloads: ``RegularRandomBond`` (bimodal +-1
+  bonds on a hypercubic lattice, src/lattice/regular_random_bond.h:13-77 with a
+  seeded generator) and ``RandomGeometricGraph2D`` (periodic unit square).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import _lib as L
+
+
+class Lattice:
+    def desc(self) -> L.LatticeDesc:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+    def size(self) -> int:  # pragma: no cover - abstract
+        raise NotImplementedError
+
+
+class RegularHypercubic(Lattice):
+    def __init__(self, len: int, dim: int):  # noqa: A002 - reference argument name
+        self.len = int(len)
+        self.dim = int(dim)
+        self.npoints = self.len ** self.dim
+
+    def size(self) -> int:
+        return self.npoints
+
+    def nbrs(self, alpha: int, i: int) -> list[int]:
+        """Neighbours in the reference order +x,-x,+y,-y,... (regular_hypercubic.h:31-66)."""
+        out = []
+        p = 1
+        for _ in range(self.dim):
+            pl = p * self.len
+            base = (i // pl) * pl
+            out.append(base + (i + p) % pl)
+            c = i - p
+            out.append(base + (c + pl) % pl if c < base else c)
+            p = pl
+        return out
+
+    def crds(self, k: int) -> list[float]:
+        """Site coordinates (x + 0.5) / len (regular_hypercubic.h:73-85)."""
+        a = 1.0 / self.len
+        out = []
+        p = 1
+        for _ in range(self.dim):
+            out.append(((k // p) % self.len) * a + 0.5 * a)
+            p *= self.len
+        return out
+
+    def desc(self) -> L.LatticeDesc:
+        return L.LatticeDesc(kind=L.LATTICE_HYPERCUBIC, dim=self.dim, len=self.len)
+
+    def to_csr(self) -> "CSRLattice":
+        n, d = self.npoints, self.dim
+        idx = np.arange(n, dtype=np.int64)
+        cols = np.empty((n, 2 * d), np.int32)
+        p = 1
+        for j in range(d):
+            pl = p * self.len
+            base = (idx // pl) * pl
+            cols[:, 2 * j] = base + (idx + p) % pl
+            c = idx - p
+            cols[:, 2 * j + 1] = np.where(c < base, base + (c + pl) % pl, c)
+            p = pl
+        rp = np.arange(0, n * 2 * d + 1, 2 * d, dtype=np.int32)
+        par = np.zeros(n, np.int64)
+        p = 1
+        for j in range(d):
+            par += (idx // p) % self.len
+            p *= self.len
+        return CSRLattice(rp, cols.reshape(-1), colours=(par & 1).astype(np.int32))
+
+
+def FixedDimRegularHypercubic(dim: int, len: int) -> RegularHypercubic:  # noqa: A002
+    """``FixedDimRegularHypercubic<dim>(len)``."""
+    return RegularHypercubic(len, dim)
+
+
+class CSRLattice(Lattice):
+    def __init__(self, row_ptr, col_idx, bonds=None, colours=None, crds=None):
+        self.row_ptr = np.ascontiguousarray(row_ptr, np.int32)
+        self.col_idx = np.ascontiguousarray(col_idx, np.int32)
+        self.bonds = None if bonds is None else np.ascontiguousarray(bonds, np.int8)
+        self.colours = None if colours is None else np.ascontiguousarray(colours, np.int32)
+        self.coords = crds
+        self.n = len(self.row_ptr) - 1
+
+    @classmethod
+    def from_nbrs(cls, lat, with_bonds: bool | None = None, colours=None) -> "CSRLattice":
+        """Lower any reference-style lattice (``size()``, ``nbrs(0, i)``, optional
+        ``bnds(0, i)``) by querying it once per site."""
+        n = int(lat.size())
+        rp = np.zeros(n + 1, np.int32)
+        cols, bnds = [], []
+        has_b = hasattr(lat, "bnds") if with_bonds is None else with_bonds
+        for i in range(n):
+            nb = list(lat.nbrs(0, i))
+            cols.extend(nb)
+            if has_b:
+                bnds.extend(list(lat.bnds(0, i)))
+            rp[i + 1] = rp[i] + len(nb)
+        return cls(rp, np.array(cols, np.int32), np.array(bnds, np.int8) if has_b else None, colours)
+
+    def size(self) -> int:
+        return self.n
+
+    def nbrs(self, alpha: int, i: int):
+        return self.col_idx[self.row_ptr[i]:self.row_ptr[i + 1]].tolist()
+
+    def bnds(self, alpha: int, i: int):
+        if self.bonds is None:
+            raise AttributeError("lattice has no bonds")
+        return self.bonds[self.row_ptr[i]:self.row_ptr[i + 1]].tolist()
+
+    def desc(self) -> L.LatticeDesc:
+        return L.LatticeDesc(kind=L.LATTICE_CSR, n=self.n, row_ptr=self.row_ptr.ctypes.data,
+                             col_idx=self.col_idx.ctypes.data,
+                             bonds=None if self.bonds is None else self.bonds.ctypes.data,
+                             colours=None if self.colours is None else self.colours.ctypes.data)
+
+    def greedy_colours(self) -> np.ndarray:
+        """Greedy colouring in site order (the engine's default)."""
+        col = np.full(self.n, -1, np.int32)
+        for i in range(self.n):
+            used = {int(col[j]) for j in self.col_idx[self.row_ptr[i]:self.row_ptr[i + 1]] if col[j] >= 0}
+            c = 0
+            while c in used:
+                c += 1
+            col[i] = c
+        return col
+
+
+def RegularRandomBond(len: int, dim: int, p: float = 0.5, seed: int = 0) -> CSRLattice:  # noqa: A002
+    """Hypercubic lattice with symmetric bimodal +-1 bonds, P(+1) = p: the
+    ``RegularRandomBond<BimodalPDF>`` lattice (regular_random_bond.h:26-55) with
+    a seeded generator instead of ``random_device``.  Each undirected bond gets
+    one draw; both of its CSR entries carry it."""
+    base = RegularHypercubic(len, dim).to_csr()
+    n = base.n
+    rng = np.random.default_rng(seed)
+    deg = 2 * dim
+    cols = base.col_idx.reshape(n, deg)
+    w = np.where(rng.random((n, dim)) < p, 1, -1).astype(np.int8)  # forward bond of each dim
+    bonds = np.empty((n, deg), np.int8)
+    for j in range(dim):
+        bonds[:, 2 * j] = w[:, j]                        # +dir bond owned by the site
+        bonds[:, 2 * j + 1] = w[cols[:, 2 * j + 1], j]   # -dir bond owned by the neighbour
+    return CSRLattice(base.row_ptr, base.col_idx, bonds.reshape(-1), base.colours)
+
+
+def RandomGeometricGraph2D(n: int, mean_degree: float = 8.0, seed: int = 0) -> CSRLattice:
+    """n points uniform in the periodic unit square, bonds between points closer
+    than r with pi r^2 n = mean_degree.  Neighbour lists sorted by id; cell-list
+    construction, O(n)."""
+    rng = np.random.default_rng(seed)
+    pts = rng.random((n, 2))
+    r = float(np.sqrt(mean_degree / (np.pi * n)))
+    nc = max(1, int(1.0 / r))
+    cell = np.minimum((pts * nc).astype(np.int64), nc - 1)
+    cid = cell[:, 0] * nc + cell[:, 1]
+    order = np.argsort(cid, kind="stable")
+    starts = np.searchsorted(cid[order], np.arange(nc * nc + 1))
+    src, dst = [], []
+    for dx in (-1, 0, 1):
+        for dy in (-1, 0, 1):
+            ncell = ((cell[:, 0] + dx) % nc) * nc + (cell[:, 1] + dy) % nc
+            cnt = starts[ncell + 1] - starts[ncell]
+            tot = int(cnt.sum())
+            if tot == 0:
+                continue
+            a = np.repeat(np.arange(n), cnt)
+            off = np.arange(tot) - np.repeat(np.cumsum(cnt) - cnt, cnt)
+            b = order[np.repeat(starts[ncell], cnt) + off]
+            d = pts[a] - pts[b]
+            d -= np.round(d)
+            keep = (a != b) & ((d * d).sum(1) < r * r)
+            src.append(a[keep])
+            dst.append(b[keep])
+    src = np.concatenate(src)
+    dst = np.concatenate(dst)
+    if nc < 3:  # small grids visit a cell more than once
+        pair = np.unique(np.stack([src, dst], 1), axis=0)
+        src, dst = pair[:, 0], pair[:, 1]
+    o = np.lexsort((dst, src))
+    src, dst = src[o], dst[o]
+    rp = np.zeros(n + 1, np.int32)
+    np.add.at(rp, src + 1, 1)
+    rp = np.cumsum(rp).astype(np.int32)
+    return CSRLattice(rp, dst.astype(np.int32), crds=pts)
+
+
+def read_graph_csv(path: str) -> CSRLattice:
+    """Read the reference's graph CSV format (src/lattice/util/io.h:34-126 as
+    used by GraphFromCSV, src/lattice/graph_from_csv.h:32-57): first line the
+    number of coordinates c; then one line per site with c tab-separated
+    coordinates followed by its neighbour ids."""
+    with open(path) as fh:
+        ncoords = int(fh.readline().strip())
+        rp, cols, crd = [0], [], []
+        for line in fh:
+            f = line.split()
+            if not f:
+                continue
+            crd.append([float(x) for x in f[:ncoords]])
+            nb = [int(x) for x in f[ncoords:]]
+            cols.extend(nb)
+            rp.append(rp[-1] + len(nb))
+    return CSRLattice(np.array(rp, np.int32), np.array(cols, np.int32), crds=np.array(crd))

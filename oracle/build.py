@@ -1,0 +1,62 @@
+"""Build recipe for the CPU oracle -- TEST INFRASTRUCTURE.
+
+* ``oracle/liboracle.so``        -- the C restatement (oracle.c), always built.
+* ``oracle/_ref/libmarqov_ref.so`` -- ref_harness.cpp compiled against the
+  reference's own headers, built only where the reference source tree exists
+  (``MARQOV_REF_SRC`` or /root/reference/src).  The output stays out of git but
+  travels with the working tree, so machines without the source can still load it.
+
+Both use a conservative ``-march=x86-64-v3`` so the binaries run on any AVX2
+host, not only the build machine, and ``-ffp-contract=off`` so every FP64
+operation of the acceptance rule is rounded as written (the engine does the
+same on host and device).
+"""
+from __future__ import annotations
+
+import os
+import subprocess
+import sys
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REF_SRC_DEFAULT = "/root/reference/src"
+ARCH = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared"]
+
+
+def _newer(out: str, srcs: list[str]) -> bool:
+    if not os.path.exists(out):
+        return False
+    t = os.path.getmtime(out)
+    return all(os.path.getmtime(s) <= t for s in srcs)
+
+
+def build_oracle(force: bool = False) -> str:
+    out = os.path.join(HERE, "liboracle.so")
+    srcs = [os.path.join(HERE, "oracle.c"), os.path.join(HERE, "oracle.h")]
+    if force or not _newer(out, srcs):
+        cmd = ["gcc", "-std=gnu11", *ARCH, "-o", out, srcs[0], "-lm"]
+        subprocess.check_call(cmd)
+    return out
+
+
+def build_ref(force: bool = False) -> str | None:
+    src_root = os.environ.get("MARQOV_REF_SRC", REF_SRC_DEFAULT)
+    out_dir = os.path.join(HERE, "_ref")
+    out = os.path.join(out_dir, "libmarqov_ref.so")
+    if not os.path.isdir(os.path.join(src_root, "libmarqov")):
+        return out if os.path.exists(out) else None
+    os.makedirs(out_dir, exist_ok=True)
+    srcs = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "oracle.c")]
+    if force or not _newer(out, srcs):
+        obj = os.path.join(out_dir, "oracle_c.o")
+        subprocess.check_call(["gcc", "-std=gnu11", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-c",
+                               "-o", obj, srcs[1]])
+        cmd = ["g++", "-std=gnu++14", *ARCH, "-w", "-I", src_root, "-o", out, srcs[0], obj,
+               "-lm", "-lpthread"]
+        subprocess.check_call(cmd)
+    return out
+
+
+if __name__ == "__main__":
+    force = "--force" in sys.argv
+    print(build_oracle(force))
+    print(build_ref(force))

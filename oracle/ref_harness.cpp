@@ -1,0 +1,508 @@
+// Reference harness -- TEST INFRASTRUCTURE (builds oracle/_ref/libmarqov_ref.so).
+//
+// Compiles MARQOV's own hot-path templates from the reference source tree
+// (include path given at build time) and drives them:
+//   * MARQOV::Metropolis<H,L>::move (src/libmarqov/metropolis.h:88-126) over
+//     the engine's colour order, with an RNGCache specialisation whose words
+//     come from the keyed Philox stream (one substream per site and sweep);
+//   * MARQOV::Wolff<H,L>::move (src/libmarqov/wolff.h:72-126 and the model
+//     specialisations) on one sequential Philox substream per cluster, for
+//     statistical comparison;
+//   * the reference observables Energy / Magnetization / PottsMagnetization;
+//   * the reference acceptance known-answer test
+//     (testsuite/components/5-metro_exp.cpp) on RNGCache<std::mt19937_64>{0};
+//   * the reference EMCS in its own random-site order on RNGCache<mt19937_64>
+//     (src/libmarqov/emcs.h:69-109), single thread or one replica per thread,
+//     as the CPU baseline.
+// Nothing here is part of the engine; only tests and bench.py's reference
+// arm load it.
+#define CACHECONTAINER_H 1
+#include <algorithm>
+#include <array>
+#include <chrono>
+#include <numeric>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <random>
+#include <string>
+#include <thread>
+#include <vector>
+
+namespace H5 { struct Group {}; }
+template <class... T> inline void dumpscalartoH5(T&&...) {}
+
+namespace MARQOV {
+// Minimal stand-in for MARQOV::Space (src/libmarqov/core.h:249-330): the
+// embedders only need the type name and operator[].
+template <class SV, class Grid>
+class Space {
+public:
+    typedef Grid Lattice;
+    typedef SV StateVector;
+    using value_type = SV;
+    explicit Space(std::size_t n) : v(n) {}
+    SV& operator[](int j) { return v[j]; }
+    const SV& operator[](int j) const { return v[j]; }
+    std::size_t size() const { return v.size(); }
+    std::vector<SV> v;
+};
+}  // namespace MARQOV
+
+#include "libmarqov/rngcache.h"
+#include "libmarqov/util/svmath.h"
+
+extern "C" uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
+                             uint32_t c1, uint32_t k);
+
+// Tag type: the keyed Philox stream.
+struct PhiloxSite {};
+
+// RNGCache over the keyed Philox stream, with the interface and semantics of
+// src/libmarqov/rngcache.h:156-206 (integer, integer(range), real(max,min)).
+template <>
+class RNGCache<PhiloxSite> {
+public:
+    uint64_t seed = 0;
+    uint32_t replica = 0, stream = 0, c0 = 0, c1 = 0, k = 0;
+    void rekey(uint32_t st, uint32_t a, uint32_t b) { stream = st; c0 = a; c1 = b; k = 0; }
+    inline uint64_t integer() noexcept { return orc_draw(seed, replica, stream, c0, c1, k++); }
+    inline uint64_t integer(uint64_t range) noexcept { return integer() % range; }
+    inline double real(double max = 1.0, double min = 0.0) noexcept
+    {
+        double ret = (integer() >> 11) * 0x1.0p-53;
+        return min + (max - min) * ret;
+    }
+};
+
+#include "libmarqov/metropolis.h"
+#include "libmarqov/wolff.h"
+#include "hamiltonian/Ising.h"
+#include "hamiltonian/Potts.h"
+#include "hamiltonian/Heisenberg.h"
+#include "hamiltonian/Phi4.h"
+#include "hamiltonian/BlumeCapel.h"
+#include "lattice/regular_hypercubic.h"
+
+enum { ST_METRO = 1, ST_INIT = 2, ST_WOLFF_SEED = 3 };
+
+// ---------------------------------------------------------------------------
+// User-side plugins written in the reference API.
+
+// A lattice given as CSR with optional per-bond weights: nbrs(a,i) and
+// bnds(a,i) as the reference lattice concept (src/lattice/regular_random_bond.h:58-67).
+struct CSRLattice {
+    int n;
+    const int32_t* rp;
+    const int32_t* ci;
+    std::vector<int> nb(int i) const { return std::vector<int>(ci + rp[i], ci + rp[i + 1]); }
+    std::vector<int> nbrs(int, int i) const { return nb(i); }
+    std::vector<int> flexnbrs(int, int i) const { return nb(i); }
+    std::size_t size() const { return n; }
+    std::vector<double> crds(int) const { return {0.0}; }
+};
+struct CSRBondLattice : CSRLattice {
+    const int8_t* bd;
+    std::vector<int> bnds(int, int i) const { return std::vector<int>(bd + rp[i], bd + rp[i + 1]); }
+};
+
+// Heisenberg with small-cap proposals: an Initializer specialisation.
+struct HeisenbergCap : public Heisenberg<float, double> {
+    explicit HeisenbergCap(double J) : Heisenberg<float, double>(J) {}
+    static double cap;
+};
+double HeisenbergCap::cap = 0.9;
+template <>
+class Initializer<HeisenbergCap> {
+public:
+    template <class R>
+    static std::array<float, 3> newsv(const std::array<float, 3>& o, R& rng)
+    {
+        double u0 = rng.real(), u1 = rng.real();
+        double ca = 1.0 - u0 * (1.0 - HeisenbergCap::cap);
+        double sa = std::sqrt(std::fmax(0.0, 1.0 - ca * ca));
+        double ph = 2.0 * M_PI * u1;
+        double dx = sa * std::cos(ph), dy = sa * std::sin(ph), dz = ca;
+        double x = o[0], y = o[1], z = o[2];
+        double sg = z < 0 ? -1.0 : 1.0;
+        double a = 1.0 / (1.0 + sg * z);
+        double bxy = -x * y * a;
+        double e1[3] = {1.0 - x * x * a, bxy, -x * sg};
+        double e2[3] = {bxy, 1.0 - y * y * a, -y * sg};
+        double nv[3];
+        for (int c = 0; c < 3; ++c) nv[c] = dx * e1[c] + dy * e2[c] + dz * (double)o[c];
+        double nn = std::sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
+        return {(float)(nv[0] / nn), (float)(nv[1] / nn), (float)(nv[2] / nn)};
+    }
+};
+
+// Scalar phi^4 (one component) in the reference's Phi4 form
+// (src/hamiltonian/Phi4.h:84-121): J = -1, onsite mass/beta phi^2 and
+// lambda/beta (phi^2-1)^2, shift proposal old + amp * real(-1,1).
+struct Phi4Scalar {
+    static constexpr int SymD = 1;
+    typedef std::array<float, 1> StateVector;
+    const double J = -1;
+    double beta, lambda, mass;
+    static double amp;
+    Standard_Interaction<StateVector> inter{-1.0};
+    Onsite_Quadratic<StateVector> q2;
+    Onsite_Fourth_Minus_One<StateVector> q4;
+    std::array<Standard_Interaction<StateVector>*, 1> interactions{&inter};
+    std::vector<OnSite<StateVector, double>*> onsite;
+    Phi4Scalar(double b, double l, double m) : beta(b), lambda(l), mass(m), q2(m / b), q4(l / b)
+    {
+        onsite.push_back(&q2);
+        onsite.push_back(&q4);
+    }
+};
+double Phi4Scalar::amp = 0.5;
+template <>
+class Initializer<Phi4Scalar> {
+public:
+    template <class R>
+    static std::array<float, 1> newsv(const std::array<float, 1>& o, R& rng)
+    {
+        double r = rng.real(-1.0, 1.0);
+        return {(float)((double)o[0] + Phi4Scalar::amp * r)};
+    }
+};
+
+// ---------------------------------------------------------------------------
+// Colour-order Metropolis through the reference templates.
+
+template <class H, class L, class SS>
+static void colour_sweep(const H& ham, const L& grid, SS& ss, RNGCache<PhiloxSite>& rng, double beta,
+                         uint32_t sweep, int ncol, const int32_t* cptr, const int32_t* order)
+{
+    for (int c = 0; c < ncol; ++c)
+        for (int32_t p = cptr[c]; p < cptr[c + 1]; ++p) {
+            const int i = order[p];
+            rng.rekey(ST_METRO, (uint32_t)i, sweep);
+            MARQOV::Metropolis<H, L>::move(ham, grid, ss, rng, beta, i);
+        }
+}
+
+extern "C" {
+
+// Metropolis sweeps for int8-state models.  kind: 1 Ising<int>, 3 Potts<3>,
+// 4 BlumeCapel, 5 Ising with bonds (EdwardsAnderson form).  Writes per-sweep
+// reference observables (e, m) when obs != NULL.
+int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const int8_t* bonds,
+                   int ncol, const int32_t* cptr, const int32_t* order, int8_t* spins,
+                   double J, double D, double beta, uint64_t seed, uint32_t replica,
+                   uint32_t sweep0, int nsweeps, double* obs)
+{
+    RNGCache<PhiloxSite> rng;
+    rng.seed = seed;
+    rng.replica = replica;
+    CSRLattice lat{n, rp, ci};
+    if (kind == 1) {
+        Ising<int> ham(J);
+        MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
+        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
+        for (int t = 0; t < nsweeps; ++t) {
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                Magnetization mo;
+                Energy<Ising<int>> eo(ham);
+                obs[2 * t] = eo.measure(ss, lat);
+                obs[2 * t + 1] = mo.measure(ss, lat);
+            }
+        }
+        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    } else if (kind == 3) {
+        Potts<3> ham(J);
+        MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
+        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
+        for (int t = 0; t < nsweeps; ++t) {
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                PottsMagnetization<3> mo;
+                obs[2 * t] = 0.0;
+                obs[2 * t + 1] = mo.measure(ss, lat);
+            }
+        }
+        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    } else if (kind == 4) {
+        BlumeCapel<int> ham(J, D);
+        MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
+        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
+        for (int t = 0; t < nsweeps; ++t) {
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                Magnetization mo;
+                obs[2 * t] = 0.0;
+                obs[2 * t + 1] = mo.measure(ss, lat);
+            }
+        }
+        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    } else if (kind == 5) {
+        CSRBondLattice blat;
+        blat.n = n; blat.rp = rp; blat.ci = ci; blat.bd = bonds;
+        Ising<int> ham(J);
+        MARQOV::Space<std::array<int, 1>, CSRBondLattice> ss(n);
+        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
+        for (int t = 0; t < nsweeps; ++t) {
+            colour_sweep(ham, blat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                Magnetization mo;
+                obs[2 * t] = 0.0;
+                obs[2 * t + 1] = mo.measure(ss, blat);
+            }
+        }
+        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    } else {
+        return -1;
+    }
+    return 0;
+}
+
+// Initial state by the reference's own initstatespace rule, one INIT
+// substream per site: Ising::initstatespace (src/hamiltonian/Ising.h:99-107)
+// for kind 1, Potts<3>::initstatespace (src/hamiltonian/Potts.h:149-156) for 3.
+int ref_init_int(int kind, int n, uint64_t seed, uint32_t replica, int8_t* out)
+{
+    RNGCache<PhiloxSite> rng;
+    rng.seed = seed;
+    rng.replica = replica;
+    FixedDimRegularHypercubic<1> one(1);
+    for (int i = 0; i < n; ++i) {
+        rng.rekey(ST_INIT, (uint32_t)i, 0);
+        MARQOV::Space<std::array<int, 1>, FixedDimRegularHypercubic<1>> ss(1);
+        if (kind == 1) Ising<int>(-1.0).initstatespace(ss, one, rng);
+        else if (kind == 3) Potts<3>(-1.0).initstatespace(ss, one, rng);
+        else return -1;
+        out[i] = (int8_t)ss[0][0];
+    }
+    return 0;
+}
+
+// Metropolis sweeps for float-state models. kind: 6 Heisenberg<float> with
+// the reference's fresh-direction proposal, 7 Heisenberg small-cap (cap =
+// cos of the cap half-angle), 8 scalar phi^4 (p0 = lambda, p1 = mass,
+// cap = shift amplitude).
+int ref_sweeps_f32(int kind, int n, const int32_t* rp, const int32_t* ci, int ncol,
+                   const int32_t* cptr, const int32_t* order, float* s, double J, double p0,
+                   double p1, double cap, double beta, uint64_t seed, uint32_t replica,
+                   uint32_t sweep0, int nsweeps, double* obs)
+{
+    RNGCache<PhiloxSite> rng;
+    rng.seed = seed;
+    rng.replica = replica;
+    CSRLattice lat{n, rp, ci};
+    if (kind == 6 || kind == 7) {
+        HeisenbergCap::cap = cap;
+        HeisenbergCap hc(J);
+        Heisenberg<float, double> hf(J);
+        MARQOV::Space<std::array<float, 3>, CSRLattice> ss(n);
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) ss[i][c] = s[3 * i + c];
+        for (int t = 0; t < nsweeps; ++t) {
+            if (kind == 6) colour_sweep(hf, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            else colour_sweep(hc, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                Magnetization mo;
+                obs[2 * t] = 0.0;
+                obs[2 * t + 1] = mo.measure(ss, lat);
+            }
+        }
+        for (int i = 0; i < n; ++i)
+            for (int c = 0; c < 3; ++c) s[3 * i + c] = ss[i][c];
+    } else if (kind == 8) {
+        Phi4Scalar::amp = cap;
+        Phi4Scalar ham(beta, p0, p1);
+        MARQOV::Space<std::array<float, 1>, CSRLattice> ss(n);
+        for (int i = 0; i < n; ++i) ss[i][0] = s[i];
+        for (int t = 0; t < nsweeps; ++t) {
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (obs) {
+                Magnetization mo;
+                obs[2 * t] = 0.0;
+                obs[2 * t + 1] = mo.measure(ss, lat);
+            }
+        }
+        for (int i = 0; i < n; ++i) s[i] = ss[i][0];
+    } else {
+        return -1;
+    }
+    return 0;
+}
+
+// Unmodified reference Wolff clusters (Wolff<Ising<int>> and Wolff<Potts<3>>)
+// on a sequential Philox substream per cluster. Returns the cluster sizes.
+int ref_wolff_int(int kind, int n, const int32_t* rp, const int32_t* ci, int8_t* spins, double J,
+                  double beta, uint64_t seed, uint32_t replica, uint32_t serial0, int nclusters,
+                  int32_t* sizes)
+{
+    RNGCache<PhiloxSite> rng;
+    rng.seed = seed;
+    rng.replica = replica;
+    CSRLattice lat{n, rp, ci};
+    MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
+    for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
+    if (kind == 1) {
+        Ising<int> ham(J);
+        MARQOV::Wolff<Ising<int>, CSRLattice> w;
+        for (int c = 0; c < nclusters; ++c) {
+            rng.rekey(ST_WOLFF_SEED, 0, serial0 + c);
+            int site = (int)rng.integer(n);
+            sizes[c] = w.move(ham, lat, ss, rng, beta, site);
+        }
+    } else if (kind == 3) {
+        Potts<3> ham(J);
+        MARQOV::Wolff<Potts<3>, CSRLattice> w;
+        for (int c = 0; c < nclusters; ++c) {
+            rng.rekey(ST_WOLFF_SEED, 0, serial0 + c);
+            int site = (int)rng.integer(n);
+            sizes[c] = w.move(ham, lat, ss, rng, beta, site);
+        }
+    } else {
+        return -1;
+    }
+    for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    return 0;
+}
+
+// testsuite/components/5-metro_exp.cpp, decision by decision: dE = 10 real()
+// for N words of RNGCache<std::mt19937_64>{0}, then `reps` passes of
+// MARQOV::metro_update_accepted at beta.  decisions[r*N+i] receives each
+// accept bit (when non-NULL); the return value is the accept count.
+long long ref_metro_exp(int N, int reps, double beta, double* dE, uint8_t* decisions)
+{
+    RNGCache<std::mt19937_64> rc{0};
+    for (int i = 0; i < N; ++i) dE[i] = 10.0 * rc.real();
+    long long acc = 0;
+    for (int r = 0; r < reps; ++r)
+        for (int i = 0; i < N; ++i) {
+            bool a = MARQOV::metro_update_accepted(dE[i], beta, rc);
+            acc += a;
+            if (decisions) decisions[(size_t)r * N + i] = a;
+        }
+    return acc;
+}
+
+// The first n words of RNGCache<std::mt19937_64>{0}.
+void ref_mt_words(long long n, uint64_t* out)
+{
+    RNGCache<std::mt19937_64> rc{0};
+    for (long long i = 0; i < n; ++i) out[i] = rc.integer();
+}
+
+// Plain-exp count of the same test (the "OLD" branch of 5-metro_exp.cpp).
+long long ref_metro_exp_plain(int N, int reps, double beta)
+{
+    RNGCache<std::mt19937_64> rc{0};
+    std::vector<double> dE(N);
+    for (int i = 0; i < N; ++i) dE[i] = 10.0 * rc.real();
+    long long acc = 0;
+    for (int r = 0; r < reps; ++r)
+        for (int i = 0; i < N; ++i) acc += (dE[i] <= 0) || (rc.real() < std::exp(-beta * dE[i]));
+    return acc;
+}
+
+}  // extern "C"
+
+// The reference rule evaluated on one explicit word (the template reads one
+// word from an RNGCache; a one-word cache supplies it).
+struct OneWordEngine {};
+
+template <>
+class RNGCache<OneWordEngine> {
+public:
+    uint64_t w = 0;
+    inline uint64_t integer() noexcept { return w; }
+    inline uint64_t integer(uint64_t r) noexcept { return w % r; }
+    inline double real(double max = 1.0, double min = 0.0) noexcept
+    {
+        double ret = (w >> 11) * 0x1.0p-53;
+        return min + (max - min) * ret;
+    }
+};
+
+extern "C" {
+int ref_update_accepted(int pref, double dE, double beta, uint64_t word)
+{
+    RNGCache<OneWordEngine> r;
+    r.w = word;
+    if (pref == 1) return MARQOV::update_accepted<1>(dE, beta, r) ? 1 : 0;
+    return MARQOV::update_accepted<2>(dE, beta, r) ? 1 : 0;
+}
+
+// ---------------------------------------------------------------------------
+// CPU baseline: the reference EMCS Metropolis loop (src/libmarqov/emcs.h:93-105)
+// in its own random-site order on RNGCache<std::mt19937_64>, 2D Ising<int8_t>
+// on FixedDimRegularHypercubic<2>.  A farm holds nthreads independent
+// replicas, one per thread, as CXX11Scheduler farms simulations
+// (src/libmarqov/marqovscheduler.h:281-285); one farm step runs `nupdates`
+// random-site updates on every replica in parallel.
+
+struct Farm {
+    typedef FixedDimRegularHypercubic<2> G;
+    typedef MARQOV::Space<std::array<int8_t, 1>, G> SS;
+    int len;
+    double beta;
+    G grid;
+    Ising<int8_t> ham{-1.0};
+    std::vector<std::unique_ptr<SS>> states;
+    std::vector<std::unique_ptr<RNGCache<std::mt19937_64>>> rngs;
+    Farm(int l, double b) : len(l), beta(b), grid(l) {}
+};
+
+static void farm_run(Farm* f, int t, long long nupdates)
+{
+    auto& ss = *f->states[t];
+    auto& rng = *f->rngs[t];
+    const int N = (int)f->grid.size();
+    for (long long i = 0; i < nupdates; ++i) {
+        const int rsite = rng.integer(N);
+        MARQOV::Metropolis<Ising<int8_t>, Farm::G>::move(f->ham, f->grid, ss, rng, f->beta, rsite);
+    }
+}
+
+void* ref_farm_create(int len, double beta, int nthreads, uint64_t seed)
+{
+    Farm* f = new Farm(len, beta);
+    f->states.resize(nthreads);
+    f->rngs.resize(nthreads);
+    std::vector<std::thread> th;
+    for (int t = 0; t < nthreads; ++t)
+        th.emplace_back([f, t, seed]() {
+            f->states[t].reset(new Farm::SS(f->grid.size()));
+            f->rngs[t].reset(new RNGCache<std::mt19937_64>(seed + 7919u * (unsigned)t));
+            f->ham.initstatespace(*f->states[t], f->grid, *f->rngs[t]);
+        });
+    for (auto& x : th) x.join();
+    return f;
+}
+
+// Runs one step; returns its wall time in seconds.
+double ref_farm_step(void* h, long long nupdates)
+{
+    Farm* f = (Farm*)h;
+    const int n = (int)f->states.size();
+    auto t0 = std::chrono::steady_clock::now();
+    if (n == 1) {
+        farm_run(f, 0, nupdates);
+    } else {
+        std::vector<std::thread> th;
+        for (int t = 0; t < n; ++t) th.emplace_back(farm_run, f, t, nupdates);
+        for (auto& x : th) x.join();
+    }
+    auto t1 = std::chrono::steady_clock::now();
+    return std::chrono::duration<double>(t1 - t0).count();
+}
+
+// Magnetisation sum of replica t (keeps the work observable).
+long long ref_farm_magnetisation(void* h, int t)
+{
+    Farm* f = (Farm*)h;
+    long long m = 0;
+    for (auto& v : f->states[t]->v) m += v[0];
+    return m;
+}
+
+void ref_farm_destroy(void* h) { delete (Farm*)h; }
+
+}  // extern "C"

@@ -1,0 +1,140 @@
+"""Generate the golden fixtures in tests/golden from the reference itself.
+
+Runs the reference's own templates (oracle/_ref/libmarqov_ref.so, built from
+the MARQOV sources by oracle/build.py) and stores their outputs as small
+.npz files, so the parity tests can check the oracle and the engine on
+machines where the reference source is absent.
+
+    python tests/golden/make_golden.py
+
+Fixtures:
+  metro_exp.npz   the acceptance known-answer test of
+                  testsuite/components/5-metro_exp.cpp (N = 1e5, 500 passes,
+                  beta = 0.44): accept counts of the MARQOV rule and of plain
+                  exp, and a SHA-256 of the 5e7 individual decisions.
+  philox_kat.npz  Philox4x32-10 known-answer vectors of the Random123
+                  distribution (published), for the engine's generator.
+  <case>.npz      Metropolis runs through MARQOV::Metropolis<H,L>::move in
+                  colour order on the keyed Philox stream: initial state (by
+                  the reference initstatespace rule where it has one), final
+                  state, per-sweep reference observables (energy, |m|).
+  wolff_*.npz     cluster-size statistics of the unmodified reference Wolff
+                  updates (sequential draws), for a statistical comparison
+                  with the bond-keyed restatement.
+"""
+from __future__ import annotations
+
+import hashlib
+import os
+import sys
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+sys.path.insert(0, ROOT)
+
+from oracle import oracle as O  # noqa: E402
+from oracle.build import build_oracle, build_ref  # noqa: E402
+
+
+def save(name, **arrs):
+    np.savez_compressed(os.path.join(HERE, name + ".npz"), **arrs)
+    print("wrote", name, {k: getattr(v, "shape", v) for k, v in arrs.items()})
+
+
+def main():
+    build_oracle()
+    if build_ref() is None:
+        raise SystemExit("reference source tree not found: cannot build oracle/_ref")
+    orc = O.Oracle()
+    ref = O.RefHarness()
+
+    # -- acceptance KAT (5-metro_exp.cpp at its own sizes)
+    N, reps, beta = 100000, 500, 0.44
+    acc, dec = ref.metro_exp(N, reps, beta, want_decisions=True)
+    plain = ref.metro_exp_plain(N, reps, beta)
+    digest = hashlib.sha256(np.packbits(dec).tobytes()).hexdigest()
+    save("metro_exp", N=np.int64(N), reps=np.int64(reps), beta=np.float64(beta), accepted=np.int64(acc),
+         accepted_plain=np.int64(plain), sha256=np.array(digest))
+    # the first words of RNGCache<mt19937_64>{0}, to pin the oracle's MT19937-64
+    save("mt19937_64_words", words=ref.mt_words(1024))
+
+    # -- Philox KAT (Random123 kat_vectors, philox4x32_10)
+    ctr = np.array([[0, 0, 0, 0], [0xffffffff] * 4, [0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344]], np.uint32)
+    key = np.array([[0, 0], [0xffffffff] * 2, [0xa4093822, 0x299f31d0]], np.uint32)
+    out = np.array([[0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8],
+                    [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd],
+                    [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]], np.uint32)
+    save("philox_kat", ctr=ctr, key=key, out=out)
+
+    # -- Metropolis cases through the reference templates
+    def int_case(name, kind, ref_kind, dim, L, J, D, beta, seed, replica, nsweeps, q=0, bonds=None,
+                 init_kind=None):
+        g = orc.hypercubic(dim, L, bonds)
+        if init_kind is not None:
+            s0 = ref.init_int(init_kind, g.n, seed, replica)
+        else:
+            m = O.OrcModel(kind=kind, q=q, J=J, h=D, k=J)
+            s0 = orc.init_int8(m, g.n, seed, replica)
+        s = s0.copy()
+        obs = ref.sweeps_int(ref_kind, g, s, J, D, beta, seed, replica, 0, nsweeps)
+        arrs = dict(kind=np.int32(kind), dim=np.int32(dim), L=np.int32(L), J=np.float64(J), D=np.float64(D),
+                    q=np.int32(q), beta=np.float64(beta), seed=np.uint64(seed), replica=np.uint32(replica),
+                    nsweeps=np.int32(nsweeps), init=s0, final=s, obs=obs)
+        if bonds is not None:
+            arrs["bonds"] = bonds
+        save(name, **arrs)
+
+    int_case("ising2d_L16", O.ISING, 1, 2, 16, -1.0, 0.0, 0.44068679, 42, 0, 64, init_kind=1)
+    int_case("ising2d_L64", O.ISING, 1, 2, 64, -1.0, 0.0, 0.44068679, 2024, 5, 40, init_kind=1)
+    int_case("ising3d_L8", O.ISING, 1, 3, 8, -1.0, 0.0, 0.2216544, 7, 1, 40, init_kind=1)
+    int_case("potts2d_L16", O.POTTS, 3, 2, 16, -1.0, 0.0, 1.0050525, 11, 2, 40, q=3, init_kind=3)
+    int_case("bc2d_L16", O.BLUME_CAPEL, 4, 2, 16, -1.0, 0.5, 0.6, 13, 0, 40)
+    # Edwards-Anderson +-J on 3D L=8 with symmetric bimodal bonds
+    L = 8
+    g = orc.hypercubic(3, L)
+    rng = np.random.default_rng(5)
+    n = g.n
+    cols = g.col_idx.reshape(n, 6)
+    w = np.where(rng.random((n, 3)) < 0.5, 1, -1).astype(np.int8)
+    bonds = np.empty((n, 6), np.int8)
+    for j in range(3):
+        bonds[:, 2 * j] = w[:, j]
+        bonds[:, 2 * j + 1] = w[cols[:, 2 * j + 1], j]
+    int_case("ea3d_L8", O.EA, 5, 3, L, -1.0, 0.0, 0.9, 17, 3, 40, bonds=bonds.reshape(-1))
+
+    # -- float cases
+    def f32_case(name, ref_kind, dim, L, J, p0, p1, cap, beta, seed, nsweeps, symd):
+        g = orc.hypercubic(dim, L)
+        kind = O.PHI4 if symd == 1 else O.HEISENBERG
+        m = O.OrcModel(kind=kind, J=J)
+        s0 = orc.init_f32(m, g.n, symd, seed, 0)
+        s = s0.copy()
+        obs = ref.sweeps_f32(ref_kind, g, s, J, p0, p1, cap, beta, seed, 0, 0, nsweeps)
+        save(name, dim=np.int32(dim), L=np.int32(L), J=np.float64(J), p0=np.float64(p0), p1=np.float64(p1),
+             cap=np.float64(cap), beta=np.float64(beta), seed=np.uint64(seed), nsweeps=np.int32(nsweeps),
+             symd=np.int32(symd), ref_kind=np.int32(ref_kind), init=s0, final=s, obs=obs)
+
+    f32_case("heis3d_L8_fresh", 6, 3, 8, -1.0, 0, 0, 0.0, 0.6930, 21, 10, 3)
+    f32_case("heis3d_L8_cap", 7, 3, 8, -1.0, 0, 0, 0.6, 0.6930, 22, 10, 3)
+    f32_case("phi4_3d_L8", 8, 3, 8, -1.0, 1.1, 1.0, 0.5, 0.37, 23, 10, 1)
+
+    # -- Wolff statistics: unmodified reference clusters on Ising L=16 and Potts L=16
+    for name, kind, okind, beta, q in (("wolff_ising_L16", 1, O.ISING, 0.44068679, 0),
+                                        ("wolff_potts_L16", 3, O.POTTS, 1.0050525, 3)):
+        g = orc.hypercubic(2, 16)
+        m = O.OrcModel(kind=okind, q=q, J=-1.0, k=-1.0)
+        s = orc.init_int8(m, g.n, 99, 0)
+        for t in range(200):
+            orc.sweep_int8(m, g, s, beta, 99, 0, t)
+        sizes = []
+        for t in range(4000):
+            sizes.append(int(ref.wolff_int(kind, g, s, -1.0, beta, 99, 0, t, 1)[0]))
+            orc.sweep_int8(m, g, s, beta, 99, 0, 1000 + t)
+        sizes = np.array(sizes, np.int32)
+        save(name, beta=np.float64(beta), q=np.int32(q), sizes=sizes)
+
+
+if __name__ == "__main__":
+    main()

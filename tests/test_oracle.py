@@ -1,0 +1,139 @@
+"""The CPU oracle against the reference: golden vectors generated from the
+reference's own templates (tests/golden/make_golden.py), the reference's
+acceptance known-answer test, and the published Philox KAT."""
+import hashlib
+import os
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+
+INT_CASES = ["ising2d_L16", "ising2d_L64", "ising3d_L8", "potts2d_L16", "bc2d_L16", "ea3d_L8"]
+F32_CASES = ["heis3d_L8_fresh", "heis3d_L8_cap", "phi4_3d_L8"]
+
+
+def model_of(g):
+    kind = int(g["kind"])
+    return O.OrcModel(kind=kind, q=int(g["q"]), J=float(g["J"]), h=float(g["D"]), k=float(g["J"]))
+
+
+def test_philox_kat(orc, golden):
+    g = golden("philox_kat")
+    for c, k, o in zip(g["ctr"], g["key"], g["out"]):
+        assert (orc.philox(c, k) == o).all()
+
+
+def test_mt19937_64_words(orc, golden):
+    g = golden("mt19937_64_words")
+    assert (orc.mt_words(0, len(g["words"])) == g["words"]).all()
+
+
+def test_metro_exp_kat(orc, golden):
+    """testsuite/components/5-metro_exp.cpp: same accept decisions, one by one."""
+    g = golden("metro_exp")
+    acc, dec = orc.metro_exp(int(g["N"]), int(g["reps"]), float(g["beta"]), want_decisions=True)
+    assert acc == int(g["accepted"])
+    assert acc == int(g["accepted_plain"])  # the reference test's own criterion
+    assert hashlib.sha256(np.packbits(dec).tobytes()).hexdigest() == str(g["sha256"])
+
+
+@pytest.mark.parametrize("pref", [1, 2])
+def test_acceptance_is_a_threshold_on_u53(orc, pref):
+    rng = np.random.default_rng(pref)
+    for _ in range(60):
+        dE = float(rng.uniform(0.01, 30))
+        beta = float(rng.uniform(0.05, 2.0))
+        t = orc.threshold(pref, dE, beta)
+        for u53 in [0, 1, max(t - 1, 0), t, min(t + 1, 2 ** 53 - 1), 2 ** 53 - 1] + \
+                list(rng.integers(0, 2 ** 53, 20)):
+            u53 = int(u53)
+            w = (u53 << 11) | int(rng.integers(0, 2 ** 11))
+            assert orc.update_accepted(pref, dE, beta, w) == (u53 < t)
+
+
+def test_acceptance_edge_cases(orc):
+    assert orc.update_accepted(1, 0.0, 1.0, 2 ** 64 - 1)
+    assert orc.update_accepted(1, -5.0, 1.0, 2 ** 64 - 1)
+    assert orc.threshold(1, -1.0, 0.5) == 2 ** 53
+    # huge action: truncation saturates, every nonzero draw is rejected
+    assert not orc.update_accepted(1, 1e300, 1e10, 1 << 40)
+    assert orc.threshold(1, 1e300, 1e10) <= 1
+
+
+@pytest.mark.parametrize("case", INT_CASES)
+def test_int_case_bit_exact(orc, golden, case):
+    g = golden(case)
+    dim, L = int(g["dim"]), int(g["L"])
+    graph = orc.hypercubic(dim, L, g.get("bonds"))
+    m = model_of(g)
+    if case.startswith(("ising", "potts")):
+        assert (orc.init_int8(m, graph.n, int(g["seed"]), int(g["replica"])) == g["init"]).all()
+    s = g["init"].copy()
+    for t in range(int(g["nsweeps"])):
+        orc.sweep_int8(m, graph, s, float(g["beta"]), int(g["seed"]), int(g["replica"]), t)
+        e, mm, _, _ = orc.measure_int8(m, graph, s)
+        assert mm == g["obs"][t, 1]
+        if case.startswith("ising"):
+            assert e == g["obs"][t, 0]
+    assert (s == g["final"]).all()
+
+
+@pytest.mark.parametrize("case", F32_CASES)
+def test_f32_case_tolerance(orc, golden, case):
+    g = golden(case)
+    dim, L, symd = int(g["dim"]), int(g["L"]), int(g["symd"])
+    graph = orc.hypercubic(dim, L)
+    rk = int(g["ref_kind"])
+    beta = float(g["beta"])
+    if rk == 8:
+        m = O.OrcModel(kind=O.PHI4, J=-1.0, h=float(g["p1"]) / beta, h2=float(g["p0"]) / beta, cap=float(g["cap"]))
+    else:
+        m = O.OrcModel(kind=O.HEISENBERG, J=-1.0, proposal=1 if rk == 7 else 0, cap=float(g["cap"]))
+    s = g["init"].copy()
+    for t in range(int(g["nsweeps"])):
+        orc.sweep_f32(m, graph, s, symd, beta, int(g["seed"]), 0, t)
+        _, mm, _, _ = orc.measure_f32(m, graph, s, symd)
+        assert abs(mm - g["obs"][t, 1]) <= 1e-5 * max(abs(g["obs"][t, 1]), 1e-3)
+    assert np.allclose(s, g["final"], rtol=0, atol=1e-5)
+
+
+def _batch_err(x, nb=20):
+    b = np.array_split(np.asarray(x, float), nb)
+    means = np.array([v.mean() for v in b])
+    return means.std(ddof=1) / np.sqrt(nb)
+
+
+@pytest.mark.parametrize("case,kind,q", [("wolff_ising_L16", O.ISING, 0), ("wolff_potts_L16", O.POTTS, 3)])
+def test_wolff_restatement_statistics(orc, golden, case, kind, q):
+    """Bond-keyed clusters have the reference clusters' size distribution."""
+    g = golden(case)
+    beta = float(g["beta"])
+    graph = orc.hypercubic(2, 16)
+    m = O.OrcModel(kind=kind, q=q, J=-1.0, k=-1.0)
+    s = orc.init_int8(m, graph.n, 99, 0)
+    for t in range(200):
+        orc.sweep_int8(m, graph, s, beta, 99, 0, t)
+    sizes = []
+    for t in range(4000):
+        sizes.append(orc.wolff_int8(m, graph, s, beta, 7, 0, t))
+        orc.sweep_int8(m, graph, s, beta, 7, 0, 1000 + t)
+    a, b = np.asarray(sizes, float), g["sizes"].astype(float)
+    err = np.hypot(_batch_err(a), _batch_err(b))
+    assert abs(a.mean() - b.mean()) < 4 * err, (a.mean(), b.mean(), err)
+
+
+def test_ref_harness_live_matches_oracle(orc):
+    """Where the reference build is present, re-check a fresh case directly."""
+    path = O.ref_path()
+    if not os.path.exists(path):
+        pytest.skip("reference build oracle/_ref not present")
+    ref = O.RefHarness(path)
+    graph = orc.hypercubic(2, 12)
+    m = O.OrcModel(kind=O.ISING, J=-1.0)
+    s = orc.init_int8(m, graph.n, 1234, 9)
+    s2 = s.copy()
+    for t in range(25):
+        orc.sweep_int8(m, graph, s, 0.3, 1234, 9, 100 + t)
+    ref.sweeps_int(1, graph, s2, -1.0, 0.0, 0.3, 1234, 9, 100, 25, want_obs=False)
+    assert (s == s2).all()
