@@ -48,16 +48,9 @@ unsigned long long accept_cut(int pref, double dE, double beta)
 
 static bool is_f32_kind(int k) { return k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ; }
 
-static void compute_thresholds(Sim* s)
-{
-    if (!s->fused_ising2d) return;
-    for (int mc = 0; mc < 2; ++mc)
-        for (int M = 0; M <= 4; ++M) {
-            const int sg = 1 - 2 * mc, sum = 4 - 2 * M;
-            const double dE = s->md.J * (double)((-2 * sg) * sum);
-            s->thr2d[mc * 5 + M] = accept_cut(1, dE, s->md.beta);
-        }
-}
+bool ising2d_supported(int L);
+cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split);
+cudaError_t launch_merge_rows(Sim* s, const void* split, void* rowmajor);
 
 struct DeviceGuard {
     int prev = -1;
@@ -95,7 +88,8 @@ static void free_sim(Sim* s)
     DeviceGuard g(s->device);
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (void* p : {s->state[0], s->state[1], (void*)s->d_rp, (void*)s->d_ci, (void*)s->d_bonds, (void*)s->d_order,
-                    (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize})
+                    (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize,
+                    (void*)s->d_status})
         if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -133,6 +127,19 @@ static mqv_status ensure_wolff(Sim* s)
     const size_t words = (size_t)((s->n + 31) / 32);
     MQV_CK(cudaMalloc(&s->d_visited, sizeof(uint32_t) * words));
     MQV_CK(cudaMemsetAsync(s->d_visited, 0, sizeof(uint32_t) * words, s->stream));
+    return MQV_OK;
+}
+
+// Reads (and clears) the device error word that bounded waits set.
+static mqv_status check_device_status(Sim* s)
+{
+    int st = 0;
+    MQV_CK(cudaMemcpyAsync(&st, s->d_status, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+    MQV_CK(cudaStreamSynchronize(s->stream));
+    if (st != 0) {
+        MQV_CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
+        return fail(st, "a device-side wait gave up (status " + std::to_string(st) + ")");
+    }
     return MQV_OK;
 }
 
@@ -395,9 +402,16 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
     } else {
         return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "unknown lattice kind"));
     }
-    s->fused_ising2d = !(params->flags & MQV_FLAG_PER_COLOUR) && !s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC && s->dim == 2 && (s->len % 16) == 0 &&
+    s->fused_ising2d = !(params->flags & MQV_FLAG_PER_COLOUR) && !s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC &&
+                       s->dim == 2 && ising2d_supported(s->len) &&
                        (s->md.kind == MQV_MODEL_ISING || s->md.kind == MQV_MODEL_ISING_EMBED);
-    compute_thresholds(s);
+    s->sten.split = s->fused_ising2d ? 1 : 0;
+    cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
+    if (cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess || cudaMemset(s->d_status, 0, sizeof(int)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of the status word failed");
+        return bail(MQV_ERR_OUT_OF_MEMORY);
+    }
     s->state_bytes = (size_t)s->n * (s->is_f32 ? sizeof(float) * s->symd : 1);
     if (cudaMalloc(&s->state[0], s->state_bytes) != cudaSuccess) {
         cudaGetLastError();
@@ -450,7 +464,6 @@ MQV_API mqv_status mqv_set_beta(mqv_sim* h, double beta)
     MQV_GUARD(s);
     if (!(beta >= 0) || !std::isfinite(beta)) return fail(MQV_ERR_INVALID_ARG, "beta must be finite and >= 0");
     s->md.beta = beta;
-    compute_thresholds(s);
     return MQV_OK;
 }
 
@@ -464,7 +477,6 @@ MQV_API mqv_status mqv_set_model(mqv_sim* h, const mqv_model_desc* m)
     mqv_status st = lower_model(s, m, s->d_bonds != nullptr);
     if (st) return st;
     s->md.beta = beta;
-    compute_thresholds(s);
     return MQV_OK;
 }
 
@@ -491,9 +503,15 @@ MQV_API mqv_status mqv_get_state(mqv_sim* h, void* host, size_t bytes)
     MQV_GUARD(s);
     if (!host || bytes != s->state_bytes)
         return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
-    MQV_CK(cudaMemcpyAsync(host, s->state[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+    if (s->fused_ising2d) {
+        // the other buffer is free between sweeps: merge the split rows into it
+        MQV_CK(launch_merge_rows(s, s->state[s->cur], s->state[s->cur ^ 1]));
+        MQV_CK(cudaMemcpyAsync(host, s->state[s->cur ^ 1], bytes, cudaMemcpyDeviceToHost, s->stream));
+    } else {
+        MQV_CK(cudaMemcpyAsync(host, s->state[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+    }
     MQV_CK(cudaStreamSynchronize(s->stream));
-    return MQV_OK;
+    return check_device_status(s);
 }
 
 MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
@@ -515,7 +533,12 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
             for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] * v[i]) != 1;
         if (bad) return fail(MQV_ERR_INVALID_ARG, "illegal spin value in the state");
     }
-    MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
+    if (s->fused_ising2d) {
+        MQV_CK(cudaMemcpyAsync(s->state[s->cur ^ 1], host, bytes, cudaMemcpyHostToDevice, s->stream));
+        MQV_CK(launch_split_rows(s, s->state[s->cur ^ 1], s->state[s->cur]));
+    } else {
+        MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
+    }
     MQV_CK(cudaStreamSynchronize(s->stream));
     s->initialised = true;
     return MQV_OK;
@@ -631,7 +654,10 @@ MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_
             csz.resize((size_t)ch * ncluster);
             MQV_CK(cudaMemcpyAsync(csz.data(), s->d_csize, sizeof(int32_t) * csz.size(), cudaMemcpyDeviceToHost, s->stream));
         }
-        if (obs || mean_cluster) MQV_CK(cudaStreamSynchronize(s->stream));
+        if (obs || mean_cluster) {
+            st = check_device_status(s);
+            if (st) return st;
+        }
         if (mean_cluster) {
             for (int e = 0; e < ch; ++e) {
                 double a = 0;
@@ -657,7 +683,7 @@ MQV_API mqv_status mqv_measure(mqv_sim* h, mqv_obs* out)
     if (st) return st;
     MQV_CK(cudaMemcpyAsync(out, s->d_obs, sizeof(double) * 4, cudaMemcpyDeviceToHost, s->stream));
     MQV_CK(cudaStreamSynchronize(s->stream));
-    return MQV_OK;
+    return check_device_status(s);
 }
 
 MQV_API mqv_status mqv_synchronize(mqv_sim* h)
@@ -665,7 +691,7 @@ MQV_API mqv_status mqv_synchronize(mqv_sim* h)
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     MQV_CK(cudaStreamSynchronize(s->stream));
-    return MQV_OK;
+    return check_device_status(s);
 }
 
 MQV_API mqv_status mqv_launch_count(mqv_sim* h, uint64_t* count)

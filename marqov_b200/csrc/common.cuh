@@ -15,7 +15,7 @@
 namespace mqv {
 
 // Stream tags, counter word 3 bits 24..31 (replica id in bits 0..23).
-enum Stream : uint32_t { kMetro = 1, kInit = 2, kWolffSeed = 3, kWolffBond = 4 };
+enum Stream : uint32_t { kMetro = 1, kInit = 2, kWolffSeed = 3, kWolffBond = 4, kAccept = 5, kAcceptFine = 6 };
 
 struct Key {
     uint32_t k0, k1;
@@ -63,6 +63,28 @@ MQV_HD uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, Key k)
 
 MQV_HD uint64_t lo64(uint4 v) { return (uint64_t)v.x | ((uint64_t)v.y << 32); }
 MQV_HD uint64_t hi64(uint4 v) { return (uint64_t)v.z | ((uint64_t)v.w << 32); }
+
+// The Metropolis acceptance word of a site: top byte = byte (site & 15) of the
+// ACCEPT block (c0 = site >> 4) -- one block serves 16 consecutive sites --
+// low 56 bits = low 56 bits of half (site & 1) of the ACCEPT_FINE block
+// (c0 = site >> 1).  A threshold test on real() is decided by the top byte
+// except on a tie with the threshold's top byte (probability 1/256).
+MQV_HD uint32_t accept_byte(uint4 blk, uint32_t site)
+{
+    const uint32_t b = site & 15u;
+    const uint32_t w = b < 4 ? blk.x : b < 8 ? blk.y : b < 12 ? blk.z : blk.w;
+    return (w >> (8 * (b & 3u))) & 0xFFu;
+}
+MQV_HD uint64_t accept_fine56(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    const uint4 f = philox(site >> 1, sweep, 0u, (kAcceptFine << 24) | (replica & 0xFFFFFFu), key);
+    return ((site & 1u) ? hi64(f) : lo64(f)) & 0x00FFFFFFFFFFFFFFull;
+}
+MQV_HD uint64_t accept_word(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    const uint4 c = philox(site >> 4, sweep, 0u, (kAccept << 24) | (replica & 0xFFFFFFu), key);
+    return ((uint64_t)accept_byte(c, site) << 56) | accept_fine56(key, site, sweep, replica);
+}
 
 // real() of RNGCache: (word >> 11) * 2^-53 (src/libmarqov/rngcache.h:202-206).
 MQV_HD double real01(uint64_t w) { return (double)(w >> 11) * 0x1.0p-53; }
@@ -159,5 +181,50 @@ MQV_HD bool update_accepted(int pref, double dE, double beta, uint64_t word)
     double remainder = MQV_DSUB(action2, trunc(action2));
     return double_of(i64) < exp2app6(remainder);
 }
+
+// ---- Blackwell async copies (bulk copy engine) and mbarriers -----------------
+__device__ __forceinline__ uint32_t smem_addr(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count)
+{
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_fence_init() { asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory"); }
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity)
+{
+    uint32_t done;
+    asm volatile(
+        "{\n .reg .pred p;\n mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n selp.u32 %0, 1, 0, p;\n}"
+        : "=r"(done)
+        : "r"(bar), "r"(parity)
+        : "memory");
+    return done != 0;
+}
+__device__ __forceinline__ uint64_t global_timer_ns()
+{
+    uint64_t t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+// global -> shared bulk copy completing on an mbarrier (16-byte aligned, size % 16 == 0)
+__device__ __forceinline__ void bulk_g2s(uint32_t dst, const void* src, uint32_t bytes, uint32_t bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(dst),
+                 "l"(src), "r"(bytes), "r"(bar)
+                 : "memory");
+}
+// shared -> global bulk copy in the issuing thread's bulk group
+__device__ __forceinline__ void bulk_s2g(void* dst, uint32_t src, uint32_t bytes)
+{
+    asm volatile("cp.async.bulk.global.shared::cta.bulk_group [%0], [%1], %2;" ::"l"(dst), "r"(src), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_commit() { asm volatile("cp.async.bulk.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait_read0() { asm volatile("cp.async.bulk.wait_group.read 0;" ::: "memory"); }
+__device__ __forceinline__ void bulk_wait0() { asm volatile("cp.async.bulk.wait_group 0;" ::: "memory"); }
+__device__ __forceinline__ void fence_proxy_async_smem() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 
 }  // namespace mqv

@@ -33,6 +33,15 @@ struct StencilDev {
     int len;
     int64_t n;
     int64_t pows[4];
+    int split;  // 2D state stored in split rows (even-x half, then odd-x half)
+    // device address of site i
+    MQV_HD int64_t addr(int64_t i) const
+    {
+        if (!split) return i;
+        const int64_t y = i / len;
+        const int64_t x = i - y * len;
+        return y * len + (x & 1) * (len >> 1) + (x >> 1);
+    }
     MQV_HD int degree(int64_t) const { return 2 * dim; }
     MQV_HD int64_t nbr(int64_t i, int slot) const
     {
@@ -50,6 +59,7 @@ struct CSRDev {
     const int32_t* rp;
     const int32_t* ci;
     const int8_t* bonds;
+    MQV_HD int64_t addr(int64_t i) const { return i; }
     MQV_HD int degree(int64_t i) const { return rp[i + 1] - rp[i]; }
     MQV_HD int64_t nbr(int64_t i, int slot) const { return ci[rp[i] + slot]; }
     MQV_HD int bond(int64_t i, int slot) const { return bonds ? bonds[rp[i] + slot] : 1; }
@@ -91,9 +101,13 @@ struct Sim {
     uint32_t replica = 0;
     uint64_t sweep = 0;
     uint64_t cluster = 0;
-    // fused 2D Ising path: accept thresholds over (minus-self, minus-neighbour count)
+    // fused 2D Ising path (ising2d.cu): state in split rows
     bool fused_ising2d = false;
-    uint64_t thr2d[10] = {};
+    int num_sms = 148;
+    int* d_status = nullptr;  // device error word of bounded waits
+    double thr_J = 0, thr_beta = -1;  // (J, beta) the cached 2D thresholds belong to
+    unsigned long long thr_cut[5] = {};
+    uint32_t thr_pools[6] = {};
     // measurement
     int nslots = 0;
     long long* d_acc = nullptr;  // nslots * kAccStride

@@ -54,9 +54,9 @@ __device__ __forceinline__ void smallcap3(SubStream& rng, const float o[3], doub
 
 template <class Lat>
 __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, float* __restrict__ s, int64_t i,
-                                         Key key, uint32_t sweep, uint32_t tg)
+                                         Key key, uint32_t sweep, uint32_t replica)
 {
-    SubStream rng(key, (uint32_t)i, sweep, tg);
+    SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
     const int deg = lat.degree(i);
     if (m.symd == 1) {
         // shift proposal old + amp * real(-1, 1) (Phi4_Initializer_Cartesian,
@@ -71,7 +71,7 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
         const double o2 = old * old, n2 = nw * nw;
         const double dE = m.J * (nw - old) * sum + m.h * (n2 - o2) +
                           m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
-        if (dE <= 0 || update_accepted(1, dE, m.beta, rng.next())) s[i] = nwf;
+        if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) s[i] = nwf;
         return;
     }
     float* so = s + 3 * i;
@@ -92,7 +92,7 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
     dE += ((double)nf[1] - (double)o[1]) * nb[1];
     dE += wz * ((double)nf[2] - (double)o[2]) * nb[2];
     dE *= m.J;
-    if (dE <= 0 || update_accepted(1, dE, m.beta, rng.next())) {
+    if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) {
         so[0] = nf[0];
         so[1] = nf[1];
         so[2] = nf[2];
@@ -108,18 +108,18 @@ __device__ __forceinline__ int64_t parity_site_f(const StencilDev& st, int64_t t
 }
 
 __global__ void metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s, int colour, Key key,
-                                  uint32_t sweep, uint32_t tg)
+                                  uint32_t sweep, uint32_t replica)
 {
     const int64_t half = st.n / 2;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < half; t += (int64_t)gridDim.x * blockDim.x)
-        f32_site(m, st, s, parity_site_f(st, t, colour), key, sweep, tg);
+        f32_site(m, st, s, parity_site_f(st, t, colour), key, sweep, replica);
 }
 
 __global__ void metro_f32_csr(ModelDev m, CSRDev g, float* __restrict__ s, const int32_t* __restrict__ order,
-                              int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t tg)
+                              int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t replica)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
-        f32_site(m, g, s, order[begin + t], key, sweep, tg);
+        f32_site(m, g, s, order[begin + t], key, sweep, replica);
 }
 
 // ---- measurement (FP64) ---------------------------------------------------------
@@ -363,12 +363,11 @@ cudaError_t launch_finalize_f32(Sim* s, int nslots, double* d_out)
 cudaError_t launch_metropolis_f32(Sim* s, int slot)
 {
     const Key key = make_key(s->seed);
-    const uint32_t tg = tag(kMetro, s->replica);
     float* st = (float*)s->state[s->cur];
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
         const int g = grid_for_f(s->n / 2, 256);
         for (int c = 0; c < 2; ++c) {
-            metro_f32_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, tg);
+            metro_f32_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, s->replica);
             s->launches++;
         }
     } else {
@@ -376,7 +375,7 @@ cudaError_t launch_metropolis_f32(Sim* s, int slot)
             const int64_t b = s->colour_ptr[c], cnt = s->colour_ptr[c + 1] - b;
             if (cnt == 0) continue;
             metro_f32_csr<<<grid_for_f(cnt, 256), 256, 0, s->stream>>>(s->md, s->csr, st, s->d_order, b, cnt, key,
-                                                                        (uint32_t)s->sweep, tg);
+                                                                        (uint32_t)s->sweep, s->replica);
             s->launches++;
         }
     }

@@ -39,7 +39,7 @@ __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* 
     if (threadIdx.x == 0) {
         SubStream rng(key, 0u, serial, tg_seed);
         const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
-        const int val = s[rsite];
+        const int val = s[lat.addr(rsite)];
         int newq = -val;
         if (w.mode == 2) {
             // Embedder<Potts<Q>>::draw: new state different from the old one
@@ -74,7 +74,7 @@ __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* 
                 int64_t j = 0;
                 if (t < deg) {
                     j = lat.nbr(cur, t);
-                    const int sj = s[j];
+                    const int sj = s[lat.addr(j)];
                     if (sj == val && !(visited[j >> 5] & (1u << (j & 31)))) {
                         const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
                         const unsigned long long u53 = lo64(philox(lo, serial, hi, tg_bond, key)) >> 11;
@@ -107,7 +107,7 @@ __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* 
     const int8_t nv = (int8_t)s_newq;
     for (int k = threadIdx.x; k < size; k += blockDim.x) {
         const int32_t i = queue[k];
-        s[i] = nv;
+        s[lat.addr(i)] = nv;
         atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
     }
     if (threadIdx.x == 0) *out_size = size;

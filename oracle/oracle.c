@@ -20,7 +20,7 @@
 #include <string.h>
 
 /* Stream tags (counter word 3, bits 24..31). */
-enum { ST_METRO = 1, ST_INIT = 2, ST_WOLFF_SEED = 3, ST_WOLFF_BOND = 4 };
+enum { ST_METRO = 1, ST_INIT = 2, ST_WOLFF_SEED = 3, ST_WOLFF_BOND = 4, ST_ACCEPT = 5, ST_ACCEPT_FINE = 6 };
 
 /* Philox4x32-10 as published by Salmon, Moraes, Dror and Shaw, "Parallel
  * random numbers: as easy as 1, 2, 3" (SC'11): ten rounds of two 32x32->64
@@ -59,6 +59,26 @@ uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
     orc_philox4x32_10(ctr, key, o);
     if (k & 1u) return (uint64_t)o[2] | ((uint64_t)o[3] << 32);
     return (uint64_t)o[0] | ((uint64_t)o[1] << 32);
+}
+
+/* The acceptance word of site i in sweep t: its top byte is byte (i & 15) of
+ * the Philox block (c0 = i >> 4, c1 = t, c2 = 0, ACCEPT stream) -- one block
+ * serves 16 consecutive sites -- and its low 56 bits are the low 56 bits of
+ * half (i & 1) of the block (c0 = i >> 1, c1 = t, c2 = 0, ACCEPT_FINE stream).
+ * A comparison of real() against a threshold is decided by the top byte
+ * unless it ties with the threshold's top byte. */
+uint64_t orc_accept_word(uint64_t seed, uint32_t replica, uint32_t site, uint32_t sweep)
+{
+    uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
+    uint32_t ctr[4] = {site >> 4, sweep, 0, (ST_ACCEPT << 24) | (replica & 0xFFFFFFu)};
+    uint32_t o[4];
+    orc_philox4x32_10(ctr, key, o);
+    const uint32_t b = site & 15u;
+    const uint64_t cb = (o[b >> 2] >> (8 * (b & 3))) & 0xFFu;
+    uint32_t ctrf[4] = {site >> 1, sweep, 0, (ST_ACCEPT_FINE << 24) | (replica & 0xFFFFFFu)};
+    orc_philox4x32_10(ctrf, key, o);
+    const uint64_t f = (site & 1u) ? ((uint64_t)o[2] | ((uint64_t)o[3] << 32)) : ((uint64_t)o[0] | ((uint64_t)o[1] << 32));
+    return (cb << 56) | (f & 0x00FFFFFFFFFFFFFFULL);
 }
 
 /* RNGCache::real(max, min) = min + (max-min) * (word >> 11) * 2^-53
@@ -225,8 +245,10 @@ static void metro_int8_site(const orc_model* m, const orc_lattice* g, int8_t* s,
         break;
     }
     }
-    /* metro_update_accepted, metropolis.h:61-64,120-124 */
-    if (dE <= 0 || orc_update_accepted(1, dE, beta, rng_integer(rng))) s[i] = (int8_t)nw;
+    /* metro_update_accepted, metropolis.h:61-64,120-124: the draw after the
+     * proposal draws is the site's acceptance word */
+    if (dE <= 0 || orc_update_accepted(1, dE, beta, orc_accept_word(rng->seed, rng->replica, rng->c0, rng->c1)))
+        s[i] = (int8_t)nw;
 }
 
 void orc_sweep_int8(const orc_model* m, const orc_lattice* g, int8_t* s, double beta,
@@ -237,6 +259,28 @@ void orc_sweep_int8(const orc_model* m, const orc_lattice* g, int8_t* s, double 
             int32_t i = g->order[p];
             orc_rng rng = {seed, replica, ST_METRO, (uint32_t)i, sweep, 0};
             metro_int8_site(m, g, s, beta, &rng, i);
+        }
+}
+
+/* One colour-order sweep of Ising<int> on FixedDimRegularHypercubic<2>(L)
+ * without a materialised neighbour list: the neighbours of
+ * src/lattice/regular_hypercubic.h:31-66 computed per site.  State in the
+ * reference layout (site = x + L y). */
+void orc_ising2d_sweep(int32_t L, double J, int8_t* s, double beta, uint64_t seed, uint32_t replica,
+                       uint32_t sweep)
+{
+    for (int c = 0; c < 2; ++c)
+        for (int64_t y = 0; y < L; ++y) {
+            const int64_t yu = (y + 1) % L, yd = (y + L - 1) % L;
+            for (int64_t x = (y + c) & 1; x < L; x += 2) {
+                const int64_t i = y * L + x;
+                const int64_t xr = (x + 1) % L, xl = (x + L - 1) % L;
+                const int old = s[i];
+                const int sum = s[y * L + xr] + s[y * L + xl] + s[yu * L + x] + s[yd * L + x];
+                const double dE = J * (double)((-2 * old) * sum);
+                if (dE <= 0 || orc_update_accepted(1, dE, beta, orc_accept_word(seed, replica, (uint32_t)i, sweep)))
+                    s[i] = (int8_t)-old;
+            }
         }
 }
 
@@ -328,7 +372,7 @@ static void metro_f32_site(const orc_model* m, const orc_lattice* g, float* s, i
         for (int c = 0; c < 3; ++c) dE += w[c] * (nw[c] - (double)so[c]) * nb[c];
         dE *= m->J;
     }
-    if (dE <= 0 || orc_update_accepted(1, dE, beta, rng_integer(rng)))
+    if (dE <= 0 || orc_update_accepted(1, dE, beta, orc_accept_word(rng->seed, rng->replica, rng->c0, rng->c1)))
         for (int c = 0; c < symd; ++c) so[c] = (float)nw[c];
 }
 

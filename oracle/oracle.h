@@ -28,6 +28,9 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
  * 2b+1 are the two halves of the Philox block with c2 = b. */
 uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
                   uint32_t c1, uint32_t k);
+/* The Metropolis acceptance word of `site` in `sweep` (top byte from a block
+ * shared by 16 sites, low 56 bits from a block shared by 2 sites). */
+uint64_t orc_accept_word(uint64_t seed, uint32_t replica, uint32_t site, uint32_t sweep);
 /* single draw keyed fully by the counter words (used for Wolff bonds) */
 uint64_t orc_draw_c2(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
                      uint32_t c1, uint32_t c2);
@@ -79,6 +82,11 @@ void orc_sweep_int8(const orc_model* m, const orc_lattice* g, int8_t* s, double 
 /* One Metropolis sweep over float state vectors (symd components AoS). */
 void orc_sweep_f32(const orc_model* m, const orc_lattice* g, float* s, int symd,
                    double beta, uint64_t seed, uint32_t replica, uint32_t sweep);
+
+/* Colour-order sweep of 2D Ising<int> on an L x L periodic lattice, neighbours
+ * computed on the fly (for lattices too large for a neighbour list). */
+void orc_ising2d_sweep(int32_t L, double J, int8_t* s, double beta, uint64_t seed, uint32_t replica,
+                       uint32_t sweep);
 
 /* Initial states from the INIT stream (reference initstatespace rules). */
 void orc_init_int8(const orc_model* m, int32_t n, int8_t* s, uint64_t seed, uint32_t replica);

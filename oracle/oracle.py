@@ -63,6 +63,8 @@ def load_oracle() -> C.CDLL:
     lib.orc_draw.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
     lib.orc_draw_c2.restype = C.c_uint64
     lib.orc_draw_c2.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]
+    lib.orc_accept_word.restype = C.c_uint64
+    lib.orc_accept_word.argtypes = [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32]
     lib.orc_exp2app6.restype = C.c_double
     lib.orc_exp2app6.argtypes = [C.c_double]
     lib.orc_update_accepted.restype = C.c_int
@@ -73,6 +75,8 @@ def load_oracle() -> C.CDLL:
                                    C.c_uint64, C.c_uint32, C.c_uint32]
     lib.orc_sweep_f32.argtypes = [C.POINTER(OrcModel), C.POINTER(OrcLattice), _f32p, C.c_int,
                                   C.c_double, C.c_uint64, C.c_uint32, C.c_uint32]
+    lib.orc_ising2d_sweep.argtypes = [C.c_int32, C.c_double, _i8p, C.c_double, C.c_uint64, C.c_uint32,
+                                      C.c_uint32]
     lib.orc_init_int8.argtypes = [C.POINTER(OrcModel), C.c_int32, _i8p, C.c_uint64, C.c_uint32]
     lib.orc_init_f32.argtypes = [C.POINTER(OrcModel), C.c_int32, _f32p, C.c_int, C.c_uint64,
                                  C.c_uint32]
@@ -137,6 +141,9 @@ class Oracle:
     def update_accepted(self, pref, dE, beta, word):
         return bool(self.lib.orc_update_accepted(pref, dE, beta, word))
 
+    def accept_word(self, seed, replica, site, sweep):
+        return int(self.lib.orc_accept_word(seed, replica, site, sweep))
+
     def threshold(self, pref, dE, beta):
         return int(self.lib.orc_accept_threshold(pref, dE, beta))
 
@@ -146,6 +153,9 @@ class Oracle:
 
     def sweep_f32(self, model: OrcModel, g: Graph, s, symd, beta, seed, replica, sweep):
         self.lib.orc_sweep_f32(C.byref(model), C.byref(g.c), s, symd, beta, seed, replica, sweep)
+
+    def ising2d_sweep(self, L, J, s, beta, seed, replica, sweep):
+        self.lib.orc_ising2d_sweep(L, J, s, beta, seed, replica, sweep)
 
     def init_int8(self, model, n, seed, replica):
         s = np.zeros(n, np.int8)

@@ -59,15 +59,27 @@ extern "C" uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, u
 // Tag type: the keyed Philox stream.
 struct PhiloxSite {};
 
+extern "C" uint64_t orc_accept_word(uint64_t seed, uint32_t replica, uint32_t site, uint32_t sweep);
+
 // RNGCache over the keyed Philox stream, with the interface and semantics of
 // src/libmarqov/rngcache.h:156-206 (integer, integer(range), real(max,min)).
+// In a Metropolis move the first `nprop` words are the proposal words of the
+// site's substream and the next word is its acceptance word.
 template <>
 class RNGCache<PhiloxSite> {
 public:
     uint64_t seed = 0;
     uint32_t replica = 0, stream = 0, c0 = 0, c1 = 0, k = 0;
-    void rekey(uint32_t st, uint32_t a, uint32_t b) { stream = st; c0 = a; c1 = b; k = 0; }
-    inline uint64_t integer() noexcept { return orc_draw(seed, replica, stream, c0, c1, k++); }
+    int nprop = -1;  // < 0: plain substream (no acceptance word)
+    void rekey(uint32_t st, uint32_t a, uint32_t b, int np = -1) { stream = st; c0 = a; c1 = b; k = 0; nprop = np; }
+    inline uint64_t integer() noexcept
+    {
+        if (nprop >= 0 && (int)k == nprop) {
+            ++k;
+            return orc_accept_word(seed, replica, c0, c1);
+        }
+        return orc_draw(seed, replica, stream, c0, c1, k++);
+    }
     inline uint64_t integer(uint64_t range) noexcept { return integer() % range; }
     inline double real(double max = 1.0, double min = 0.0) noexcept
     {
@@ -172,14 +184,21 @@ public:
 // ---------------------------------------------------------------------------
 // Colour-order Metropolis through the reference templates.
 
+// Proposal words drawn by Initializer<H>::newsv before the acceptance word.
+template <class H> struct NProp { static constexpr int value = 0; };
+template <> struct NProp<Potts<3>> { static constexpr int value = 1; };
+template <> struct NProp<BlumeCapel<int>> { static constexpr int value = 1; };
+template <> struct NProp<Heisenberg<float, double>> { static constexpr int value = 2; };
+template <> struct NProp<Phi4Scalar> { static constexpr int value = 1; };
+
 template <class H, class L, class SS>
 static void colour_sweep(const H& ham, const L& grid, SS& ss, RNGCache<PhiloxSite>& rng, double beta,
-                         uint32_t sweep, int ncol, const int32_t* cptr, const int32_t* order)
+                         uint32_t sweep, int ncol, const int32_t* cptr, const int32_t* order, int nprop)
 {
     for (int c = 0; c < ncol; ++c)
         for (int32_t p = cptr[c]; p < cptr[c + 1]; ++p) {
             const int i = order[p];
-            rng.rekey(ST_METRO, (uint32_t)i, sweep);
+            rng.rekey(ST_METRO, (uint32_t)i, sweep, nprop);
             MARQOV::Metropolis<H, L>::move(ham, grid, ss, rng, beta, i);
         }
 }
@@ -203,7 +222,7 @@ int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const 
         MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
         for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
         for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
             if (obs) {
                 Magnetization mo;
                 Energy<Ising<int>> eo(ham);
@@ -217,7 +236,7 @@ int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const 
         MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
         for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
         for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
             if (obs) {
                 PottsMagnetization<3> mo;
                 obs[2 * t] = 0.0;
@@ -230,7 +249,7 @@ int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const 
         MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
         for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
         for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
             if (obs) {
                 Magnetization mo;
                 obs[2 * t] = 0.0;
@@ -245,7 +264,7 @@ int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const 
         MARQOV::Space<std::array<int, 1>, CSRBondLattice> ss(n);
         for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
         for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, blat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            colour_sweep(ham, blat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 0);
             if (obs) {
                 Magnetization mo;
                 obs[2 * t] = 0.0;
@@ -300,8 +319,8 @@ int ref_sweeps_f32(int kind, int n, const int32_t* rp, const int32_t* ci, int nc
         for (int i = 0; i < n; ++i)
             for (int c = 0; c < 3; ++c) ss[i][c] = s[3 * i + c];
         for (int t = 0; t < nsweeps; ++t) {
-            if (kind == 6) colour_sweep(hf, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
-            else colour_sweep(hc, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            if (kind == 6) colour_sweep(hf, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 2);
+            else colour_sweep(hc, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 2);
             if (obs) {
                 Magnetization mo;
                 obs[2 * t] = 0.0;
@@ -316,7 +335,7 @@ int ref_sweeps_f32(int kind, int n, const int32_t* rp, const int32_t* ci, int nc
         MARQOV::Space<std::array<float, 1>, CSRLattice> ss(n);
         for (int i = 0; i < n; ++i) ss[i][0] = s[i];
         for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order);
+            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
             if (obs) {
                 Magnetization mo;
                 obs[2 * t] = 0.0;

@@ -101,7 +101,7 @@ def test_philox_matches_oracle_and_curand(orc):
         assert (eng == cur.reshape(n, 4)).all(), "engine Philox differs from cuRAND Philox4_32_10"
 
 
-@pytest.mark.parametrize("L", [16, 48, 64, 96])
+@pytest.mark.parametrize("L", [16, 32, 48, 64, 96, 320, 512])
 @pytest.mark.parametrize("spintype", ["int", "int8"])
 def test_fused_tiles_equal_per_colour_and_oracle(orc, L, spintype):
     M = mb()
