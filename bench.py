@@ -299,10 +299,10 @@ def run_engine(args, ws, rank, local):
     per_launch_s = ms * 1e-3 / (args.steps * args.nmetro)
     alg_bytes = 2 * n  # one int8 read + one int8 write per site update
     achieved = alg_bytes / per_launch_s / 1e9
-    tr = profiled_traffic("ising2d_fused")
+    tr = profiled_traffic("ising2d_sweep")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None if tr is None else tr.get("bytes_per_launch"),
-            "kernel": "ising2d_fused<256,32>", "peak_source": f"{peak_kind} hbm_gbs",
+            "kernel": "ising2d_sweep<512,32,256>", "peak_source": f"{peak_kind} hbm_gbs",
             "algorithmic_bytes_per_launch": alg_bytes}
 
     line = {

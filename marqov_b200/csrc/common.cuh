@@ -64,17 +64,15 @@ MQV_HD uint4 philox(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, Key k)
 MQV_HD uint64_t lo64(uint4 v) { return (uint64_t)v.x | ((uint64_t)v.y << 32); }
 MQV_HD uint64_t hi64(uint4 v) { return (uint64_t)v.z | ((uint64_t)v.w << 32); }
 
-// The Metropolis acceptance word of a site: top byte = byte (site & 15) of the
-// ACCEPT block (c0 = site >> 4) -- one block serves 16 consecutive sites --
-// low 56 bits = low 56 bits of half (site & 1) of the ACCEPT_FINE block
-// (c0 = site >> 1).  A threshold test on real() is decided by the top byte
-// except on a tie with the threshold's top byte (probability 1/256).
-MQV_HD uint32_t accept_byte(uint4 blk, uint32_t site)
-{
-    const uint32_t b = site & 15u;
-    const uint32_t w = b < 4 ? blk.x : b < 8 ? blk.y : b < 12 ? blk.z : blk.w;
-    return (w >> (8 * (b & 3u))) & 0xFFu;
-}
+// The Metropolis acceptance word of a site.  Top byte, bit-sliced: sites are
+// grouped by G(i) = ((i >> 6) << 1) | (i & 1) (32 sites of equal parity in an
+// aligned run of 64); bit b of the byte is bit ((i >> 1) & 31) of plane b,
+// planes 0..3 = Philox(G, sweep, 0, ACCEPT), planes 4..7 = Philox(G, sweep, 1,
+// ACCEPT).  Low 56 bits: low 56 bits of half (i & 1) of Philox(i >> 1, sweep,
+// 0, ACCEPT_FINE).  A threshold test on real() is decided by the top byte
+// except on a tie with the threshold's top byte (probability 1/256), so
+// kernels draw two Philox blocks per 32 sites and the fine block rarely.
+MQV_HD uint32_t accept_group(uint32_t site) { return ((site >> 6) << 1) | (site & 1u); }
 MQV_HD uint64_t accept_fine56(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
 {
     const uint4 f = philox(site >> 1, sweep, 0u, (kAcceptFine << 24) | (replica & 0xFFFFFFu), key);
@@ -82,8 +80,14 @@ MQV_HD uint64_t accept_fine56(Key key, uint32_t site, uint32_t sweep, uint32_t r
 }
 MQV_HD uint64_t accept_word(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
 {
-    const uint4 c = philox(site >> 4, sweep, 0u, (kAccept << 24) | (replica & 0xFFFFFFu), key);
-    return ((uint64_t)accept_byte(c, site) << 56) | accept_fine56(key, site, sweep, replica);
+    const uint32_t g = accept_group(site), q = (site >> 1) & 31u;
+    const uint32_t c3 = (kAccept << 24) | (replica & 0xFFFFFFu);
+    const uint4 a = philox(g, sweep, 0u, c3, key);
+    const uint4 b = philox(g, sweep, 1u, c3, key);
+    const uint32_t cb = ((a.x >> q) & 1u) | (((a.y >> q) & 1u) << 1) | (((a.z >> q) & 1u) << 2) |
+                        (((a.w >> q) & 1u) << 3) | (((b.x >> q) & 1u) << 4) | (((b.y >> q) & 1u) << 5) |
+                        (((b.z >> q) & 1u) << 6) | (((b.w >> q) & 1u) << 7);
+    return ((uint64_t)cb << 56) | accept_fine56(key, site, sweep, replica);
 }
 
 // real() of RNGCache: (word >> 11) * 2^-53 (src/libmarqov/rngcache.h:202-206).

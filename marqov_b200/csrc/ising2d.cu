@@ -1,32 +1,32 @@
-// Fused checkerboard Metropolis sweep for the 2D Ising model on sm_100a.
+// Fused checkerboard Metropolis sweep for the 2D Ising model on sm_100a,
+// bit-sliced in shared memory.
 //
-// Layout in HBM ("split rows"): row y of the L x L lattice is stored as its
-// L/2 even-x sites followed by its L/2 odd-x sites.  In a colour phase every
-// byte of a 32-bit word of the active half is a site of the active colour, and
-// its four neighbours are the same word of the rows above and below plus the
-// same (or the one-site shifted) word of the other half of its own row.
+// HBM layout ("split rows"): row y of the L x L lattice is stored as its L/2
+// even-x sites followed by its L/2 odd-x sites, int8 +-1.  Sites of one colour
+// in a row are then contiguous, and the neighbours of element j of one half
+// are element j of the same half in the rows above and below and elements
+// j-1, j (even half) or j, j+1 (odd half) of the other half of the row.
 //
-// One persistent CTA per SM slot loops over TY x TX tiles with a two-stage
-// pipeline: while it updates tile n, the bulk-copy engine (cp.async.bulk,
-// completion on an mbarrier) stages tile n+1 with a two-row / 32-column halo
-// of the old state, and updated tiles leave shared memory by bulk stores.  In
-// shared memory the CTA updates colour 0 on the tile plus its one-site ring
-// (re-deriving the neighbouring tiles' updates, which are deterministic), then
-// colour 1 on the tile, and writes the tile to the other state buffer: one HBM
-// read and one write per site update.
+// Pipeline: one persistent CTA per SM slot loops over TY x TX tiles.  While it
+// updates tile n, the bulk-copy engine (cp.async.bulk completing on an
+// mbarrier) stages tile n+1 plus a two-row / 64-column halo of the old state;
+// updated tiles leave shared memory by bulk stores to the other state buffer.
+// Every site is read from HBM once and written once per sweep (2 bytes).
 //
-// Randomness: a site's acceptance word has its top byte in a Philox block
-// shared by 16 consecutive sites (see accept_word in common.cuh).  The CTA
-// fills a shared-memory tile of those bytes -- one Philox4x32-10 per 16 sites --
-// while the bulk copies are in flight.  A decision compares the byte with the
-// top byte of the u53 threshold of the site's class (number of aligned
-// neighbours); only on a tie (1/256) is the second block evaluated.  The
-// decision equals update_accepted<1>(dE, beta, word) for the full word.
+// In shared memory each staged half-row is packed to one bit per site (1 =
+// spin -1) in 32-site words.  Colour 0 is updated on the tile and its
+// one-site ring (re-deriving the neighbouring tiles' updates, which are
+// deterministic), then colour 1 on the tile; a 32-site word costs a few dozen
+// logic instructions: neighbour counts by a carry-save adder on the bit
+// planes, the site class (number of aligned neighbours) by plane masks, and the
+// 8-bit random-versus-threshold comparison by a bit-serial borrow chain.
 //
-// Per word of 4 sites: neighbour minus-counts by byte-wise adds, the aligned
-// count by a byte select, thresholds by byte-permute lookups, decisions by
-// byte-wise compares, flips by one XOR.  Energy (sum over bonds, each bond
-// seen once from its colour-1 end) and magnetisation are reduced in phase 2.
+// Randomness: the top byte of a site's acceptance word is bit-sliced -- eight
+// planes from two Philox4x32-10 blocks per 32 sites (accept_word in
+// common.cuh) -- so the planes of a word are exactly the kernel's operands.  The
+// decision u53 < T(class) is taken on the top byte; a tie with the
+// threshold's top byte (probability 1/256) is resolved with the site's fine
+// block.  The result equals update_accepted<1>(dE, beta, word) bit for bit.
 #include <cuda_runtime.h>
 
 #include "engine.h"
@@ -42,29 +42,38 @@ struct Ising2DArgs {
     Key key;
     uint32_t sweep;
     uint32_t replica;
-    uint32_t t8lo, t8hi;    // top byte of the threshold per aligned count a = 0..4 (clamped to 255)
-    uint32_t alwlo, alwhi;  // 0xFF where class a always accepts
-    uint32_t ztlo, ztlhi;   // 0xFF where a top-byte tie rejects without the low bits
-    unsigned long long thr[5];
+    // the (at most two) aligned-neighbour classes with dE > 0 that need a test
+    int clsA, clsB;             // aligned count, -1 when unused
+    uint32_t tA8, tB8;          // threshold top bytes
+    uint32_t ztA, ztB;          // 1 when a top-byte tie rejects without the fine bits
+    unsigned long long tA, tB;  // full u53 thresholds
     long long* acc;
     int* status;
 };
 
-#define MQV_ISING_THREADS 256
-
 template <int TX, int TY>
 struct TileGeom {
-    static constexpr int H2 = TX / 2;      // interior bytes of a half row
-    static constexpr int PH = H2 + 32;     // half pitch: 16 halo + interior + 16 halo
-    static constexpr int P = 2 * PH;       // row pitch
-    static constexpr int R = TY + 4;       // staged rows: y0-2 .. y0+TY+1
-    static constexpr int RR = TY + 2;      // rows with random bytes: y0-1 .. y0+TY
-    static constexpr int NG = TX / 16 + 2; // 16-site Philox groups per random row
+    static constexpr int NWI = TX / 64;  // interior 32-site words per half-row
+    static constexpr int NWB = NWI + 2;  // with one halo word on each side
+    static constexpr int H2 = TX / 2;    // interior sites per half-row
+    static constexpr int PH = NWB * 32;  // staged bytes per half-row
+    static constexpr int P = 2 * PH;     // staged bytes per row
+    static constexpr int R = TY + 4;     // staged rows y0-2 .. y0+TY+1
+    static constexpr int RR = TY + 2;    // rows with random planes y0-1 .. y0+TY
     static constexpr int STAGE = R * P;
-    static constexpr int RND = RR * P;
+    static constexpr int BITS = R * 2 * NWB * 4;
+    static constexpr int PLANES = RR * 2 * NWB * 32;
     static constexpr uint32_t TX_BYTES = (uint32_t)(R * P);
-    static constexpr int SMEM = 2 * STAGE + RND + 64;
+    static constexpr int SMEM = 2 * STAGE + BITS + PLANES + 64;
 };
+
+// CTAs per SM that shared memory admits (228 KB per SM, 1 KB reserved per CTA)
+template <int TX, int TY, int NT>
+constexpr int min_blocks()
+{
+    return (228 * 1024) / (TileGeom<TX, TY>::SMEM + 1024) < 2048 / NT ? (228 * 1024) / (TileGeom<TX, TY>::SMEM + 1024)
+                                                                      : 2048 / NT;
+}
 
 __device__ __forceinline__ int wrapi(int v, int L)
 {
@@ -72,119 +81,152 @@ __device__ __forceinline__ int wrapi(int v, int L)
     return v >= L ? v - L : v;
 }
 
-// Resolve the tie bytes of one word with the fine block.
-__device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t cbw, uint32_t aw, int j0, int half, int y, int x0,
-                                              int L, Key key, uint32_t sweep, uint32_t replica,
-                                              const unsigned long long* thr)
+// uniform all-ones / all-zeros mask of bit b of t
+__device__ __forceinline__ uint32_t bitmask(uint32_t t, int b) { return 0u - ((t >> b) & 1u); }
+
+// sites (bits) whose neighbour minus-count equals v: planes m0 m1 m2 of M <= 4
+__device__ __forceinline__ uint32_t eq_count(uint32_t m0, uint32_t m1, uint32_t m2, int v)
 {
-    uint32_t accm = 0;
-    for (int b = 0; b < 4; ++b) {
-        if (!((tie >> (8 * b)) & 0xFFu)) continue;
-        const int x = wrapi(x0 - 32 + 2 * (j0 + b) + half, L);
+    return ~(m0 ^ bitmask((uint32_t)v, 0)) & ~(m1 ^ bitmask((uint32_t)v, 1)) & ~(m2 ^ bitmask((uint32_t)v, 2));
+}
+
+// sites of class `cls` (aligned neighbours): minus sites with M == cls, plus
+// sites with M == 4 - cls
+__device__ __forceinline__ uint32_t class_mask(uint32_t A, uint32_t m0, uint32_t m1, uint32_t m2, int cls)
+{
+    if (cls < 0) return 0u;
+    return (A & eq_count(m0, m1, m2, cls)) | (~A & eq_count(m0, m1, m2, 4 - cls));
+}
+
+// Tie bits: compare the full acceptance word with the class threshold.
+__device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, const uint32_t* spl, int w, int half, int y,
+                                              int x0, int L, Key key, uint32_t sweep, uint32_t replica,
+                                              unsigned long long tA, unsigned long long tB)
+{
+    uint32_t acc = 0;
+    while (tie) {
+        const int b = __ffs(tie) - 1;
+        tie &= tie - 1;
+        const int x = wrapi(x0 - 64 + 2 * (32 * w + b) + half, L);
         const uint32_t site = (uint32_t)y * (uint32_t)L + (uint32_t)x;
-        const uint64_t cb = (cbw >> (8 * b)) & 0xFFu;
+        uint64_t cb = 0;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) cb |= (uint64_t)((spl[k] >> b) & 1u) << k;
         const uint64_t u53 = ((cb << 56) | accept_fine56(key, site, sweep, replica)) >> 11;
-        const int cls = (aw >> (8 * b)) & 0xFF;
-        if (u53 < thr[cls]) accm |= 0xFFu << (8 * b);
+        const unsigned long long T = ((maskA >> b) & 1u) ? tA : tB;
+        if (u53 < T) acc |= 1u << b;
     }
-    return accm;
+    return acc;
 }
 
-// One colour phase over rows [r0, r0 + NR) and words [w0, w0 + NW) of the
-// active half of each row.
-template <int TX, int TY, int COL, int NR, int NW, bool MEAS>
-__device__ __forceinline__ void phase(uint8_t* st, const uint8_t* rnd, int r0, int w0, int x0, int y0,
-                                      const Ising2DArgs& a, const unsigned long long* sthr, int& esum, int& msum)
+// Update the active-colour sites of one 32-site word; returns the new word.
+template <bool MEAS>
+__device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb,
+                                                const uint32_t* spl, int w, int half, int y, int x0,
+                                                const Ising2DArgs& a, int& esum)
 {
-    using G = TileGeom<TX, TY>;
-    for (int t = threadIdx.x; t < NR * NW; t += MQV_ISING_THREADS) {
-        const int r = r0 + t / NW;
-        const int w = w0 + t % NW;
-        const int p = (COL + r) & 1;  // active half: x parity of colour COL in this row
-        uint32_t* H = reinterpret_cast<uint32_t*>(st + r * G::P + p * G::PH);
-        const uint32_t* Gr = reinterpret_cast<const uint32_t*>(st + r * G::P + (1 - p) * G::PH);
-        const uint32_t A = H[w];
-        const uint32_t U = reinterpret_cast<const uint32_t*>(st + (r - 1) * G::P + p * G::PH)[w];
-        const uint32_t D = reinterpret_cast<const uint32_t*>(st + (r + 1) * G::P + p * G::PH)[w];
-        const uint32_t G0 = Gr[w];
-        uint32_t Lw, Rw;
-        if (p == 0) {
-            Lw = __funnelshift_l(Gr[w - 1], G0, 8);
-            Rw = G0;
-        } else {
-            Lw = G0;
-            Rw = __funnelshift_r(G0, Gr[w + 1], 8);
-        }
-        const uint32_t m1 = 0x01010101u;
-        const uint32_t mA = (A >> 1) & m1;
-        const uint32_t M = ((U >> 1) & m1) + ((D >> 1) & m1) + ((Lw >> 1) & m1) + ((Rw >> 1) & m1);
-        const uint32_t sel = mA * 0xFFu;
-        const uint32_t aw = (M & sel) | ((0x04040404u - M) & ~sel);  // aligned neighbours per byte
-        const uint32_t tt = aw | (aw >> 4);
-        const uint32_t nib = (tt & 0xFFu) | ((tt >> 8) & 0xFF00u);
-        const uint32_t T8 = __byte_perm(a.t8lo, a.t8hi, nib);
-        const uint32_t ALW = __byte_perm(a.alwlo, a.alwhi, nib);
-        const uint32_t cbw = reinterpret_cast<const uint32_t*>(rnd + (r - 1) * G::P + p * G::PH)[w];
-        uint32_t accm = __vcmpltu4(cbw, T8) | ALW;
-        const uint32_t tie = __vcmpeq4(cbw, T8) & ~ALW & ~__byte_perm(a.ztlo, a.ztlhi, nib);
-        if (tie)
-            accm |= resolve_ties(tie, cbw, aw, 4 * w, p, wrapi(y0 - 2 + r, a.L), x0, a.L, a.key, a.sweep, a.replica, sthr);
-        const uint32_t An = A ^ (accm & 0xFEFEFEFEu);
-        if (accm) H[w] = An;
-        if (MEAS) {
-            // bond sum seen from the colour-1 end, and both colours' spins
-            esum = __dp4a((int)An, (int)__vsub4(0x04040404u, M + M), esum);
-            msum = __dp4a((int)An, 0x01010101, msum);
-            msum = __dp4a((int)G0, 0x01010101, msum);
-        }
+    // the word's eight random planes (shared memory)
+    const uint4 q0 = reinterpret_cast<const uint4*>(spl)[0], q1 = reinterpret_cast<const uint4*>(spl)[1];
+    const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
+    // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder)
+    const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
+    const uint32_t m0 = s1 ^ s2, c3 = s1 & s2;
+    const uint32_t m1 = c1 ^ c2 ^ c3;
+    const uint32_t m2 = (c1 & c2) | (c3 & (c1 | c2));
+    const uint32_t maskA = class_mask(A, m0, m1, m2, a.clsA);
+    const uint32_t maskB = class_mask(A, m0, m1, m2, a.clsB);
+    // per-site threshold bits, then X < T by a borrow chain and X == T
+    uint32_t borrow = 0, eq = ~0u;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        const uint32_t tb = (maskA & bitmask(a.tA8, b)) | (maskB & bitmask(a.tB8, b));
+        const uint32_t nx = ~pl[b];
+        borrow = (nx & tb) | (nx & borrow) | (tb & borrow);
+        eq &= ~(pl[b] ^ tb);
     }
+    const uint32_t test = maskA | maskB;
+    uint32_t acc = ~test | borrow;
+    const uint32_t zt = (maskA & (0u - a.ztA)) | (maskB & (0u - a.ztB));
+    const uint32_t tie = eq & test & ~zt;
+    if (tie) acc |= resolve_ties(tie, maskA, spl, w, half, y, x0, a.L, a.key, a.sweep, a.replica, a.tA, a.tB);
+    const uint32_t An = A ^ acc;
+    if (MEAS) {
+        // sum over the word's bonds s * sum(nbrs) = sum (1 - 2a)(4 - 2M)
+        const int sM = __popc(m0) + 2 * __popc(m1) + 4 * __popc(m2);
+        const int sAM = __popc(An & m0) + 2 * __popc(An & m1) + 4 * __popc(An & m2);
+        esum += 128 - 2 * sM - 8 * __popc(An) + 4 * sAM;
+    }
+    return An;
 }
 
-template <int TX, int TY, bool MEAS>
-__global__ void __launch_bounds__(MQV_ISING_THREADS, 4) ising2d_sweep(const __grid_constant__ Ising2DArgs a)
+// 32 staged bytes (+-1) -> 32 bits (1 = -1)
+__device__ __forceinline__ uint32_t pack32(const uint8_t* p)
+{
+    const uint4 v0 = *reinterpret_cast<const uint4*>(p);
+    const uint4 v1 = *reinterpret_cast<const uint4*>(p + 16);
+    const unsigned long long M = 0x0101010101010101ull, G = 0x0102040810204080ull;
+    const unsigned long long q0 = ((((unsigned long long)v0.y << 32) | v0.x) >> 1) & M;
+    const unsigned long long q1 = ((((unsigned long long)v0.w << 32) | v0.z) >> 1) & M;
+    const unsigned long long q2 = ((((unsigned long long)v1.y << 32) | v1.x) >> 1) & M;
+    const unsigned long long q3 = ((((unsigned long long)v1.w << 32) | v1.z) >> 1) & M;
+    return (uint32_t)((q0 * G) >> 56) | ((uint32_t)((q1 * G) >> 56) << 8) | ((uint32_t)((q2 * G) >> 56) << 16) |
+           ((uint32_t)((q3 * G) >> 56) << 24);
+}
+
+// 32 bits -> 32 staged bytes (+1 -> 0x01, -1 -> 0xFF)
+__device__ __forceinline__ void unpack32(uint32_t bits, uint8_t* p)
+{
+    uint32_t o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t n = (bits >> (4 * k)) & 0xFu;
+        o[k] = 0x01010101u + ((n * 0x00204081u) & 0x01010101u) * 0xFEu;
+    }
+    *reinterpret_cast<uint4*>(p) = make_uint4(o[0], o[1], o[2], o[3]);
+    *reinterpret_cast<uint4*>(p + 16) = make_uint4(o[4], o[5], o[6], o[7]);
+}
+
+template <int TX, int TY, int NT, bool MEAS>
+__global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(const __grid_constant__ Ising2DArgs a)
 {
     using G = TileGeom<TX, TY>;
+    constexpr int NWI = G::NWI, NWB = G::NWB;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* stage0 = smem;
-    uint8_t* rnd = smem + 2 * G::STAGE;
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * G::STAGE + G::RND);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE);             // [R][2][NWB]
+    uint32_t* planes = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE + G::BITS);  // [RR][2][NWB][8]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * G::STAGE + G::BITS + G::PLANES);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
-    const int L = a.L;
-    const int Lh = L >> 1;
+    const int L = a.L, Lh = L >> 1;
     const uint32_t tg_acc = tag(kAccept, a.replica);
-    __shared__ unsigned long long sthr[5];
     if (tid == 0) {
         mbar_init(smem_addr(&bars[0]), 1);
         mbar_init(smem_addr(&bars[1]), 1);
         mbar_fence_init();
-#pragma unroll
-        for (int k = 0; k < 5; ++k) sthr[k] = a.thr[k];
     }
     __syncthreads();
 
     auto issue_load = [&](int tile, int stg) {
-        // warp 0: stage rows y0-2 .. y0+TY+1 of both halves, columns x0-32 .. x0+TX+31
-        const int tx = tile % a.ntx, ty = tile / a.ntx;
-        const int x0 = tx * TX, y0 = ty * TY;
+        // warp 0: rows y0-2 .. y0+TY+1 of both halves, columns x0-64 .. x0+TX+63
+        const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
         uint8_t* sb = stage0 + stg * G::STAGE;
         const uint32_t bar = smem_addr(&bars[stg]);
         if (lane == 0) mbar_expect_tx(bar, G::TX_BYTES);
         __syncwarp();
         const bool inner = x0 > 0 && x0 + TX < L;
+        const int j0 = (x0 >> 1) - 32;
         for (int task = lane; task < 2 * G::R; task += 32) {
             const int r = task >> 1, h = task & 1;
-            const int gy = wrapi(y0 - 2 + r, L);
-            const int8_t* row = a.src + (size_t)gy * L + (size_t)h * Lh;
+            const int8_t* row = a.src + (size_t)wrapi(y0 - 2 + r, L) * L + (size_t)h * Lh;
             const uint32_t d = smem_addr(sb + r * G::P + h * G::PH);
-            const int j0 = (x0 >> 1) - 16;
             if (inner) {
                 bulk_g2s(d, row + j0, G::PH, bar);
             } else {
-                bulk_g2s(d, row + (j0 < 0 ? j0 + Lh : j0), 16, bar);
-                bulk_g2s(d + 16, row + (x0 >> 1), G::H2, bar);
+                bulk_g2s(d, row + (j0 < 0 ? j0 + Lh : j0), 32, bar);
+                bulk_g2s(d + 32, row + (x0 >> 1), G::H2, bar);
                 const int jr = (x0 >> 1) + G::H2;
-                bulk_g2s(d + 16 + G::H2, row + (jr >= Lh ? jr - Lh : jr), 16, bar);
+                bulk_g2s(d + 32 + G::H2, row + (jr >= Lh ? jr - Lh : jr), 32, bar);
             }
         }
     };
@@ -195,26 +237,33 @@ __global__ void __launch_bounds__(MQV_ISING_THREADS, 4) ising2d_sweep(const __gr
     for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
         const int stg = it & 1;
         uint8_t* sb = stage0 + stg * G::STAGE;
-        const int tx = tile % a.ntx, ty = tile / a.ntx;
-        const int x0 = tx * TX, y0 = ty * TY;
-        // prefetch the next tile into the other stage once its stores have read it
+        const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
         const int next = tile + gridDim.x;
         if (warp == 0 && next < a.ntiles) {
-            bulk_wait_read0();
+            bulk_wait_read0();  // the stores of the other stage have read it
             __syncwarp();
             issue_load(next, stg ^ 1);
         }
-        // random top bytes of this tile's updated sites, split by x parity
-        for (int task = tid; task < G::RR * G::NG; task += MQV_ISING_THREADS) {
-            const int rr = task / G::NG, g = task % G::NG;
-            const int gy = wrapi(y0 - 1 + rr, L);
-            const int gx = wrapi(x0 - 16 + 16 * g, L);
-            const uint32_t site0 = (uint32_t)gy * (uint32_t)L + (uint32_t)gx;
-            const uint4 v = philox(site0 >> 4, a.sweep, 0u, tg_acc, a.key);
-            uint8_t* rrow = rnd + rr * G::P + 8 * g + 8;
-            *reinterpret_cast<uint2*>(rrow) = make_uint2(__byte_perm(v.x, v.y, 0x6420), __byte_perm(v.z, v.w, 0x6420));
-            *reinterpret_cast<uint2*>(rrow + G::PH) =
-                make_uint2(__byte_perm(v.x, v.y, 0x7531), __byte_perm(v.z, v.w, 0x7531));
+        // random planes of the updated words (overlaps the copies in flight):
+        // both halves' interior words, and the one ring word colour 0 needs
+        for (int task = tid; task < G::RR * (2 * NWI + 1); task += NT) {
+            const int rr = task / (2 * NWI + 1), k = task % (2 * NWI + 1);
+            int h, w;
+            if (k < 2 * NWI) {
+                h = k / NWI;
+                w = 1 + k % NWI;
+            } else {
+                h = (rr + 1) & 1;
+                w = h ? 0 : NWI + 1;
+            }
+            const int y = wrapi(y0 - 1 + rr, L);
+            const int x = wrapi(x0 - 64 + 64 * w + h, L);
+            const uint32_t g = accept_group((uint32_t)y * (uint32_t)L + (uint32_t)x);
+            const uint4 p0 = philox(g, a.sweep, 0u, tg_acc, a.key);
+            const uint4 p1 = philox(g, a.sweep, 1u, tg_acc, a.key);
+            uint4* dst = reinterpret_cast<uint4*>(planes + ((rr * 2 + h) * NWB + w) * 8);
+            dst[0] = p0;
+            dst[1] = p1;
         }
         // wait for the staged tile (bounded: a stuck copy sets an error status)
         {
@@ -236,24 +285,59 @@ __global__ void __launch_bounds__(MQV_ISING_THREADS, 4) ising2d_sweep(const __gr
                 break;
             }
         }
-        // colour 0 on the tile and its ring (rows 1..TY+2), then colour 1 on the tile
-        phase<TX, TY, 0, TY + 2, TX / 8 + 2, false>(sb, rnd, 1, 3, x0, y0, a, sthr, esum, msum);
+        // pack the staged bytes to bit words
+        for (int task = tid; task < G::R * 2 * NWB; task += NT) {
+            const int r = task / (2 * NWB), rem = task % (2 * NWB), h = rem / NWB, w = rem % NWB;
+            bits[(r * 2 + h) * NWB + w] = pack32(sb + r * G::P + h * G::PH + 32 * w);
+        }
         __syncthreads();
-        phase<TX, TY, 1, TY, TX / 8, MEAS>(sb, rnd, 2, 4, x0, y0, a, sthr, esum, msum);
+        // colour 0 on the tile and its ring: rows 1..TY+2, interior words + one halo word
+        for (int task = tid; task < (TY + 2) * (NWI + 1); task += NT) {
+            const int r = 1 + task / (NWI + 1), k = task % (NWI + 1);
+            const int p = r & 1;
+            const int w = k < NWI ? 1 + k : (p ? 0 : NWI + 1);
+            uint32_t* Hr = bits + (r * 2 + p) * NWB;
+            const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
+            const uint32_t Gw = Gr[w];
+            const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
+            const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
+            const uint32_t* spl = planes + (((r - 1) * 2 + p) * NWB + w) * 8;
+            int dummy = 0;
+            Hr[w] = update_word<false>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w], bits[((r + 1) * 2 + p) * NWB + w], Lb,
+                                       Rb, spl, w, p, wrapi(y0 - 2 + r, L), x0, a, dummy);
+        }
+        __syncthreads();
+        // colour 1 on the tile, then both colours of the tile back to bytes
+        for (int task = tid; task < TY * NWI; task += NT) {
+            const int r = 2 + task / NWI, w = 1 + task % NWI;
+            const int p = (r + 1) & 1;
+            uint32_t* Hr = bits + (r * 2 + p) * NWB;
+            const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
+            const uint32_t Gw = Gr[w];
+            const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
+            const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
+            const uint32_t* spl = planes + (((r - 1) * 2 + p) * NWB + w) * 8;
+            const uint32_t An = update_word<MEAS>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w],
+                                                  bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, spl, w, p,
+                                                  wrapi(y0 - 2 + r, L), x0, a, esum);
+            if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+            unpack32(An, sb + r * G::P + p * G::PH + 32 * w);
+            unpack32(Gw, sb + r * G::P + (1 - p) * G::PH + 32 * w);
+        }
         fence_proxy_async_smem();
         __syncthreads();
         if (warp == 0) {
             for (int task = lane; task < 2 * TY; task += 32) {
                 const int r = 2 + (task >> 1), h = task & 1;
                 int8_t* drow = a.dst + (size_t)(y0 + r - 2) * L + (size_t)h * Lh + (x0 >> 1);
-                bulk_s2g(drow, smem_addr(sb + r * G::P + h * G::PH + 16), G::H2);
+                bulk_s2g(drow, smem_addr(sb + r * G::P + h * G::PH + 32), G::H2);
             }
             bulk_commit();
         }
     }
     if (warp == 0) bulk_wait0();
     if (MEAS) {
-        __shared__ long long red[2][MQV_ISING_THREADS / 32];
+        __shared__ long long red[2][NT / 32];
         long long e = esum, m = msum;
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
@@ -267,7 +351,7 @@ __global__ void __launch_bounds__(MQV_ISING_THREADS, 4) ising2d_sweep(const __gr
         __syncthreads();
         if (tid == 0) {
             long long es = 0, ms = 0;
-            for (int k = 0; k < MQV_ISING_THREADS / 32; ++k) {
+            for (int k = 0; k < NT / 32; ++k) {
                 es += red[0][k];
                 ms += red[1][k];
             }
@@ -308,61 +392,37 @@ constexpr int kIsingTY = 32;
 
 static int tile_width(int L)
 {
-    for (int tx : {256, 128, 64, 32})
+    for (int tx : {512, 256, 128, 64})
         if (L % tx == 0) return tx;
     return 0;
 }
 
-bool ising2d_supported(int L) { return L >= 32 && L % 32 == 0 && tile_width(L) > 0; }
+bool ising2d_supported(int L) { return L >= 64 && L % 64 == 0; }
 
-template <int TX, bool MEAS>
+template <int TX, int NT, bool MEAS>
 static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
     using G = TileGeom<TX, kIsingTY>;
-    auto kern = ising2d_sweep<TX, kIsingTY, MEAS>;
+    auto kern = ising2d_sweep<TX, kIsingTY, NT, MEAS>;
     static int cps = 0;  // resident CTAs per SM for this instantiation
     if (cps == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         if (e != cudaSuccess) return e;
         int c = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, MQV_ISING_THREADS, G::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NT, G::SMEM);
         if (e != cudaSuccess) return e;
         cps = c < 1 ? 1 : c;
     }
     int grid = nsm * cps;
     if (grid > a.ntiles) grid = a.ntiles;
-    kern<<<grid, MQV_ISING_THREADS, G::SMEM, stream>>>(a);
+    kern<<<grid, NT, G::SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 
-template <int TX>
+template <int TX, int NT>
 static cudaError_t launch_tx(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
-    return a.acc ? launch_t<TX, true>(a, nsm, stream) : launch_t<TX, false>(a, nsm, stream);
-}
-
-// Thresholds per aligned-neighbour count a: dE = J (s_new - s_old) sum_nbrs =
-// J (8 - 4a), the cut of update_accepted<1> on u53, its top byte and flags.
-void ising2d_thresholds(double J, double beta, unsigned long long thr[5], uint32_t pools[6])
-{
-    uint32_t t8[2] = {0, 0}, alw[2] = {0, 0}, zt[2] = {0, 0};
-    for (int k = 0; k < 5; ++k) {
-        const double dE = J * (double)(8 - 4 * k);
-        const unsigned long long T = accept_cut(1, dE, beta);
-        thr[k] = T;
-        const unsigned long long hi = T >> 45;
-        const uint32_t c = hi > 255 ? 255u : (uint32_t)hi;
-        const int wd = k >> 2, sh = 8 * (k & 3);
-        t8[wd] |= c << sh;
-        if (T >= (1ull << 53)) alw[wd] |= 0xFFu << sh;
-        if ((T & ((1ull << 45) - 1)) == 0) zt[wd] |= 0xFFu << sh;
-    }
-    pools[0] = t8[0];
-    pools[1] = t8[1];
-    pools[2] = alw[0];
-    pools[3] = alw[1];
-    pools[4] = zt[0];
-    pools[5] = zt[1];
+    return a.acc ? launch_t<TX, NT, true>(a, nsm, stream) : launch_t<TX, NT, false>(a, nsm, stream);
 }
 
 cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
@@ -377,27 +437,34 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
     a.key = make_key(s->seed);
     a.sweep = (uint32_t)s->sweep;
     a.replica = s->replica;
+    // cuts of update_accepted<1> on u53 per aligned-neighbour count k:
+    // dE = J (s_new - s_old) sum_nbrs = J (8 - 4k)
     if (s->thr_J != s->md.J || s->thr_beta != s->md.beta) {
-        ising2d_thresholds(s->md.J, s->md.beta, s->thr_cut, s->thr_pools);
+        for (int k = 0; k < 5; ++k) s->thr_cut[k] = accept_cut(1, s->md.J * (double)(8 - 4 * k), s->md.beta);
         s->thr_J = s->md.J;
         s->thr_beta = s->md.beta;
     }
-    const uint32_t* pools = s->thr_pools;
-    for (int k = 0; k < 5; ++k) a.thr[k] = s->thr_cut[k];
-    a.t8lo = pools[0];
-    a.t8hi = pools[1];
-    a.alwlo = pools[2];
-    a.alwhi = pools[3];
-    a.ztlo = pools[4];
-    a.ztlhi = pools[5];
+    // classes with a nontrivial test: dE > 0 and not every u53 accepted
+    int cls[2] = {-1, -1}, nc = 0;
+    for (int k = 0; k < 5 && nc < 2; ++k)
+        if (s->md.J * (double)(8 - 4 * k) > 0 && s->thr_cut[k] < (1ull << 53)) cls[nc++] = k;
+    const unsigned long long TA = cls[0] >= 0 ? s->thr_cut[cls[0]] : 0, TB = cls[1] >= 0 ? s->thr_cut[cls[1]] : 0;
+    a.clsA = cls[0];
+    a.clsB = cls[1];
+    a.tA = TA;
+    a.tB = TB;
+    a.tA8 = (uint32_t)(TA >> 45);
+    a.tB8 = (uint32_t)(TB >> 45);
+    a.ztA = (TA & ((1ull << 45) - 1)) == 0;
+    a.ztB = (TB & ((1ull << 45) - 1)) == 0;
     a.acc = acc;
     a.status = s->d_status;
     const int nsm = s->num_sms;
     switch (TX) {
-    case 256: return launch_tx<256>(a, nsm, s->stream);
-    case 128: return launch_tx<128>(a, nsm, s->stream);
-    case 64: return launch_tx<64>(a, nsm, s->stream);
-    default: return launch_tx<32>(a, nsm, s->stream);
+    case 512: return launch_tx<512, 256>(a, nsm, s->stream);
+    case 256: return launch_tx<256, 128>(a, nsm, s->stream);
+    case 128: return launch_tx<128, 128>(a, nsm, s->stream);
+    default: return launch_tx<64, 64>(a, nsm, s->stream);
     }
 }
 

@@ -61,20 +61,30 @@ uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
     return (uint64_t)o[0] | ((uint64_t)o[1] << 32);
 }
 
-/* The acceptance word of site i in sweep t: its top byte is byte (i & 15) of
- * the Philox block (c0 = i >> 4, c1 = t, c2 = 0, ACCEPT stream) -- one block
- * serves 16 consecutive sites -- and its low 56 bits are the low 56 bits of
- * half (i & 1) of the block (c0 = i >> 1, c1 = t, c2 = 0, ACCEPT_FINE stream).
- * A comparison of real() against a threshold is decided by the top byte
- * unless it ties with the threshold's top byte. */
+/* The acceptance word of site i in sweep t.  Its top byte is bit-sliced:
+ * sites are grouped by G(i) = ((i >> 6) << 1) | (i & 1) -- 32 sites of equal
+ * index parity in an aligned run of 64 -- and bit b of the byte is bit
+ * ((i >> 1) & 31) of plane b, where planes 0..3 are the Philox block
+ * (c0 = G(i), c1 = t, c2 = 0, ACCEPT stream) and planes 4..7 the block with
+ * c2 = 1.  Its low 56 bits are the low 56 bits of half (i & 1) of the block
+ * (c0 = i >> 1, c1 = t, c2 = 0, ACCEPT_FINE stream).  A comparison of real()
+ * against a threshold is decided by the top byte unless it ties with the
+ * threshold's top byte. */
 uint64_t orc_accept_word(uint64_t seed, uint32_t replica, uint32_t site, uint32_t sweep)
 {
     uint32_t key[2] = {(uint32_t)seed, (uint32_t)(seed >> 32)};
-    uint32_t ctr[4] = {site >> 4, sweep, 0, (ST_ACCEPT << 24) | (replica & 0xFFFFFFu)};
+    const uint32_t g = ((site >> 6) << 1) | (site & 1u), q = (site >> 1) & 31u;
+    uint32_t p0[4], p1[4];
+    uint32_t ctr0[4] = {g, sweep, 0, (ST_ACCEPT << 24) | (replica & 0xFFFFFFu)};
+    uint32_t ctr1[4] = {g, sweep, 1, (ST_ACCEPT << 24) | (replica & 0xFFFFFFu)};
+    orc_philox4x32_10(ctr0, key, p0);
+    orc_philox4x32_10(ctr1, key, p1);
+    uint64_t cb = 0;
+    for (int b = 0; b < 8; ++b) {
+        const uint32_t plane = b < 4 ? p0[b] : p1[b - 4];
+        cb |= (uint64_t)((plane >> q) & 1u) << b;
+    }
     uint32_t o[4];
-    orc_philox4x32_10(ctr, key, o);
-    const uint32_t b = site & 15u;
-    const uint64_t cb = (o[b >> 2] >> (8 * (b & 3))) & 0xFFu;
     uint32_t ctrf[4] = {site >> 1, sweep, 0, (ST_ACCEPT_FINE << 24) | (replica & 0xFFFFFFu)};
     orc_philox4x32_10(ctrf, key, o);
     const uint64_t f = (site & 1u) ? ((uint64_t)o[2] | ((uint64_t)o[3] << 32)) : ((uint64_t)o[0] | ((uint64_t)o[1] << 32));

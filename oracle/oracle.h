@@ -28,8 +28,9 @@ void orc_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
  * 2b+1 are the two halves of the Philox block with c2 = b. */
 uint64_t orc_draw(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
                   uint32_t c1, uint32_t k);
-/* The Metropolis acceptance word of `site` in `sweep` (top byte from a block
- * shared by 16 sites, low 56 bits from a block shared by 2 sites). */
+/* The Metropolis acceptance word of `site` in `sweep` (top byte bit-sliced
+ * from two Philox blocks shared by 32 sites, low 56 bits from a block shared
+ * by 2 sites). */
 uint64_t orc_accept_word(uint64_t seed, uint32_t replica, uint32_t site, uint32_t sweep);
 /* single draw keyed fully by the counter words (used for Wolff bonds) */
 uint64_t orc_draw_c2(uint64_t seed, uint32_t replica, uint32_t stream, uint32_t c0,
