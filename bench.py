@@ -259,6 +259,7 @@ def run_engine(args, ws, rank, local):
         torch.cuda.synchronize()
         barrier()
     launches = core.launches - l0
+    kernel_desc = core.describe()
     ms = ev0.elapsed_time(ev1)
     ms_max = max_over_ranks(ms)
     updates = n * args.nmetro * args.steps
@@ -302,7 +303,7 @@ def run_engine(args, ws, rank, local):
     tr = profiled_traffic("ising2d_sweep")
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None if tr is None else tr.get("bytes_per_launch"),
-            "kernel": "ising2d_sweep<512,32,256>", "peak_source": f"{peak_kind} hbm_gbs",
+            "kernel": kernel_desc.split("kernel=")[-1], "peak_source": f"{peak_kind} hbm_gbs",
             "algorithmic_bytes_per_launch": alg_bytes}
 
     line = {

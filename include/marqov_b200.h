@@ -174,6 +174,9 @@ MQV_API mqv_status mqv_emcs(mqv_sim* sim, int32_t n_emcs, int32_t ncluster, int3
 /* Observables of the current state. */
 MQV_API mqv_status mqv_measure(mqv_sim* sim, mqv_obs* out);
 MQV_API mqv_status mqv_synchronize(mqv_sim* sim);
+/* Human-readable description of the handle's kernel path (e.g. the autotuned
+ * fused-sweep configuration), NUL-terminated. */
+MQV_API mqv_status mqv_describe(mqv_sim* sim, char* buf, size_t len);
 /* Number of engine kernel launches issued by this handle so far. */
 MQV_API mqv_status mqv_launch_count(mqv_sim* sim, uint64_t* count);
 

@@ -88,6 +88,7 @@ SIGNATURES = {
     "mqv_measure": (C.c_int32, [_vp, C.POINTER(Obs)]),
     "mqv_synchronize": (C.c_int32, [_vp]),
     "mqv_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
+    "mqv_describe": (C.c_int32, [_vp, C.c_char_p, C.c_size_t]),
     "mqv_selftest_philox": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                         _vp, _vp]),
 }

@@ -207,6 +207,11 @@ class Core:
     def counters(self, v):
         L.check(self._lib.mqv_set_counters(self._h, int(v[0]), int(v[1])))
 
+    def describe(self) -> str:
+        buf = C.create_string_buffer(256)
+        L.check(self._lib.mqv_describe(self._h, buf, len(buf)))
+        return buf.value.decode()
+
     @property
     def launches(self) -> int:
         c = C.c_uint64()

@@ -49,6 +49,7 @@ unsigned long long accept_cut(int pref, double dE, double beta)
 static bool is_f32_kind(int k) { return k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ; }
 
 bool ising2d_supported(int L);
+const char* ising2d_config_name(Sim* s, char* buf, int len);
 cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split);
 cudaError_t launch_merge_rows(Sim* s, const void* split, void* rowmajor);
 
@@ -692,6 +693,19 @@ MQV_API mqv_status mqv_synchronize(mqv_sim* h)
     MQV_GUARD(s);
     MQV_CK(cudaStreamSynchronize(s->stream));
     return check_device_status(s);
+}
+
+MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !buf || len == 0) return fail(MQV_ERR_INVALID_ARG, "bad arguments");
+    char cfg[96] = "";
+    if (s->fused_ising2d) ising2d_config_name(s, cfg, sizeof(cfg));
+    std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s", s->md.kind,
+                  s->lat_kind == MQV_LATTICE_HYPERCUBIC ? "hypercubic" : "csr", (long long)s->n,
+                  s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8"),
+                  cfg[0] ? " kernel=" : "", cfg);
+    return MQV_OK;
 }
 
 MQV_API mqv_status mqv_launch_count(mqv_sim* h, uint64_t* count)

@@ -25,16 +25,12 @@ MQV_HD Key make_key(uint64_t seed) { return Key{(uint32_t)seed, (uint32_t)(seed 
 
 MQV_HD uint32_t tag(uint32_t stream, uint32_t replica) { return (stream << 24) | (replica & 0xFFFFFFu); }
 
+// 32 x 32 -> 64-bit product (one wide multiply-add on the GPU)
 MQV_HD void mulhilo(uint32_t a, uint32_t b, uint32_t& hi, uint32_t& lo)
 {
-#ifdef __CUDA_ARCH__
-    hi = __umulhi(a, b);
-    lo = a * b;
-#else
-    uint64_t p = (uint64_t)a * b;
+    const uint64_t p = (uint64_t)a * b;
     hi = (uint32_t)(p >> 32);
     lo = (uint32_t)p;
-#endif
 }
 
 // Philox4x32-10 (Salmon et al., SC'11): 10 rounds, multipliers 0xD2511F53 /

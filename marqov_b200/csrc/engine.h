@@ -107,7 +107,7 @@ struct Sim {
     int* d_status = nullptr;  // device error word of bounded waits
     double thr_J = 0, thr_beta = -1;  // (J, beta) the cached 2D thresholds belong to
     unsigned long long thr_cut[5] = {};
-    uint32_t thr_pools[6] = {};
+    int sweep_cfg = -1;  // autotuned fused-sweep configuration (-1: not chosen yet)
     // measurement
     int nslots = 0;
     long long* d_acc = nullptr;  // nslots * kAccStride

@@ -9,9 +9,11 @@
 //
 // Pipeline: one persistent CTA per SM slot loops over TY x TX tiles.  While it
 // updates tile n, the bulk-copy engine (cp.async.bulk completing on an
-// mbarrier) stages tile n+1 plus a two-row / 64-column halo of the old state;
-// updated tiles leave shared memory by bulk stores to the other state buffer.
-// Every site is read from HBM once and written once per sweep (2 bytes).
+// mbarrier) stages tile n+1 plus a two-row / 64-column halo of the old state
+// in the other input stage; updated tiles are unpacked into an output stage
+// and leave by bulk stores to the other state buffer.  Every site is read from
+// HBM once and written once per sweep (2 bytes).  Tile shape and CTA size are
+// picked per lattice size by timing the candidates on the first sweep.
 //
 // In shared memory each staged half-row is packed to one bit per site (1 =
 // spin -1) in 32-site words.  Colour 0 is updated on the tile and its
@@ -28,6 +30,8 @@
 // threshold's top byte (probability 1/256) is resolved with the site's fine
 // block.  The result equals update_accepted<1>(dE, beta, word) bit for bit.
 #include <cuda_runtime.h>
+
+#include <cstdio>
 
 #include "engine.h"
 
@@ -59,12 +63,11 @@ struct TileGeom {
     static constexpr int PH = NWB * 32;  // staged bytes per half-row
     static constexpr int P = 2 * PH;     // staged bytes per row
     static constexpr int R = TY + 4;     // staged rows y0-2 .. y0+TY+1
-    static constexpr int RR = TY + 2;    // rows with random planes y0-1 .. y0+TY
-    static constexpr int STAGE = R * P;
+    static constexpr int STAGE = R * P;  // one input stage
+    static constexpr int OUT = TY * TX;  // output stage: interior rows, both halves
     static constexpr int BITS = R * 2 * NWB * 4;
-    static constexpr int PLANES = RR * 2 * NWB * 32;
     static constexpr uint32_t TX_BYTES = (uint32_t)(R * P);
-    static constexpr int SMEM = 2 * STAGE + BITS + PLANES + 64;
+    static constexpr int SMEM = 2 * STAGE + OUT + BITS + 64;
 };
 
 // CTAs per SM that shared memory admits (228 KB per SM, 1 KB reserved per CTA)
@@ -99,11 +102,12 @@ __device__ __forceinline__ uint32_t class_mask(uint32_t A, uint32_t m0, uint32_t
 }
 
 // Tie bits: compare the full acceptance word with the class threshold.
-__device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, const uint32_t* spl, int w, int half, int y,
+__device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, uint4 q0, uint4 q1, int w, int half, int y,
                                               int x0, int L, Key key, uint32_t sweep, uint32_t replica,
                                               unsigned long long tA, unsigned long long tB)
 {
     uint32_t acc = 0;
+    const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     while (tie) {
         const int b = __ffs(tie) - 1;
         tie &= tie - 1;
@@ -111,7 +115,7 @@ __device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, cons
         const uint32_t site = (uint32_t)y * (uint32_t)L + (uint32_t)x;
         uint64_t cb = 0;
 #pragma unroll
-        for (int k = 0; k < 8; ++k) cb |= (uint64_t)((spl[k] >> b) & 1u) << k;
+        for (int k = 0; k < 8; ++k) cb |= (uint64_t)((pl[k] >> b) & 1u) << k;
         const uint64_t u53 = ((cb << 56) | accept_fine56(key, site, sweep, replica)) >> 11;
         const unsigned long long T = ((maskA >> b) & 1u) ? tA : tB;
         if (u53 < T) acc |= 1u << b;
@@ -121,12 +125,15 @@ __device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, cons
 
 // Update the active-colour sites of one 32-site word; returns the new word.
 template <bool MEAS>
-__device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb,
-                                                const uint32_t* spl, int w, int half, int y, int x0,
-                                                const Ising2DArgs& a, int& esum)
+__device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb, int w,
+                                                int half, int y, int x0, uint32_t tg_acc, const Ising2DArgs& a,
+                                                int& esum)
 {
-    // the word's eight random planes (shared memory)
-    const uint4 q0 = reinterpret_cast<const uint4*>(spl)[0], q1 = reinterpret_cast<const uint4*>(spl)[1];
+    // the word's eight random planes: two Philox blocks of its 32-site group
+    const int x = wrapi(x0 - 64 + 64 * w + half, a.L);
+    const uint32_t g = accept_group((uint32_t)y * (uint32_t)a.L + (uint32_t)x);
+    const uint4 q0 = philox(g, a.sweep, 0u, tg_acc, a.key);
+    const uint4 q1 = philox(g, a.sweep, 1u, tg_acc, a.key);
     const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder)
     const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
@@ -148,7 +155,7 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
     uint32_t acc = ~test | borrow;
     const uint32_t zt = (maskA & (0u - a.ztA)) | (maskB & (0u - a.ztB));
     const uint32_t tie = eq & test & ~zt;
-    if (tie) acc |= resolve_ties(tie, maskA, spl, w, half, y, x0, a.L, a.key, a.sweep, a.replica, a.tA, a.tB);
+    if (tie) acc |= resolve_ties(tie, maskA, q0, q1, w, half, y, x0, a.L, a.key, a.sweep, a.replica, a.tA, a.tB);
     const uint32_t An = A ^ acc;
     if (MEAS) {
         // sum over the word's bonds s * sum(nbrs) = sum (1 - 2a)(4 - 2M)
@@ -159,18 +166,13 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
     return An;
 }
 
-// 32 staged bytes (+-1) -> 32 bits (1 = -1)
-__device__ __forceinline__ uint32_t pack32(const uint8_t* p)
+// 16 staged bytes (+-1) -> 16 bits (1 = -1)
+__device__ __forceinline__ uint32_t pack16(uint4 v)
 {
-    const uint4 v0 = *reinterpret_cast<const uint4*>(p);
-    const uint4 v1 = *reinterpret_cast<const uint4*>(p + 16);
     const unsigned long long M = 0x0101010101010101ull, G = 0x0102040810204080ull;
-    const unsigned long long q0 = ((((unsigned long long)v0.y << 32) | v0.x) >> 1) & M;
-    const unsigned long long q1 = ((((unsigned long long)v0.w << 32) | v0.z) >> 1) & M;
-    const unsigned long long q2 = ((((unsigned long long)v1.y << 32) | v1.x) >> 1) & M;
-    const unsigned long long q3 = ((((unsigned long long)v1.w << 32) | v1.z) >> 1) & M;
-    return (uint32_t)((q0 * G) >> 56) | ((uint32_t)((q1 * G) >> 56) << 8) | ((uint32_t)((q2 * G) >> 56) << 16) |
-           ((uint32_t)((q3 * G) >> 56) << 24);
+    const unsigned long long q0 = ((((unsigned long long)v.y << 32) | v.x) >> 1) & M;
+    const unsigned long long q1 = ((((unsigned long long)v.w << 32) | v.z) >> 1) & M;
+    return (uint32_t)((q0 * G) >> 56) | ((uint32_t)((q1 * G) >> 56) << 8);
 }
 
 // 32 bits -> 32 staged bytes (+1 -> 0x01, -1 -> 0xFF)
@@ -192,10 +194,10 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
     using G = TileGeom<TX, TY>;
     constexpr int NWI = G::NWI, NWB = G::NWB;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* stage0 = smem;
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE);             // [R][2][NWB]
-    uint32_t* planes = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE + G::BITS);  // [RR][2][NWB][8]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * G::STAGE + G::BITS + G::PLANES);
+    uint8_t* stage0 = smem;                                                       // [2][R][2][PH]
+    uint8_t* out = smem + 2 * G::STAGE;                                           // [TY][2][H2]
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE + G::OUT);  // [R][2][NWB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * G::STAGE + G::OUT + G::BITS);
     const int tid = threadIdx.x;
     const int warp = tid >> 5, lane = tid & 31;
     const int L = a.L, Lh = L >> 1;
@@ -212,6 +214,7 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
         const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
         uint8_t* sb = stage0 + stg * G::STAGE;
         const uint32_t bar = smem_addr(&bars[stg]);
+        fence_proxy_async_smem();
         if (lane == 0) mbar_expect_tx(bar, G::TX_BYTES);
         __syncwarp();
         const bool inner = x0 > 0 && x0 + TX < L;
@@ -236,40 +239,16 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
     if (tile < a.ntiles && warp == 0) issue_load(tile, 0);
     for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
         const int stg = it & 1;
-        uint8_t* sb = stage0 + stg * G::STAGE;
+        const uint8_t* sb = stage0 + stg * G::STAGE;
         const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
         const int next = tile + gridDim.x;
-        if (warp == 0 && next < a.ntiles) {
-            bulk_wait_read0();  // the stores of the other stage have read it
-            __syncwarp();
-            issue_load(next, stg ^ 1);
-        }
-        // random planes of the updated words (overlaps the copies in flight):
-        // both halves' interior words, and the one ring word colour 0 needs
-        for (int task = tid; task < G::RR * (2 * NWI + 1); task += NT) {
-            const int rr = task / (2 * NWI + 1), k = task % (2 * NWI + 1);
-            int h, w;
-            if (k < 2 * NWI) {
-                h = k / NWI;
-                w = 1 + k % NWI;
-            } else {
-                h = (rr + 1) & 1;
-                w = h ? 0 : NWI + 1;
-            }
-            const int y = wrapi(y0 - 1 + rr, L);
-            const int x = wrapi(x0 - 64 + 64 * w + h, L);
-            const uint32_t g = accept_group((uint32_t)y * (uint32_t)L + (uint32_t)x);
-            const uint4 p0 = philox(g, a.sweep, 0u, tg_acc, a.key);
-            const uint4 p1 = philox(g, a.sweep, 1u, tg_acc, a.key);
-            uint4* dst = reinterpret_cast<uint4*>(planes + ((rr * 2 + h) * NWB + w) * 8);
-            dst[0] = p0;
-            dst[1] = p1;
-        }
-        // wait for the staged tile (bounded: a stuck copy sets an error status)
-        {
+        if (warp == 0 && next < a.ntiles) issue_load(next, stg ^ 1);
+        // one thread waits for the staged tile (bounded: a stuck copy sets an
+        // error status); the barrier publishes the data to the CTA
+        int timed_out = 0;
+        if (tid == 0) {
             const uint32_t bar = smem_addr(&bars[stg]);
             const uint32_t par = (uint32_t)(it >> 1) & 1u;
-            int timed_out = 0;
             if (!mbar_try_wait(bar, par)) {
                 const uint64_t t0 = global_timer_ns();
                 for (uint32_t k = 1;; ++k) {
@@ -280,15 +259,17 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
                     }
                 }
             }
-            if (__syncthreads_or(timed_out)) {
-                if (tid == 0) atomicExch(a.status, MQV_ERR_TIMEOUT);
-                break;
-            }
         }
-        // pack the staged bytes to bit words
-        for (int task = tid; task < G::R * 2 * NWB; task += NT) {
-            const int r = task / (2 * NWB), rem = task % (2 * NWB), h = rem / NWB, w = rem % NWB;
-            bits[(r * 2 + h) * NWB + w] = pack32(sb + r * G::P + h * G::PH + 32 * w);
+        if (__syncthreads_or(timed_out)) {
+            if (tid == 0) atomicExch(a.status, MQV_ERR_TIMEOUT);
+            break;
+        }
+        // pack: one 16-byte chunk per thread, lane pairs form a 32-site word
+        for (int base = 0; base < G::STAGE / 16; base += NT) {
+            const int c = base + tid;
+            const uint32_t h16 = c < G::STAGE / 16 ? pack16(reinterpret_cast<const uint4*>(sb)[c]) : 0u;
+            const uint32_t hi = __shfl_down_sync(0xffffffffu, h16, 1);
+            if (!(c & 1) && c < G::STAGE / 16) bits[c >> 1] = h16 | (hi << 16);
         }
         __syncthreads();
         // colour 0 on the tile and its ring: rows 1..TY+2, interior words + one halo word
@@ -301,13 +282,13 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
             const uint32_t Gw = Gr[w];
             const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
             const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
-            const uint32_t* spl = planes + (((r - 1) * 2 + p) * NWB + w) * 8;
             int dummy = 0;
             Hr[w] = update_word<false>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w], bits[((r + 1) * 2 + p) * NWB + w], Lb,
-                                       Rb, spl, w, p, wrapi(y0 - 2 + r, L), x0, a, dummy);
+                                       Rb, w, p, wrapi(y0 - 2 + r, L), x0, tg_acc, a, dummy);
         }
+        if (warp == 0) bulk_wait_read0();  // the previous tile's stores have read the output stage
         __syncthreads();
-        // colour 1 on the tile, then both colours of the tile back to bytes
+        // colour 1 on the tile, then both colours of the tile to the output stage
         for (int task = tid; task < TY * NWI; task += NT) {
             const int r = 2 + task / NWI, w = 1 + task % NWI;
             const int p = (r + 1) & 1;
@@ -316,21 +297,21 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
             const uint32_t Gw = Gr[w];
             const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
             const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
-            const uint32_t* spl = planes + (((r - 1) * 2 + p) * NWB + w) * 8;
             const uint32_t An = update_word<MEAS>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w],
-                                                  bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, spl, w, p,
-                                                  wrapi(y0 - 2 + r, L), x0, a, esum);
+                                                  bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, w, p,
+                                                  wrapi(y0 - 2 + r, L), x0, tg_acc, a, esum);
             if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
-            unpack32(An, sb + r * G::P + p * G::PH + 32 * w);
-            unpack32(Gw, sb + r * G::P + (1 - p) * G::PH + 32 * w);
+            uint8_t* orow = out + (r - 2) * TX;
+            unpack32(An, orow + p * G::H2 + 32 * (w - 1));
+            unpack32(Gw, orow + (1 - p) * G::H2 + 32 * (w - 1));
         }
         fence_proxy_async_smem();
         __syncthreads();
         if (warp == 0) {
             for (int task = lane; task < 2 * TY; task += 32) {
-                const int r = 2 + (task >> 1), h = task & 1;
-                int8_t* drow = a.dst + (size_t)(y0 + r - 2) * L + (size_t)h * Lh + (x0 >> 1);
-                bulk_s2g(drow, smem_addr(sb + r * G::P + h * G::PH + 32), G::H2);
+                const int r = task >> 1, h = task & 1;
+                int8_t* drow = a.dst + (size_t)(y0 + r) * L + (size_t)h * Lh + (x0 >> 1);
+                bulk_s2g(drow, smem_addr(out + r * TX + h * G::H2), G::H2);
             }
             bulk_commit();
         }
@@ -388,22 +369,15 @@ __global__ void merge_rows(const int8_t* __restrict__ in, int8_t* __restrict__ o
 
 // ---- host side ------------------------------------------------------------------
 
-constexpr int kIsingTY = 32;
-
-static int tile_width(int L)
-{
-    for (int tx : {512, 256, 128, 64})
-        if (L % tx == 0) return tx;
-    return 0;
-}
-
 bool ising2d_supported(int L) { return L >= 64 && L % 64 == 0; }
 
-template <int TX, int NT, bool MEAS>
+typedef cudaError_t (*SweepLauncher)(const Ising2DArgs&, int, cudaStream_t);
+
+template <int TX, int TY, int NT, bool MEAS>
 static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
-    using G = TileGeom<TX, kIsingTY>;
-    auto kern = ising2d_sweep<TX, kIsingTY, NT, MEAS>;
+    using G = TileGeom<TX, TY>;
+    auto kern = ising2d_sweep<TX, TY, NT, MEAS>;
     static int cps = 0;  // resident CTAs per SM for this instantiation
     if (cps == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
@@ -419,21 +393,31 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-template <int TX, int NT>
-static cudaError_t launch_tx(const Ising2DArgs& a, int nsm, cudaStream_t stream)
-{
-    return a.acc ? launch_t<TX, NT, true>(a, nsm, stream) : launch_t<TX, NT, false>(a, nsm, stream);
-}
+// Candidate tile shapes and CTA sizes.  Every candidate computes the same
+// result; the autotuner keeps the fastest for a lattice size.
+struct SweepConfig {
+    int tx, ty, nt;
+    SweepLauncher plain, meas;
+};
 
-cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
+#define MQV_CFG(TX, TY, NT) \
+    SweepConfig{TX, TY, NT, launch_t<TX, TY, NT, false>, launch_t<TX, TY, NT, true>}
+
+static const SweepConfig kConfigs[] = {
+    MQV_CFG(512, 32, 256), MQV_CFG(512, 32, 320), MQV_CFG(256, 32, 128), MQV_CFG(256, 32, 160),
+    MQV_CFG(256, 64, 256), MQV_CFG(128, 32, 128), MQV_CFG(64, 32, 64),
+};
+constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
+
+static bool config_fits(const SweepConfig& c, int L) { return L % c.tx == 0 && L % c.ty == 0; }
+
+static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs& a)
 {
-    const int TX = tile_width(s->len);
-    Ising2DArgs a{};
     a.src = (const int8_t*)s->state[s->cur];
     a.dst = (int8_t*)s->state[s->cur ^ 1];
     a.L = s->len;
-    a.ntx = s->len / TX;
-    a.ntiles = a.ntx * (s->len / kIsingTY);
+    a.ntx = s->len / c.tx;
+    a.ntiles = a.ntx * (s->len / c.ty);
     a.key = make_key(s->seed);
     a.sweep = (uint32_t)s->sweep;
     a.replica = s->replica;
@@ -459,13 +443,68 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
     a.ztB = (TB & ((1ull << 45) - 1)) == 0;
     a.acc = acc;
     a.status = s->d_status;
-    const int nsm = s->num_sms;
-    switch (TX) {
-    case 512: return launch_tx<512, 256>(a, nsm, s->stream);
-    case 256: return launch_tx<256, 128>(a, nsm, s->stream);
-    case 128: return launch_tx<128, 128>(a, nsm, s->stream);
-    default: return launch_tx<64, 64>(a, nsm, s->stream);
+}
+
+// Time every fitting candidate on this lattice (two sweeps each into the
+// scratch buffer; the state is not modified) and keep the fastest.  Small
+// lattices take the first fitting candidate.
+static int pick_config(Sim* s)
+{
+    int first = -1;
+    for (int k = 0; k < kNumConfigs; ++k)
+        if (config_fits(kConfigs[k], s->len)) {
+            first = k;
+            break;
+        }
+    if (s->len < 2048 || first < 0) return first;
+    cudaEvent_t e0, e1;
+    if (cudaEventCreate(&e0) != cudaSuccess) return first;
+    if (cudaEventCreate(&e1) != cudaSuccess) {
+        cudaEventDestroy(e0);
+        return first;
     }
+    int best = first;
+    float best_ms = 1e30f;
+    for (int k = 0; k < kNumConfigs; ++k) {
+        if (!config_fits(kConfigs[k], s->len)) continue;
+        Ising2DArgs a{};
+        fill_args(s, kConfigs[k], nullptr, a);
+        if (kConfigs[k].plain(a, s->num_sms, s->stream) != cudaSuccess) continue;  // warm-up
+        cudaEventRecord(e0, s->stream);
+        kConfigs[k].plain(a, s->num_sms, s->stream);
+        kConfigs[k].plain(a, s->num_sms, s->stream);
+        cudaEventRecord(e1, s->stream);
+        s->launches += 3;
+        float ms = 0;
+        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+            best_ms = ms;
+            best = k;
+        }
+    }
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    return best;
+}
+
+cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
+{
+    if (s->sweep_cfg < 0) {
+        s->sweep_cfg = pick_config(s);
+        if (s->sweep_cfg < 0) return cudaErrorInvalidValue;
+    }
+    const SweepConfig& c = kConfigs[s->sweep_cfg];
+    Ising2DArgs a{};
+    fill_args(s, c, acc, a);
+    return acc ? c.meas(a, s->num_sms, s->stream) : c.plain(a, s->num_sms, s->stream);
+}
+
+const char* ising2d_config_name(Sim* s, char* buf, int len)
+{
+    if (s->sweep_cfg < 0) return "";
+    const SweepConfig& c = kConfigs[s->sweep_cfg];
+    snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nt);
+    return buf;
 }
 
 cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split)
