@@ -90,7 +90,7 @@ static void free_sim(Sim* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (void* p : {s->state[0], s->state[1], (void*)s->d_rp, (void*)s->d_ci, (void*)s->d_bonds, (void*)s->d_order,
                     (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize,
-                    (void*)s->d_status})
+                    (void*)s->d_status, (void*)s->d_counter})
         if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -408,7 +408,8 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
                        (s->md.kind == MQV_MODEL_ISING || s->md.kind == MQV_MODEL_ISING_EMBED);
     s->sten.split = s->fused_ising2d ? 1 : 0;
     cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
-    if (cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess || cudaMemset(s->d_status, 0, sizeof(int)) != cudaSuccess) {
+    if (cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess || cudaMemset(s->d_status, 0, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&s->d_counter, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of the status word failed");
         return bail(MQV_ERR_OUT_OF_MEMORY);

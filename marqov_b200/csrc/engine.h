@@ -104,7 +104,8 @@ struct Sim {
     // fused 2D Ising path (ising2d.cu): state in split rows
     bool fused_ising2d = false;
     int num_sms = 148;
-    int* d_status = nullptr;  // device error word of bounded waits
+    int* d_status = nullptr;   // device error word of bounded waits
+    int* d_counter = nullptr;  // tile counter of the fused sweep
     double thr_J = 0, thr_beta = -1;  // (J, beta) the cached 2D thresholds belong to
     unsigned long long thr_cut[5] = {};
     int sweep_cfg = -1;  // autotuned fused-sweep configuration (-1: not chosen yet)

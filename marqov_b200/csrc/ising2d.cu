@@ -7,16 +7,19 @@
 // are element j of the same half in the rows above and below and elements
 // j-1, j (even half) or j, j+1 (odd half) of the other half of the row.
 //
-// Pipeline: one persistent CTA per SM slot loops over TY x TX tiles.  While it
-// updates tile n, the bulk-copy engine (cp.async.bulk completing on an
-// mbarrier) stages tile n+1 plus a two-row / 64-column halo of the old state
-// in the other input stage; updated tiles are unpacked into an output stage
-// and leave by bulk stores to the other state buffer.  Every site is read from
-// HBM once and written once per sweep (2 bytes).  Tile shape and CTA size are
-// picked per lattice size by timing the candidates on the first sweep.
+// Pipeline: every warp is an independent worker with its own shared-memory
+// partition.  It takes TY x TX tiles from a global tile counter; the rows of a
+// tile plus a two-row / 64-column halo of the old state stream in through an
+// 8-row staging ring filled by the bulk-copy engine (cp.async.bulk, one
+// mbarrier per slot), are packed to bits as they arrive, and the updated rows
+// leave through an output ring drained by bulk stores to the other state
+// buffer.  Loads for the next tile are in flight while the warp updates the
+// current one; the warp only ever synchronises with itself.  Every site is
+// read from HBM once and written once per sweep (2 bytes).  Tile shape and
+// warps per CTA are picked per lattice size by timing the candidates.
 //
-// In shared memory each staged half-row is packed to one bit per site (1 =
-// spin -1) in 32-site words.  Colour 0 is updated on the tile and its
+// Each staged half-row is packed to one bit per site (1 = spin -1) in 32-site
+// words.  Colour 0 is updated on the tile and its
 // one-site ring (re-deriving the neighbouring tiles' updates, which are
 // deterministic), then colour 1 on the tile; a 32-site word costs a few dozen
 // logic instructions: neighbour counts by a carry-save adder on the bit
@@ -53,30 +56,27 @@ struct Ising2DArgs {
     unsigned long long tA, tB;  // full u53 thresholds
     long long* acc;
     int* status;
+    int* counter;  // next tile (zeroed before the launch)
 };
 
-template <int TX, int TY>
+template <int TX, int TY, int NWARP>
 struct TileGeom {
-    static constexpr int NWI = TX / 64;  // interior 32-site words per half-row
-    static constexpr int NWB = NWI + 2;  // with one halo word on each side
-    static constexpr int H2 = TX / 2;    // interior sites per half-row
-    static constexpr int PH = NWB * 32;  // staged bytes per half-row
-    static constexpr int P = 2 * PH;     // staged bytes per row
-    static constexpr int R = TY + 4;     // staged rows y0-2 .. y0+TY+1
-    static constexpr int STAGE = R * P;  // one input stage
-    static constexpr int OUT = TY * TX;  // output stage: interior rows, both halves
+    static constexpr int NWI = TX / 64;         // interior 32-site words per half-row
+    static constexpr int NWB = NWI + 2;         // with one halo word on each side
+    static constexpr int H2 = TX / 2;           // interior sites per half-row
+    static constexpr int PH = NWB * 32;         // staged bytes per half-row
+    static constexpr int P = 2 * PH;            // staged bytes per row
+    static constexpr int R = TY + 4;            // staged rows y0-2 .. y0+TY+1
+    static constexpr int NS = 8;                // staging ring rows
+    static constexpr int RPG = 32 / NWI;        // rows per 32 colour-1 words
+    static constexpr int NO = 2 * RPG;          // output ring rows (two store groups)
     static constexpr int BITS = R * 2 * NWB * 4;
-    static constexpr uint32_t TX_BYTES = (uint32_t)(R * P);
-    static constexpr int SMEM = 2 * STAGE + OUT + BITS + 64;
+    static constexpr int STAGE = NS * P;
+    static constexpr int OUT = NO * TX;
+    static constexpr int WARP = ((STAGE + OUT + BITS + NS * 8) + 127) / 128 * 128;  // per-warp partition
+    static constexpr int SMEM = NWARP * WARP;
+    static_assert(R % 4 == 0 && 32 % NWI == 0, "tile shape");
 };
-
-// CTAs per SM that shared memory admits (228 KB per SM, 1 KB reserved per CTA)
-template <int TX, int TY, int NT>
-constexpr int min_blocks()
-{
-    return (228 * 1024) / (TileGeom<TX, TY>::SMEM + 1024) < 2048 / NT ? (228 * 1024) / (TileGeom<TX, TY>::SMEM + 1024)
-                                                                      : 2048 / NT;
-}
 
 __device__ __forceinline__ int wrapi(int v, int L)
 {
@@ -188,92 +188,118 @@ __device__ __forceinline__ void unpack32(uint32_t bits, uint8_t* p)
     *reinterpret_cast<uint4*>(p + 16) = make_uint4(o[4], o[5], o[6], o[7]);
 }
 
-template <int TX, int TY, int NT, bool MEAS>
-__global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(const __grid_constant__ Ising2DArgs a)
+template <int TX, int TY, int NWARP, bool MEAS>
+__global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constant__ Ising2DArgs a)
 {
-    using G = TileGeom<TX, TY>;
-    constexpr int NWI = G::NWI, NWB = G::NWB;
+    using G = TileGeom<TX, TY, NWARP>;
+    constexpr int NWI = G::NWI, NWB = G::NWB, R = G::R, NS = G::NS;
     extern __shared__ __align__(128) uint8_t smem[];
-    uint8_t* stage0 = smem;                                                       // [2][R][2][PH]
-    uint8_t* out = smem + 2 * G::STAGE;                                           // [TY][2][H2]
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + 2 * G::STAGE + G::OUT);  // [R][2][NWB]
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * G::STAGE + G::OUT + G::BITS);
-    const int tid = threadIdx.x;
-    const int warp = tid >> 5, lane = tid & 31;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint8_t* part = smem + warp * G::WARP;
+    uint8_t* stage = part;                                                   // [NS][2][PH]
+    uint8_t* out = part + G::STAGE;                                          // [NO][2][H2]
+    uint32_t* bits = reinterpret_cast<uint32_t*>(part + G::STAGE + G::OUT);  // [R][2][NWB]
+    uint64_t* bars = reinterpret_cast<uint64_t*>(part + G::STAGE + G::OUT + G::BITS);
     const int L = a.L, Lh = L >> 1;
     const uint32_t tg_acc = tag(kAccept, a.replica);
-    if (tid == 0) {
-        mbar_init(smem_addr(&bars[0]), 1);
-        mbar_init(smem_addr(&bars[1]), 1);
+    if (lane == 0) {
+        for (int k = 0; k < NS; ++k) mbar_init(smem_addr(&bars[k]), 1);
         mbar_fence_init();
     }
-    __syncthreads();
+    __syncwarp();
 
-    auto issue_load = [&](int tile, int stg) {
-        // warp 0: rows y0-2 .. y0+TY+1 of both halves, columns x0-64 .. x0+TX+63
+    // staged row q of this warp's row sequence: row r of tile `tile` into slot q % NS
+    auto issue_row = [&](int tile, int r, int q) {
         const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
-        uint8_t* sb = stage0 + stg * G::STAGE;
-        const uint32_t bar = smem_addr(&bars[stg]);
-        fence_proxy_async_smem();
-        if (lane == 0) mbar_expect_tx(bar, G::TX_BYTES);
-        __syncwarp();
-        const bool inner = x0 > 0 && x0 + TX < L;
+        const int slot = q % NS;
+        uint8_t* sb = stage + slot * G::P;
+        const uint32_t bar = smem_addr(&bars[slot]);
+        mbar_expect_tx(bar, (uint32_t)G::P);
+        const int8_t* row = a.src + (size_t)wrapi(y0 - 2 + r, L) * L;
         const int j0 = (x0 >> 1) - 32;
-        for (int task = lane; task < 2 * G::R; task += 32) {
-            const int r = task >> 1, h = task & 1;
-            const int8_t* row = a.src + (size_t)wrapi(y0 - 2 + r, L) * L + (size_t)h * Lh;
-            const uint32_t d = smem_addr(sb + r * G::P + h * G::PH);
-            if (inner) {
-                bulk_g2s(d, row + j0, G::PH, bar);
+        for (int h = 0; h < 2; ++h) {
+            const int8_t* rh = row + (size_t)h * Lh;
+            const uint32_t d = smem_addr(sb + h * G::PH);
+            if (x0 > 0 && x0 + TX < L) {
+                bulk_g2s(d, rh + j0, G::PH, bar);
             } else {
-                bulk_g2s(d, row + (j0 < 0 ? j0 + Lh : j0), 32, bar);
-                bulk_g2s(d + 32, row + (x0 >> 1), G::H2, bar);
+                bulk_g2s(d, rh + (j0 < 0 ? j0 + Lh : j0), 32, bar);
+                bulk_g2s(d + 32, rh + (x0 >> 1), G::H2, bar);
                 const int jr = (x0 >> 1) + G::H2;
-                bulk_g2s(d + 32 + G::H2, row + (jr >= Lh ? jr - Lh : jr), 32, bar);
+                bulk_g2s(d + 32 + G::H2, rh + (jr >= Lh ? jr - Lh : jr), 32, bar);
             }
         }
     };
+    auto grab = [&]() {
+        int t = 0;
+        if (lane == 0) t = atomicAdd(a.counter, 1);
+        return __shfl_sync(0xffffffffu, t, 0);
+    };
 
     int esum = 0, msum = 0;
-    int tile = blockIdx.x;
-    if (tile < a.ntiles && warp == 0) issue_load(tile, 0);
-    for (int it = 0; tile < a.ntiles; ++it, tile += gridDim.x) {
-        const int stg = it & 1;
-        const uint8_t* sb = stage0 + stg * G::STAGE;
-        const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
-        const int next = tile + gridDim.x;
-        if (warp == 0 && next < a.ntiles) issue_load(next, stg ^ 1);
-        // one thread waits for the staged tile (bounded: a stuck copy sets an
-        // error status); the barrier publishes the data to the CTA
-        int timed_out = 0;
-        if (tid == 0) {
-            const uint32_t bar = smem_addr(&bars[stg]);
-            const uint32_t par = (uint32_t)(it >> 1) & 1u;
-            if (!mbar_try_wait(bar, par)) {
-                const uint64_t t0 = global_timer_ns();
-                for (uint32_t k = 1;; ++k) {
-                    if (mbar_try_wait(bar, par)) break;
-                    if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
-                        timed_out = 1;
-                        break;
+    uint32_t gq = 0;  // store groups issued by this warp: output-ring half = gq & 1
+    int cur = grab();
+    int nxt = cur < a.ntiles ? grab() : a.ntiles;
+    int base = 0;  // sequence number of the current tile's row 0
+    if (lane == 0 && cur < a.ntiles) {
+        fence_proxy_async_smem();
+        for (int r = 0; r < NS; ++r) issue_row(cur, r, r);
+    }
+    bool stop = false;
+    while (cur < a.ntiles && !stop) {
+        const int x0 = (cur % a.ntx) * TX, y0 = (cur / a.ntx) * TY;
+        // stream the staged rows in, four at a time, packing them to bits
+        for (int r0 = 0; r0 < R; r0 += 4) {
+            int timed_out = 0;
+            if (lane == 0) {
+                for (int i = 0; i < 4 && !timed_out; ++i) {
+                    const int q = base + r0 + i;
+                    const uint32_t bar = smem_addr(&bars[q % NS]);
+                    const uint32_t par = (uint32_t)(q / NS) & 1u;
+                    if (!mbar_try_wait(bar, par)) {
+                        const uint64_t t0 = global_timer_ns();
+                        for (uint32_t k = 1;; ++k) {
+                            if (mbar_try_wait(bar, par)) break;
+                            if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
+                                timed_out = 1;
+                                break;
+                            }
+                        }
                     }
                 }
             }
+            if (__shfl_sync(0xffffffffu, timed_out, 0)) {
+                if (lane == 0) atomicExch(a.status, MQV_ERR_TIMEOUT);
+                stop = true;
+                break;
+            }
+            // 4 rows x 2 halves x NWB words = 8 NWB words = 16 NWB chunks of 16 bytes
+            for (int c0 = 0; c0 < 16 * NWB; c0 += 32) {
+                const int c = c0 + lane;
+                uint32_t h16 = 0;
+                if (c < 16 * NWB) {
+                    const int i = c / (4 * NWB), cr = c % (4 * NWB);
+                    const uint8_t* sb = stage + ((base + r0 + i) % NS) * G::P;
+                    h16 = pack16(reinterpret_cast<const uint4*>(sb)[cr]);
+                }
+                const uint32_t hi = __shfl_down_sync(0xffffffffu, h16, 1);
+                if (!(c & 1) && c < 16 * NWB) bits[(r0 * 2 * NWB) + (c >> 1)] = h16 | (hi << 16);
+            }
+            __syncwarp();
+            // refill the four freed slots: rows NS ahead in this tile or the next
+            if (lane == 0) {
+                fence_proxy_async_smem();
+                for (int i = 0; i < 4; ++i) {
+                    const int r = r0 + i + NS;
+                    if (r < R) issue_row(cur, r, base + r);
+                    else if (nxt < a.ntiles) issue_row(nxt, r - R, base + r);
+                }
+            }
         }
-        if (__syncthreads_or(timed_out)) {
-            if (tid == 0) atomicExch(a.status, MQV_ERR_TIMEOUT);
-            break;
-        }
-        // pack: one 16-byte chunk per thread, lane pairs form a 32-site word
-        for (int base = 0; base < G::STAGE / 16; base += NT) {
-            const int c = base + tid;
-            const uint32_t h16 = c < G::STAGE / 16 ? pack16(reinterpret_cast<const uint4*>(sb)[c]) : 0u;
-            const uint32_t hi = __shfl_down_sync(0xffffffffu, h16, 1);
-            if (!(c & 1) && c < G::STAGE / 16) bits[c >> 1] = h16 | (hi << 16);
-        }
-        __syncthreads();
+        if (stop) break;
+        __syncwarp();
         // colour 0 on the tile and its ring: rows 1..TY+2, interior words + one halo word
-        for (int task = tid; task < (TY + 2) * (NWI + 1); task += NT) {
+        for (int task = lane; task < (TY + 2) * (NWI + 1); task += 32) {
             const int r = 1 + task / (NWI + 1), k = task % (NWI + 1);
             const int p = r & 1;
             const int w = k < NWI ? 1 + k : (p ? 0 : NWI + 1);
@@ -286,10 +312,10 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
             Hr[w] = update_word<false>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w], bits[((r + 1) * 2 + p) * NWB + w], Lb,
                                        Rb, w, p, wrapi(y0 - 2 + r, L), x0, tg_acc, a, dummy);
         }
-        if (warp == 0) bulk_wait_read0();  // the previous tile's stores have read the output stage
-        __syncthreads();
-        // colour 1 on the tile, then both colours of the tile to the output stage
-        for (int task = tid; task < TY * NWI; task += NT) {
+        __syncwarp();
+        // colour 1 on the tile, 32 words (RPG rows) at a time, then those rows out
+        for (int t0 = 0; t0 < TY * NWI; t0 += 32) {
+            const int task = t0 + lane;
             const int r = 2 + task / NWI, w = 1 + task % NWI;
             const int p = (r + 1) & 1;
             uint32_t* Hr = bits + (r * 2 + p) * NWB;
@@ -301,24 +327,32 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
                                                   bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, w, p,
                                                   wrapi(y0 - 2 + r, L), x0, tg_acc, a, esum);
             if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
-            uint8_t* orow = out + (r - 2) * TX;
+            // the output-ring half this group uses must have been read by its last store
+            if (lane == 0) bulk_wait_read1();
+            __syncwarp();
+            uint8_t* orow = out + ((gq & 1u) * G::RPG + lane / NWI) * TX;
             unpack32(An, orow + p * G::H2 + 32 * (w - 1));
             unpack32(Gw, orow + (1 - p) * G::H2 + 32 * (w - 1));
-        }
-        fence_proxy_async_smem();
-        __syncthreads();
-        if (warp == 0) {
-            for (int task = lane; task < 2 * TY; task += 32) {
-                const int r = task >> 1, h = task & 1;
-                int8_t* drow = a.dst + (size_t)(y0 + r) * L + (size_t)h * Lh + (x0 >> 1);
-                bulk_s2g(drow, smem_addr(out + r * TX + h * G::H2), G::H2);
+            fence_proxy_async_smem();
+            __syncwarp();
+            if (lane == 0) {
+                for (int i = 0; i < G::RPG; ++i) {
+                    const int rr = 2 + t0 / NWI + i;
+                    const uint8_t* src = out + ((gq & 1u) * G::RPG + i) * TX;
+                    int8_t* drow = a.dst + (size_t)(y0 + rr - 2) * L + (x0 >> 1);
+                    bulk_s2g(drow, smem_addr(src), G::H2);
+                    bulk_s2g(drow + Lh, smem_addr(src + G::H2), G::H2);
+                }
+                bulk_commit();
             }
-            bulk_commit();
+            ++gq;
         }
+        base += R;
+        cur = nxt;
+        nxt = cur < a.ntiles ? grab() : a.ntiles;
     }
-    if (warp == 0) bulk_wait0();
+    if (lane == 0) bulk_wait0();
     if (MEAS) {
-        __shared__ long long red[2][NT / 32];
         long long e = esum, m = msum;
 #pragma unroll
         for (int o = 16; o; o >>= 1) {
@@ -326,19 +360,9 @@ __global__ void __launch_bounds__(NT, (min_blocks<TX, TY, NT>())) ising2d_sweep(
             m += __shfl_xor_sync(0xffffffffu, m, o);
         }
         if (lane == 0) {
-            red[0][warp] = e;
-            red[1][warp] = m;
-        }
-        __syncthreads();
-        if (tid == 0) {
-            long long es = 0, ms = 0;
-            for (int k = 0; k < NT / 32; ++k) {
-                es += red[0][k];
-                ms += red[1][k];
-            }
             // enepart = sum_i sum_{j in nbrs(i)} s_i s_j counts every bond twice
-            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccEne), (unsigned long long)(2 * es));
-            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccMag), (unsigned long long)ms);
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccEne), (unsigned long long)(2 * e));
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccMag), (unsigned long long)m);
         }
     }
 }
@@ -373,39 +397,40 @@ bool ising2d_supported(int L) { return L >= 64 && L % 64 == 0; }
 
 typedef cudaError_t (*SweepLauncher)(const Ising2DArgs&, int, cudaStream_t);
 
-template <int TX, int TY, int NT, bool MEAS>
+template <int TX, int TY, int NWARP, bool MEAS>
 static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
-    using G = TileGeom<TX, TY>;
-    auto kern = ising2d_sweep<TX, TY, NT, MEAS>;
+    using G = TileGeom<TX, TY, NWARP>;
+    auto kern = ising2d_sweep<TX, TY, NWARP, MEAS>;
     static int cps = 0;  // resident CTAs per SM for this instantiation
     if (cps == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         if (e != cudaSuccess) return e;
         int c = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NT, G::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NWARP * 32, G::SMEM);
         if (e != cudaSuccess) return e;
         cps = c < 1 ? 1 : c;
     }
-    int grid = nsm * cps;
-    if (grid > a.ntiles) grid = a.ntiles;
-    kern<<<grid, NT, G::SMEM, stream>>>(a);
+    long long grid = (long long)nsm * cps;
+    const long long need = (a.ntiles + NWARP - 1) / NWARP;
+    if (grid > need) grid = need;
+    kern<<<(int)grid, NWARP * 32, G::SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 
-// Candidate tile shapes and CTA sizes.  Every candidate computes the same
+// Candidate tile shapes and warps per CTA.  Every candidate computes the same
 // result; the autotuner keeps the fastest for a lattice size.
 struct SweepConfig {
-    int tx, ty, nt;
+    int tx, ty, nwarp;
     SweepLauncher plain, meas;
 };
 
-#define MQV_CFG(TX, TY, NT) \
-    SweepConfig{TX, TY, NT, launch_t<TX, TY, NT, false>, launch_t<TX, TY, NT, true>}
+#define MQV_CFG(TX, TY, NW) \
+    SweepConfig{TX, TY, NW, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
 
 static const SweepConfig kConfigs[] = {
-    MQV_CFG(512, 32, 256), MQV_CFG(512, 32, 320), MQV_CFG(256, 32, 128), MQV_CFG(256, 32, 160),
-    MQV_CFG(256, 64, 256), MQV_CFG(128, 32, 128), MQV_CFG(64, 32, 64),
+    MQV_CFG(512, 32, 4), MQV_CFG(256, 32, 4), MQV_CFG(512, 32, 2), MQV_CFG(256, 32, 8),
+    MQV_CFG(1024, 32, 2), MQV_CFG(128, 32, 4), MQV_CFG(64, 32, 4),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
@@ -443,6 +468,7 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
     a.ztB = (TB & ((1ull << 45) - 1)) == 0;
     a.acc = acc;
     a.status = s->d_status;
+    a.counter = s->d_counter;
 }
 
 // Time every fitting candidate on this lattice (two sweeps each into the
@@ -469,9 +495,12 @@ static int pick_config(Sim* s)
         if (!config_fits(kConfigs[k], s->len)) continue;
         Ising2DArgs a{};
         fill_args(s, kConfigs[k], nullptr, a);
+        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
         if (kConfigs[k].plain(a, s->num_sms, s->stream) != cudaSuccess) continue;  // warm-up
         cudaEventRecord(e0, s->stream);
+        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
         kConfigs[k].plain(a, s->num_sms, s->stream);
+        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
         kConfigs[k].plain(a, s->num_sms, s->stream);
         cudaEventRecord(e1, s->stream);
         s->launches += 3;
@@ -496,6 +525,8 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
     const SweepConfig& c = kConfigs[s->sweep_cfg];
     Ising2DArgs a{};
     fill_args(s, c, acc, a);
+    const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
+    if (e != cudaSuccess) return e;
     return acc ? c.meas(a, s->num_sms, s->stream) : c.plain(a, s->num_sms, s->stream);
 }
 
@@ -503,7 +534,7 @@ const char* ising2d_config_name(Sim* s, char* buf, int len)
 {
     if (s->sweep_cfg < 0) return "";
     const SweepConfig& c = kConfigs[s->sweep_cfg];
-    snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nt);
+    snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
     return buf;
 }
 
