@@ -208,26 +208,37 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
     }
     __syncwarp();
 
-    // staged row q of this warp's row sequence: row r of tile `tile` into slot q % NS
-    auto issue_row = [&](int tile, int r, int q) {
+    // staged row q of this warp's row sequence (row r of tile `tile`) lands in
+    // slot q % NS: the slot's byte count is armed once, then the copies of one
+    // half-row are issued by the calling lane
+    auto arm_row = [&](int q) { mbar_expect_tx(smem_addr(&bars[q % NS]), (uint32_t)G::P); };
+    auto copy_half = [&](int tile, int r, int q, int h) {
         const int x0 = (tile % a.ntx) * TX, y0 = (tile / a.ntx) * TY;
-        const int slot = q % NS;
-        uint8_t* sb = stage + slot * G::P;
-        const uint32_t bar = smem_addr(&bars[slot]);
-        mbar_expect_tx(bar, (uint32_t)G::P);
-        const int8_t* row = a.src + (size_t)wrapi(y0 - 2 + r, L) * L;
+        const uint32_t bar = smem_addr(&bars[q % NS]);
+        const int8_t* rh = a.src + (size_t)wrapi(y0 - 2 + r, L) * L + (size_t)h * Lh;
+        const uint32_t d = smem_addr(stage + (q % NS) * G::P + h * G::PH);
         const int j0 = (x0 >> 1) - 32;
-        for (int h = 0; h < 2; ++h) {
-            const int8_t* rh = row + (size_t)h * Lh;
-            const uint32_t d = smem_addr(sb + h * G::PH);
-            if (x0 > 0 && x0 + TX < L) {
-                bulk_g2s(d, rh + j0, G::PH, bar);
-            } else {
-                bulk_g2s(d, rh + (j0 < 0 ? j0 + Lh : j0), 32, bar);
-                bulk_g2s(d + 32, rh + (x0 >> 1), G::H2, bar);
-                const int jr = (x0 >> 1) + G::H2;
-                bulk_g2s(d + 32 + G::H2, rh + (jr >= Lh ? jr - Lh : jr), 32, bar);
-            }
+        if (x0 > 0 && x0 + TX < L) {
+            bulk_g2s(d, rh + j0, G::PH, bar);
+        } else {
+            bulk_g2s(d, rh + (j0 < 0 ? j0 + Lh : j0), 32, bar);
+            bulk_g2s(d + 32, rh + (x0 >> 1), G::H2, bar);
+            const int jr = (x0 >> 1) + G::H2;
+            bulk_g2s(d + 32 + G::H2, rh + (jr >= Lh ? jr - Lh : jr), 32, bar);
+        }
+    };
+    // rows q0 .. q0+n-1 (rows r0.. of `tile`, continuing into `tile2` past R):
+    // lanes 0..n-1 arm, lanes 0..2n-1 copy one half-row each
+    auto issue_rows = [&](int tile, int tile2, int r0, int q0, int n) {
+        if (lane < n) {
+            const int r = r0 + lane;
+            if (r < R || tile2 < a.ntiles) arm_row(q0 + lane);
+        }
+        __syncwarp();
+        if (lane < 2 * n) {
+            const int i = lane >> 1, r = r0 + i;
+            if (r < R) copy_half(tile, r, q0 + i, lane & 1);
+            else if (tile2 < a.ntiles) copy_half(tile2, r - R, q0 + i, lane & 1);
         }
     };
     auto grab = [&]() {
@@ -241,34 +252,33 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
     int cur = grab();
     int nxt = cur < a.ntiles ? grab() : a.ntiles;
     int base = 0;  // sequence number of the current tile's row 0
-    if (lane == 0 && cur < a.ntiles) {
+    if (cur < a.ntiles) {
         fence_proxy_async_smem();
-        for (int r = 0; r < NS; ++r) issue_row(cur, r, r);
+        issue_rows(cur, a.ntiles, 0, 0, NS);
     }
     bool stop = false;
     while (cur < a.ntiles && !stop) {
         const int x0 = (cur % a.ntx) * TX, y0 = (cur / a.ntx) * TY;
         // stream the staged rows in, four at a time, packing them to bits
         for (int r0 = 0; r0 < R; r0 += 4) {
+            // every lane waits for the four rows (bounded: a stuck copy sets an error status)
             int timed_out = 0;
-            if (lane == 0) {
-                for (int i = 0; i < 4 && !timed_out; ++i) {
-                    const int q = base + r0 + i;
-                    const uint32_t bar = smem_addr(&bars[q % NS]);
-                    const uint32_t par = (uint32_t)(q / NS) & 1u;
-                    if (!mbar_try_wait(bar, par)) {
-                        const uint64_t t0 = global_timer_ns();
-                        for (uint32_t k = 1;; ++k) {
-                            if (mbar_try_wait(bar, par)) break;
-                            if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
-                                timed_out = 1;
-                                break;
-                            }
+            for (int i = 0; i < 4 && !timed_out; ++i) {
+                const int q = base + r0 + i;
+                const uint32_t bar = smem_addr(&bars[q % NS]);
+                const uint32_t par = (uint32_t)(q / NS) & 1u;
+                if (!mbar_try_wait(bar, par)) {
+                    const uint64_t t0 = global_timer_ns();
+                    for (uint32_t k = 1;; ++k) {
+                        if (mbar_try_wait(bar, par)) break;
+                        if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
+                            timed_out = 1;
+                            break;
                         }
                     }
                 }
             }
-            if (__shfl_sync(0xffffffffu, timed_out, 0)) {
+            if (__any_sync(0xffffffffu, timed_out)) {
                 if (lane == 0) atomicExch(a.status, MQV_ERR_TIMEOUT);
                 stop = true;
                 break;
@@ -287,14 +297,8 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
             }
             __syncwarp();
             // refill the four freed slots: rows NS ahead in this tile or the next
-            if (lane == 0) {
-                fence_proxy_async_smem();
-                for (int i = 0; i < 4; ++i) {
-                    const int r = r0 + i + NS;
-                    if (r < R) issue_row(cur, r, base + r);
-                    else if (nxt < a.ntiles) issue_row(nxt, r - R, base + r);
-                }
-            }
+            fence_proxy_async_smem();
+            issue_rows(cur, nxt, r0 + NS, base + r0 + NS, 4);
         }
         if (stop) break;
         __syncwarp();
@@ -327,22 +331,21 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
                                                   bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, w, p,
                                                   wrapi(y0 - 2 + r, L), x0, tg_acc, a, esum);
             if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
-            // the output-ring half this group uses must have been read by its last store
-            if (lane == 0) bulk_wait_read1();
+            // the output-ring half this group uses must have been read by its
+            // last stores (each storing lane waits for its own bulk groups)
+            if (lane < 2 * G::RPG) bulk_wait_read1();
             __syncwarp();
             uint8_t* orow = out + ((gq & 1u) * G::RPG + lane / NWI) * TX;
             unpack32(An, orow + p * G::H2 + 32 * (w - 1));
             unpack32(Gw, orow + (1 - p) * G::H2 + 32 * (w - 1));
             fence_proxy_async_smem();
             __syncwarp();
-            if (lane == 0) {
-                for (int i = 0; i < G::RPG; ++i) {
-                    const int rr = 2 + t0 / NWI + i;
-                    const uint8_t* src = out + ((gq & 1u) * G::RPG + i) * TX;
-                    int8_t* drow = a.dst + (size_t)(y0 + rr - 2) * L + (x0 >> 1);
-                    bulk_s2g(drow, smem_addr(src), G::H2);
-                    bulk_s2g(drow + Lh, smem_addr(src + G::H2), G::H2);
-                }
+            if (lane < 2 * G::RPG) {
+                const int i = lane >> 1, h = lane & 1;
+                const int rr = 2 + t0 / NWI + i;
+                const uint8_t* src = out + ((gq & 1u) * G::RPG + i) * TX + h * G::H2;
+                int8_t* drow = a.dst + (size_t)(y0 + rr - 2) * L + (size_t)h * Lh + (x0 >> 1);
+                bulk_s2g(drow, smem_addr(src), G::H2);
                 bulk_commit();
             }
             ++gq;
@@ -351,7 +354,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
         cur = nxt;
         nxt = cur < a.ntiles ? grab() : a.ntiles;
     }
-    if (lane == 0) bulk_wait0();
+    bulk_wait0();
     if (MEAS) {
         long long e = esum, m = msum;
 #pragma unroll
