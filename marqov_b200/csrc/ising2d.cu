@@ -341,11 +341,13 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
             fence_proxy_async_smem();
             __syncwarp();
             if (lane < 2 * G::RPG) {
-                const int i = lane >> 1, h = lane & 1;
-                const int rr = 2 + t0 / NWI + i;
-                const uint8_t* src = out + ((gq & 1u) * G::RPG + i) * TX + h * G::H2;
-                int8_t* drow = a.dst + (size_t)(y0 + rr - 2) * L + (size_t)h * Lh + (x0 >> 1);
-                bulk_s2g(drow, smem_addr(src), G::H2);
+                for (int k = lane; k < 2 * G::RPG; k += 32) {
+                    const int i = k >> 1, h = k & 1;
+                    const int rr = 2 + t0 / NWI + i;
+                    const uint8_t* src = out + ((gq & 1u) * G::RPG + i) * TX + h * G::H2;
+                    int8_t* drow = a.dst + (size_t)(y0 + rr - 2) * L + (size_t)h * Lh + (x0 >> 1);
+                    bulk_s2g(drow, smem_addr(src), G::H2);
+                }
                 bulk_commit();
             }
             ++gq;
