@@ -49,8 +49,11 @@ struct Ising2DArgs {
     Key key;
     uint32_t sweep;
     uint32_t replica;
-    // the (at most two) aligned-neighbour classes with dE > 0 that need a test
-    int clsA, clsB;             // aligned count, -1 when unused
+    // The two aligned-neighbour classes with dE > 0: mode 0 (J < 0) tests
+    // a = 3 (class A, dE = -4J) and a = 4 (class B, dE = -8J); mode 1 (J > 0)
+    // tests a = 1 (A, dE = 4J) and a = 0 (B, dE = 8J); mode 2: no test.
+    int mode;
+    uint32_t useA, useB;        // 1 when the class needs a test (cut below 2^53)
     uint32_t tA8, tB8;          // threshold top bytes
     uint32_t ztA, ztB;          // 1 when a top-byte tie rejects without the fine bits
     unsigned long long tA, tB;  // full u53 thresholds
@@ -84,21 +87,27 @@ __device__ __forceinline__ int wrapi(int v, int L)
     return v >= L ? v - L : v;
 }
 
-// uniform all-ones / all-zeros mask of bit b of t
-__device__ __forceinline__ uint32_t bitmask(uint32_t t, int b) { return 0u - ((t >> b) & 1u); }
+// Per-launch constants of the decision, as all-ones / all-zeros lane masks.
+struct Thr {
+    uint32_t tA[8], tB[8];  // bit b of the class thresholds' top bytes
+    uint32_t useA, useB, ztA, ztB;
+    int mode;
+};
 
-// sites (bits) whose neighbour minus-count equals v: planes m0 m1 m2 of M <= 4
-__device__ __forceinline__ uint32_t eq_count(uint32_t m0, uint32_t m1, uint32_t m2, int v)
+__device__ __forceinline__ Thr make_thr(const Ising2DArgs& a)
 {
-    return ~(m0 ^ bitmask((uint32_t)v, 0)) & ~(m1 ^ bitmask((uint32_t)v, 1)) & ~(m2 ^ bitmask((uint32_t)v, 2));
-}
-
-// sites of class `cls` (aligned neighbours): minus sites with M == cls, plus
-// sites with M == 4 - cls
-__device__ __forceinline__ uint32_t class_mask(uint32_t A, uint32_t m0, uint32_t m1, uint32_t m2, int cls)
-{
-    if (cls < 0) return 0u;
-    return (A & eq_count(m0, m1, m2, cls)) | (~A & eq_count(m0, m1, m2, 4 - cls));
+    Thr t;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) {
+        t.tA[b] = 0u - ((a.tA8 >> b) & 1u);
+        t.tB[b] = 0u - ((a.tB8 >> b) & 1u);
+    }
+    t.useA = 0u - a.useA;
+    t.useB = 0u - a.useB;
+    t.ztA = 0u - a.ztA;
+    t.ztB = 0u - a.ztB;
+    t.mode = a.mode;
+    return t;
 }
 
 // Tie bits: compare the full acceptance word with the class threshold.
@@ -127,7 +136,7 @@ __device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, uint
 template <bool MEAS>
 __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb, int w,
                                                 int half, int y, int x0, uint32_t tg_acc, const Ising2DArgs& a,
-                                                int& esum)
+                                                const Thr& th, int& esum)
 {
     // the word's eight random planes: two Philox blocks of its 32-site group
     const int x = wrapi(x0 - 64 + 64 * w + half, a.L);
@@ -135,25 +144,37 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
     const uint4 q0 = philox(g, a.sweep, 0u, tg_acc, a.key);
     const uint4 q1 = philox(g, a.sweep, 1u, tg_acc, a.key);
     const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder)
+    // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder; M <= 4)
     const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
     const uint32_t m0 = s1 ^ s2, c3 = s1 & s2;
     const uint32_t m1 = c1 ^ c2 ^ c3;
     const uint32_t m2 = (c1 & c2) | (c3 & (c1 | c2));
-    const uint32_t maskA = class_mask(A, m0, m1, m2, a.clsA);
-    const uint32_t maskB = class_mask(A, m0, m1, m2, a.clsB);
-    // per-site threshold bits, then X < T by a borrow chain and X == T
-    uint32_t borrow = 0, eq = ~0u;
+    // the two tested classes (aligned count a = M for a -1 site, 4 - M for +1)
+    uint32_t maskA, maskB;
+    if (th.mode == 0) {
+        maskA = m0 & ~(A ^ m1);                    // a = 3
+        maskB = (A & m2) | (~A & ~(m0 | m1 | m2));  // a = 4
+    } else if (th.mode == 1) {
+        maskA = m0 & (A ^ m1);                     // a = 1
+        maskB = (~A & m2) | (A & ~(m0 | m1 | m2));  // a = 0
+    } else {
+        maskA = 0u;
+        maskB = 0u;
+    }
+    maskA &= th.useA;
+    maskB &= th.useB;
+    // X < T and X == T for the per-site threshold byte T (class A or B)
+    uint32_t borrow = 0u, eq = ~0u;
 #pragma unroll
     for (int b = 0; b < 8; ++b) {
-        const uint32_t tb = (maskA & bitmask(a.tA8, b)) | (maskB & bitmask(a.tB8, b));
+        const uint32_t tb = (maskA & th.tA[b]) | (~maskA & th.tB[b]);
         const uint32_t nx = ~pl[b];
-        borrow = (nx & tb) | (nx & borrow) | (tb & borrow);
+        borrow = (nx & (tb | borrow)) | (tb & borrow);
         eq &= ~(pl[b] ^ tb);
     }
     const uint32_t test = maskA | maskB;
     uint32_t acc = ~test | borrow;
-    const uint32_t zt = (maskA & (0u - a.ztA)) | (maskB & (0u - a.ztB));
+    const uint32_t zt = (maskA & th.ztA) | (~maskA & th.ztB);
     const uint32_t tie = eq & test & ~zt;
     if (tie) acc |= resolve_ties(tie, maskA, q0, q1, w, half, y, x0, a.L, a.key, a.sweep, a.replica, a.tA, a.tB);
     const uint32_t An = A ^ acc;
@@ -202,6 +223,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
     uint64_t* bars = reinterpret_cast<uint64_t*>(part + G::STAGE + G::OUT + G::BITS);
     const int L = a.L, Lh = L >> 1;
     const uint32_t tg_acc = tag(kAccept, a.replica);
+    const Thr th = make_thr(a);
     if (lane == 0) {
         for (int k = 0; k < NS; ++k) mbar_init(smem_addr(&bars[k]), 1);
         mbar_fence_init();
@@ -268,8 +290,10 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
                 const uint32_t bar = smem_addr(&bars[q % NS]);
                 const uint32_t par = (uint32_t)(q / NS) & 1u;
                 if (!mbar_try_wait(bar, par)) {
+                    // back off so that waiting warps leave their issue slots to others
                     const uint64_t t0 = global_timer_ns();
                     for (uint32_t k = 1;; ++k) {
+                        __nanosleep(64);
                         if (mbar_try_wait(bar, par)) break;
                         if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
                             timed_out = 1;
@@ -314,7 +338,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
             const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
             int dummy = 0;
             Hr[w] = update_word<false>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w], bits[((r + 1) * 2 + p) * NWB + w], Lb,
-                                       Rb, w, p, wrapi(y0 - 2 + r, L), x0, tg_acc, a, dummy);
+                                       Rb, w, p, wrapi(y0 - 2 + r, L), x0, tg_acc, a, th, dummy);
         }
         __syncwarp();
         // colour 1 on the tile, 32 words (RPG rows) at a time, then those rows out
@@ -329,7 +353,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
             const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
             const uint32_t An = update_word<MEAS>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w],
                                                   bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, w, p,
-                                                  wrapi(y0 - 2 + r, L), x0, tg_acc, a, esum);
+                                                  wrapi(y0 - 2 + r, L), x0, tg_acc, a, th, esum);
             if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
             // the output-ring half this group uses must have been read by its
             // last stores (each storing lane waits for its own bulk groups)
@@ -458,17 +482,17 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
         s->thr_J = s->md.J;
         s->thr_beta = s->md.beta;
     }
-    // classes with a nontrivial test: dE > 0 and not every u53 accepted
-    int cls[2] = {-1, -1}, nc = 0;
-    for (int k = 0; k < 5 && nc < 2; ++k)
-        if (s->md.J * (double)(8 - 4 * k) > 0 && s->thr_cut[k] < (1ull << 53)) cls[nc++] = k;
-    const unsigned long long TA = cls[0] >= 0 ? s->thr_cut[cls[0]] : 0, TB = cls[1] >= 0 ? s->thr_cut[cls[1]] : 0;
-    a.clsA = cls[0];
-    a.clsB = cls[1];
+    // the tested classes: aligned counts 3 and 4 for J < 0, 1 and 0 for J > 0
+    const double J = s->md.J;
+    const int ka = J < 0 ? 3 : 1, kb = J < 0 ? 4 : 0;
+    a.mode = J < 0 ? 0 : (J > 0 ? 1 : 2);
+    const unsigned long long TA = s->thr_cut[ka], TB = s->thr_cut[kb];
+    a.useA = TA < (1ull << 53);
+    a.useB = TB < (1ull << 53);
     a.tA = TA;
     a.tB = TB;
-    a.tA8 = (uint32_t)(TA >> 45);
-    a.tB8 = (uint32_t)(TB >> 45);
+    a.tA8 = (uint32_t)(TA >> 45) & 0xFFu;
+    a.tB8 = (uint32_t)(TB >> 45) & 0xFFu;
     a.ztA = (TA & ((1ull << 45) - 1)) == 0;
     a.ztB = (TB & ((1ull << 45) - 1)) == 0;
     a.acc = acc;
