@@ -76,7 +76,8 @@ struct TileGeom {
     static constexpr int BITS = R * 2 * NWB * 4;
     static constexpr int STAGE = NS * P;
     static constexpr int OUT = NO * TX;
-    static constexpr int WARP = ((STAGE + OUT + BITS + NS * 8) + 127) / 128 * 128;  // per-warp partition
+    static constexpr int TIECAP = 96;           // tie-list entries
+    static constexpr int WARP = ((STAGE + OUT + BITS + NS * 8 + TIECAP * 20) + 127) / 128 * 128;  // per-warp partition
     static constexpr int SMEM = NWARP * WARP;
     static_assert(R % 4 == 0 && 32 % NWI == 0, "tile shape");
 };
@@ -110,36 +111,23 @@ __device__ __forceinline__ Thr make_thr(const Ising2DArgs& a)
     return t;
 }
 
-// Tie bits: compare the full acceptance word with the class threshold.
-__device__ __noinline__ uint32_t resolve_ties(uint32_t tie, uint32_t maskA, uint4 q0, uint4 q1, int w, int half, int y,
-                                              int x0, int L, Key key, uint32_t sweep, uint32_t replica,
-                                              unsigned long long tA, unsigned long long tB)
-{
-    uint32_t acc = 0;
-    const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
-    while (tie) {
-        const int b = __ffs(tie) - 1;
-        tie &= tie - 1;
-        const int x = wrapi(x0 - 64 + 2 * (32 * w + b) + half, L);
-        const uint32_t site = (uint32_t)y * (uint32_t)L + (uint32_t)x;
-        uint64_t cb = 0;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) cb |= (uint64_t)((pl[k] >> b) & 1u) << k;
-        const uint64_t u53 = ((cb << 56) | accept_fine56(key, site, sweep, replica)) >> 11;
-        const unsigned long long T = ((maskA >> b) & 1u) ? tA : tB;
-        if (u53 < T) acc |= 1u << b;
-    }
-    return acc;
-}
+// A word whose tested sites include top-byte ties is recorded in the warp's
+// tie list and resolved after the pass: a tie site's top byte equals its
+// class threshold's top byte, so only its fine block is needed.
+struct TieEntry {
+    uint32_t pos;    // word position in the bit tile: (r * 2 + half) * NWB + w
+    uint32_t tie;    // tie sites of the word
+    uint32_t inA;    // tie sites of class A (others are class B)
+    int32_t y, x;    // lattice coordinates of the word's first site
+};
 
-// Update the active-colour sites of one 32-site word; returns the new word.
-template <bool MEAS>
-__device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb, int w,
-                                                int half, int y, int x0, uint32_t tg_acc, const Ising2DArgs& a,
-                                                const Thr& th, int& esum)
+// Update the active-colour sites of one 32-site word: returns the word with
+// the decided flips applied; `tie` and `inA` receive the undecided sites.
+__device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb, int x,
+                                                int y, uint32_t tg_acc, const Ising2DArgs& a, const Thr& th,
+                                                uint32_t& tie, uint32_t& inA)
 {
     // the word's eight random planes: two Philox blocks of its 32-site group
-    const int x = wrapi(x0 - 64 + 64 * w + half, a.L);
     const uint32_t g = accept_group((uint32_t)y * (uint32_t)a.L + (uint32_t)x);
     const uint4 q0 = philox(g, a.sweep, 0u, tg_acc, a.key);
     const uint4 q1 = philox(g, a.sweep, 1u, tg_acc, a.key);
@@ -173,18 +161,22 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
         eq &= ~(pl[b] ^ tb);
     }
     const uint32_t test = maskA | maskB;
-    uint32_t acc = ~test | borrow;
     const uint32_t zt = (maskA & th.ztA) | (~maskA & th.ztB);
-    const uint32_t tie = eq & test & ~zt;
-    if (tie) acc |= resolve_ties(tie, maskA, q0, q1, w, half, y, x0, a.L, a.key, a.sweep, a.replica, a.tA, a.tB);
-    const uint32_t An = A ^ acc;
-    if (MEAS) {
-        // sum over the word's bonds s * sum(nbrs) = sum (1 - 2a)(4 - 2M)
-        const int sM = __popc(m0) + 2 * __popc(m1) + 4 * __popc(m2);
-        const int sAM = __popc(An & m0) + 2 * __popc(An & m1) + 4 * __popc(An & m2);
-        esum += 128 - 2 * sM - 8 * __popc(An) + 4 * sAM;
-    }
-    return An;
+    tie = eq & test & ~zt;
+    inA = tie & maskA;
+    return A ^ (~test | borrow);
+}
+
+// Bond sum s * sum(nbrs) = sum (1 - 2a)(4 - 2M) over the sites of a word
+__device__ __forceinline__ int word_bonds(uint32_t An, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb)
+{
+    const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
+    const uint32_t m0 = s1 ^ s2, c3 = s1 & s2;
+    const uint32_t m1 = c1 ^ c2 ^ c3;
+    const uint32_t m2 = (c1 & c2) | (c3 & (c1 | c2));
+    const int sM = __popc(m0) + 2 * __popc(m1) + 4 * __popc(m2);
+    const int sAM = __popc(An & m0) + 2 * __popc(An & m1) + 4 * __popc(An & m2);
+    return 128 - 2 * sM - 8 * __popc(An) + 4 * sAM;
 }
 
 // 16 staged bytes (+-1) -> 16 bits (1 = -1)
@@ -269,6 +261,35 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
         return __shfl_sync(0xffffffffu, t, 0);
     };
 
+    // the warp's tie list: entries appended with a ballot, resolved in bulk
+    TieEntry* tl = reinterpret_cast<TieEntry*>(part + G::STAGE + G::OUT + G::BITS + NS * 8);
+    int ntie = 0;
+    auto flush_ties = [&]() {
+        __syncwarp();
+        for (int e = lane; e < ntie; e += 32) {
+            const TieEntry t = tl[e];
+            uint32_t m = t.tie, flips = 0u;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const bool inA = (t.inA >> b) & 1u;
+                const uint32_t site = (uint32_t)t.y * (uint32_t)L + (uint32_t)(t.x + 2 * b);
+                const uint64_t u53 = ((uint64_t)(inA ? a.tA8 : a.tB8) << 45) |
+                                     (accept_fine56(a.key, site, a.sweep, a.replica) >> 11);
+                if (u53 < (inA ? a.tA : a.tB)) flips |= 1u << b;
+            }
+            if (flips) bits[t.pos] ^= flips;
+        }
+        __syncwarp();
+        ntie = 0;
+    };
+    auto record_ties = [&](uint32_t tie, uint32_t inA, uint32_t pos, int yy, int xx) {
+        const uint32_t has = __ballot_sync(0xffffffffu, tie != 0u);
+        if (tie) tl[ntie + __popc(has & ((1u << lane) - 1u))] = TieEntry{pos, tie, inA, yy, xx};
+        ntie += __popc(has);
+        if (ntie > G::TIECAP - 32) flush_ties();
+    };
+
     int esum = 0, msum = 0;
     uint32_t gq = 0;  // store groups issued by this warp: output-ring half = gq & 1
     int cur = grab();
@@ -327,34 +348,58 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
         if (stop) break;
         __syncwarp();
         // colour 0 on the tile and its ring: rows 1..TY+2, interior words + one halo word
-        for (int task = lane; task < (TY + 2) * (NWI + 1); task += 32) {
-            const int r = 1 + task / (NWI + 1), k = task % (NWI + 1);
-            const int p = r & 1;
-            const int w = k < NWI ? 1 + k : (p ? 0 : NWI + 1);
-            uint32_t* Hr = bits + (r * 2 + p) * NWB;
-            const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
-            const uint32_t Gw = Gr[w];
-            const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
-            const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
-            int dummy = 0;
-            Hr[w] = update_word<false>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w], bits[((r + 1) * 2 + p) * NWB + w], Lb,
-                                       Rb, w, p, wrapi(y0 - 2 + r, L), x0, tg_acc, a, th, dummy);
+        for (int t0 = 0; t0 < (TY + 2) * (NWI + 1); t0 += 32) {
+            const int task = t0 + lane;
+            uint32_t tie = 0u, inA = 0u, pos = 0u;
+            int yy = 0, xx = 0;
+            if (task < (TY + 2) * (NWI + 1)) {
+                const int r = 1 + task / (NWI + 1), k = task % (NWI + 1);
+                const int p = r & 1;
+                const int w = k < NWI ? 1 + k : (p ? 0 : NWI + 1);
+                pos = (uint32_t)((r * 2 + p) * NWB + w);
+                const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
+                const uint32_t Gw = Gr[w];
+                const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
+                const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
+                yy = wrapi(y0 - 2 + r, L);
+                xx = wrapi(x0 - 64 + 64 * w + p, L);
+                bits[pos] = update_word(bits[pos], bits[pos - 2 * NWB], bits[pos + 2 * NWB], Lb, Rb, xx, yy, tg_acc,
+                                        a, th, tie, inA);
+            }
+            record_ties(tie, inA, pos, yy, xx);
         }
-        __syncwarp();
-        // colour 1 on the tile, 32 words (RPG rows) at a time, then those rows out
+        flush_ties();
+        // colour 1 on the tile
         for (int t0 = 0; t0 < TY * NWI; t0 += 32) {
             const int task = t0 + lane;
             const int r = 2 + task / NWI, w = 1 + task % NWI;
             const int p = (r + 1) & 1;
-            uint32_t* Hr = bits + (r * 2 + p) * NWB;
+            const uint32_t pos = (uint32_t)((r * 2 + p) * NWB + w);
             const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
             const uint32_t Gw = Gr[w];
             const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
             const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
-            const uint32_t An = update_word<MEAS>(Hr[w], bits[((r - 1) * 2 + p) * NWB + w],
-                                                  bits[((r + 1) * 2 + p) * NWB + w], Lb, Rb, w, p,
-                                                  wrapi(y0 - 2 + r, L), x0, tg_acc, a, th, esum);
-            if (MEAS) msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+            const int yy = wrapi(y0 - 2 + r, L), xx = wrapi(x0 - 64 + 64 * w + p, L);
+            uint32_t tie, inA;
+            bits[pos] = update_word(bits[pos], bits[pos - 2 * NWB], bits[pos + 2 * NWB], Lb, Rb, xx, yy, tg_acc, a,
+                                    th, tie, inA);
+            record_ties(tie, inA, pos, yy, xx);
+        }
+        flush_ties();
+        // the tile's rows to the output ring and out, RPG rows (32 words) at a time
+        for (int t0 = 0; t0 < TY * NWI; t0 += 32) {
+            const int task = t0 + lane;
+            const int r = 2 + task / NWI, w = 1 + task % NWI;
+            const int p = (r + 1) & 1;
+            const uint32_t pos = (uint32_t)((r * 2 + p) * NWB + w);
+            const uint32_t* Gr = bits + (r * 2 + (1 - p)) * NWB;
+            const uint32_t An = bits[pos], Gw = Gr[w];
+            if (MEAS) {
+                const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[w - 1], Gw, 1);
+                const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[w + 1], 1) : Gw;
+                esum += word_bonds(An, bits[pos - 2 * NWB], bits[pos + 2 * NWB], Lb, Rb);
+                msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+            }
             // the output-ring half this group uses must have been read by its
             // last stores (each storing lane waits for its own bulk groups)
             if (lane < 2 * G::RPG) bulk_wait_read1();
