@@ -12,8 +12,8 @@ Fixtures:
                   testsuite/components/5-metro_exp.cpp (N = 1e5, 500 passes,
                   beta = 0.44): accept counts of the MARQOV rule and of plain
                   exp, and a SHA-256 of the 5e7 individual decisions.
-  philox_kat.npz  Philox4x32-10 known-answer vectors of the Random123
-                  distribution (published), for the engine's generator.
+  (philox_curand.npz, cuRAND Philox4_32_10 blocks, is made on a GPU machine
+  by make_philox_curand.py.)
   <case>.npz      Metropolis runs through MARQOV::Metropolis<H,L>::move in
                   colour order on the keyed Philox stream: initial state (by
                   the reference initstatespace rule where it has one), final
@@ -59,14 +59,6 @@ def main():
          accepted_plain=np.int64(plain), sha256=np.array(digest))
     # the first words of RNGCache<mt19937_64>{0}, to pin the oracle's MT19937-64
     save("mt19937_64_words", words=ref.mt_words(1024))
-
-    # -- Philox KAT (Random123 kat_vectors, philox4x32_10)
-    ctr = np.array([[0, 0, 0, 0], [0xffffffff] * 4, [0x243f6a88, 0x85a308d3, 0x13198a2e, 0x03707344]], np.uint32)
-    key = np.array([[0, 0], [0xffffffff] * 2, [0xa4093822, 0x299f31d0]], np.uint32)
-    out = np.array([[0x6627e8d5, 0xe169c58d, 0xbc57ac4c, 0x9b00dbd8],
-                    [0x408f276d, 0x41c83b0e, 0xa20bc7c6, 0x6d5451fd],
-                    [0xd16cfe09, 0x94fdcceb, 0x5001e420, 0x24126ea1]], np.uint32)
-    save("philox_kat", ctr=ctr, key=key, out=out)
 
     # -- Metropolis cases through the reference templates
     def int_case(name, kind, ref_kind, dim, L, J, D, beta, seed, replica, nsweeps, q=0, bonds=None,

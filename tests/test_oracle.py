@@ -18,10 +18,12 @@ def model_of(g):
     return O.OrcModel(kind=kind, q=int(g["q"]), J=float(g["J"]), h=float(g["D"]), k=float(g["J"]))
 
 
-def test_philox_kat(orc, golden):
-    g = golden("philox_kat")
-    for c, k, o in zip(g["ctr"], g["key"], g["out"]):
-        assert (orc.philox(c, k) == o).all()
+def test_philox_matches_curand_fixture(orc, golden):
+    """The oracle's Philox4x32-10 against cuRAND's Philox4_32_10 blocks."""
+    g = golden("philox_curand")
+    for seed, c, o in zip(g["seed"], g["ctr"], g["out"]):
+        seed = int(seed)
+        assert (orc.philox(c, [seed & 0xFFFFFFFF, seed >> 32]) == o).all()
 
 
 def test_mt19937_64_words(orc, golden):
