@@ -166,6 +166,20 @@ MQV_API mqv_status mqv_metropolis(mqv_sim* sim, int32_t nsweeps);
 /* nclusters Wolff clusters; sizes (host, may be NULL) receives each size
  * (synchronises when sizes != NULL). */
 MQV_API mqv_status mqv_wolff(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
+/* No counterpart in the reference.  mqv_wolff for int8 models (Ising,
+ * embedded Ising, Potts) that allocates no device memory: the queue, the
+ * visited bitmap and the size slots live in one static device array sized
+ * for lattices of at most 1,048,576 sites (larger lattices are rejected with
+ * MQV_ERR_INVALID_ARG).  For hosts that cannot have device memory allocated
+ * while they run clusters (HBM budgeted up front for resident lattices, or
+ * no cudaMalloc/cudaFree stalls allowed between their streams).  Same
+ * clusters, sizes and counters as mqv_wolff.  The bitmap starts at zero
+ * (module load) and every cluster leaves it zero.  The array is shared by
+ * all handles on a device: calls whose kernels may overlap race on it and
+ * must be serialised by the caller.  The first call on a device looks up the
+ * array's address and may load the module, so it must come before any
+ * stream capture. */
+MQV_API mqv_status mqv_wolff_noalloc(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
 /* n_emcs elementary MC steps (ncluster clusters then nmetro sweeps each),
  * measuring after every step.  obs (host, may be NULL) receives n_emcs
  * records; mean_cluster (host, may be NULL) receives n_emcs mean sizes. */

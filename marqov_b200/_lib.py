@@ -84,6 +84,7 @@ SIGNATURES = {
     "mqv_set_counters": (C.c_int32, [_vp, C.c_uint64, C.c_uint64]),
     "mqv_metropolis": (C.c_int32, [_vp, C.c_int32]),
     "mqv_wolff": (C.c_int32, [_vp, C.c_int32, _vp]),
+    "mqv_wolff_noalloc": (C.c_int32, [_vp, C.c_int32, _vp]),
     "mqv_emcs": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp]),
     "mqv_measure": (C.c_int32, [_vp, C.POINTER(Obs)]),
     "mqv_synchronize": (C.c_int32, [_vp]),

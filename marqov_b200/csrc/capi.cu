@@ -30,6 +30,11 @@ cudaError_t launch_metropolis_f32(Sim* s, int slot);
 cudaError_t launch_measure_f32(Sim* s, int slot);
 cudaError_t launch_finalize_f32(Sim* s, int nslots, double* d_out);
 cudaError_t launch_wolff_f32(Sim* s, int slot);
+int64_t wolff_noalloc_max_sites();
+int wolff_noalloc_max_clusters();
+cudaError_t wolff_noalloc_scratch(int device, uint32_t** out);
+cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot);
+const int32_t* wolff_noalloc_sizes(const uint32_t* scratch);
 
 // Smallest u53 rejected by update_accepted<pref>(dE, beta, .), 2^53 when all
 // are accepted: the rule accepts exactly the words with u53 below a cut.
@@ -605,6 +610,38 @@ MQV_API mqv_status mqv_wolff(mqv_sim* h, int32_t nclusters, int32_t* sizes)
         }
         if (sizes) {
             MQV_CK(cudaMemcpyAsync(sizes + done, s->d_csize, sizeof(int32_t) * chunk, cudaMemcpyDeviceToHost, s->stream));
+            MQV_CK(cudaStreamSynchronize(s->stream));
+        }
+        done += chunk;
+    }
+    return MQV_OK;
+}
+
+// mqv_wolff without any device allocation: the clusters run on the static
+// scratch of wolff.cu (int8 models, lattices of up to 2^20 sites).
+MQV_API mqv_status mqv_wolff_noalloc(mqv_sim* h, int32_t nclusters, int32_t* sizes)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (nclusters < 0) return fail(MQV_ERR_INVALID_ARG, "nclusters < 0");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    mqv_status st = check_wolff_supported(s);
+    if (st) return st;
+    if (s->is_f32)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "mqv_wolff_noalloc: int8 models only (Ising, embedded Ising, Potts)");
+    if (s->n > wolff_noalloc_max_sites())
+        return fail(MQV_ERR_INVALID_ARG, "mqv_wolff_noalloc: lattice of " + std::to_string(s->n) +
+                                             " sites exceeds the static scratch limit of " +
+                                             std::to_string(wolff_noalloc_max_sites()) + " sites");
+    uint32_t* scratch = nullptr;
+    MQV_CK(wolff_noalloc_scratch(s->device, &scratch));
+    int done = 0;
+    while (done < nclusters) {
+        const int chunk = std::min(nclusters - done, wolff_noalloc_max_clusters());
+        for (int c = 0; c < chunk; ++c) MQV_CK(launch_wolff_int8_noalloc(s, scratch, c));
+        if (sizes) {
+            MQV_CK(cudaMemcpyAsync(sizes + done, wolff_noalloc_sizes(scratch), sizeof(int32_t) * chunk,
+                                   cudaMemcpyDeviceToHost, s->stream));
             MQV_CK(cudaStreamSynchronize(s->stream));
         }
         done += chunk;

@@ -17,6 +17,8 @@
 // the bitmap is zero again for the next cluster.
 #include <cuda_runtime.h>
 
+#include <mutex>
+
 #include "engine.h"
 
 namespace mqv {
@@ -156,6 +158,107 @@ cudaError_t launch_wolff_int8(Sim* s, int slot)
     s->launches++;
     s->cluster++;
     return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Wolff clusters for int8 models with scratch that is never allocated.
+//
+// mqv_wolff takes its queue, visited bitmap and cluster-size slots from
+// device memory that the handle allocates on its first cluster.  A host that
+// cannot have device memory allocated at that point -- one that budgets the
+// whole of HBM up front for many resident lattices, or that must not let a
+// cudaMalloc/cudaFree stall its other streams in the middle of a run -- uses
+// mqv_wolff_noalloc instead, which draws the same clusters with the scratch
+// below: one file-scope device array, sized for lattices of up to
+// kNoAllocMaxSites sites, that exists from module load.
+//
+// What must start at zero: the visited bitmap.  The module load zero-fills
+// the array, and every cluster clears the bits of its members before its
+// kernel returns, so the bitmap is zero again between clusters.  The queue
+// and size slots are written before they are read.
+//
+// The array is shared by every handle on a device: calls whose kernels may
+// overlap (two streams, two host threads, two handles without ordering
+// between them) race on it and must be serialised by the caller.
+constexpr int64_t kNoAllocMaxSites = 1 << 20;  // 1,048,576 sites: 4 MiB queue + 128 KiB bitmap
+constexpr int kNoAllocMaxClusters = 4096;      // size slots per chunk of clusters
+constexpr size_t kNoAllocWords = (size_t)kNoAllocMaxSites + (size_t)kNoAllocMaxSites / 32 + kNoAllocMaxClusters;
+
+static __device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocWords];
+
+namespace {
+constexpr int kNoAllocMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_addr[kNoAllocMaxDevices] = {};
+}  // namespace
+
+int64_t wolff_noalloc_max_sites() { return kNoAllocMaxSites; }
+int wolff_noalloc_max_clusters() { return kNoAllocMaxClusters; }
+
+// Device address of the scratch on `device`, looked up once per device with
+// that device current (the caller makes it current).  The first lookup may
+// load the module, so the first call on a device has to come before any
+// stream capture begins.
+cudaError_t wolff_noalloc_scratch(int device, uint32_t** out)
+{
+    if (device < 0 || device >= kNoAllocMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[device]) {
+        void* p = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_addr[device] = static_cast<uint32_t*>(p);
+    }
+    *out = g_noalloc_addr[device];
+    return cudaSuccess;
+}
+
+// One cluster of the int8 Wolff update on the static scratch; the activation
+// rule and the draws are those of launch_wolff_int8, so the cluster is the
+// same.  The size lands in size slot `slot` of the scratch.
+cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot)
+{
+    WolffDev w{};
+    const double beta = s->md.beta;
+    if (s->md.kind == MQV_MODEL_ISING) {
+        w.mode = 0;
+        const double prob = -expm1(2.0 * beta * s->md.J);
+        if (!(prob > 0)) w.thr = 0;
+        else {
+            const double x = prob * 9007199254740992.0;
+            unsigned long long c = (unsigned long long)x;
+            if ((double)c < x) ++c;
+            w.thr = c > (1ull << 53) ? (1ull << 53) : c;
+        }
+    } else if (s->md.kind == MQV_MODEL_POTTS) {
+        w.mode = 2;
+        w.q = s->md.q;
+        w.thr = accept_cut(2, s->md.k * -0.5, beta);
+    } else {
+        w.mode = 1;
+        w.thr = accept_cut(2, -s->md.J, beta);
+    }
+    int32_t* queue = reinterpret_cast<int32_t*>(scratch);
+    uint32_t* visited = scratch + kNoAllocMaxSites;
+    int32_t* sizes = reinterpret_cast<int32_t*>(visited + kNoAllocMaxSites / 32);
+    int8_t* st = (int8_t*)s->state[s->cur];
+    const Key key = make_key(s->seed);
+    const uint32_t serial = (uint32_t)s->cluster;
+    if (s->lat_kind == MQV_LATTICE_HYPERCUBIC)
+        wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->sten, st, visited, queue, sizes + slot, key, serial,
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+    else
+        wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->csr, st, visited, queue, sizes + slot, key, serial,
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+    s->launches++;
+    s->cluster++;
+    return cudaGetLastError();
+}
+
+// Size slots of the scratch (for the copy of a chunk's sizes to the host).
+const int32_t* wolff_noalloc_sizes(const uint32_t* scratch)
+{
+    return reinterpret_cast<const int32_t*>(scratch + kNoAllocMaxSites + kNoAllocMaxSites / 32);
 }
 
 }  // namespace mqv
