@@ -34,6 +34,9 @@
 // block.  The result equals update_accepted<1>(dE, beta, word) bit for bit.
 #include <cuda_runtime.h>
 
+#include <cstdlib>
+#include <cstring>
+
 #include <cstdio>
 
 #include "engine.h"
@@ -441,6 +444,242 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
     }
 }
 
+// ---- band kernel: one CTA spans the lattice width --------------------------------
+//
+// Thread t owns word column t of both halves of every row (64 sites: 32 even-x
+// and 32 odd-x), so a CTA of L/64 threads covers whole rows and needs no
+// horizontal halo.  CTA c streams down its band of rows [y0, y1) (bands split
+// the L rows evenly over the grid) with two halo rows above and below: staged
+// row r is lattice row y0 - 2 + r, r = 0 .. H + 3.  Step k of the pipeline
+//   packs staged row k (one bulk copy per row, ring of NSB slots) into the bit
+//   ring, updates colour 0 of row k - 1, colour 1 of row k - 2 - S, and writes
+//   row k - 2 - 2S out.
+// Top-byte ties of both colours are resolved in bulk every S steps, so a word
+// is final at most S - 1 steps after its update: colour 1 lags colour 0 by S
+// rows and the output lags colour 1 by S rows, which keeps every neighbour a
+// word reads final.  The bit ring keeps the last RB >= 2S + 4 rows.
+
+constexpr int band_ring(int S)
+{
+    int r = 1;
+    while (r < 2 * S + 4) r <<= 1;
+    return r;
+}
+
+template <int NT, int S>  // NT = L / 64 threads per CTA; ties resolved every S steps
+struct BandGeom {
+    static constexpr int NW = NT / 32;
+    static constexpr int NSB = 4;                // staged row slots
+    static constexpr int RB = band_ring(S);      // bit ring rows
+    static constexpr int L = NT * 64;
+    static constexpr int STAGE = NSB * L;
+    static constexpr int BITS = RB * 2 * NT * 4;
+    static constexpr int TIECAP = 96;            // tie entries per warp
+    static constexpr int TIES = NW * TIECAP * 16;
+    static constexpr int SMEM = STAGE + BITS + TIES + NSB * 8;
+    static_assert(NT % 32 == 0 && S >= 1, "band shape");
+};
+
+struct BandTie {
+    uint32_t pos;  // word position in the bit ring: (slot * 2 + half) * NT + t
+    uint32_t tie;  // undecided sites of the word
+    uint32_t inA;  // those of class A
+    int32_t y;     // lattice row
+};
+
+// 32 bits -> 32 bytes (+1 -> 0x01, -1 -> 0xFF) as two 16-byte vectors
+__device__ __forceinline__ void unpack32_regs(uint32_t bits, uint4& lo, uint4& hi)
+{
+    uint32_t o[8];
+#pragma unroll
+    for (int k = 0; k < 8; ++k) {
+        const uint32_t n = (bits >> (4 * k)) & 0xFu;
+        o[k] = 0x01010101u + ((n * 0x00204081u) & 0x01010101u) * 0xFEu;
+    }
+    lo = make_uint4(o[0], o[1], o[2], o[3]);
+    hi = make_uint4(o[4], o[5], o[6], o[7]);
+}
+
+template <int NT, int S, bool MEAS>
+__global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising2DArgs a)
+{
+    using G = BandGeom<NT, S>;
+    constexpr int RB = G::RB, NSB = G::NSB, L = G::L, Lh = L / 2;
+    extern __shared__ __align__(128) uint8_t smem[];
+    uint8_t* stage = smem;
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + G::STAGE);
+    BandTie* ties = reinterpret_cast<BandTie*>(smem + G::STAGE + G::BITS);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::STAGE + G::BITS + G::TIES);
+    const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const int y0 = (int)(((long long)blockIdx.x * L) / gridDim.x);
+    const int y1 = (int)(((long long)(blockIdx.x + 1) * L) / gridDim.x);
+    const int NR = y1 - y0 + 4;  // staged rows
+    const uint32_t tg_acc = tag(kAccept, a.replica);
+    const Thr th = make_thr(a);
+    const int tl_ = t == 0 ? NT - 1 : t - 1, tr_ = t == NT - 1 ? 0 : t + 1;
+
+    if (t == 0) {
+        for (int k = 0; k < NSB; ++k) mbar_init(smem_addr(&bars[k]), 1);
+        mbar_fence_init();
+    }
+    __syncthreads();
+    // staged row r -> slot r % NSB (thread 0)
+    auto issue = [&](int r) {
+        const int y = wrapi(y0 - 2 + r, L);
+        const uint32_t bar = smem_addr(&bars[r % NSB]);
+        mbar_expect_tx(bar, (uint32_t)L);
+        bulk_g2s(smem_addr(stage + (r % NSB) * L), a.src + (size_t)y * L, (uint32_t)L, bar);
+    };
+    if (t == 0)
+        for (int r = 0; r < NSB && r < NR; ++r) issue(r);
+
+    BandTie* tl = ties + warp * G::TIECAP;
+    int ntie = 0;
+    auto record = [&](uint32_t tie, uint32_t inA, uint32_t pos, int y) {
+        const uint32_t has = __ballot_sync(0xffffffffu, tie != 0u);
+        if (tie) tl[ntie + __popc(has & ((1u << lane) - 1u))] = BandTie{pos, tie, inA, y};
+        ntie += __popc(has);
+    };
+    auto flush = [&]() {
+        __syncwarp();
+        for (int e = lane; e < ntie; e += 32) {
+            const BandTie te = tl[e];
+            const uint32_t w = te.pos % NT, h = (te.pos / NT) & 1u;
+            const uint32_t site0 = (uint32_t)te.y * (uint32_t)L + 64u * w + h;
+            uint32_t m = te.tie, flips = 0u;
+            while (m) {
+                const int b = __ffs(m) - 1;
+                m &= m - 1;
+                const bool inA = (te.inA >> b) & 1u;
+                const uint64_t u53 = ((uint64_t)(inA ? a.tA8 : a.tB8) << 45) |
+                                     (accept_fine56(a.key, site0 + 2u * (uint32_t)b, a.sweep, a.replica) >> 11);
+                if (u53 < (inA ? a.tA : a.tB)) flips |= 1u << b;
+            }
+            if (flips) bits[te.pos] ^= flips;
+        }
+        __syncwarp();
+        ntie = 0;
+    };
+    // update the word of column t in half p of staged row r (lattice row y)
+    auto update = [&](int r, int p, int y) {
+        const int sl = r & (RB - 1), su = (r - 1) & (RB - 1), sd = (r + 1) & (RB - 1);
+        const uint32_t pos = (uint32_t)((sl * 2 + p) * NT + t);
+        const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NT;
+        const uint32_t Gw = Gr[t];
+        const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
+        const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
+        uint32_t tie, inA;
+        bits[pos] = update_word(bits[pos], bits[(su * 2 + p) * NT + t], bits[(sd * 2 + p) * NT + t], Lb, Rb,
+                                64 * t + p, y, tg_acc, a, th, tie, inA);
+        record(tie, inA, pos, y);
+    };
+
+    int esum = 0, msum = 0;
+    int k = 0;
+    bool stop = false;
+    for (; k < NR + 2 * S; ++k) {
+        int timed_out = 0;
+        if (k < NR) {
+            // every thread waits for row k (bounded: a stuck copy sets an error status)
+            const uint32_t bar = smem_addr(&bars[k % NSB]);
+            const uint32_t par = (uint32_t)(k / NSB) & 1u;
+            if (!mbar_try_wait(bar, par)) {
+                const uint64_t t0 = global_timer_ns();
+                for (uint32_t i = 1;; ++i) {
+                    __nanosleep(64);
+                    if (mbar_try_wait(bar, par)) break;
+                    if ((i & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
+                        timed_out = 1;
+                        break;
+                    }
+                }
+            }
+        }
+        if (__syncthreads_or(timed_out)) {
+            stop = true;
+            break;
+        }
+        if (k < NR) {
+            const uint8_t* row = stage + (k % NSB) * L;
+            uint32_t* brow = bits + (k & (RB - 1)) * 2 * NT;
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * t);
+                brow[h * NT + t] = pack16(q[0]) | (pack16(q[1]) << 16);
+            }
+        }
+        __syncthreads();  // slot k consumed, row k's bits visible
+        if (t == 0 && k + NSB < NR) {
+            fence_proxy_async_smem();
+            issue(k + NSB);
+        }
+        // colour 0 of row k - 1 (staged rows 1 .. NR - 2)
+        if (k - 1 >= 1 && k - 1 <= NR - 2) {
+            const int y = wrapi(y0 - 3 + k, L);
+            update(k - 1, y & 1, y);
+        }
+        // colour 1 of row k - 2 - S (staged rows 2 .. NR - 3)
+        const int r1 = k - 2 - S;
+        if (r1 >= 2 && r1 <= NR - 3) {
+            const int y = y0 - 2 + r1;
+            update(r1, 1 - (y & 1), y);
+        }
+        if (k % S == S - 1 || ntie > G::TIECAP - 64) flush();
+        // row k - 2 - 2S out
+        const int r2 = k - 2 - 2 * S;
+        if (r2 >= 2 && r2 <= NR - 3) {
+            const int y = y0 - 2 + r2;
+            const int sl = r2 & (RB - 1);
+            const uint32_t w0 = bits[(sl * 2) * NT + t], w1 = bits[(sl * 2 + 1) * NT + t];
+            int8_t* drow = a.dst + (size_t)y * L + 32 * t;
+            uint4 lo, hi;
+            unpack32_regs(w0, lo, hi);
+            reinterpret_cast<uint4*>(drow)[0] = lo;
+            reinterpret_cast<uint4*>(drow)[1] = hi;
+            unpack32_regs(w1, lo, hi);
+            reinterpret_cast<uint4*>(drow + Lh)[0] = lo;
+            reinterpret_cast<uint4*>(drow + Lh)[1] = hi;
+            if (MEAS) {
+                const int p1 = 1 - (y & 1);
+                const uint32_t An = p1 ? w1 : w0, Gw = p1 ? w0 : w1;
+                const uint32_t* Gr = bits + (sl * 2 + (1 - p1)) * NT;
+                const uint32_t Lb = p1 ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
+                const uint32_t Rb = p1 ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
+                const uint32_t U = bits[((((r2 - 1) & (RB - 1)) * 2) + p1) * NT + t];
+                const uint32_t D = bits[((((r2 + 1) & (RB - 1)) * 2) + p1) * NT + t];
+                esum += word_bonds(An, U, D, Lb, Rb);
+                msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+            }
+        }
+        __syncthreads();  // the step's words final for the next step's readers
+    }
+    if (stop) {
+        // wait (bounded) for the copies still in flight before the CTA leaves
+        if (t == 0) {
+            atomicExch(a.status, MQV_ERR_TIMEOUT);
+            const uint64_t t0 = global_timer_ns();
+            for (int r = k; r < NR && r < k + NSB; ++r) {
+                const uint32_t bar = smem_addr(&bars[r % NSB]);
+                const uint32_t par = (uint32_t)(r / NSB) & 1u;
+                while (!mbar_try_wait(bar, par) && global_timer_ns() - t0 < 1000000000ull) __nanosleep(1000);
+            }
+        }
+        return;
+    }
+    if (MEAS) {
+        long long e = esum, m = msum;
+#pragma unroll
+        for (int o = 16; o; o >>= 1) {
+            e += __shfl_xor_sync(0xffffffffu, e, o);
+            m += __shfl_xor_sync(0xffffffffu, m, o);
+        }
+        if (lane == 0) {
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccEne), (unsigned long long)(2 * e));
+            atomicAdd(reinterpret_cast<unsigned long long*>(a.acc + kAccMag), (unsigned long long)m);
+        }
+    }
+}
+
 // ---- layout conversion: row-major <-> split rows -----------------------------
 
 __global__ void split_rows(const int8_t* __restrict__ in, int8_t* __restrict__ out, int L)
@@ -492,31 +731,62 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-// Candidate tile shapes and warps per CTA.  Every candidate computes the same
-// result; the autotuner keeps the fastest for a lattice size.
+template <int NT, int S, bool MEAS>
+static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t stream)
+{
+    using G = BandGeom<NT, S>;
+    auto kern = ising2d_band<NT, S, MEAS>;
+    static int cps = 0;  // resident CTAs per SM for this instantiation
+    if (cps == 0) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        if (e != cudaSuccess) return e;
+        int c = 0;
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NT, G::SMEM);
+        if (e != cudaSuccess) return e;
+        cps = c < 1 ? 1 : c;
+    }
+    // one band per CTA, at least 8 rows each
+    long long grid = (long long)nsm * cps;
+    if (grid > G::L / 8) grid = G::L / 8;
+    kern<<<(int)grid, NT, G::SMEM, stream>>>(a);
+    return cudaGetLastError();
+}
+
+// Candidate kernels: tiles (tx x ty sites, nwarp independent warps per CTA)
+// or bands (band = NT threads spanning a lattice of side 64 NT, ties resolved
+// every S steps).  Every candidate computes the same result; the autotuner
+// keeps the fastest for a lattice size.
 struct SweepConfig {
-    int tx, ty, nwarp;
+    int tx, ty, nwarp;  // tile shape (band: tx = L, ty = S, nwarp = NT / 32)
+    bool band;
     SweepLauncher plain, meas;
 };
 
 #define MQV_CFG(TX, TY, NW) \
-    SweepConfig{TX, TY, NW, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
+    SweepConfig{TX, TY, NW, false, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
+#define MQV_BAND(NT, S) \
+    SweepConfig{64 * NT, S, NT / 32, true, launch_band<NT, S, false>, launch_band<NT, S, true>}
 
 static const SweepConfig kConfigs[] = {
     MQV_CFG(512, 32, 4), MQV_CFG(256, 32, 4), MQV_CFG(512, 32, 2), MQV_CFG(256, 32, 8),
     MQV_CFG(1024, 32, 2), MQV_CFG(128, 32, 4), MQV_CFG(64, 32, 4),
+    MQV_BAND(256, 2), MQV_BAND(256, 4), MQV_BAND(128, 2), MQV_BAND(128, 4),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
-static bool config_fits(const SweepConfig& c, int L) { return L % c.tx == 0 && L % c.ty == 0; }
+static bool config_fits(const SweepConfig& c, int L)
+{
+    if (c.band) return L == c.tx;
+    return L % c.tx == 0 && L % c.ty == 0;
+}
 
 static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs& a)
 {
     a.src = (const int8_t*)s->state[s->cur];
     a.dst = (int8_t*)s->state[s->cur ^ 1];
     a.L = s->len;
-    a.ntx = s->len / c.tx;
-    a.ntiles = a.ntx * (s->len / c.ty);
+    a.ntx = c.band ? 1 : s->len / c.tx;
+    a.ntiles = c.band ? 0 : a.ntx * (s->len / c.ty);
     a.key = make_key(s->seed);
     a.sweep = (uint32_t)s->sweep;
     a.replica = s->replica;
@@ -548,8 +818,23 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
 // Time every fitting candidate on this lattice (two sweeps each into the
 // scratch buffer; the state is not modified) and keep the fastest.  Small
 // lattices take the first fitting candidate.
+static void config_name(const SweepConfig& c, char* buf, int len)
+{
+    if (c.band) snprintf(buf, len, "ising2d_band<%d,%d>", c.nwarp * 32, c.ty);
+    else snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
+}
+
 static int pick_config(Sim* s)
 {
+    // MARQOV_B200_SWEEP_CONFIG=<name> (as mqv_describe prints it) forces one
+    // candidate, when it fits the lattice: for tests of each kernel shape
+    if (const char* want = getenv("MARQOV_B200_SWEEP_CONFIG")) {
+        char buf[64];
+        for (int k = 0; k < kNumConfigs; ++k) {
+            config_name(kConfigs[k], buf, sizeof buf);
+            if (config_fits(kConfigs[k], s->len) && strcmp(buf, want) == 0) return k;
+        }
+    }
     int first = -1;
     for (int k = 0; k < kNumConfigs; ++k)
         if (config_fits(kConfigs[k], s->len)) {
@@ -607,8 +892,7 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
 const char* ising2d_config_name(Sim* s, char* buf, int len)
 {
     if (s->sweep_cfg < 0) return "";
-    const SweepConfig& c = kConfigs[s->sweep_cfg];
-    snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
+    config_name(kConfigs[s->sweep_cfg], buf, len);
     return buf;
 }
 
