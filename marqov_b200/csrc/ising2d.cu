@@ -63,7 +63,35 @@ struct Ising2DArgs {
     long long* acc;
     int* status;
     int* counter;  // next tile (zeroed before the launch)
+    uint32_t rk0[10], rk1[10];  // Philox round keys of `key`
 };
+
+// Philox4x32-10 with the round keys taken from the launch arguments (the
+// same function as philox() in common.cuh, whose key schedule is computed
+// once on the host)
+__device__ __forceinline__ uint4 philox_rk(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3, const Ising2DArgs& a)
+{
+#pragma unroll
+    for (int r = 0; r < 10; ++r) {
+        uint32_t hi0, lo0, hi1, lo1;
+        mulhilo(0xD2511F53u, c0, hi0, lo0);
+        mulhilo(0xCD9E8D57u, c2, hi1, lo1);
+        const uint32_t n0 = hi1 ^ c1 ^ a.rk0[r];
+        const uint32_t n2 = hi0 ^ c3 ^ a.rk1[r];
+        c0 = n0;
+        c1 = lo1;
+        c2 = n2;
+        c3 = lo0;
+    }
+    return make_uint4(c0, c1, c2, c3);
+}
+
+// low 56 bits of the acceptance word of `site` (accept_fine56 of common.cuh)
+__device__ __forceinline__ uint64_t fine56_rk(uint32_t site, const Ising2DArgs& a)
+{
+    const uint4 f = philox_rk(site >> 1, a.sweep, 0u, (kAcceptFine << 24) | (a.replica & 0xFFFFFFu), a);
+    return ((site & 1u) ? hi64(f) : lo64(f)) & 0x00FFFFFFFFFFFFFFull;
+}
 
 template <int TX, int TY, int NWARP>
 struct TileGeom {
@@ -132,8 +160,8 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
 {
     // the word's eight random planes: two Philox blocks of its 32-site group
     const uint32_t g = accept_group((uint32_t)y * (uint32_t)a.L + (uint32_t)x);
-    const uint4 q0 = philox(g, a.sweep, 0u, tg_acc, a.key);
-    const uint4 q1 = philox(g, a.sweep, 1u, tg_acc, a.key);
+    const uint4 q0 = philox_rk(g, a.sweep, 0u, tg_acc, a);
+    const uint4 q1 = philox_rk(g, a.sweep, 1u, tg_acc, a);
     const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder; M <= 4)
     const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
@@ -278,7 +306,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
                 const bool inA = (t.inA >> b) & 1u;
                 const uint32_t site = (uint32_t)t.y * (uint32_t)L + (uint32_t)(t.x + 2 * b);
                 const uint64_t u53 = ((uint64_t)(inA ? a.tA8 : a.tB8) << 45) |
-                                     (accept_fine56(a.key, site, a.sweep, a.replica) >> 11);
+                                     (fine56_rk(site, a) >> 11);
                 if (u53 < (inA ? a.tA : a.tB)) flips |= 1u << b;
             }
             if (flips) bits[t.pos] ^= flips;
@@ -457,20 +485,13 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
 // Top-byte ties of both colours are resolved in bulk every S steps, so a word
 // is final at most S - 1 steps after its update: colour 1 lags colour 0 by S
 // rows and the output lags colour 1 by S rows, which keeps every neighbour a
-// word reads final.  The bit ring keeps the last RB >= 2S + 4 rows.
+// word reads final.  The bit ring keeps the last RB = 2S + 4 rows.
 
-constexpr int band_ring(int S)
-{
-    int r = 1;
-    while (r < 2 * S + 4) r <<= 1;
-    return r;
-}
-
-template <int NT, int S>  // NT = L / 64 threads per CTA; ties resolved every S steps
+template <int NT, int S, int NSB_>  // NT = L / 64 threads; ties every S steps; NSB_ staged rows
 struct BandGeom {
     static constexpr int NW = NT / 32;
-    static constexpr int NSB = 4;                // staged row slots
-    static constexpr int RB = band_ring(S);      // bit ring rows
+    static constexpr int NSB = NSB_;             // staged row slots
+    static constexpr int RB = 2 * S + 4;         // bit ring rows
     static constexpr int L = NT * 64;
     static constexpr int STAGE = NSB * L;
     static constexpr int BITS = RB * 2 * NT * 4;
@@ -500,10 +521,10 @@ __device__ __forceinline__ void unpack32_regs(uint32_t bits, uint4& lo, uint4& h
     hi = make_uint4(o[4], o[5], o[6], o[7]);
 }
 
-template <int NT, int S, bool MEAS>
+template <int NT, int S, int NSB_, bool MEAS>
 __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising2DArgs a)
 {
-    using G = BandGeom<NT, S>;
+    using G = BandGeom<NT, S, NSB_>;
     constexpr int RB = G::RB, NSB = G::NSB, L = G::L, Lh = L / 2;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* stage = smem;
@@ -552,7 +573,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 m &= m - 1;
                 const bool inA = (te.inA >> b) & 1u;
                 const uint64_t u53 = ((uint64_t)(inA ? a.tA8 : a.tB8) << 45) |
-                                     (accept_fine56(a.key, site0 + 2u * (uint32_t)b, a.sweep, a.replica) >> 11);
+                                     (fine56_rk(site0 + 2u * (uint32_t)b, a) >> 11);
                 if (u53 < (inA ? a.tA : a.tB)) flips |= 1u << b;
             }
             if (flips) bits[te.pos] ^= flips;
@@ -562,7 +583,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     };
     // update the word of column t in half p of staged row r (lattice row y)
     auto update = [&](int r, int p, int y) {
-        const int sl = r & (RB - 1), su = (r - 1) & (RB - 1), sd = (r + 1) & (RB - 1);
+        const int sl = r % RB, su = (r - 1) % RB, sd = (r + 1) % RB;
         const uint32_t pos = (uint32_t)((sl * 2 + p) * NT + t);
         const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NT;
         const uint32_t Gw = Gr[t];
@@ -601,7 +622,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         }
         if (k < NR) {
             const uint8_t* row = stage + (k % NSB) * L;
-            uint32_t* brow = bits + (k & (RB - 1)) * 2 * NT;
+            uint32_t* brow = bits + (k % RB) * 2 * NT;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * t);
@@ -629,7 +650,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         const int r2 = k - 2 - 2 * S;
         if (r2 >= 2 && r2 <= NR - 3) {
             const int y = y0 - 2 + r2;
-            const int sl = r2 & (RB - 1);
+            const int sl = r2 % RB;
             const uint32_t w0 = bits[(sl * 2) * NT + t], w1 = bits[(sl * 2 + 1) * NT + t];
             int8_t* drow = a.dst + (size_t)y * L + 32 * t;
             uint4 lo, hi;
@@ -645,13 +666,14 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 const uint32_t* Gr = bits + (sl * 2 + (1 - p1)) * NT;
                 const uint32_t Lb = p1 ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
                 const uint32_t Rb = p1 ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
-                const uint32_t U = bits[((((r2 - 1) & (RB - 1)) * 2) + p1) * NT + t];
-                const uint32_t D = bits[((((r2 + 1) & (RB - 1)) * 2) + p1) * NT + t];
+                const uint32_t U = bits[(((r2 - 1) % RB) * 2 + p1) * NT + t];
+                const uint32_t D = bits[(((r2 + 1) % RB) * 2 + p1) * NT + t];
                 esum += word_bonds(An, U, D, Lb, Rb);
                 msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
             }
         }
-        __syncthreads();  // the step's words final for the next step's readers
+        // the next step's __syncthreads_or makes this step's words visible
+        // to their readers before any of them is read
     }
     if (stop) {
         // wait (bounded) for the copies still in flight before the CTA leaves
@@ -731,11 +753,11 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-template <int NT, int S, bool MEAS>
+template <int NT, int S, int NSB, bool MEAS>
 static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
-    using G = BandGeom<NT, S>;
-    auto kern = ising2d_band<NT, S, MEAS>;
+    using G = BandGeom<NT, S, NSB>;
+    auto kern = ising2d_band<NT, S, NSB, MEAS>;
     static int cps = 0;  // resident CTAs per SM for this instantiation
     if (cps == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
@@ -759,18 +781,20 @@ static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t strea
 struct SweepConfig {
     int tx, ty, nwarp;  // tile shape (band: tx = L, ty = S, nwarp = NT / 32)
     bool band;
+    int nsb;            // band: staged row slots
     SweepLauncher plain, meas;
 };
 
 #define MQV_CFG(TX, TY, NW) \
-    SweepConfig{TX, TY, NW, false, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
-#define MQV_BAND(NT, S) \
-    SweepConfig{64 * NT, S, NT / 32, true, launch_band<NT, S, false>, launch_band<NT, S, true>}
+    SweepConfig{TX, TY, NW, false, 0, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
+#define MQV_BAND(NT, S, NSB) \
+    SweepConfig{64 * NT, S, NT / 32, true, NSB, launch_band<NT, S, NSB, false>, launch_band<NT, S, NSB, true>}
 
 static const SweepConfig kConfigs[] = {
     MQV_CFG(512, 32, 4), MQV_CFG(256, 32, 4), MQV_CFG(512, 32, 2), MQV_CFG(256, 32, 8),
     MQV_CFG(1024, 32, 2), MQV_CFG(128, 32, 4), MQV_CFG(64, 32, 4),
-    MQV_BAND(256, 2), MQV_BAND(256, 4), MQV_BAND(128, 2), MQV_BAND(128, 4),
+    MQV_BAND(256, 4, 2), MQV_BAND(256, 2, 2), MQV_BAND(256, 4, 3), MQV_BAND(256, 4, 4),
+    MQV_BAND(128, 4, 2), MQV_BAND(128, 4, 4),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
@@ -788,6 +812,10 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
     a.ntx = c.band ? 1 : s->len / c.tx;
     a.ntiles = c.band ? 0 : a.ntx * (s->len / c.ty);
     a.key = make_key(s->seed);
+    for (int r = 0; r < 10; ++r) {
+        a.rk0[r] = a.key.k0 + (uint32_t)r * 0x9E3779B9u;
+        a.rk1[r] = a.key.k1 + (uint32_t)r * 0xBB67AE85u;
+    }
     a.sweep = (uint32_t)s->sweep;
     a.replica = s->replica;
     // cuts of update_accepted<1> on u53 per aligned-neighbour count k:
@@ -820,7 +848,7 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
 // lattices take the first fitting candidate.
 static void config_name(const SweepConfig& c, char* buf, int len)
 {
-    if (c.band) snprintf(buf, len, "ising2d_band<%d,%d>", c.nwarp * 32, c.ty);
+    if (c.band) snprintf(buf, len, "ising2d_band<%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb);
     else snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
 }
 

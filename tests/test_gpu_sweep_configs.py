@@ -11,10 +11,12 @@ pytestmark = pytest.mark.gpu
 BETA = 0.44068679
 
 CONFIGS = [
-    ("ising2d_band<256,2>", 16384),
-    ("ising2d_band<256,4>", 16384),
-    ("ising2d_band<128,2>", 8192),
-    ("ising2d_band<128,4>", 8192),
+    ("ising2d_band<256,4,2>", 16384),
+    ("ising2d_band<256,2,2>", 16384),
+    ("ising2d_band<256,4,3>", 16384),
+    ("ising2d_band<256,4,4>", 16384),
+    ("ising2d_band<128,4,2>", 8192),
+    ("ising2d_band<128,4,4>", 8192),
     ("ising2d_sweep<512,32,4>", 8192),
     ("ising2d_sweep<256,32,4>", 8192),
     ("ising2d_sweep<512,32,2>", 8192),
