@@ -152,7 +152,11 @@ MQV_API mqv_status mqv_init_state(mqv_sim* sim);
  * components per site; int8 for integer models, float32 otherwise. */
 MQV_API mqv_status mqv_get_state(mqv_sim* sim, void* host, size_t bytes);
 MQV_API mqv_status mqv_set_state(mqv_sim* sim, const void* host, size_t bytes);
-/* Device pointer of the current state (valid until the next engine call). */
+/* Device pointer of the current state (valid until the next engine call).
+ * Layout: the reference site order, except on the fused 2D Ising path, whose
+ * rows hold the even-x sites, then the odd-x sites, with the 32 bytes of each
+ * 32-site group transposed (site s of a group at byte 4 (s & 7) + (s >> 3));
+ * mqv_get_state / mqv_set_state convert. */
 MQV_API mqv_status mqv_state_device_ptr(mqv_sim* sim, void** dev, size_t* bytes);
 MQV_API mqv_status mqv_state_bytes(mqv_sim* sim, size_t* bytes);
 

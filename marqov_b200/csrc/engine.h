@@ -26,6 +26,17 @@ struct ModelDev {
     double beta;
 };
 
+// Layout of the fused 2D Ising path: row y holds its even-x sites, then its
+// odd-x sites (split rows); within each half, the 32 sites of a word (32
+// consecutive sites of that parity, 32 bytes) are stored transposed, site s
+// of the word at byte 4 (s & 7) + (s >> 3), so that bit 1 of byte k of the
+// word's 32-bit lane i belongs to site 8k + i.
+MQV_HD int64_t split_addr(int64_t y, int x, int len)
+{
+    const int m = x >> 1;
+    return y * len + (x & 1) * (len >> 1) + (m & ~31) + 4 * (m & 7) + ((m >> 3) & 3);
+}
+
 // Periodic hypercubic stencil: neighbour order +x,-x,+y,-y,... of
 // FixedDimRegularHypercubic::nbrs (src/lattice/regular_hypercubic.h:31-66).
 struct StencilDev {
@@ -33,14 +44,13 @@ struct StencilDev {
     int len;
     int64_t n;
     int64_t pows[4];
-    int split;  // 2D state stored in split rows (even-x half, then odd-x half)
+    int split;  // 2D state stored in split rows (see split_addr)
     // device address of site i
     MQV_HD int64_t addr(int64_t i) const
     {
         if (!split) return i;
         const int64_t y = i / len;
-        const int64_t x = i - y * len;
-        return y * len + (x & 1) * (len >> 1) + (x >> 1);
+        return split_addr(y, (int)(i - y * len), len);
     }
     MQV_HD int degree(int64_t) const { return 2 * dim; }
     MQV_HD int64_t nbr(int64_t i, int slot) const

@@ -210,26 +210,47 @@ __device__ __forceinline__ int word_bonds(uint32_t An, uint32_t U, uint32_t D, u
     return 128 - 2 * sM - 8 * __popc(An) + 4 * sAM;
 }
 
-// 16 staged bytes (+-1) -> 16 bits (1 = -1)
-__device__ __forceinline__ uint32_t pack16(uint4 v)
+// Packing between the staged bytes (+1 -> 0x01, -1 -> 0xFF, one word of 32
+// sites stored transposed, see split_addr) and 32-bit words (bit s = site s,
+// 1 = spin -1): bit 1 of byte k of the word's 32-bit lane i is site 8k + i.
+//
+// lanes 0..3 of a word -> bits 8k + i, i < 4 (shift by 4 for lanes 4..7)
+__device__ __forceinline__ uint32_t pack_lanes4(uint4 v)
 {
-    const unsigned long long M = 0x0101010101010101ull, G = 0x0102040810204080ull;
-    const unsigned long long q0 = ((((unsigned long long)v.y << 32) | v.x) >> 1) & M;
-    const unsigned long long q1 = ((((unsigned long long)v.w << 32) | v.z) >> 1) & M;
-    return (uint32_t)((q0 * G) >> 56) | ((uint32_t)((q1 * G) >> 56) << 8);
+    const uint32_t M = 0x01010101u;
+    uint32_t t = (v.x >> 1) & M;
+    t |= v.y & (M << 1);
+    t |= (v.z << 1) & (M << 2);
+    t |= (v.w << 2) & (M << 3);
+    return t;
 }
 
-// 32 bits -> 32 staged bytes (+1 -> 0x01, -1 -> 0xFF)
+__device__ __forceinline__ uint32_t pack_word(uint4 lo, uint4 hi)
+{
+    return pack_lanes4(lo) | (pack_lanes4(hi) << 4);
+}
+
+// 32 bits -> the word's 32 bytes as two 16-byte vectors (lanes 0..3, 4..7)
+__device__ __forceinline__ void unpack_word(uint32_t t, uint4& lo, uint4& hi)
+{
+    const uint32_t M = 0x01010101u;
+    lo.x = (t & M) * 0xFEu + M;
+    lo.y = ((t >> 1) & M) * 0xFEu + M;
+    lo.z = ((t >> 2) & M) * 0xFEu + M;
+    lo.w = ((t >> 3) & M) * 0xFEu + M;
+    hi.x = ((t >> 4) & M) * 0xFEu + M;
+    hi.y = ((t >> 5) & M) * 0xFEu + M;
+    hi.z = ((t >> 6) & M) * 0xFEu + M;
+    hi.w = ((t >> 7) & M) * 0xFEu + M;
+}
+
+// 32 bits -> 32 bytes at p (16-byte aligned)
 __device__ __forceinline__ void unpack32(uint32_t bits, uint8_t* p)
 {
-    uint32_t o[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const uint32_t n = (bits >> (4 * k)) & 0xFu;
-        o[k] = 0x01010101u + ((n * 0x00204081u) & 0x01010101u) * 0xFEu;
-    }
-    *reinterpret_cast<uint4*>(p) = make_uint4(o[0], o[1], o[2], o[3]);
-    *reinterpret_cast<uint4*>(p + 16) = make_uint4(o[4], o[5], o[6], o[7]);
+    uint4 lo, hi;
+    unpack_word(bits, lo, hi);
+    *reinterpret_cast<uint4*>(p) = lo;
+    *reinterpret_cast<uint4*>(p + 16) = hi;
 }
 
 template <int TX, int TY, int NWARP, bool MEAS>
@@ -366,10 +387,10 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
                 if (c < 16 * NWB) {
                     const int i = c / (4 * NWB), cr = c % (4 * NWB);
                     const uint8_t* sb = stage + ((base + r0 + i) % NS) * G::P;
-                    h16 = pack16(reinterpret_cast<const uint4*>(sb)[cr]);
+                    h16 = pack_lanes4(reinterpret_cast<const uint4*>(sb)[cr]) << (4 * (c & 1));
                 }
                 const uint32_t hi = __shfl_down_sync(0xffffffffu, h16, 1);
-                if (!(c & 1) && c < 16 * NWB) bits[(r0 * 2 * NWB) + (c >> 1)] = h16 | (hi << 16);
+                if (!(c & 1) && c < 16 * NWB) bits[(r0 * 2 * NWB) + (c >> 1)] = h16 | hi;
             }
             __syncwarp();
             // refill the four freed slots: rows NS ahead in this tile or the next
@@ -508,19 +529,6 @@ struct BandTie {
     int32_t y;     // lattice row
 };
 
-// 32 bits -> 32 bytes (+1 -> 0x01, -1 -> 0xFF) as two 16-byte vectors
-__device__ __forceinline__ void unpack32_regs(uint32_t bits, uint4& lo, uint4& hi)
-{
-    uint32_t o[8];
-#pragma unroll
-    for (int k = 0; k < 8; ++k) {
-        const uint32_t n = (bits >> (4 * k)) & 0xFu;
-        o[k] = 0x01010101u + ((n * 0x00204081u) & 0x01010101u) * 0xFEu;
-    }
-    lo = make_uint4(o[0], o[1], o[2], o[3]);
-    hi = make_uint4(o[4], o[5], o[6], o[7]);
-}
-
 template <int NT, int S, int NSB_, bool MEAS>
 __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising2DArgs a)
 {
@@ -626,7 +634,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * t);
-                brow[h * NT + t] = pack16(q[0]) | (pack16(q[1]) << 16);
+                brow[h * NT + t] = pack_word(q[0], q[1]);
             }
         }
         __syncthreads();  // slot k consumed, row k's bits visible
@@ -654,10 +662,10 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
             const uint32_t w0 = bits[(sl * 2) * NT + t], w1 = bits[(sl * 2 + 1) * NT + t];
             int8_t* drow = a.dst + (size_t)y * L + 32 * t;
             uint4 lo, hi;
-            unpack32_regs(w0, lo, hi);
+            unpack_word(w0, lo, hi);
             reinterpret_cast<uint4*>(drow)[0] = lo;
             reinterpret_cast<uint4*>(drow)[1] = hi;
-            unpack32_regs(w1, lo, hi);
+            unpack_word(w1, lo, hi);
             reinterpret_cast<uint4*>(drow + Lh)[0] = lo;
             reinterpret_cast<uint4*>(drow + Lh)[1] = hi;
             if (MEAS) {
@@ -707,22 +715,20 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
 __global__ void split_rows(const int8_t* __restrict__ in, int8_t* __restrict__ out, int L)
 {
     const int64_t n = (int64_t)L * L;
-    const int Lh = L >> 1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t y = i / L;
         const int x = (int)(i - y * L);
-        out[y * L + (x & 1) * Lh + (x >> 1)] = in[i];
+        out[split_addr(y, x, L)] = in[i];
     }
 }
 
 __global__ void merge_rows(const int8_t* __restrict__ in, int8_t* __restrict__ out, int L)
 {
     const int64_t n = (int64_t)L * L;
-    const int Lh = L >> 1;
     for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const int64_t y = i / L;
         const int x = (int)(i - y * L);
-        out[i] = in[y * L + (x & 1) * Lh + (x >> 1)];
+        out[i] = in[split_addr(y, x, L)];
     }
 }
 
