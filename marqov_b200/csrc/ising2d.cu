@@ -589,18 +589,29 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         __syncwarp();
         ntie = 0;
     };
-    // update the word of column t in half p of staged row r (lattice row y)
-    auto update = [&](int r, int p, int y) {
+    // inputs of the word of column t in half p of staged row r
+    struct WordIn {
+        uint32_t A, U, D, Lb, Rb, pos;
+    };
+    auto word_in = [&](int r, int p) {
         const int sl = r % RB, su = (r - 1) % RB, sd = (r + 1) % RB;
-        const uint32_t pos = (uint32_t)((sl * 2 + p) * NT + t);
+        WordIn w;
+        w.pos = (uint32_t)((sl * 2 + p) * NT + t);
         const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NT;
         const uint32_t Gw = Gr[t];
-        const uint32_t Lb = p ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
-        const uint32_t Rb = p ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
+        w.Lb = p ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
+        w.Rb = p ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
+        w.A = bits[w.pos];
+        w.U = bits[(su * 2 + p) * NT + t];
+        w.D = bits[(sd * 2 + p) * NT + t];
+        return w;
+    };
+    // update the word of column t in half p of staged row r (lattice row y)
+    auto update = [&](int r, int p, int y) {
+        const WordIn w = word_in(r, p);
         uint32_t tie, inA;
-        bits[pos] = update_word(bits[pos], bits[(su * 2 + p) * NT + t], bits[(sd * 2 + p) * NT + t], Lb, Rb,
-                                64 * t + p, y, tg_acc, a, th, tie, inA);
-        record(tie, inA, pos, y);
+        bits[w.pos] = update_word(w.A, w.U, w.D, w.Lb, w.Rb, 64 * t + p, y, tg_acc, a, th, tie, inA);
+        record(tie, inA, w.pos, y);
     };
 
     int esum = 0, msum = 0;
@@ -642,16 +653,26 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
             fence_proxy_async_smem();
             issue(k + NSB);
         }
-        // colour 0 of row k - 1 (staged rows 1 .. NR - 2)
-        if (k - 1 >= 1 && k - 1 <= NR - 2) {
-            const int y = wrapi(y0 - 3 + k, L);
-            update(k - 1, y & 1, y);
-        }
-        // colour 1 of row k - 2 - S (staged rows 2 .. NR - 3)
+        // colour 0 of row k - 1 (staged rows 1 .. NR - 2) and colour 1 of row
+        // k - 2 - S (staged rows 2 .. NR - 3): independent words, updated
+        // side by side in the steady state
         const int r1 = k - 2 - S;
-        if (r1 >= 2 && r1 <= NR - 3) {
-            const int y = y0 - 2 + r1;
-            update(r1, 1 - (y & 1), y);
+        const bool do0 = k - 1 >= 1 && k - 1 <= NR - 2, do1 = r1 >= 2 && r1 <= NR - 3;
+        const int ya = wrapi(y0 - 3 + k, L), yb = y0 - 2 + r1;
+        if (do0 && do1) {
+            const int pa = ya & 1, pb = 1 - (yb & 1);
+            const WordIn wa = word_in(k - 1, pa), wb = word_in(r1, pb);
+            uint32_t ta, ia, tb, ib;
+            const uint32_t na = update_word(wa.A, wa.U, wa.D, wa.Lb, wa.Rb, 64 * t + pa, ya, tg_acc, a, th, ta, ia);
+            const uint32_t nb = update_word(wb.A, wb.U, wb.D, wb.Lb, wb.Rb, 64 * t + pb, yb, tg_acc, a, th, tb, ib);
+            bits[wa.pos] = na;
+            bits[wb.pos] = nb;
+            record(ta, ia, wa.pos, ya);
+            record(tb, ib, wb.pos, yb);
+        } else if (do0) {
+            update(k - 1, ya & 1, ya);
+        } else if (do1) {
+            update(r1, 1 - (yb & 1), yb);
         }
         if (k % S == S - 1 || ntie > G::TIECAP - 64) flush();
         // row k - 2 - 2S out
