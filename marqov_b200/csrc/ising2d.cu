@@ -164,10 +164,9 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
     const uint4 q1 = philox_rk(g, a.sweep, 1u, tg_acc, a);
     const uint32_t pl[8] = {q0.x, q0.y, q0.z, q0.w, q1.x, q1.y, q1.z, q1.w};
     // minus-neighbour count M = m0 + 2 m1 + 4 m2 (carry-save adder; M <= 4)
-    const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
-    const uint32_t m0 = s1 ^ s2, c3 = s1 & s2;
-    const uint32_t m1 = c1 ^ c2 ^ c3;
-    const uint32_t m2 = (c1 & c2) | (c3 & (c1 | c2));
+    const uint32_t s3 = U ^ D ^ Lb, c3 = (U & D) | (Lb & (U | D));  // full adder of three
+    const uint32_t m0 = s3 ^ Rb, c4 = s3 & Rb;                        // plus the fourth
+    const uint32_t m1 = c3 ^ c4, m2 = c3 & c4;
     // the two tested classes (aligned count a = M for a -1 site, 4 - M for +1)
     uint32_t maskA, maskB;
     if (th.mode == 0) {
@@ -201,10 +200,9 @@ __device__ __forceinline__ uint32_t update_word(uint32_t A, uint32_t U, uint32_t
 // Bond sum s * sum(nbrs) = sum (1 - 2a)(4 - 2M) over the sites of a word
 __device__ __forceinline__ int word_bonds(uint32_t An, uint32_t U, uint32_t D, uint32_t Lb, uint32_t Rb)
 {
-    const uint32_t s1 = U ^ D, c1 = U & D, s2 = Lb ^ Rb, c2 = Lb & Rb;
-    const uint32_t m0 = s1 ^ s2, c3 = s1 & s2;
-    const uint32_t m1 = c1 ^ c2 ^ c3;
-    const uint32_t m2 = (c1 & c2) | (c3 & (c1 | c2));
+    const uint32_t s3 = U ^ D ^ Lb, c3 = (U & D) | (Lb & (U | D));  // full adder of three
+    const uint32_t m0 = s3 ^ Rb, c4 = s3 & Rb;                        // plus the fourth
+    const uint32_t m1 = c3 ^ c4, m2 = c3 & c4;
     const int sM = __popc(m0) + 2 * __popc(m1) + 4 * __popc(m2);
     const int sAM = __popc(An & m0) + 2 * __popc(An & m1) + 4 * __popc(An & m2);
     return 128 - 2 * sM - 8 * __popc(An) + 4 * sAM;
@@ -227,7 +225,18 @@ __device__ __forceinline__ uint32_t pack_lanes4(uint4 v)
 
 __device__ __forceinline__ uint32_t pack_word(uint4 lo, uint4 hi)
 {
-    return pack_lanes4(lo) | (pack_lanes4(hi) << 4);
+    // Horner's rule over lanes 6 .. 0 puts lane i's bit 1 of byte k at bit
+    // 8k + 1 + i (multiply-adds); lane 7 is placed separately so that nothing
+    // runs past bit 31
+    const uint32_t m = 0x02020202u;  // bit 1 of each byte: set for spin -1
+    uint32_t h = hi.z & m;
+    h = h * 2u + (hi.y & m);
+    h = h * 2u + (hi.x & m);
+    h = h * 2u + (lo.w & m);
+    h = h * 2u + (lo.z & m);
+    h = h * 2u + (lo.y & m);
+    h = h * 2u + (lo.x & m);
+    return (h >> 1) | ((hi.w & m) << 6);
 }
 
 // 32 bits -> the word's 32 bytes as two 16-byte vectors (lanes 0..3, 4..7)
@@ -593,8 +602,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     struct WordIn {
         uint32_t A, U, D, Lb, Rb, pos;
     };
-    auto word_in = [&](int r, int p) {
-        const int sl = r % RB, su = (r - 1) % RB, sd = (r + 1) % RB;
+    auto word_in = [&](int sl, int su, int sd, int p) {
         WordIn w;
         w.pos = (uint32_t)((sl * 2 + p) * NT + t);
         const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NT;
@@ -607,8 +615,8 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         return w;
     };
     // update the word of column t in half p of staged row r (lattice row y)
-    auto update = [&](int r, int p, int y) {
-        const WordIn w = word_in(r, p);
+    auto update = [&](int sl, int su, int sd, int p, int y) {
+        const WordIn w = word_in(sl, su, sd, p);
         uint32_t tie, inA;
         bits[w.pos] = update_word(w.A, w.U, w.D, w.Lb, w.Rb, 64 * t + p, y, tg_acc, a, th, tie, inA);
         record(tie, inA, w.pos, y);
@@ -616,8 +624,14 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
 
     int esum = 0, msum = 0;
     int k = 0;
+    int sk = 0;  // k % RB: the bit-ring slot of staged row k
+    // slot of staged row k - d (0 <= d < RB)
+    auto back = [&](int d) {
+        const int v = sk - d;
+        return v < 0 ? v + RB : v;
+    };
     bool stop = false;
-    for (; k < NR + 2 * S; ++k) {
+    for (; k < NR + 2 * S; ++k, sk = sk + 1 == RB ? 0 : sk + 1) {
         int timed_out = 0;
         if (k < NR) {
             // every thread waits for row k (bounded: a stuck copy sets an error status)
@@ -641,7 +655,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         }
         if (k < NR) {
             const uint8_t* row = stage + (k % NSB) * L;
-            uint32_t* brow = bits + (k % RB) * 2 * NT;
+            uint32_t* brow = bits + sk * 2 * NT;
 #pragma unroll
             for (int h = 0; h < 2; ++h) {
                 const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * t);
@@ -661,7 +675,8 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         const int ya = wrapi(y0 - 3 + k, L), yb = y0 - 2 + r1;
         if (do0 && do1) {
             const int pa = ya & 1, pb = 1 - (yb & 1);
-            const WordIn wa = word_in(k - 1, pa), wb = word_in(r1, pb);
+            const WordIn wa = word_in(back(1), back(2), sk, pa);
+            const WordIn wb = word_in(back(2 + S), back(3 + S), back(1 + S), pb);
             uint32_t ta, ia, tb, ib;
             const uint32_t na = update_word(wa.A, wa.U, wa.D, wa.Lb, wa.Rb, 64 * t + pa, ya, tg_acc, a, th, ta, ia);
             const uint32_t nb = update_word(wb.A, wb.U, wb.D, wb.Lb, wb.Rb, 64 * t + pb, yb, tg_acc, a, th, tb, ib);
@@ -670,16 +685,16 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
             record(ta, ia, wa.pos, ya);
             record(tb, ib, wb.pos, yb);
         } else if (do0) {
-            update(k - 1, ya & 1, ya);
+            update(back(1), back(2), sk, ya & 1, ya);
         } else if (do1) {
-            update(r1, 1 - (yb & 1), yb);
+            update(back(2 + S), back(3 + S), back(1 + S), 1 - (yb & 1), yb);
         }
         if (k % S == S - 1 || ntie > G::TIECAP - 64) flush();
         // row k - 2 - 2S out
         const int r2 = k - 2 - 2 * S;
         if (r2 >= 2 && r2 <= NR - 3) {
             const int y = y0 - 2 + r2;
-            const int sl = r2 % RB;
+            const int sl = back(2 + 2 * S);
             const uint32_t w0 = bits[(sl * 2) * NT + t], w1 = bits[(sl * 2 + 1) * NT + t];
             int8_t* drow = a.dst + (size_t)y * L + 32 * t;
             uint4 lo, hi;
@@ -695,8 +710,8 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 const uint32_t* Gr = bits + (sl * 2 + (1 - p1)) * NT;
                 const uint32_t Lb = p1 ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
                 const uint32_t Rb = p1 ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
-                const uint32_t U = bits[(((r2 - 1) % RB) * 2 + p1) * NT + t];
-                const uint32_t D = bits[(((r2 + 1) % RB) * 2 + p1) * NT + t];
+                const uint32_t U = bits[(back(3 + 2 * S) * 2 + p1) * NT + t];
+                const uint32_t D = bits[(back(1 + 2 * S) * 2 + p1) * NT + t];
                 esum += word_bonds(An, U, D, Lb, Rb);
                 msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
             }
