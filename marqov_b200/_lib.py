@@ -104,7 +104,7 @@ def load() -> C.CDLL:
         return _lib
     if not os.path.exists(LIB_PATH):
         raise ImportError(f"marqov_b200 engine library not built: {LIB_PATH} "
-                          "(run `python -m marqov_b200.build` or __graft_entry__.build())")
+                          "(run `python marqov_b200/build.py` or __graft_entry__.build())")
     lib = C.CDLL(LIB_PATH)
     for name, (res, args) in SIGNATURES.items():
         fn = getattr(lib, name)
