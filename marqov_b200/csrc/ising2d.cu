@@ -649,9 +649,15 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 }
             }
         }
+        // one barrier per step: the previous step's words are visible to their
+        // readers, and every warp has packed row k - 1, so its slot is free
         if (__syncthreads_or(timed_out)) {
             stop = true;
             break;
+        }
+        if (t == 0 && k >= 1 && k - 1 + NSB < NR) {
+            fence_proxy_async_smem();
+            issue(k - 1 + NSB);
         }
         if (k < NR) {
             const uint8_t* row = stage + (k % NSB) * L;
@@ -662,11 +668,9 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 brow[h * NT + t] = pack_word(q[0], q[1]);
             }
         }
-        __syncthreads();  // slot k consumed, row k's bits visible
-        if (t == 0 && k + NSB < NR) {
-            fence_proxy_async_smem();
-            issue(k + NSB);
-        }
+        // row k's bits are read in this step only by their own thread (the D
+        // neighbour of colour 0 in row k - 1); other warps read them from the
+        // next step on, after its barrier
         // colour 0 of row k - 1 (staged rows 1 .. NR - 2) and colour 1 of row
         // k - 2 - S (staged rows 2 .. NR - 3): independent words, updated
         // side by side in the steady state
@@ -716,15 +720,14 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
             }
         }
-        // the next step's __syncthreads_or makes this step's words visible
-        // to their readers before any of them is read
     }
     if (stop) {
         // wait (bounded) for the copies still in flight before the CTA leaves
         if (t == 0) {
             atomicExch(a.status, MQV_ERR_TIMEOUT);
             const uint64_t t0 = global_timer_ns();
-            for (int r = k; r < NR && r < k + NSB; ++r) {
+            const int issued = k == 0 ? NSB : k - 1 + NSB;  // rows issued before the stop
+            for (int r = k; r < NR && r < issued; ++r) {
                 const uint32_t bar = smem_addr(&bars[r % NSB]);
                 const uint32_t par = (uint32_t)(r / NSB) & 1u;
                 while (!mbar_try_wait(bar, par) && global_timer_ns() - t0 < 1000000000ull) __nanosleep(1000);
