@@ -135,7 +135,8 @@ def measured_peaks():
 
 
 def profiled_traffic(kernel: str):
-    """DRAM bytes per launch from the committed ncu summary, if any."""
+    """DRAM bytes per launch of `kernel` (e.g. "ising2d_band<256,4,2>") from
+    the committed ncu summary, if it holds that kernel."""
     path = os.path.join(ROOT, "profiles", "traffic.json")
     try:
         with open(path) as fh:
@@ -300,7 +301,7 @@ def run_engine(args, ws, rank, local):
     per_launch_s = ms * 1e-3 / (args.steps * args.nmetro)
     alg_bytes = 2 * n  # one int8 read + one int8 write per site update
     achieved = alg_bytes / per_launch_s / 1e9
-    tr = profiled_traffic("ising2d_sweep")
+    tr = profiled_traffic(kernel_desc.split("kernel=")[-1])
     roof = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
             "traffic": None if tr is None else tr.get("bytes_per_launch"),
             "kernel": kernel_desc.split("kernel=")[-1], "peak_source": f"{peak_kind} hbm_gbs",

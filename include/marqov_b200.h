@@ -198,6 +198,38 @@ MQV_API mqv_status mqv_describe(mqv_sim* sim, char* buf, size_t len);
 /* Number of engine kernel launches issued by this handle so far. */
 MQV_API mqv_status mqv_launch_count(mqv_sim* sim, uint64_t* count);
 
+/* ---- batches ------------------------------------------------------------
+ * Many independent simulations on one GPU, advanced together: the farm of
+ * MARQOV's scheduler (one Core per thread, src/libmarqov/marqovscheduler.h:
+ * 64-494, createSimfromParameter / start at :75-144, 223-273) as one set of
+ * batched kernels per EMCS, captured once in a CUDA graph and replayed.
+ * Members: int8 models (Ising, embedded Ising, Potts, Blume-Capel) on
+ * hypercubic lattices of any sizes, each with its own coefficients, beta,
+ * seed and replica id.  A batched run produces the same states, cluster
+ * sizes and observables as running each member handle with mqv_emcs. */
+typedef struct mqv_sim_spec {
+    mqv_model_desc model;
+    mqv_lattice_desc lattice;
+    mqv_run_params params; /* the same device for every member */
+} mqv_sim_spec;
+
+typedef struct mqv_batch mqv_batch;
+
+MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_batch** out);
+MQV_API mqv_status mqv_batch_destroy(mqv_batch* batch);
+/* Member i as an ordinary handle (state, counters, measurement); owned by
+ * the batch and bound to its stream. */
+MQV_API mqv_status mqv_batch_member(mqv_batch* batch, int32_t i, mqv_sim** sim);
+MQV_API mqv_status mqv_batch_init_state(mqv_batch* batch);
+/* EMCS per graph launch (1 .. 256; default 8). */
+MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* batch, int32_t steps);
+/* n_emcs EMCS of every member (ncluster clusters, then nmetro sweeps, then a
+ * measurement).  obs (host, may be NULL): n_emcs * n records, EMCS-major
+ * (record e * n + i is member i after EMCS e); mean_cluster likewise. */
+MQV_API mqv_status mqv_batch_emcs(mqv_batch* batch, int32_t n_emcs, int32_t ncluster, int32_t nmetro, mqv_obs* obs,
+                                  double* mean_cluster);
+MQV_API mqv_status mqv_batch_launch_count(mqv_batch* batch, uint64_t* count);
+
 /* Self test: Philox blocks for n counters (c0 = i, other words given) computed
  * on the device by the engine and by cuRAND's Philox4_32_10; out_engine and
  * out_curand receive 4n words each (host). */

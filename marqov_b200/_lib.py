@@ -56,6 +56,10 @@ class Obs(C.Structure):
     _fields_ = [("e", C.c_double), ("m", C.c_double), ("m2", C.c_double), ("m4", C.c_double)]
 
 
+class SimSpec(C.Structure):
+    _fields_ = [("model", ModelDesc), ("lattice", LatticeDesc), ("params", RunParams)]
+
+
 class MarqovError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(f"[marqov_b200] {STATUS_NAMES.get(status, status)}: {msg}")
@@ -90,6 +94,13 @@ SIGNATURES = {
     "mqv_synchronize": (C.c_int32, [_vp]),
     "mqv_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
     "mqv_describe": (C.c_int32, [_vp, C.c_char_p, C.c_size_t]),
+    "mqv_batch_create": (C.c_int32, [C.POINTER(SimSpec), C.c_int32, C.POINTER(_vp)]),
+    "mqv_batch_destroy": (C.c_int32, [_vp]),
+    "mqv_batch_member": (C.c_int32, [_vp, C.c_int32, C.POINTER(_vp)]),
+    "mqv_batch_init_state": (C.c_int32, [_vp]),
+    "mqv_batch_set_graph_steps": (C.c_int32, [_vp, C.c_int32]),
+    "mqv_batch_emcs": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp]),
+    "mqv_batch_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
     "mqv_selftest_philox": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                         _vp, _vp]),
 }

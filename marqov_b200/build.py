@@ -7,6 +7,7 @@ acceptance-rule thresholds computed on the host round like the device code.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import glob
 import os
 import subprocess
@@ -43,13 +44,13 @@ def build(force: bool = False, verbose: bool = False) -> str:
         return OUT
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
     extra = ["-Xptxas", "-v"] if verbose else []
-    for src in sources():
-        obj = os.path.join(objdir, os.path.basename(src)[:-3] + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, *extra, "-dc" if False else "-c", "-o", obj, src]
-        subprocess.check_call(cmd)
-        objs.append(obj)
+    objs = [os.path.join(objdir, os.path.basename(src)[:-3] + ".o") for src in sources()]
+    cmds = [[NVCC, *ARCH, *FLAGS, *extra, "-c", "-o", obj, src] for src, obj in zip(sources(), objs)]
+    # one nvcc per translation unit, side by side
+    with concurrent.futures.ThreadPoolExecutor(max_workers=min(len(cmds), os.cpu_count() or 1)) as ex:
+        for f in [ex.submit(subprocess.check_call, c) for c in cmds]:
+            f.result()
     tmp = OUT + ".tmp"
     subprocess.check_call([NVCC, *ARCH, "-shared", "-o", tmp, *objs])
     os.replace(tmp, OUT)

@@ -90,17 +90,33 @@ class Core:
                          replica=int(config.repid), device=int(config.device),
                          flags=L.FLAG_PER_COLOUR if config.per_colour else 0)
         L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
+        self._owner = None
+        self._setup(lattice, ham)
+
+    def _setup(self, lattice: Lattice, ham: Hamiltonian):
         self.n = int(lattice.size())
         self.symd = ham.SymD
         self.dtype = ham.dtype
         self.obs = TimeSeries()
         self.step = 0
 
+    @classmethod
+    def _member(cls, handle: C.c_void_p, owner, lattice: Lattice, config: Config, ham: Hamiltonian,
+                beta: float) -> "Core":
+        """A view of a handle owned by `owner` (a Batch member)."""
+        c = cls.__new__(cls)
+        c._lib = L.load()
+        c.lattice, c.config, c.ham, c.beta = lattice, config, ham, float(beta)
+        c._h = handle
+        c._owner = owner
+        c._setup(lattice, ham)
+        return c
+
     # -- lifecycle
     def close(self):
-        if self._h:
+        if self._h and self._owner is None:
             self._lib.mqv_destroy(self._h)
-            self._h = C.c_void_p()
+        self._h = C.c_void_p()
 
     def __del__(self):
         try:
@@ -222,3 +238,76 @@ class Core:
 def makeCore(lattice: Lattice, config: Config, ham: Hamiltonian, beta: float) -> Core:
     """``MARQOV::makeCore`` (core.h:1223-1246)."""
     return Core(lattice, config, ham, beta)
+
+
+class Batch:
+    """Many independent simulations advanced together on one GPU.
+
+    The farm MARQOV's scheduler runs as one ``Core`` per thread
+    (src/libmarqov/marqovscheduler.h:64-494) becomes batched kernels per EMCS
+    replayed from a CUDA graph; every member sees exactly the states and
+    observables it would have on its own.  ``members`` lists
+    ``(lattice, config, hamiltonian, beta)``; int8 models on hypercubic
+    lattices.
+    """
+
+    def __init__(self, members, graph_steps: int = 8):
+        lib = L.load()
+        self._lib = lib
+        self._h = C.c_void_p()
+        specs = (L.SimSpec * len(members))()
+        self._members_args = list(members)
+        for i, (lat, cfg, ham, beta) in enumerate(members):
+            specs[i].model = ham.desc(float(beta))
+            specs[i].lattice = lat.desc()
+            specs[i].params = L.RunParams(beta=float(beta), seed=int(cfg.seed) & (2 ** 64 - 1),
+                                          replica=int(cfg.repid), device=int(cfg.device), flags=0)
+        L.check(lib.mqv_batch_create(specs, len(members), C.byref(self._h)))
+        L.check(lib.mqv_batch_set_graph_steps(self._h, int(graph_steps)))
+        self.n = len(members)
+        self._views = []
+        for i, (lat, cfg, ham, beta) in enumerate(members):
+            m = C.c_void_p()
+            L.check(lib.mqv_batch_member(self._h, i, C.byref(m)))
+            self._views.append(Core._member(m, self, lat, cfg, ham, beta))
+
+    def close(self):
+        if self._h:
+            for v in self._views:
+                v._h = C.c_void_p()
+            self._lib.mqv_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __len__(self):
+        return self.n
+
+    def member(self, i: int) -> Core:
+        return self._views[i]
+
+    def init(self):
+        L.check(self._lib.mqv_batch_init_state(self._h))
+
+    def emcs(self, n: int, ncluster: int = 1, nmetro: int = 1):
+        """n EMCS of every member; returns (obs [n, members, 4], mean cluster [n, members])."""
+        obs = np.zeros((n, self.n, 4), np.float64)
+        mc = np.zeros((n, self.n), np.float64)
+        L.check(self._lib.mqv_batch_emcs(self._h, int(n), int(ncluster), int(nmetro), obs.ctypes.data, mc.ctypes.data))
+        return obs, mc
+
+    @property
+    def launches(self) -> int:
+        c = C.c_uint64()
+        L.check(self._lib.mqv_batch_launch_count(self._h, C.byref(c)))
+        return int(c.value)

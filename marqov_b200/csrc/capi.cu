@@ -12,6 +12,7 @@
 #include <string>
 #include <vector>
 
+#include "batch.h"
 #include "engine.h"
 
 namespace mqv {
@@ -767,6 +768,337 @@ MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, 
     cudaFree(de);
     cudaFree(dc);
     MQV_CK(e);
+    return MQV_OK;
+}
+
+}  // extern "C"
+
+// ---- batches -----------------------------------------------------------------------
+
+namespace mqv {
+
+struct Batch {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    std::vector<Sim*> sims;
+    int nrep = 0;
+    std::vector<BatchRep> reps;  // host copy of the replica table (kept alive for the upload)
+    BatchRep* d_reps = nullptr;
+    int64_t* d_half_prefix = nullptr;
+    int32_t* d_block_rep = nullptr;
+    BatchCtr* d_ctr = nullptr;
+    long long* d_acc = nullptr;
+    double* d_obs = nullptr;
+    int32_t* d_csize = nullptr;
+    int cap_slots = 0;   // measurement slots in d_acc / d_obs (per replica)
+    int cap_cslots = 0;  // cluster-size slots in d_csize (per replica)
+    BatchLaunch L{};
+    cudaGraphExec_t g_one = nullptr, g_many = nullptr;
+    int g_ncluster = -1, g_nmetro = -1, g_steps = 0;
+    int graph_steps = 8;  // EMCS per graph launch
+    uint64_t launches = 0;
+};
+
+static void free_graphs(Batch* b)
+{
+    if (b->g_one) cudaGraphExecDestroy(b->g_one);
+    if (b->g_many) cudaGraphExecDestroy(b->g_many);
+    b->g_one = b->g_many = nullptr;
+    b->g_ncluster = b->g_nmetro = -1;
+}
+
+static void free_batch(Batch* b)
+{
+    if (!b) return;
+    DeviceGuard g(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    free_graphs(b);
+    for (Sim* s : b->sims) free_sim(s);
+    for (void* p : {(void*)b->d_reps, (void*)b->d_half_prefix, (void*)b->d_block_rep, (void*)b->d_ctr, (void*)b->d_acc,
+                    (void*)b->d_obs, (void*)b->d_csize})
+        if (p) cudaFree(p);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+}
+
+static mqv_status batch_capacity(Batch* b, int slots, int cslots)
+{
+    if (slots > b->cap_slots) {
+        if (b->d_acc) cudaFree(b->d_acc);
+        if (b->d_obs) cudaFree(b->d_obs);
+        b->d_acc = nullptr;
+        b->d_obs = nullptr;
+        b->cap_slots = 0;
+        MQV_CK(cudaMalloc(&b->d_acc, sizeof(long long) * kAccStride * (size_t)slots * b->nrep));
+        MQV_CK(cudaMalloc(&b->d_obs, sizeof(double) * 4 * (size_t)slots * b->nrep));
+        b->cap_slots = slots;
+    }
+    if (cslots > b->cap_cslots) {
+        if (b->d_csize) cudaFree(b->d_csize);
+        b->d_csize = nullptr;
+        b->cap_cslots = 0;
+        MQV_CK(cudaMalloc(&b->d_csize, sizeof(int32_t) * (size_t)cslots * b->nrep));
+        b->cap_cslots = cslots;
+    }
+    b->L.acc = b->d_acc;
+    b->L.csize = b->d_csize;
+    return MQV_OK;
+}
+
+// Capture `steps` EMCS of the batch into an executable graph.
+static mqv_status batch_capture(Batch* b, int steps, int ncluster, int nmetro, cudaGraphExec_t* out)
+{
+    cudaGraph_t graph = nullptr;
+    uint64_t dummy = 0;
+    MQV_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int k = 0; k < steps && e == cudaSuccess; ++k) e = batch_launch_emcs(b->L, b->stream, ncluster, nmetro, &dummy);
+    const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
+    MQV_CK(e);
+    MQV_CK(e2);
+    e = cudaGraphInstantiate(out, graph, 0);
+    cudaGraphDestroy(graph);
+    MQV_CK(e);
+    return MQV_OK;
+}
+
+}  // namespace mqv
+
+extern "C" {
+
+MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_batch** out)
+{
+    if (!specs || !out) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    if (n < 1 || n > 65535) return fail(MQV_ERR_INVALID_ARG, "batch size must be in [1, 65535]");
+    *out = nullptr;
+    const int device = specs[0].params.device;
+    for (int i = 0; i < n; ++i) {
+        const int k = specs[i].model.kind;
+        if (!(k == MQV_MODEL_ISING || k == MQV_MODEL_ISING_EMBED || k == MQV_MODEL_POTTS || k == MQV_MODEL_BLUME_CAPEL))
+            return fail(MQV_ERR_UNSUPPORTED_TERM, "batches take int8 models (Ising, embedded Ising, Potts, Blume-Capel)");
+        if (specs[i].lattice.kind != MQV_LATTICE_HYPERCUBIC)
+            return fail(MQV_ERR_UNSUPPORTED_TERM, "batches take hypercubic lattices");
+        if (specs[i].params.device != device) return fail(MQV_ERR_INVALID_ARG, "all members of a batch share one device");
+    }
+    Batch* b = new (std::nothrow) Batch();
+    if (!b) return fail(MQV_ERR_OUT_OF_MEMORY, "host allocation failed");
+    b->device = device;
+    auto bail = [&](mqv_status st) {
+        free_batch(b);
+        return st;
+    };
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        delete b;
+        return fail(MQV_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) {
+        delete b;
+        return fail(MQV_ERR_INVALID_ARG, "device ordinal out of range");
+    }
+    DeviceGuard g(device);
+    if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
+        set_error("cudaStreamCreate failed");
+        return bail(MQV_ERR_CUDA);
+    }
+    // members: ordinary handles on the batch's stream, one launch per colour
+    // class (reference site order, no fused two-colour layout)
+    b->nrep = n;
+    b->sims.reserve((size_t)n);
+    for (int i = 0; i < n; ++i) {
+        mqv_run_params p = specs[i].params;
+        p.flags |= MQV_FLAG_PER_COLOUR;
+        mqv_sim* h = nullptr;
+        mqv_status st = mqv_create(&specs[i].model, &specs[i].lattice, &p, &h);
+        if (st) {
+            const std::string msg = "batch member " + std::to_string(i) + ": " + g_err;
+            return bail(fail(st, msg));
+        }
+        b->sims.push_back(reinterpret_cast<Sim*>(h));
+        st = mqv_set_stream(h, b->stream);
+        if (st) return bail(st);
+    }
+    // flattened half-site work of the colour launches
+    std::vector<int64_t> prefix((size_t)n + 1, 0);
+    int64_t nmax = 0;
+    for (int i = 0; i < n; ++i) {
+        prefix[i + 1] = prefix[i] + b->sims[i]->n / 2;
+        nmax = std::max(nmax, b->sims[i]->n);
+    }
+    const int64_t total = prefix[n];
+    const int64_t blocks = (total + kBatchMetroThreads - 1) / kBatchMetroThreads;
+    if (blocks >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
+    std::vector<int32_t> brep((size_t)blocks);
+    for (int64_t k = 0, r = 0; k < blocks; ++k) {
+        const int64_t first = k * kBatchMetroThreads;
+        while (first >= prefix[r + 1]) ++r;
+        brep[(size_t)k] = (int32_t)r;
+    }
+    auto dcopy = [&](void** dst, const void* src, size_t bytes) -> mqv_status {
+        MQV_CK(cudaMalloc(dst, bytes));
+        MQV_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        return MQV_OK;
+    };
+    mqv_status st = dcopy((void**)&b->d_half_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
+    if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
+    if (st) return bail(st);
+    if (cudaMalloc(&b->d_reps, sizeof(BatchRep) * (size_t)n) != cudaSuccess ||
+        cudaMalloc(&b->d_ctr, sizeof(BatchCtr)) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of the batch tables failed");
+        return bail(MQV_ERR_OUT_OF_MEMORY);
+    }
+    b->L.reps = b->d_reps;
+    b->L.half_prefix = b->d_half_prefix;
+    b->L.block_rep = b->d_block_rep;
+    b->L.total_half = total;
+    b->L.metro_blocks = (int)blocks;
+    b->L.meas_parts = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 4095) / 4096));
+    b->L.nrep = n;
+    b->L.ctr = b->d_ctr;
+    *out = reinterpret_cast<mqv_batch*>(b);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_destroy(mqv_batch* h)
+{
+    free_batch(reinterpret_cast<Batch*>(h));
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_member(mqv_batch* h, int32_t i, mqv_sim** sim)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b || !sim) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    if (i < 0 || i >= b->nrep) return fail(MQV_ERR_INVALID_ARG, "member index out of range");
+    *sim = reinterpret_cast<mqv_sim*>(b->sims[(size_t)i]);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_init_state(mqv_batch* h)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    for (Sim* s : b->sims) {
+        const mqv_status st = mqv_init_state(reinterpret_cast<mqv_sim*>(s));
+        if (st) return st;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* h, int32_t steps)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (steps < 1 || steps > 256) return fail(MQV_ERR_INVALID_ARG, "graph steps must be in [1, 256]");
+    b->graph_steps = steps;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_emcs(mqv_batch* h, int32_t n_emcs, int32_t ncluster, int32_t nmetro, mqv_obs* obs,
+                                  double* mean_cluster)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    DeviceGuard guard_(b->device);
+    if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
+    if (ncluster > 64 || nmetro > 64) return fail(MQV_ERR_INVALID_ARG, "at most 64 clusters and 64 sweeps per EMCS");
+    for (Sim* s : b->sims) {
+        if (!s->initialised) return fail(MQV_ERR_STATE, "state of a batch member not initialised");
+        if (ncluster > 0) {
+            mqv_status st = check_wolff_supported(s);
+            if (st) return st;
+            st = ensure_wolff(s);
+            if (st) return st;
+        }
+    }
+    // replica table at the start of the run
+    b->reps.assign((size_t)b->nrep, BatchRep{});
+    for (int i = 0; i < b->nrep; ++i) {
+        const Sim* s = b->sims[(size_t)i];
+        BatchRep& r = b->reps[(size_t)i];
+        r.md = s->md;
+        r.st = s->sten;
+        r.w = wolff_int8_params(s->md);
+        r.key = make_key(s->seed);
+        r.replica = s->replica;
+        r.sweep0 = (uint32_t)s->sweep;
+        r.cluster0 = (uint32_t)s->cluster;
+        r.s = (int8_t*)s->state[s->cur];
+        r.visited = s->d_visited;
+        r.queue = s->d_queue;
+    }
+    MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+    const int CH = 256;  // EMCS per chunk of measurements
+    const int slots = std::min(CH, std::max(n_emcs, 1));
+    const long long* acc0 = b->d_acc;
+    const int32_t* csize0 = b->d_csize;
+    mqv_status st = batch_capacity(b, slots, slots * std::max(ncluster, 1));
+    if (st) return st;
+    if (b->d_acc != acc0 || b->d_csize != csize0) free_graphs(b);  // graphs hold the old pointers
+    const int K = std::max(1, std::min(b->graph_steps, CH));
+    if (b->g_ncluster != ncluster || b->g_nmetro != nmetro || b->g_steps != K || !b->g_one) {
+        free_graphs(b);
+        MQV_CK(cudaStreamSynchronize(b->stream));
+        st = batch_capture(b, 1, ncluster, nmetro, &b->g_one);
+        if (!st && K > 1) st = batch_capture(b, K, ncluster, nmetro, &b->g_many);
+        if (st) {
+            free_graphs(b);
+            return st;
+        }
+        b->g_ncluster = ncluster;
+        b->g_nmetro = nmetro;
+        b->g_steps = K;
+    }
+    const uint64_t per_emcs = (uint64_t)ncluster + 2ull * (uint64_t)nmetro + 2ull;
+    std::vector<int32_t> csz;
+    int done = 0;
+    while (done < n_emcs) {
+        const int ch = std::min(n_emcs - done, CH);
+        MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
+        MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
+        b->launches++;
+        int k = 0;
+        if (K > 1)
+            for (; k + K <= ch; k += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
+        for (; k < ch; ++k) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
+        b->launches += per_emcs * (uint64_t)ch;
+        MQV_CK(batch_launch_finalize(b->L, b->stream, ch, b->d_obs));
+        b->launches++;
+        if (obs)
+            MQV_CK(cudaMemcpyAsync(obs + (size_t)done * b->nrep, b->d_obs, sizeof(double) * 4 * (size_t)ch * b->nrep,
+                                   cudaMemcpyDeviceToHost, b->stream));
+        if (mean_cluster && ncluster > 0) {
+            csz.resize((size_t)ch * ncluster * b->nrep);
+            MQV_CK(cudaMemcpyAsync(csz.data(), b->d_csize, sizeof(int32_t) * csz.size(), cudaMemcpyDeviceToHost,
+                                   b->stream));
+        }
+        MQV_CK(cudaStreamSynchronize(b->stream));
+        if (mean_cluster) {
+            for (int e = 0; e < ch; ++e)
+                for (int r = 0; r < b->nrep; ++r) {
+                    double a = 0;
+                    for (int c = 0; c < ncluster; ++c) a += (double)csz[((size_t)e * ncluster + c) * b->nrep + r];
+                    mean_cluster[(size_t)(done + e) * b->nrep + r] = ncluster > 0 ? a / ncluster : 0.0;
+                }
+        }
+        done += ch;
+    }
+    MQV_CK(cudaStreamSynchronize(b->stream));
+    for (Sim* s : b->sims) {
+        s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
+        s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_launch_count(mqv_batch* h, uint64_t* count)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b || !count) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    *count = b->launches;
     return MQV_OK;
 }
 

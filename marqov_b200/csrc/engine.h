@@ -75,6 +75,15 @@ struct CSRDev {
     MQV_HD int bond(int64_t i, int slot) const { return bonds ? bonds[rp[i] + slot] : 1; }
 };
 
+// Wolff activation rule of the int8 models.
+struct WolffDev {
+    int mode;               // 0 Ising exact, 1 embedded (threshold rule), 2 Potts
+    unsigned long long thr; // Ising exact: u53 < thr adds; embedded/Potts: u53 >= thr adds
+    int q;
+};
+// Activation rule of an int8 model (host side, wolff.cu).
+WolffDev wolff_int8_params(const ModelDev& md);
+
 struct Sim;
 // Smallest u53 rejected by update_accepted<pref>(dE, beta, .) (2^53: all accepted).
 unsigned long long accept_cut(int pref, double dE, double beta);

@@ -957,8 +957,10 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
     const SweepConfig& c = kConfigs[s->sweep_cfg];
     Ising2DArgs a{};
     fill_args(s, c, acc, a);
-    const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
-    if (e != cudaSuccess) return e;
+    if (!c.band) {  // tiles are taken from a counter; bands are fixed per CTA
+        const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
+        if (e != cudaSuccess) return e;
+    }
     return acc ? c.meas(a, s->num_sms, s->stream) : c.plain(a, s->num_sms, s->stream);
 }
 

@@ -19,15 +19,9 @@
 
 #include <mutex>
 
-#include "engine.h"
+#include "wolff_int8.cuh"
 
 namespace mqv {
-
-struct WolffDev {
-    int mode;               // 0 Ising exact, 1 embedded (threshold rule), 2 Potts
-    unsigned long long thr; // Ising exact: u53 < thr adds; embedded/Potts: u53 >= thr adds
-    int q;
-};
 
 template <class Lat>
 __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* __restrict__ s,
@@ -35,84 +29,7 @@ __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* 
                                                    int32_t* __restrict__ out_size, Key key, uint32_t serial,
                                                    uint32_t tg_seed, uint32_t tg_bond)
 {
-    __shared__ int s_head, s_tail, s_next;
-    __shared__ int s_val, s_newq;
-    const int64_t n = lat.n;
-    if (threadIdx.x == 0) {
-        SubStream rng(key, 0u, serial, tg_seed);
-        const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
-        const int val = s[lat.addr(rsite)];
-        int newq = -val;
-        if (w.mode == 2) {
-            // Embedder<Potts<Q>>::draw: new state different from the old one
-            int tries = 0;
-            do {
-                newq = (int)(rng.next() % (uint64_t)w.q);
-            } while (newq == val && ++tries < 256);
-            if (newq == val) newq = (val + 1) % w.q;
-        }
-        s_val = val;
-        s_newq = newq;
-        queue[0] = (int32_t)rsite;
-        atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
-        s_head = 0;
-        s_tail = 1;
-        s_next = 1;
-    }
-    __syncthreads();
-    const int val = s_val;
-    const unsigned lane = threadIdx.x & 31;
-    while (true) {
-        const int head = s_head, tail = s_tail;
-        if (head >= tail) break;
-        for (int base = head; base < tail; base += blockDim.x) {
-            const int idx = base + threadIdx.x;
-            const bool live = idx < tail;
-            const int64_t cur = live ? queue[idx] : 0;
-            const int deg = live ? lat.degree(cur) : 0;
-            int maxdeg = __reduce_max_sync(0xffffffffu, deg);
-            for (int t = 0; t < maxdeg; ++t) {
-                bool add = false;
-                int64_t j = 0;
-                if (t < deg) {
-                    j = lat.nbr(cur, t);
-                    const int sj = s[lat.addr(j)];
-                    if (sj == val && !(visited[j >> 5] & (1u << (j & 31)))) {
-                        const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
-                        const unsigned long long u53 = lo64(philox(lo, serial, hi, tg_bond, key)) >> 11;
-                        bool act;
-                        if (w.mode == 0) act = u53 < w.thr;
-                        else act = u53 >= w.thr;
-                        if (act) {
-                            const uint32_t old = atomicOr(&visited[j >> 5], 1u << (j & 31));
-                            add = !(old & (1u << (j & 31)));
-                        }
-                    }
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, add);
-                if (mask) {
-                    int pos = 0;
-                    if (lane == 0) pos = atomicAdd(&s_next, __popc(mask));
-                    pos = __shfl_sync(0xffffffffu, pos, 0);
-                    if (add) queue[pos + __popc(mask & ((1u << lane) - 1))] = (int32_t)j;
-                }
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            s_head = tail;
-            s_tail = s_next;
-        }
-        __syncthreads();
-    }
-    const int size = s_tail;
-    const int8_t nv = (int8_t)s_newq;
-    for (int k = threadIdx.x; k < size; k += blockDim.x) {
-        const int32_t i = queue[k];
-        s[lat.addr(i)] = nv;
-        atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
-    }
-    if (threadIdx.x == 0) *out_size = size;
+    wolff_int8_cluster(w, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond);
 }
 
 unsigned long long accept_cut(int pref, double dE, double beta);
@@ -120,13 +37,13 @@ unsigned long long accept_cut(int pref, double dE, double beta);
 // Wolff activation thresholds on u53 = word >> 11:
 //  Ising<int>: add iff real() < prob, prob = -expm1(2 beta J): u53 < ceil(prob 2^53)
 //  embedded Ising / Potts: add iff !update_accepted<2>(cpl): u53 >= cut(cpl)
-cudaError_t launch_wolff_int8(Sim* s, int slot)
+WolffDev wolff_int8_params(const ModelDev& md)
 {
     WolffDev w{};
-    const double beta = s->md.beta;
-    if (s->md.kind == MQV_MODEL_ISING) {
+    const double beta = md.beta;
+    if (md.kind == MQV_MODEL_ISING) {
         w.mode = 0;
-        const double prob = -expm1(2.0 * beta * s->md.J);
+        const double prob = -expm1(2.0 * beta * md.J);
         if (!(prob > 0)) w.thr = 0;
         else {
             // smallest u53 with u53 * 2^-53 >= prob
@@ -135,16 +52,22 @@ cudaError_t launch_wolff_int8(Sim* s, int slot)
             if ((double)c < x) ++c;
             w.thr = c > (1ull << 53) ? (1ull << 53) : c;
         }
-    } else if (s->md.kind == MQV_MODEL_POTTS) {
+    } else if (md.kind == MQV_MODEL_POTTS) {
         w.mode = 2;
-        w.q = s->md.q;
+        w.q = md.q;
         // coupling k * (-0.5) for a neighbour in the seed's old state
-        w.thr = accept_cut(2, s->md.k * -0.5, beta);
+        w.thr = accept_cut(2, md.k * -0.5, beta);
     } else {
         // embedded Ising: cpl = J * (s_cur flipped) * s_nbr = -J for an aligned neighbour
         w.mode = 1;
-        w.thr = accept_cut(2, -s->md.J, beta);
+        w.thr = accept_cut(2, -md.J, beta);
     }
+    return w;
+}
+
+cudaError_t launch_wolff_int8(Sim* s, int slot)
+{
+    const WolffDev w = wolff_int8_params(s->md);
     int8_t* st = (int8_t*)s->state[s->cur];
     const Key key = make_key(s->seed);
     const uint32_t serial = (uint32_t)s->cluster;
@@ -218,26 +141,7 @@ cudaError_t wolff_noalloc_scratch(int device, uint32_t** out)
 // same.  The size lands in size slot `slot` of the scratch.
 cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot)
 {
-    WolffDev w{};
-    const double beta = s->md.beta;
-    if (s->md.kind == MQV_MODEL_ISING) {
-        w.mode = 0;
-        const double prob = -expm1(2.0 * beta * s->md.J);
-        if (!(prob > 0)) w.thr = 0;
-        else {
-            const double x = prob * 9007199254740992.0;
-            unsigned long long c = (unsigned long long)x;
-            if ((double)c < x) ++c;
-            w.thr = c > (1ull << 53) ? (1ull << 53) : c;
-        }
-    } else if (s->md.kind == MQV_MODEL_POTTS) {
-        w.mode = 2;
-        w.q = s->md.q;
-        w.thr = accept_cut(2, s->md.k * -0.5, beta);
-    } else {
-        w.mode = 1;
-        w.thr = accept_cut(2, -s->md.J, beta);
-    }
+    const WolffDev w = wolff_int8_params(s->md);
     int32_t* queue = reinterpret_cast<int32_t*>(scratch);
     uint32_t* visited = scratch + kNoAllocMaxSites;
     int32_t* sizes = reinterpret_cast<int32_t*>(visited + kNoAllocMaxSites / 32);

@@ -1,0 +1,99 @@
+// The int8 Wolff cluster update as a device function, shared by the per-handle
+// kernel (wolff.cu) and the batched kernel (batch.cu).  Reference semantics:
+// src/libmarqov/wolff.h:72-126, src/hamiltonian/Ising.h:126-168,
+// src/hamiltonian/Potts.h:220-320 (draws keyed by the undirected bond).
+#pragma once
+#include "engine.h"
+
+namespace mqv {
+
+
+// One cluster grown and flipped by the calling CTA (any block size that is a
+// multiple of 32); the visited bits of its members are cleared before return.
+template <class Lat>
+__device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat& lat, int8_t* __restrict__ s,
+                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
+                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
+                                                   uint32_t tg_seed, uint32_t tg_bond)
+{
+    __shared__ int s_head, s_tail, s_next;
+    __shared__ int s_val, s_newq;
+    const int64_t n = lat.n;
+    if (threadIdx.x == 0) {
+        SubStream rng(key, 0u, serial, tg_seed);
+        const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
+        const int val = s[lat.addr(rsite)];
+        int newq = -val;
+        if (w.mode == 2) {
+            // Embedder<Potts<Q>>::draw: new state different from the old one
+            int tries = 0;
+            do {
+                newq = (int)(rng.next() % (uint64_t)w.q);
+            } while (newq == val && ++tries < 256);
+            if (newq == val) newq = (val + 1) % w.q;
+        }
+        s_val = val;
+        s_newq = newq;
+        queue[0] = (int32_t)rsite;
+        atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
+        s_head = 0;
+        s_tail = 1;
+        s_next = 1;
+    }
+    __syncthreads();
+    const int val = s_val;
+    const unsigned lane = threadIdx.x & 31;
+    while (true) {
+        const int head = s_head, tail = s_tail;
+        if (head >= tail) break;
+        for (int base = head; base < tail; base += blockDim.x) {
+            const int idx = base + threadIdx.x;
+            const bool live = idx < tail;
+            const int64_t cur = live ? queue[idx] : 0;
+            const int deg = live ? lat.degree(cur) : 0;
+            int maxdeg = __reduce_max_sync(0xffffffffu, deg);
+            for (int t = 0; t < maxdeg; ++t) {
+                bool add = false;
+                int64_t j = 0;
+                if (t < deg) {
+                    j = lat.nbr(cur, t);
+                    const int sj = s[lat.addr(j)];
+                    if (sj == val && !(visited[j >> 5] & (1u << (j & 31)))) {
+                        const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
+                        const unsigned long long u53 = lo64(philox(lo, serial, hi, tg_bond, key)) >> 11;
+                        bool act;
+                        if (w.mode == 0) act = u53 < w.thr;
+                        else act = u53 >= w.thr;
+                        if (act) {
+                            const uint32_t old = atomicOr(&visited[j >> 5], 1u << (j & 31));
+                            add = !(old & (1u << (j & 31)));
+                        }
+                    }
+                }
+                const unsigned mask = __ballot_sync(0xffffffffu, add);
+                if (mask) {
+                    int pos = 0;
+                    if (lane == 0) pos = atomicAdd(&s_next, __popc(mask));
+                    pos = __shfl_sync(0xffffffffu, pos, 0);
+                    if (add) queue[pos + __popc(mask & ((1u << lane) - 1))] = (int32_t)j;
+                }
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            s_head = tail;
+            s_tail = s_next;
+        }
+        __syncthreads();
+    }
+    const int size = s_tail;
+    const int8_t nv = (int8_t)s_newq;
+    for (int k = threadIdx.x; k < size; k += blockDim.x) {
+        const int32_t i = queue[k];
+        s[lat.addr(i)] = nv;
+        atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
+    }
+    if (threadIdx.x == 0) *out_size = size;
+}
+
+}  // namespace mqv

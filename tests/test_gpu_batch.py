@@ -1,0 +1,86 @@
+"""Batched EMCS (mqv_batch_*): a batch of members with uneven lattice sizes,
+models and temperatures equals the same members run one handle at a time,
+bit for bit -- states, per-EMCS observables and cluster sizes -- over
+consecutive calls and for every number of EMCS per graph launch."""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+TC_POTTS3 = 1.0 / np.log(1.0 + np.sqrt(3.0))
+
+
+def members(M):
+    out = []
+    rng = np.random.default_rng(7)
+    sizes = [16, 24, 32, 48, 10, 64]
+    for i, L in enumerate(sizes):
+        beta = 1.0 / (TC_POTTS3 * rng.uniform(0.9, 1.1))
+        out.append((M.RegularHypercubic(L, 2), M.Config(seed=100 + i, repid=i), M.Potts(3, -1.0), beta))
+    out.append((M.RegularHypercubic(64, 2), M.Config(seed=11, repid=40), M.Ising(-1.0), 0.44068679))
+    out.append((M.RegularHypercubic(8, 3), M.Config(seed=12, repid=41), M.Ising(-1.0), 0.2216))
+    out.append((M.RegularHypercubic(20, 2), M.Config(seed=13, repid=42), M.Ising(-1.0, "int8"), 0.42))
+    return out
+
+
+def solo(M, m):
+    lat, cfg, ham, beta = m
+    return M.makeCore(lat, cfg, ham, beta)
+
+
+@pytest.mark.parametrize("graph_steps", [1, 3, 8])
+def test_batch_equals_single_handles(graph_steps):
+    import marqov_b200 as M
+    ms = members(M)
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms, graph_steps=graph_steps) as b:
+            b.init()
+            for c in singles:
+                c.init()
+            for i, c in enumerate(singles):
+                assert (b.member(i).state == c.state).all()
+            for call, n in enumerate((7, 5)):
+                obs, mc = b.emcs(n, ncluster=1, nmetro=2)
+                for i, c in enumerate(singles):
+                    o, m = c.emcs(n, ncluster=1, nmetro=2)
+                    assert (obs[:, i, :] == o).all(), f"call {call} member {i}: observables differ"
+                    assert (mc[:, i] == m).all(), f"call {call} member {i}: cluster sizes differ"
+                    assert (b.member(i).state == c.state).all(), f"call {call} member {i}: states differ"
+                    assert b.member(i).counters == c.counters
+            assert b.launches > 0
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_blume_capel_metropolis_only():
+    import marqov_b200 as M
+    ms = [(M.RegularHypercubic(L, 2), M.Config(seed=5 + L, repid=L), M.BlumeCapel(-1.0, 0.5), 0.6)
+          for L in (8, 12, 16)]
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms) as b:
+            b.init()
+            for c in singles:
+                c.init()
+            obs, mc = b.emcs(6, ncluster=0, nmetro=3)
+            assert (mc == 0).all()
+            for i, c in enumerate(singles):
+                o, _ = c.emcs(6, ncluster=0, nmetro=3)
+                assert (obs[:, i, :] == o).all()
+                assert (b.member(i).state == c.state).all()
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_rejects_unsupported_members():
+    import marqov_b200 as M
+    with pytest.raises(M.MarqovError) as ei:
+        M.Batch([(M.RegularHypercubic(8, 3), M.Config(), M.Heisenberg(-1.0), 0.7)])
+    assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
+    lat = M.RegularRandomBond(8, 2, seed=1)
+    with pytest.raises(M.MarqovError) as ei:
+        M.Batch([(lat, M.Config(), M.EdwardsAndersonIsing(-1.0), 0.7)])
+    assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
