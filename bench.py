@@ -54,8 +54,8 @@ def parse():
     p.add_argument("--L", type=int, default=16384)
     p.add_argument("--nmetro", type=int, default=20, help="sweeps per step (one EMCS)")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["ising2d", "potts-batch"], default="ising2d",
-                   help="ising2d: the headline line; potts-batch: the batched-farm line alone")
+    p.add_argument("--workload", choices=["ising2d", "potts-batch", "secondary"], default="ising2d",
+                   help="ising2d: the headline line; potts-batch / secondary: those lines alone")
     p.add_argument("--no-secondary", action="store_true",
                    help="leave the secondary workloads out of the headline line")
     return p.parse_args()
@@ -295,11 +295,114 @@ def workload_potts_batch(M, torch, emcs_batched=100, emcs_plain=4, warmup=5):
     }
 
 
+def timed(torch, stream, fn):
+    """Device time (s) of fn()'s work on `stream` (CUDA events)."""
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    ev0.record(stream)
+    fn()
+    ev1.record(stream)
+    torch.cuda.synchronize()
+    return ev0.elapsed_time(ev1) * 1e-3
+
+
+def hbm_frac(bytes_per_update, rate_per_ns):
+    peak, _ = measured_peaks()
+    return bytes_per_update * rate_per_ns / peak
+
+
+def workload_heisenberg(M, torch, sweeps=20, clusters=20):
+    """Config 2: 3D Heisenberg L=128 at beta=0.693, small-cap proposals tuned
+    to ~50% acceptance during thermalisation, Wolff plane reflections."""
+    L, beta = 128, 0.6930
+    st = torch.cuda.Stream()
+    with M.makeCore(M.RegularHypercubic(L, 3), M.Config(seed=31, repid=0), M.Heisenberg(-1.0, "smallcap", 0.5),
+                    beta) as c:
+        c.set_stream(st.cuda_stream)
+        c.init()
+        cap = M.tune_small_cap(c, 0.5, iters=10)
+        c.emcs(5, ncluster=1, nmetro=5, measure=False)
+        n = c.n
+        t_m = timed(torch, st, lambda: c.metropolis(sweeps))
+        sizes = []
+        t_w = timed(torch, st, lambda: sizes.append(c.wolff(clusters)))
+        t_e = timed(torch, st, lambda: c.emcs(4, ncluster=1, nmetro=5, measure=True))
+        obs, _ = c.emcs(1, ncluster=0, nmetro=1)
+    rate = n * sweeps / (t_m * 1e9)
+    return {"workload": "3D Heisenberg L=128 (2,097,152 sites), beta=0.693, small-cap Metropolis",
+            "unit": UNIT, "value": rate, "dtype": "f32 (FP64 dE and acceptance)",
+            "cap_cos_half_angle": cap,
+            "roofline": {"bytes_per_update": 24, "frac_of_hbm": hbm_frac(24, rate),
+                         "note": "25 MB state: largely L2-resident"},
+            "wolff_cluster_spins_per_ns": float(np.sum(sizes)) / (t_w * 1e9),
+            "emcs_per_s": 4 / t_e, "energy_per_site": float(obs[0, 0])}
+
+
+def workload_rgg(M, torch, sweeps=20):
+    """Config 5a: Ising on a 2D random geometric graph, N = 2^20, mean degree 8,
+    CSR with greedy colouring, beta = 0.5, Metropolis only."""
+    n = 1 << 20
+    t0 = time.perf_counter()
+    lat = M.RandomGeometricGraph2D(n, 8.0, seed=5)
+    build_s = time.perf_counter() - t0
+    st = torch.cuda.Stream()
+    with M.makeCore(lat, M.Config(seed=41, repid=0), M.Ising(-1.0, "int8"), 0.5) as c:
+        c.set_stream(st.cuda_stream)
+        c.init()
+        c.metropolis(3)
+        t_m = timed(torch, st, lambda: c.metropolis(sweeps))
+    rate = n * sweeps / (t_m * 1e9)
+    deg = float(lat.col_idx.size) / n
+    bpu = 1 + 1 + 4 + 4 * deg + deg
+    return {"workload": f"Ising on a 2D random geometric graph, N=2^20, mean degree {deg:.2f}, beta=0.5",
+            "unit": UNIT, "value": rate, "graph_build_s": build_s,
+            "roofline": {"bytes_per_update": bpu, "frac_of_hbm": hbm_frac(bpu, rate)}}
+
+
+def workload_ea(M, torch, sweeps=20, realisations=32):
+    """Config 5b: 32 +-J Edwards-Anderson realisations on 3D L=32, beta=0.9,
+    Metropolis only."""
+    st = torch.cuda.Stream()
+    cores = []
+    try:
+        for r in range(realisations):
+            c = M.makeCore(M.RegularRandomBond(32, 3, 0.5, seed=100 + r), M.Config(seed=500 + r, repid=r),
+                           M.EdwardsAndersonIsing(-1.0), 0.9)
+            c.set_stream(st.cuda_stream)
+            c.init()
+            c.metropolis(2)
+            cores.append(c)
+        t_m = timed(torch, st, lambda: [c.metropolis(sweeps) for c in cores])
+    finally:
+        for c in cores:
+            c.close()
+    n = 32 ** 3 * realisations
+    rate = n * sweeps / (t_m * 1e9)
+    return {"workload": "32 +-J Edwards-Anderson realisations, 3D L=32, beta=0.9 (one handle each)",
+            "unit": UNIT, "value": rate,
+            "roofline": {"bytes_per_update": 5, "frac_of_hbm": hbm_frac(5, rate), "note": "L2-resident"}}
+
+
+def secondary(M, torch):
+    out = {}
+    for name, fn in (("potts_batch", workload_potts_batch), ("heisenberg3d_L128", workload_heisenberg),
+                     ("rgg_ising_N1M", workload_rgg), ("ea_3d_L32x32", workload_ea)):
+        try:
+            out[name] = fn(M, torch)
+        except Exception as exc:  # a secondary line never hides the headline
+            out[name] = {"error": f"{type(exc).__name__}: {exc}"}
+    return out
+
+
 def run_workload(args, ws, rank, local):
     import torch
 
     import marqov_b200 as M
     torch.cuda.set_device(local)
+    if args.workload == "secondary":
+        if rank == 0:
+            print(json.dumps({"secondary": secondary(M, torch)}))
+        return 0
     res = workload_potts_batch(M, torch)
     line = {"metric": METRIC, "value": res["batched"]["value"], "unit": UNIT, "n_gpus": 1,
             "steps": res["batched"]["emcs"], "warmup": 5, "ms_per_step": 1e3 * res["batched"]["seconds_device"] /
@@ -420,6 +523,8 @@ def run_engine(args, ws, rank, local):
         "e2e": e2e, "e2e_host_state": e2e_host, "roofline": roof, "gpu_launches": launches,
         "clocks": clk.summary(),
     }
+    if rank == 0 and ws == 1 and not args.no_secondary:
+        line["secondary"] = secondary(M, torch)
     if rank == 0 and ws == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline(L)

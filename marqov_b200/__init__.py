@@ -7,7 +7,7 @@ Core interface.  Importing it loads the engine library; there is no CPU path.
 """
 from . import _lib
 from ._lib import MarqovError
-from .core import Batch, Config, Core, makeCore
+from .core import Batch, Config, Core, makeCore, tune_small_cap
 from .hamiltonians import (BlumeCapel, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising, Phi4, Potts,
                            XXZAntiferro)
 from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
@@ -15,7 +15,7 @@ from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGra
 
 _lib.load()
 
-__all__ = ["Batch", "Config", "Core", "makeCore", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
+__all__ = ["Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
            "Potts", "BlumeCapel", "Heisenberg", "XXZAntiferro", "Phi4", "CSRLattice",
            "FixedDimRegularHypercubic", "RegularHypercubic", "RegularRandomBond", "RandomGeometricGraph2D",
            "read_graph_csv"]

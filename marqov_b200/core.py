@@ -193,6 +193,12 @@ class Core:
         self.beta = float(beta)
         L.check(self._lib.mqv_set_beta(self._h, self.beta))
 
+    def set_model(self, ham: Hamiltonian):
+        """Replace the model coefficients (same model kind), e.g. a new
+        proposal width."""
+        L.check(self._lib.mqv_set_model(self._h, C.byref(ham.desc(self.beta))))
+        self.ham = ham
+
     def set_stream(self, stream_ptr: int):
         L.check(self._lib.mqv_set_stream(self._h, C.c_void_p(stream_ptr)))
 
@@ -311,3 +317,32 @@ class Batch:
         c = C.c_uint64()
         L.check(self._lib.mqv_batch_launch_count(self._h, C.byref(c)))
         return int(c.value)
+
+
+def tune_small_cap(core: Core, target: float = 0.5, iters: int = 10, sweeps: int = 1) -> float:
+    """Tune the small-cap proposal of an O(3) model to a Metropolis acceptance
+    rate near `target` by bisection on cap = cos(half-angle) during
+    thermalisation; returns the frozen cap (also set on the core).
+
+    The acceptance rate of a sweep is measured as the fraction of sites whose
+    spin changed (an accepted cap move always changes the spin).  This tuning
+    has no counterpart in the reference, which draws fresh directions."""
+    import copy
+    lo, hi = -1.0, 0.9999
+    ham = copy.copy(core.ham)
+    ham.proposal = "smallcap"
+    for _ in range(iters):
+        mid = 0.5 * (lo + hi)
+        ham.cap = mid
+        core.set_model(ham)
+        before = core.state.reshape(-1, core.symd)
+        core.metropolis(sweeps)
+        after = core.state.reshape(-1, core.symd)
+        acc = float(np.mean(np.any(before != after, axis=1))) ** (1.0 / sweeps)
+        if acc < target:
+            lo = mid  # too few accepted: narrower cone (larger cap)
+        else:
+            hi = mid
+    ham.cap = 0.5 * (lo + hi)
+    core.set_model(ham)
+    return ham.cap
