@@ -321,7 +321,8 @@ def workload_heisenberg(M, torch, sweeps=20, clusters=20):
         c.set_stream(st.cuda_stream)
         c.init()
         cap = M.tune_small_cap(c, 0.5, iters=10)
-        c.emcs(5, ncluster=1, nmetro=5, measure=False)
+        # thermalise with clusters, so that cluster sizes approach their critical scale
+        c.emcs(20, ncluster=10, nmetro=5, measure=False)
         n = c.n
         t_m = timed(torch, st, lambda: c.metropolis(sweeps))
         sizes = []
@@ -335,6 +336,7 @@ def workload_heisenberg(M, torch, sweeps=20, clusters=20):
             "roofline": {"bytes_per_update": 24, "frac_of_hbm": hbm_frac(24, rate),
                          "note": "25 MB state: largely L2-resident"},
             "wolff_cluster_spins_per_ns": float(np.sum(sizes)) / (t_w * 1e9),
+            "wolff_mean_cluster": float(np.mean(sizes)), "wolff_us_per_cluster": 1e6 * t_w / clusters,
             "emcs_per_s": 4 / t_e, "energy_per_site": float(obs[0, 0])}
 
 

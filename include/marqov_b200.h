@@ -189,6 +189,24 @@ MQV_API mqv_status mqv_wolff_noalloc(mqv_sim* sim, int32_t nclusters, int32_t* s
  * records; mean_cluster (host, may be NULL) receives n_emcs mean sizes. */
 MQV_API mqv_status mqv_emcs(mqv_sim* sim, int32_t n_emcs, int32_t ncluster, int32_t nmetro,
                             mqv_obs* obs, double* mean_cluster);
+/* No counterpart in the reference.  mqv_emcs that keeps the raw lattice sums
+ * of every EMCS on the device for gradient estimators: d_samples (DEVICE
+ * pointer, n_emcs * 4 doubles) receives per EMCS the interaction sum
+ * sum_i s_i sum_{j in nbrs(i)} s_j, sum_i s_i, sum_i s_i^2 and
+ * sum_i (s_i^2 - 1)^2 (x components for vectors; 0 for the last sum of
+ * integer models).  Asynchronous on the handle's stream. */
+MQV_API mqv_status mqv_emcs_samples(mqv_sim* sim, int32_t n_emcs, int32_t ncluster, int32_t nmetro, double* d_samples);
+/* No counterpart in the reference.  Fluctuation-dissipation gradients of
+ * scalar phi^4 in the reference form (src/hamiltonian/Phi4.h:84-121),
+ * S = -beta sum_<ij> phi_i phi_j + sum_i [mass phi_i^2 + lambda (phi_i^2 - 1)^2],
+ * from the samples of nrep runs (d_samples: [nrep][nsamp][4] as written by
+ * mqv_emcs_samples).  All arrays are DEVICE pointers: d_beta, d_lambda [nrep];
+ * d_obs [nrep][3] = (<E>, <|m|>, U4); d_jac [nrep][3][2] = d obs / d(beta,
+ * lambda); optional d_gout [nrep][3] and d_grads [nrep][2] = gout . jac.
+ * stream: cudaStream_t (NULL = default stream). */
+MQV_API mqv_status mqv_phi4_fdt(const double* d_samples, int32_t nrep, int32_t nsamp, int64_t nsites, double mass,
+                                const double* d_beta, const double* d_lambda, double* d_obs, double* d_jac,
+                                const double* d_gout, double* d_grads, void* stream);
 /* Observables of the current state. */
 MQV_API mqv_status mqv_measure(mqv_sim* sim, mqv_obs* out);
 MQV_API mqv_status mqv_synchronize(mqv_sim* sim);

@@ -91,6 +91,9 @@ SIGNATURES = {
     "mqv_wolff_noalloc": (C.c_int32, [_vp, C.c_int32, _vp]),
     "mqv_emcs": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp]),
     "mqv_measure": (C.c_int32, [_vp, C.POINTER(Obs)]),
+    "mqv_emcs_samples": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
+    "mqv_phi4_fdt": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int64, C.c_double, _vp, _vp, _vp, _vp, _vp, _vp,
+                                 _vp]),
     "mqv_synchronize": (C.c_int32, [_vp]),
     "mqv_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
     "mqv_describe": (C.c_int32, [_vp, C.c_char_p, C.c_size_t]),

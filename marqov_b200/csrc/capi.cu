@@ -36,6 +36,10 @@ int wolff_noalloc_max_clusters();
 cudaError_t wolff_noalloc_scratch(int device, uint32_t** out);
 cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot);
 const int32_t* wolff_noalloc_sizes(const uint32_t* scratch);
+cudaError_t launch_acc_to_samples(const long long* acc, int is_f32, int nslots, double* out, cudaStream_t st);
+cudaError_t launch_phi4_fdt(const double* samples, int nrep, int nsamp, double invN, const double* beta,
+                            const double* lam, double mass, double* obs, double* jac, const double* gout,
+                            double* grads, cudaStream_t st);
 
 // Smallest u53 rejected by update_accepted<pref>(dE, beta, .), 2^53 when all
 // are accepted: the rule accepts exactly the words with u53 below a cut.
@@ -707,6 +711,61 @@ MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_
         }
         done += ch;
     }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_emcs_samples(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_t nmetro, double* d_samples)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
+    if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
+    if (n_emcs > 0 && !d_samples) return fail(MQV_ERR_INVALID_ARG, "null sample buffer");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    if (ncluster > 0) {
+        mqv_status st = check_wolff_supported(s);
+        if (st) return st;
+    }
+    const int CH = 1024;
+    int done = 0;
+    while (done < n_emcs) {
+        const int ch = std::min(n_emcs - done, CH);
+        mqv_status st = ensure_slots(s, ch);
+        if (st) return st;
+        if (ncluster > 0) {
+            st = ensure_cslots(s, ch * ncluster);
+            if (st) return st;
+        }
+        MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch, s->stream));
+        for (int e = 0; e < ch; ++e) {
+            for (int c = 0; c < ncluster; ++c) {
+                st = launch_cluster(s, e * ncluster + c);
+                if (st) return st;
+            }
+            for (int j = 0; j < nmetro; ++j) {
+                st = launch_sweep(s, j == nmetro - 1 ? e : -1);
+                if (st) return st;
+            }
+            if (nmetro == 0) {
+                st = launch_measure(s, e);
+                if (st) return st;
+            }
+        }
+        MQV_CK(launch_acc_to_samples(s->d_acc, s->is_f32 ? 1 : 0, ch, d_samples + 4 * (size_t)done, s->stream));
+        s->launches++;
+        done += ch;
+    }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_phi4_fdt(const double* d_samples, int32_t nrep, int32_t nsamp, int64_t nsites, double mass,
+                                const double* d_beta, const double* d_lambda, double* d_obs, double* d_jac,
+                                const double* d_gout, double* d_grads, void* stream)
+{
+    if (!d_samples || !d_beta || !d_lambda || !d_obs || !d_jac) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    if (nrep < 1 || nsamp < 2 || nsites < 1) return fail(MQV_ERR_INVALID_ARG, "need nrep >= 1, nsamp >= 2, nsites >= 1");
+    if ((d_gout == nullptr) != (d_grads == nullptr)) return fail(MQV_ERR_INVALID_ARG, "gout and grads go together");
+    MQV_CK(launch_phi4_fdt(d_samples, nrep, nsamp, 1.0 / (double)nsites, d_beta, d_lambda, mass, d_obs, d_jac, d_gout,
+                           d_grads, (cudaStream_t)stream));
     return MQV_OK;
 }
 
