@@ -385,10 +385,35 @@ def workload_ea(M, torch, sweeps=20, realisations=32):
             "roofline": {"bytes_per_update": 5, "frac_of_hbm": hbm_frac(5, rate), "note": "L2-resident"}}
 
 
+def workload_phi4_autograd(M, torch, n_therm=10, n_meas=40):
+    """Config 4: 3D phi^4 L=64 for 64 beta values uniform in [0.36, 0.38],
+    lambda = 1.1: forward (chains + device samples) and backward (the FDT
+    kernel) of <E>, <|m|>, U4; bounded EMCS counts."""
+    import marqov_b200.autograd as A
+    R = 64
+    rng = np.random.default_rng(17)
+    beta = torch.tensor(np.sort(rng.uniform(0.36, 0.38, R)), dtype=torch.float64, requires_grad=True)
+    lam = torch.full((R,), 1.1, dtype=torch.float64, requires_grad=True)
+    ens = A.Phi4Ensemble(L=64, dim=3, n_therm=n_therm, n_meas=n_meas, seed=23)
+    st = torch.cuda.current_stream()
+    fwd = []
+    t_f = timed(torch, st, lambda: fwd.append(A.phi4_observables(beta, lam, ens)))
+    obs = fwd[0]
+    t_b = timed(torch, st, lambda: obs[:, 0].sum().backward())
+    sites = R * ens.sites
+    rate = sites * (n_therm + n_meas) / (t_f * 1e9)
+    return {"workload": "3D phi^4 L=64 x 64 beta in [0.36,0.38], lambda=1.1, EMCS = 1 Wolff + 1 sweep",
+            "unit": UNIT, "value": rate, "emcs_per_chain": n_therm + n_meas,
+            "roofline": {"bytes_per_update": 8, "frac_of_hbm": hbm_frac(8, rate)},
+            "backward_ms": 1e3 * t_b, "dE_dbeta_mean": float(beta.grad.mean()),
+            "forward_includes": "chain runs from a random start, device samples, FDT observables"}
+
+
 def secondary(M, torch):
     out = {}
     for name, fn in (("potts_batch", workload_potts_batch), ("heisenberg3d_L128", workload_heisenberg),
-                     ("rgg_ising_N1M", workload_rgg), ("ea_3d_L32x32", workload_ea)):
+                     ("phi4_autograd_64xL64", workload_phi4_autograd), ("rgg_ising_N1M", workload_rgg),
+                     ("ea_3d_L32x32", workload_ea)):
         try:
             out[name] = fn(M, torch)
         except Exception as exc:  # a secondary line never hides the headline

@@ -34,7 +34,7 @@ __global__ void batch_metro_int8(const BatchRep* __restrict__ reps, const int64_
     while (g >= half_prefix[r + 1]) ++r;
     const BatchRep& R = reps[r];
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
-    int8_site(R.md, R.st, R.s, parity_site(R.st, g - half_prefix[r], colour), R.key, sweep, R.replica);
+    int8_site(R.md, R.st, R.s, parity_site(R.st, g - half_prefix[r], colour), R.key, sweep, R.replica, R.cuts, R.D);
 }
 
 __global__ void __launch_bounds__(1024) batch_wolff_int8(const BatchRep* __restrict__ reps,

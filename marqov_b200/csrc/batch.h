@@ -15,6 +15,8 @@ struct BatchRep {
     int8_t* s;                  // state (reference site order)
     uint32_t* visited;          // Wolff scratch of the member handle
     int32_t* queue;
+    const unsigned long long* cuts;  // the member's Metropolis cut table
+    int D;                           // its maximum degree
 };
 
 // Device counters of a run: EMCS done, first EMCS of the current chunk

@@ -26,6 +26,7 @@ cudaError_t launch_metropolis_int8(Sim* s, int slot);
 cudaError_t launch_measure_int8(Sim* s, int slot);
 cudaError_t launch_finalize_int8(Sim* s, int nslots, double* d_out);
 cudaError_t launch_wolff_int8(Sim* s, int slot);
+cudaError_t ensure_cuts(Sim* s);
 cudaError_t launch_init_f32(Sim* s);
 cudaError_t launch_metropolis_f32(Sim* s, int slot);
 cudaError_t launch_measure_f32(Sim* s, int slot);
@@ -100,7 +101,7 @@ static void free_sim(Sim* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (void* p : {s->state[0], s->state[1], (void*)s->d_rp, (void*)s->d_ci, (void*)s->d_bonds, (void*)s->d_order,
                     (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize,
-                    (void*)s->d_status, (void*)s->d_counter})
+                    (void*)s->d_status, (void*)s->d_counter, (void*)s->d_cuts})
         if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -404,6 +405,9 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         s->sten.dim = lattice->dim;
         s->sten.len = lattice->len;
         s->sten.n = n;
+        s->sten.lg = -1;
+        for (int b = 0; b < 31; ++b)
+            if ((1 << b) == lattice->len) s->sten.lg = b;
         s->max_degree = 2 * lattice->dim;
         s->colour_ptr = {0, (int32_t)(n / 2), (int32_t)n};
     } else if (lattice->kind == MQV_LATTICE_CSR) {
@@ -1065,6 +1069,7 @@ MQV_API mqv_status mqv_batch_emcs(mqv_batch* h, int32_t n_emcs, int32_t ncluster
     if (ncluster > 64 || nmetro > 64) return fail(MQV_ERR_INVALID_ARG, "at most 64 clusters and 64 sweeps per EMCS");
     for (Sim* s : b->sims) {
         if (!s->initialised) return fail(MQV_ERR_STATE, "state of a batch member not initialised");
+        MQV_CK(ensure_cuts(s));
         if (ncluster > 0) {
             mqv_status st = check_wolff_supported(s);
             if (st) return st;
@@ -1087,6 +1092,8 @@ MQV_API mqv_status mqv_batch_emcs(mqv_batch* h, int32_t n_emcs, int32_t ncluster
         r.s = (int8_t*)s->state[s->cur];
         r.visited = s->d_visited;
         r.queue = s->d_queue;
+        r.cuts = s->d_cuts;
+        r.D = s->max_degree;
     }
     MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
                            b->stream));

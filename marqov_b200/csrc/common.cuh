@@ -74,16 +74,28 @@ MQV_HD uint64_t accept_fine56(Key key, uint32_t site, uint32_t sweep, uint32_t r
     const uint4 f = philox(site >> 1, sweep, 0u, (kAcceptFine << 24) | (replica & 0xFFFFFFu), key);
     return ((site & 1u) ? hi64(f) : lo64(f)) & 0x00FFFFFFFFFFFFFFull;
 }
-MQV_HD uint64_t accept_word(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+MQV_HD uint32_t accept_top8(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
 {
     const uint32_t g = accept_group(site), q = (site >> 1) & 31u;
     const uint32_t c3 = (kAccept << 24) | (replica & 0xFFFFFFu);
     const uint4 a = philox(g, sweep, 0u, c3, key);
     const uint4 b = philox(g, sweep, 1u, c3, key);
-    const uint32_t cb = ((a.x >> q) & 1u) | (((a.y >> q) & 1u) << 1) | (((a.z >> q) & 1u) << 2) |
-                        (((a.w >> q) & 1u) << 3) | (((b.x >> q) & 1u) << 4) | (((b.y >> q) & 1u) << 5) |
-                        (((b.z >> q) & 1u) << 6) | (((b.w >> q) & 1u) << 7);
-    return ((uint64_t)cb << 56) | accept_fine56(key, site, sweep, replica);
+    return ((a.x >> q) & 1u) | (((a.y >> q) & 1u) << 1) | (((a.z >> q) & 1u) << 2) | (((a.w >> q) & 1u) << 3) |
+           (((b.x >> q) & 1u) << 4) | (((b.y >> q) & 1u) << 5) | (((b.z >> q) & 1u) << 6) | (((b.w >> q) & 1u) << 7);
+}
+MQV_HD uint64_t accept_word(Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    return ((uint64_t)accept_top8(key, site, sweep, replica) << 56) | accept_fine56(key, site, sweep, replica);
+}
+// u53 < cut on the site's acceptance word (cut = accept_cut of the move's dE):
+// the fine half is drawn only when the top byte ties the cut's
+MQV_HD bool accept_below(uint64_t cut, Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    if (cut >= (1ull << 53)) return true;
+    if (cut == 0) return false;
+    const uint32_t top = accept_top8(key, site, sweep, replica), t8 = (uint32_t)(cut >> 45);
+    if (top != t8) return top < t8;
+    return (((uint64_t)top << 45) | (accept_fine56(key, site, sweep, replica) >> 11)) < cut;
 }
 
 // real() of RNGCache: (word >> 11) * 2^-53 (src/libmarqov/rngcache.h:202-206).

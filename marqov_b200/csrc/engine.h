@@ -42,22 +42,29 @@ MQV_HD int64_t split_addr(int64_t y, int x, int len)
 struct StencilDev {
     int dim;
     int len;
-    int64_t n;
+    int64_t n;  // < 2^31: site indices fit 32 bits
     int64_t pows[4];
     int split;  // 2D state stored in split rows (see split_addr)
+    int lg;     // log2(len) when len is a power of two, else -1
+    // coordinate j of site i (32-bit arithmetic; shifts for power-of-two sides)
+    MQV_HD int coord(int64_t i, int j) const
+    {
+        const uint32_t u = (uint32_t)i;
+        if (lg >= 0) return (int)((u >> (lg * j)) & (uint32_t)(len - 1));
+        return (int)((u / (uint32_t)pows[j]) % (uint32_t)len);
+    }
     // device address of site i
     MQV_HD int64_t addr(int64_t i) const
     {
         if (!split) return i;
-        const int64_t y = i / len;
-        return split_addr(y, (int)(i - y * len), len);
+        return split_addr(coord(i, 1), coord(i, 0), len);  // split layouts are 2D
     }
     MQV_HD int degree(int64_t) const { return 2 * dim; }
     MQV_HD int64_t nbr(int64_t i, int slot) const
     {
         const int j = slot >> 1;
         const int64_t p = pows[j];
-        const int64_t x = (i / p) % len;
+        const int x = coord(i, j);
         if ((slot & 1) == 0) return x == len - 1 ? i - (int64_t)(len - 1) * p : i + p;
         return x == 0 ? i + (int64_t)(len - 1) * p : i - p;
     }
@@ -81,6 +88,9 @@ struct WolffDev {
     unsigned long long thr; // Ising exact: u53 < thr adds; embedded/Potts: u53 >= thr adds
     int q;
 };
+// u53 cuts of an int8 model's Metropolis moves for lattices of maximum degree
+// D, indexed as int8_site computes its dE index (host side).
+std::vector<unsigned long long> int8_cut_table(const ModelDev& md, int D);
 // Activation rule of an int8 model (host side, wolff.cu).
 WolffDev wolff_int8_params(const ModelDev& md);
 
@@ -128,6 +138,10 @@ struct Sim {
     double thr_J = 0, thr_beta = -1;  // (J, beta) the cached 2D thresholds belong to
     unsigned long long thr_cut[5] = {};
     int sweep_cfg = -1;  // autotuned fused-sweep configuration (-1: not chosen yet)
+    // int8 models: u53 cut of every possible dE (int8_cut_table), on the device
+    unsigned long long* d_cuts = nullptr;
+    int n_cuts = 0;
+    double cuts_for[5] = {0, 0, 0, -1, 0};  // (J, h, k, beta, kind) the table belongs to
     // measurement
     int nslots = 0;
     long long* d_acc = nullptr;  // nslots * kAccStride

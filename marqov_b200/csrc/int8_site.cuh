@@ -10,16 +10,19 @@ namespace mqv {
 // ---------------------------------------------------------------------------
 // generic per-site update (Metropolis<H,L>::move, src/libmarqov/metropolis.h:88-126)
 
+// `cuts`: the u53 cut of every dE the model can produce, indexed as
+// int8_cut_index (host table int8_cut_table); the decision equals
+// update_accepted<1>(dE, beta, word) on the site's acceptance word.
 template <class Lat>
 __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int8_t* __restrict__ s, int64_t i,
-                                          Key key, uint32_t sweep, uint32_t replica)
+                                          Key key, uint32_t sweep, uint32_t replica,
+                                          const unsigned long long* __restrict__ cuts, int D)
 {
     SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
     const int64_t ai = lat.addr(i);
     const int old = s[ai];
     const int deg = lat.degree(i);
-    int nw;
-    double dE;
+    int nw, k;
     if (m.kind == MQV_MODEL_POTTS) {
         // Initializer<Potts<Q>>::newsv (src/hamiltonian/Potts.h:170-177) and
         // PottsInteraction::diff (src/hamiltonian/Potts.h:86-107)
@@ -30,7 +33,7 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int
             eo += (v == old);
             en += (v == nw);
         }
-        dE = MQV_DMUL(m.k, (double)(en - eo));
+        k = en - eo + D;
     } else if (m.kind == MQV_MODEL_BLUME_CAPEL) {
         // Spin1_Initializer::newsv (src/hamiltonian/util/initializers.h:99-118)
         int st = old;
@@ -39,18 +42,18 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int
         nw = st;
         int sum = 0;
         for (int t = 0; t < deg; ++t) sum += s[lat.addr(lat.nbr(i, t))];
-        dE = MQV_DADD(MQV_DMUL(m.J, (double)((nw - old) * sum)), MQV_DMUL(m.h, (double)(nw * nw - old * old)));
+        k = (((nw - old) + 2) * (2 * D + 1) + (sum + D)) * 3 + (nw * nw - old * old + 1);
     } else {
         // spin flip (src/hamiltonian/util/initializers.h:52-58), neighbourhood
         // sum with optional bonds (src/libmarqov/metropolishelpers.h:456-537)
         nw = -old;
         int sum = 0;
         for (int t = 0; t < deg; ++t) sum += lat.bond(i, t) * s[lat.addr(lat.nbr(i, t))];
-        dE = MQV_DMUL(m.J, (double)((nw - old) * sum));
+        k = old * sum + D;
     }
     // metro_update_accepted (src/libmarqov/metropolis.h:61-64,120-124) on the
     // site's acceptance word
-    if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) s[ai] = (int8_t)nw;
+    if (accept_below(cuts[k], key, (uint32_t)i, sweep, replica)) s[ai] = (int8_t)nw;
 }
 
 // Site of colour `colour` in pair t of a parity-coloured hypercubic lattice
@@ -60,7 +63,7 @@ __device__ __forceinline__ int64_t parity_site(const StencilDev& st, int64_t t, 
 {
     const int64_t i0 = 2 * t;
     int par = 0;
-    for (int j = 1; j < st.dim; ++j) par += (int)((i0 / st.pows[j]) % st.len);
+    for (int j = 1; j < st.dim; ++j) par += st.coord(i0, j);
     return i0 + (((par & 1) != colour) ? 1 : 0);
 }
 

@@ -103,7 +103,7 @@ __device__ __forceinline__ int64_t parity_site_f(const StencilDev& st, int64_t t
 {
     const int64_t i0 = 2 * t;
     int par = 0;
-    for (int j = 1; j < st.dim; ++j) par += (int)((i0 / st.pows[j]) % st.len);
+    for (int j = 1; j < st.dim; ++j) par += st.coord(i0, j);
     return i0 + (((par & 1) != colour) ? 1 : 0);
 }
 

@@ -11,23 +11,73 @@
 // lattice's addr() maps for every other kernel.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <vector>
+
 #include "int8_site.cuh"
 
 namespace mqv {
 
 __global__ void metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict__ s, int colour, Key key,
-                                   uint32_t sweep, uint32_t replica)
+                                   uint32_t sweep, uint32_t replica, const unsigned long long* __restrict__ cuts,
+                                   int D)
 {
     const int64_t half = st.n / 2;
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < half; t += (int64_t)gridDim.x * blockDim.x)
-        int8_site(m, st, s, parity_site(st, t, colour), key, sweep, replica);
+        int8_site(m, st, s, parity_site(st, t, colour), key, sweep, replica, cuts, D);
 }
 
 __global__ void metro_int8_csr(ModelDev m, CSRDev g, int8_t* __restrict__ s, const int32_t* __restrict__ order,
-                               int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t replica)
+                               int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t replica,
+                               const unsigned long long* __restrict__ cuts, int D)
 {
     for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
-        int8_site(m, g, s, order[begin + t], key, sweep, replica);
+        int8_site(m, g, s, order[begin + t], key, sweep, replica, cuts, D);
+}
+
+// dE of every move index of int8_site, with the kernel's own FP64 operations
+std::vector<unsigned long long> int8_cut_table(const ModelDev& m, int D)
+{
+    std::vector<unsigned long long> t;
+    if (m.kind == MQV_MODEL_BLUME_CAPEL) {
+        t.resize((size_t)5 * (2 * D + 1) * 3);
+        for (int dn = -2; dn <= 2; ++dn)
+            for (int sum = -D; sum <= D; ++sum)
+                for (int dq = -1; dq <= 1; ++dq) {
+                    const double dE = MQV_DADD(MQV_DMUL(m.J, (double)(dn * sum)), MQV_DMUL(m.h, (double)dq));
+                    t[(size_t)(((dn + 2) * (2 * D + 1) + (sum + D)) * 3 + (dq + 1))] = accept_cut(1, dE, m.beta);
+                }
+    } else {
+        t.resize((size_t)2 * D + 1);
+        for (int k = 0; k <= 2 * D; ++k) {
+            const double dE = m.kind == MQV_MODEL_POTTS ? MQV_DMUL(m.k, (double)(k - D))
+                                                        : MQV_DMUL(m.J, (double)(-2 * (k - D)));
+            t[(size_t)k] = accept_cut(1, dE, m.beta);
+        }
+    }
+    return t;
+}
+
+// the handle's cut table, rebuilt when the model or beta changed
+cudaError_t ensure_cuts(Sim* s)
+{
+    const double key[5] = {s->md.J, s->md.h, s->md.k, s->md.beta, (double)s->md.kind};
+    if (s->d_cuts && std::equal(key, key + 5, s->cuts_for)) return cudaSuccess;
+    const std::vector<unsigned long long> t = int8_cut_table(s->md, s->max_degree);
+    if ((int)t.size() > s->n_cuts) {
+        if (s->d_cuts) cudaFree(s->d_cuts);
+        s->d_cuts = nullptr;
+        s->n_cuts = 0;
+        const cudaError_t e = cudaMalloc(&s->d_cuts, sizeof(unsigned long long) * t.size());
+        if (e != cudaSuccess) return e;
+        s->n_cuts = (int)t.size();
+    }
+    // stream-ordered with the sweeps that read the previous table
+    const cudaError_t e = cudaMemcpyAsync(s->d_cuts, t.data(), sizeof(unsigned long long) * t.size(),
+                                          cudaMemcpyHostToDevice, s->stream);
+    if (e != cudaSuccess) return e;
+    std::copy(key, key + 5, s->cuts_for);
+    return cudaStreamSynchronize(s->stream);  // the host table goes out of scope
 }
 
 template <class Lat>
@@ -102,6 +152,7 @@ cudaError_t launch_finalize_int8(Sim* s, int nslots, double* d_out)
 }
 
 cudaError_t launch_ising2d_sweep(Sim* s, long long* acc);
+unsigned long long accept_cut(int pref, double dE, double beta);
 
 // One Metropolis sweep; when slot >= 0 the new state's observables are
 // accumulated into that slot.
@@ -118,10 +169,13 @@ cudaError_t launch_metropolis_int8(Sim* s, int slot)
         return err;
     }
     int8_t* st = (int8_t*)s->state[s->cur];
+    err = ensure_cuts(s);
+    if (err != cudaSuccess) return err;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
         const int g = grid_for(s->n / 2, 256);
         for (int c = 0; c < 2; ++c) {
-            metro_int8_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, s->replica);
+            metro_int8_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, s->replica,
+                                                          s->d_cuts, s->max_degree);
             s->launches++;
         }
     } else {
@@ -129,7 +183,8 @@ cudaError_t launch_metropolis_int8(Sim* s, int slot)
             const int64_t b = s->colour_ptr[c], cnt = s->colour_ptr[c + 1] - b;
             if (cnt == 0) continue;
             metro_int8_csr<<<grid_for(cnt, 256), 256, 0, s->stream>>>(s->md, s->csr, st, s->d_order, b, cnt, key,
-                                                                       (uint32_t)s->sweep, s->replica);
+                                                                       (uint32_t)s->sweep, s->replica, s->d_cuts,
+                                                                       s->max_degree);
             s->launches++;
         }
     }
