@@ -442,29 +442,18 @@ def run_workload(args, ws, rank, local):
 
 def run_engine(args, ws, rank, local):
     import torch
-    import torch.distributed as dist
 
     import marqov_b200 as M
     from marqov_b200 import _lib
+    from marqov_b200.replicas import ReplicaGroup
 
     torch.cuda.set_device(local)
-    if ws > 1:
-        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
-
-    def barrier():
-        if ws > 1:
-            dist.barrier()
-
-    def max_over_ranks(x: float) -> float:
-        if ws == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    group = ReplicaGroup("nccl")
+    barrier, max_over_ranks = group.barrier, group.max
 
     L = args.L
     n = L * L
-    cfg = M.Config(seed=20240601, repid=rank, ncluster=0, nmetro=args.nmetro, device=local)
+    cfg = M.Config(seed=20240601, repid=group.replica_id(), ncluster=0, nmetro=args.nmetro, device=local)
     core = M.makeCore(M.RegularHypercubic(L, 2), cfg, M.Ising(-1.0), BETA_C)
     stream = torch.cuda.Stream()
     core.set_stream(stream.cuda_stream)
@@ -560,9 +549,7 @@ def run_engine(args, ws, rank, local):
                                     "sample": f"unavailable: {exc}"}
     if rank == 0:
         print(json.dumps(line))
-    if ws > 1:
-        dist.barrier()
-        dist.destroy_process_group()
+    group.close()
     return 0
 
 
