@@ -237,6 +237,9 @@ class RefHarness:
         lib.ref_farm_magnetisation.restype = C.c_longlong
         lib.ref_farm_magnetisation.argtypes = [C.c_void_p, C.c_int]
         lib.ref_farm_destroy.argtypes = [C.c_void_p]
+        lib.ref_emcs_ising2d.restype = C.c_int
+        lib.ref_emcs_ising2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int,
+                                         C.c_int, _f64p, _f64p]
         self.lib = lib
 
     def sweeps_int(self, kind, g: Graph, s, J, D, beta, seed, replica, sweep0, nsweeps, want_obs=True):
@@ -285,6 +288,14 @@ class RefHarness:
         out = np.zeros(n, np.uint64)
         self.lib.ref_mt_words(n, out)
         return out
+
+    def emcs_ising2d(self, L, J, beta, seed, ncluster, nmetro, ntherm, nmeas):
+        """The reference's own EMCS loop (random-site order, mt19937_64):
+        per measured EMCS (E, |m|) and mean cluster size."""
+        obs = np.zeros(2 * nmeas, np.float64)
+        mc = np.zeros(nmeas, np.float64)
+        assert self.lib.ref_emcs_ising2d(L, J, beta, seed, ncluster, nmetro, ntherm, nmeas, obs, mc) == 0
+        return obs.reshape(nmeas, 2), mc
 
     def farm(self, length, beta, nthreads, seed=12345):
         return RefFarm(self.lib, length, beta, nthreads, seed)

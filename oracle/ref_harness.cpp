@@ -524,4 +524,44 @@ long long ref_farm_magnetisation(void* h, int t)
 
 void ref_farm_destroy(void* h) { delete (Farm*)h; }
 
+// The reference's own EMCS (the loop of src/libmarqov/emcs.h:69-109: ncluster
+// Wolff<Ising<int>> clusters seeded at rng.integer(N), then N random-site
+// Metropolis<Ising<int>> moves per sweep) for the 2D Ising model on
+// FixedDimRegularHypercubic<2> with RNGCache<mt19937_64>, from the
+// reference's initstatespace; obs receives (Energy, Magnetization) after each
+// of the nmeas measured EMCS, mean_cluster the mean cluster size per EMCS.
+int ref_emcs_ising2d(int len, double J, double beta, uint64_t seed, int ncluster, int nmetro, int ntherm,
+                     int nmeas, double* obs, double* mean_cluster)
+{
+    typedef FixedDimRegularHypercubic<2> G;
+    G grid(len);
+    Ising<int> ham(J);
+    MARQOV::Space<std::array<int, 1>, G> ss(grid.size());
+    RNGCache<std::mt19937_64> rng(seed);
+    ham.initstatespace(ss, grid, rng);
+    MARQOV::Wolff<Ising<int>, G> wolff;
+    const int N = (int)grid.size();
+    for (int t = 0; t < ntherm + nmeas; ++t) {
+        double avg = 0;
+        for (int c = 0; c < ncluster; ++c) {
+            const int site = rng.integer(N);
+            avg += (double)wolff.move(ham, grid, ss, rng, beta, site);
+        }
+        for (int j = 0; j < nmetro; ++j)
+            for (int i = 0; i < N; ++i) {
+                const int rsite = rng.integer(N);
+                MARQOV::Metropolis<Ising<int>, G>::move(ham, grid, ss, rng, beta, rsite);
+            }
+        if (t >= ntherm) {
+            const int k = t - ntherm;
+            Magnetization mo;
+            Energy<Ising<int>> eo(ham);
+            obs[2 * k] = eo.measure(ss, grid);
+            obs[2 * k + 1] = mo.measure(ss, grid);
+            if (mean_cluster) mean_cluster[k] = ncluster ? avg / ncluster : 0.0;
+        }
+    }
+    return 0;
+}
+
 }  // extern "C"
