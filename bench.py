@@ -363,25 +363,18 @@ def workload_rgg(M, torch, sweeps=20):
 
 def workload_ea(M, torch, sweeps=20, realisations=32):
     """Config 5b: 32 +-J Edwards-Anderson realisations on 3D L=32, beta=0.9,
-    Metropolis only."""
-    st = torch.cuda.Stream()
-    cores = []
-    try:
-        for r in range(realisations):
-            c = M.makeCore(M.RegularRandomBond(32, 3, 0.5, seed=100 + r), M.Config(seed=500 + r, repid=r),
-                           M.EdwardsAndersonIsing(-1.0), 0.9)
-            c.set_stream(st.cuda_stream)
-            c.init()
-            c.metropolis(2)
-            cores.append(c)
-        t_m = timed(torch, st, lambda: [c.metropolis(sweeps) for c in cores])
-    finally:
-        for c in cores:
-            c.close()
+    Metropolis only, as one batch (CSR members with their own bonds)."""
+    members = [(M.RegularRandomBond(32, 3, 0.5, seed=100 + r), M.Config(seed=500 + r, repid=r),
+                M.EdwardsAndersonIsing(-1.0), 0.9) for r in range(realisations)]
+    with M.Batch(members, graph_steps=sweeps) as b:
+        b.init()
+        b.emcs(2, ncluster=0, nmetro=1)
+        st = torch.cuda.ExternalStream(stream_of(b.member(0)))
+        t_m = timed(torch, st, lambda: b.emcs(sweeps, ncluster=0, nmetro=1))
     n = 32 ** 3 * realisations
     rate = n * sweeps / (t_m * 1e9)
-    return {"workload": "32 +-J Edwards-Anderson realisations, 3D L=32, beta=0.9 (one handle each)",
-            "unit": UNIT, "value": rate,
+    return {"workload": "32 +-J Edwards-Anderson realisations, 3D L=32, beta=0.9, one batch",
+            "unit": UNIT, "value": rate, "includes": "a measurement per sweep (EMCS = 1 sweep)",
             "roofline": {"bytes_per_update": 5, "frac_of_hbm": hbm_frac(5, rate), "note": "L2-resident"}}
 
 
@@ -402,7 +395,7 @@ def workload_phi4_autograd(M, torch, n_therm=10, n_meas=40):
     t_b = timed(torch, st, lambda: obs[:, 0].sum().backward())
     sites = R * ens.sites
     rate = sites * (n_therm + n_meas) / (t_f * 1e9)
-    return {"workload": "3D phi^4 L=64 x 64 beta in [0.36,0.38], lambda=1.1, EMCS = 1 Wolff + 1 sweep",
+    return {"workload": "3D phi^4 L=64 x 64 beta in [0.36,0.38], lambda=1.1, EMCS = 1 Wolff + 1 sweep, one batch",
             "unit": UNIT, "value": rate, "emcs_per_chain": n_therm + n_meas,
             "roofline": {"bytes_per_update": 8, "frac_of_hbm": hbm_frac(8, rate)},
             "backward_ms": 1e3 * t_b, "dE_dbeta_mean": float(beta.grad.mean()),

@@ -221,10 +221,12 @@ MQV_API mqv_status mqv_launch_count(mqv_sim* sim, uint64_t* count);
  * MARQOV's scheduler (one Core per thread, src/libmarqov/marqovscheduler.h:
  * 64-494, createSimfromParameter / start at :75-144, 223-273) as one set of
  * batched kernels per EMCS, captured once in a CUDA graph and replayed.
- * Members: int8 models (Ising, embedded Ising, Potts, Blume-Capel) on
- * hypercubic lattices of any sizes, each with its own coefficients, beta,
- * seed and replica id.  A batched run produces the same states, cluster
- * sizes and observables as running each member handle with mqv_emcs. */
+ * Members: any model on hypercubic or CSR lattices of any sizes, each with
+ * its own coefficients, beta, seed, replica id and bonds (disorder
+ * realisations); one batch holds either int8 members (Ising, embedded Ising,
+ * Potts, Blume-Capel, Edwards-Anderson) or float members (Heisenberg, XXZ,
+ * phi^4).  A batched run produces the same states, cluster sizes and
+ * observables as running each member handle with mqv_emcs. */
 typedef struct mqv_sim_spec {
     mqv_model_desc model;
     mqv_lattice_desc lattice;
@@ -246,6 +248,11 @@ MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* batch, int32_t steps);
  * (record e * n + i is member i after EMCS e); mean_cluster likewise. */
 MQV_API mqv_status mqv_batch_emcs(mqv_batch* batch, int32_t n_emcs, int32_t ncluster, int32_t nmetro, mqv_obs* obs,
                                   double* mean_cluster);
+/* No counterpart in the reference.  mqv_batch_emcs that keeps each member's
+ * raw lattice sums on the device (as mqv_emcs_samples): d_samples is a
+ * DEVICE pointer to [n][n_emcs][4] doubles. */
+MQV_API mqv_status mqv_batch_emcs_samples(mqv_batch* batch, int32_t n_emcs, int32_t ncluster, int32_t nmetro,
+                                          double* d_samples);
 MQV_API mqv_status mqv_batch_launch_count(mqv_batch* batch, uint64_t* count);
 
 /* Self test: Philox blocks for n counters (c0 = i, other words given) computed

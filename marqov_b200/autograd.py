@@ -24,7 +24,7 @@ from dataclasses import dataclass
 import torch
 
 from . import _lib as L
-from .core import Config, makeCore
+from .core import Batch, Config
 from .hamiltonians import Phi4
 from .lattices import RegularHypercubic
 
@@ -58,20 +58,20 @@ class Phi4Ensemble:
             raise ValueError("beta and lambda need one entry per chain")
         dev = torch.device("cuda", self.device)
         out = torch.empty((b.numel(), self.n_meas, 4), dtype=torch.float64, device=dev)
-        stream = torch.cuda.current_stream(dev)
-        lib = L.load()
+        members = []
         for r in range(b.numel()):
             rep = 0 if self.common_random_numbers else r
             cfg = Config(seed=self.seed, repid=rep, device=self.device, ncluster=self.ncluster, nmetro=self.nmetro)
-            ham = Phi4(float(b[r]), float(lm[r]), self.mass, self.amp)
-            with makeCore(RegularHypercubic(self.L, self.dim), cfg, ham, float(b[r])) as core:
-                core.set_stream(stream.cuda_stream)
-                core.init()
-                if self.n_therm:
-                    core.emcs(self.n_therm, measure=False)
-                L.check(lib.mqv_emcs_samples(core.handle, self.n_meas, self.ncluster, self.nmetro,
-                                             C.c_void_p(out[r].data_ptr())))
-                core.synchronize()
+            members.append((RegularHypercubic(self.L, self.dim), cfg,
+                            Phi4(float(b[r]), float(lm[r]), self.mass, self.amp), float(b[r])))
+        torch.cuda.current_stream(dev).synchronize()
+        # all chains in one batch (batched kernels replayed from a CUDA graph)
+        with Batch(members) as bt:
+            bt.init()
+            if self.n_therm:
+                bt.emcs(self.n_therm, self.ncluster, self.nmetro)
+            L.check(L.load().mqv_batch_emcs_samples(bt._h, self.n_meas, self.ncluster, self.nmetro,
+                                                    C.c_void_p(out.data_ptr())))
         return out
 
 

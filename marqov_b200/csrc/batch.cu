@@ -1,59 +1,98 @@
-// Batched elementary Monte Carlo steps over many independent int8
-// simulations (replicas, temperatures, lattice sizes) on one GPU.
+// Batched elementary Monte Carlo steps over many independent simulations
+// (replicas, temperatures, disorder realisations, lattice sizes) on one GPU.
 //
 // MARQOV runs such a farm as one simulation per CPU thread
 // (src/libmarqov/marqovscheduler.h:64-494); on the GPU the same farm is a
-// handful of kernels per EMCS that each cover every replica:
-//   batch_wolff_int8    one CTA per replica grows and flips its cluster,
-//   batch_metro_int8    one launch per colour over the sites of that colour of
-//                       all replicas (flattened, block -> first replica table),
-//   batch_measure_int8  CTAs (part, replica) accumulate each replica's
-//                       observables,
-//   batch_tick          advances the EMCS counter.
+// handful of kernels per EMCS that each cover every member:
+//   batch_wolff      one CTA per member grows and flips/reflects its cluster,
+//   batch_metro      one launch per colour over the sites of that colour of
+//                    all members (flattened, block -> first member table);
+//                    members on hypercubic lattices use the checkerboard,
+//                    CSR members their own colouring,
+//   batch_measure    CTAs (part, member) accumulate each member's observables,
+//   batch_tick       advances the EMCS counter.
 // Every per-step number (sweep and cluster serials, measurement slot) is
 // derived on the device from that counter, so the kernels of one EMCS form a
-// fixed sequence: it is captured once into a CUDA graph and replayed.
-// The per-replica arithmetic is that of the per-handle kernels, keyed by each
-// replica's (seed, replica id, sweep, site), so a batched run equals running
-// every member handle on its own, bit for bit.
+// fixed sequence: it is captured once into a CUDA graph and replayed.  The
+// per-member arithmetic is that of the per-handle kernels, keyed by each
+// member's (seed, replica id, sweep, site), so a batched run equals running
+// every member handle on its own, bit for bit.  A batch holds either int8 or
+// float members.
 #include <cuda_runtime.h>
 
 #include "batch.h"
+#include "f32_site.cuh"
 #include "int8_site.cuh"
 #include "wolff_int8.cuh"
 
 namespace mqv {
 
-__global__ void batch_metro_int8(const BatchRep* __restrict__ reps, const int64_t* __restrict__ half_prefix,
-                                 const int32_t* __restrict__ block_rep, int64_t total, int colour,
-                                 const BatchCtr* __restrict__ ctr, int nmetro, int j)
+template <bool F32, class Lat>
+__device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep)
+{
+    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica);
+    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D);
+}
+
+template <bool F32>
+__global__ void batch_metro(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                            const int32_t* __restrict__ block_rep, const int32_t* __restrict__ cbegin, int ncol,
+                            int64_t total, int colour, const BatchCtr* __restrict__ ctr, int nmetro, int j)
 {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (g >= total) return;
     int r = block_rep[blockIdx.x];
-    while (g >= half_prefix[r + 1]) ++r;
+    while (g >= prefix[r + 1]) ++r;
     const BatchRep& R = reps[r];
+    const int64_t t = g - prefix[r];
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
-    int8_site(R.md, R.st, R.s, parity_site(R.st, g - half_prefix[r], colour), R.key, sweep, R.replica, R.cuts, R.D);
+    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
+        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep);
+    else
+        batch_site<F32>(R, R.csr, (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t], sweep);
 }
 
-__global__ void __launch_bounds__(1024) batch_wolff_int8(const BatchRep* __restrict__ reps,
-                                                         const BatchCtr* __restrict__ ctr, int ncluster, int c,
-                                                         int32_t* __restrict__ csize, int nrep)
+template <bool F32>
+__global__ void __launch_bounds__(1024) batch_wolff(const BatchRep* __restrict__ reps,
+                                                    const BatchCtr* __restrict__ ctr, int ncluster, int c,
+                                                    int32_t* __restrict__ csize, int nrep)
 {
     const BatchRep& R = reps[blockIdx.x];
     const uint32_t e = ctr->e, slot = e - ctr->ebase;
     const uint32_t serial = R.cluster0 + e * (uint32_t)ncluster + (uint32_t)c;
-    wolff_int8_cluster(R.w, R.st, R.s, R.visited, R.queue, csize + ((size_t)slot * ncluster + c) * nrep + blockIdx.x,
-                       R.key, serial, tag(kWolffSeed, R.replica), tag(kWolffBond, R.replica));
+    int32_t* out = csize + ((size_t)slot * ncluster + c) * nrep + blockIdx.x;
+    const uint32_t tgs = tag(kWolffSeed, R.replica), tgb = tag(kWolffBond, R.replica);
+    if (F32) {
+        if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
+            wolff_f32_cluster(R.md, R.st, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+        else
+            wolff_f32_cluster(R.md, R.csr, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+    } else {
+        if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
+            wolff_int8_cluster(R.w, R.st, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+        else
+            wolff_int8_cluster(R.w, R.csr, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+    }
 }
 
-__global__ void batch_measure_int8(const BatchRep* __restrict__ reps, const BatchCtr* __restrict__ ctr,
-                                   long long* __restrict__ acc, int nrep)
+template <bool F32>
+__global__ void batch_measure(const BatchRep* __restrict__ reps, const BatchCtr* __restrict__ ctr,
+                              long long* __restrict__ acc, int nrep)
 {
     const BatchRep& R = reps[blockIdx.y];
     const uint32_t slot = ctr->e - ctr->ebase;
-    measure_int8_part(R.md, R.st, R.s, acc + ((size_t)slot * nrep + blockIdx.y) * kAccStride, blockIdx.x, gridDim.x);
+    long long* a = acc + ((size_t)slot * nrep + blockIdx.y) * kAccStride;
+    if (F32) {
+        if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
+            measure_f32_part(R.md, R.st, (const float*)R.s, (double*)a, blockIdx.x, gridDim.x);
+        else
+            measure_f32_part(R.md, R.csr, (const float*)R.s, (double*)a, blockIdx.x, gridDim.x);
+    } else {
+        if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
+            measure_int8_part(R.md, R.st, (const int8_t*)R.s, a, blockIdx.x, gridDim.x);
+        else
+            measure_int8_part(R.md, R.csr, (const int8_t*)R.s, a, blockIdx.x, gridDim.x);
+    }
 }
 
 __global__ void batch_tick(BatchCtr* ctr) { ctr->e += 1u; }
@@ -64,33 +103,63 @@ __global__ void batch_chunk_start(BatchCtr* ctr, uint32_t e)
     ctr->ebase = e;
 }
 
-// acc/out: slot-major, entry k = slot * nrep + replica
-__global__ void batch_finalize_int8(const BatchRep* __restrict__ reps, const long long* __restrict__ acc, int nslots,
-                                    int nrep, double* __restrict__ out)
+// acc/out: slot-major, entry k = slot * nrep + member
+__global__ void batch_finalize(const BatchRep* __restrict__ reps, const long long* __restrict__ acc, int nslots,
+                               int nrep, int f32, double* __restrict__ out)
 {
     const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= (int64_t)nslots * nrep) return;
     const BatchRep& R = reps[k % nrep];
-    finalize_int8_one(R.md, R.st.n, acc + (size_t)k * kAccStride, out + 4 * (size_t)k);
+    const int64_t n = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.n : R.csr.n;
+    if (f32) finalize_f32_one(R.md, n, (const double*)(acc + (size_t)k * kAccStride), out + 4 * (size_t)k);
+    else finalize_int8_one(R.md, n, acc + (size_t)k * kAccStride, out + 4 * (size_t)k);
+}
+
+// raw sums (interaction, sum s, sum s^2, sum (s^2 - 1)^2) -> samples[r][e0 + slot][4]
+__global__ void batch_samples(const long long* __restrict__ acc, int nslots, int nrep, int f32, int e0, int n_total,
+                              double* __restrict__ out)
+{
+    const int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= (int64_t)nslots * nrep) return;
+    const int slot = (int)(k / nrep), r = (int)(k % nrep);
+    const long long* a = acc + (size_t)k * kAccStride;
+    double* o = out + ((size_t)r * n_total + e0 + slot) * 4;
+    if (f32) {
+        const double* d = (const double*)a;
+        o[0] = d[kAccEne];
+        o[1] = d[kAccMag];
+        o[2] = d[kAccSq];
+        o[3] = d[kAccQ4];
+    } else {
+        o[0] = (double)a[kAccEne];
+        o[1] = (double)a[kAccMag];
+        o[2] = (double)a[kAccSq];
+        o[3] = 0.0;
+    }
 }
 
 // ---- launchers (stream-ordered; all capturable) ------------------------------------
 
-cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro, uint64_t* launches)
+template <bool F32>
+static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro)
 {
-    for (int c = 0; c < ncluster; ++c) {
-        batch_wolff_int8<<<b.nrep, 1024, 0, st>>>(b.reps, b.ctr, ncluster, c, b.csize, b.nrep);
-        ++*launches;
-    }
+    for (int c = 0; c < ncluster; ++c)
+        batch_wolff<F32><<<b.nrep, 1024, 0, st>>>(b.reps, b.ctr, ncluster, c, b.csize, b.nrep);
     for (int j = 0; j < nmetro; ++j)
-        for (int colour = 0; colour < 2; ++colour) {
-            batch_metro_int8<<<b.metro_blocks, kBatchMetroThreads, 0, st>>>(b.reps, b.half_prefix, b.block_rep,
-                                                                             b.total_half, colour, b.ctr, nmetro, j);
-            ++*launches;
+        for (int colour = 0; colour < b.ncol; ++colour) {
+            if (b.total[colour] == 0) continue;
+            batch_metro<F32><<<b.blocks[colour], kBatchMetroThreads, 0, st>>>(
+                b.reps, b.prefix + (size_t)colour * (b.nrep + 1), b.block_rep + b.block_off[colour], b.cbegin, b.ncol,
+                b.total[colour], colour, b.ctr, nmetro, j);
         }
-    batch_measure_int8<<<dim3(b.meas_parts, b.nrep), 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep);
+    batch_measure<F32><<<dim3(b.meas_parts, b.nrep), 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep);
     batch_tick<<<1, 1, 0, st>>>(b.ctr);
-    *launches += 2;
+}
+
+cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro)
+{
+    if (b.f32) launch_emcs_t<true>(b, st, ncluster, nmetro);
+    else launch_emcs_t<false>(b, st, ncluster, nmetro);
     return cudaGetLastError();
 }
 
@@ -103,7 +172,15 @@ cudaError_t batch_launch_chunk_start(const BatchLaunch& b, cudaStream_t st, uint
 cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nslots, double* out)
 {
     const int64_t n = (int64_t)nslots * b.nrep;
-    batch_finalize_int8<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(b.reps, b.acc, nslots, b.nrep, out);
+    batch_finalize<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(b.reps, b.acc, nslots, b.nrep, b.f32, out);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_launch_samples(const BatchLaunch& b, cudaStream_t st, int nslots, int e0, int n_total,
+                                 double* samples)
+{
+    const int64_t n = (int64_t)nslots * b.nrep;
+    batch_samples<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(b.acc, nslots, b.nrep, b.f32, e0, n_total, samples);
     return cudaGetLastError();
 }
 

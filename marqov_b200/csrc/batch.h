@@ -4,19 +4,22 @@
 
 namespace mqv {
 
-// One replica of a batch as the batched kernels see it.
+// One member of a batch as the batched kernels see it.
 struct BatchRep {
     ModelDev md;
-    StencilDev st;
-    WolffDev w;
+    StencilDev st;              // hypercubic members
+    CSRDev csr;                 // CSR members
+    int lat_kind;               // MQV_LATTICE_*
+    const int32_t* order;       // CSR: sites grouped by colour
+    WolffDev w;                 // int8 activation rule
     Key key;
     uint32_t replica;
     uint32_t sweep0, cluster0;  // the member handle's counters when the run started
-    int8_t* s;                  // state (reference site order)
+    void* s;                    // state: int8_t or float, reference site order
     uint32_t* visited;          // Wolff scratch of the member handle
     int32_t* queue;
-    const unsigned long long* cuts;  // the member's Metropolis cut table
-    int D;                           // its maximum degree
+    const unsigned long long* cuts;  // int8: the member's Metropolis cut table
+    int D;                           // int8: its maximum degree
 };
 
 // Device counters of a run: EMCS done, first EMCS of the current chunk
@@ -28,22 +31,39 @@ struct BatchCtr {
 
 constexpr int kBatchMetroThreads = 256;
 
-// Device pointers and shapes the launchers need.
+// Device tables and shapes the launchers need.  Colour c's work is the
+// concatenation over members of their colour-c sites: prefix + c * (nrep + 1)
+// holds its prefix sums, block_rep + block_off[c] the first member of each of
+// its blocks, cbegin[r * ncol + c] member r's offset into its colour order.
 struct BatchLaunch {
     const BatchRep* reps;
-    const int64_t* half_prefix;  // nrep + 1 prefix sums of n / 2
-    const int32_t* block_rep;    // first replica of each metropolis block
-    int64_t total_half;
-    int metro_blocks;
-    int meas_parts;              // measurement CTAs per replica
     int nrep;
+    int f32;                     // float members (else int8)
+    int ncol;                    // colours of the member with the most
+    const int64_t* prefix;       // [ncol][nrep + 1]
+    const int32_t* block_rep;    // [sum of blocks]
+    const int32_t* cbegin;       // [nrep][ncol]
+    const int* block_off;        // host: [ncol] offsets into block_rep
+    const int* blocks;           // host: [ncol] blocks of each colour
+    const int64_t* total;        // host: [ncol] work items of each colour
+    int meas_parts;              // measurement CTAs per member
     BatchCtr* ctr;
-    long long* acc;              // slot-major accumulators
+    long long* acc;              // slot-major accumulators (int64, or FP64 in the same words)
     int32_t* csize;              // cluster sizes: (slot * ncluster + c) * nrep + r
 };
 
-cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro, uint64_t* launches);
+cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro);
 cudaError_t batch_launch_chunk_start(const BatchLaunch& b, cudaStream_t st, uint32_t e);
 cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nslots, double* out);
+// raw sums of the chunk's slots -> samples[r][e0 + slot][4] (n_total EMCS per member)
+cudaError_t batch_launch_samples(const BatchLaunch& b, cudaStream_t st, int nslots, int e0, int n_total,
+                                 double* samples);
+// kernel launches of one EMCS
+inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int nmetro)
+{
+    int live = 0;
+    for (int c = 0; c < b.ncol; ++c) live += b.total[c] > 0;
+    return (uint64_t)ncluster + (uint64_t)nmetro * (uint64_t)live + 2ull;
+}
 
 }  // namespace mqv

@@ -845,16 +845,20 @@ struct Batch {
     cudaStream_t stream = nullptr;
     std::vector<Sim*> sims;
     int nrep = 0;
-    std::vector<BatchRep> reps;  // host copy of the replica table (kept alive for the upload)
+    bool f32 = false;
+    std::vector<BatchRep> reps;  // host copy of the member table (kept alive for the upload)
     BatchRep* d_reps = nullptr;
-    int64_t* d_half_prefix = nullptr;
+    int64_t* d_prefix = nullptr;
     int32_t* d_block_rep = nullptr;
+    int32_t* d_cbegin = nullptr;
+    std::vector<int> block_off, blocks;
+    std::vector<int64_t> total;
     BatchCtr* d_ctr = nullptr;
     long long* d_acc = nullptr;
     double* d_obs = nullptr;
     int32_t* d_csize = nullptr;
-    int cap_slots = 0;   // measurement slots in d_acc / d_obs (per replica)
-    int cap_cslots = 0;  // cluster-size slots in d_csize (per replica)
+    int cap_slots = 0;   // measurement slots in d_acc / d_obs (per member)
+    int cap_cslots = 0;  // cluster-size slots in d_csize (per member)
     BatchLaunch L{};
     cudaGraphExec_t g_one = nullptr, g_many = nullptr;
     int g_ncluster = -1, g_nmetro = -1, g_steps = 0;
@@ -877,8 +881,8 @@ static void free_batch(Batch* b)
     if (b->stream) cudaStreamSynchronize(b->stream);
     free_graphs(b);
     for (Sim* s : b->sims) free_sim(s);
-    for (void* p : {(void*)b->d_reps, (void*)b->d_half_prefix, (void*)b->d_block_rep, (void*)b->d_ctr, (void*)b->d_acc,
-                    (void*)b->d_obs, (void*)b->d_csize})
+    for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin, (void*)b->d_ctr,
+                    (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize})
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -912,16 +916,130 @@ static mqv_status batch_capacity(Batch* b, int slots, int cslots)
 static mqv_status batch_capture(Batch* b, int steps, int ncluster, int nmetro, cudaGraphExec_t* out)
 {
     cudaGraph_t graph = nullptr;
-    uint64_t dummy = 0;
     MQV_CK(cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
-    for (int k = 0; k < steps && e == cudaSuccess; ++k) e = batch_launch_emcs(b->L, b->stream, ncluster, nmetro, &dummy);
+    for (int k = 0; k < steps && e == cudaSuccess; ++k) e = batch_launch_emcs(b->L, b->stream, ncluster, nmetro);
     const cudaError_t e2 = cudaStreamEndCapture(b->stream, &graph);
     MQV_CK(e);
     MQV_CK(e2);
     e = cudaGraphInstantiate(out, graph, 0);
     cudaGraphDestroy(graph);
     MQV_CK(e);
+    return MQV_OK;
+}
+
+static bool batch_kind_ok(int k)
+{
+    return k == MQV_MODEL_ISING || k == MQV_MODEL_ISING_EMBED || k == MQV_MODEL_POTTS || k == MQV_MODEL_BLUME_CAPEL ||
+           k == MQV_MODEL_EA || k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ;
+}
+
+// n_emcs EMCS of every member; observables / cluster means to the host, raw
+// sums to the device samples buffer ([member][n_emcs][4]), each when given.
+static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_obs* obs, double* mean_cluster,
+                            double* d_samples)
+{
+    DeviceGuard guard_(b->device);
+    if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
+    if (ncluster > 64 || nmetro > 64) return fail(MQV_ERR_INVALID_ARG, "at most 64 clusters and 64 sweeps per EMCS");
+    for (Sim* s : b->sims) {
+        if (!s->initialised) return fail(MQV_ERR_STATE, "state of a batch member not initialised");
+        if (!b->f32) MQV_CK(ensure_cuts(s));
+        if (ncluster > 0) {
+            mqv_status st = check_wolff_supported(s);
+            if (st) return st;
+            st = ensure_wolff(s);
+            if (st) return st;
+        }
+    }
+    // member table at the start of the run
+    b->reps.assign((size_t)b->nrep, BatchRep{});
+    for (int i = 0; i < b->nrep; ++i) {
+        const Sim* s = b->sims[(size_t)i];
+        BatchRep& r = b->reps[(size_t)i];
+        r.md = s->md;
+        r.st = s->sten;
+        r.csr = s->csr;
+        r.lat_kind = s->lat_kind;
+        r.order = s->d_order;
+        if (!b->f32) r.w = wolff_int8_params(s->md);
+        r.key = make_key(s->seed);
+        r.replica = s->replica;
+        r.sweep0 = (uint32_t)s->sweep;
+        r.cluster0 = (uint32_t)s->cluster;
+        r.s = s->state[s->cur];
+        r.visited = s->d_visited;
+        r.queue = s->d_queue;
+        r.cuts = s->d_cuts;
+        r.D = s->max_degree;
+    }
+    MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
+                           b->stream));
+    const int CH = 256;  // EMCS per chunk of measurements
+    const int slots = std::min(CH, std::max(n_emcs, 1));
+    const long long* acc0 = b->d_acc;
+    const int32_t* csize0 = b->d_csize;
+    mqv_status st = batch_capacity(b, slots, slots * std::max(ncluster, 1));
+    if (st) return st;
+    if (b->d_acc != acc0 || b->d_csize != csize0) free_graphs(b);  // graphs hold the old pointers
+    const int K = std::max(1, std::min(b->graph_steps, CH));
+    if (b->g_ncluster != ncluster || b->g_nmetro != nmetro || b->g_steps != K || !b->g_one) {
+        free_graphs(b);
+        MQV_CK(cudaStreamSynchronize(b->stream));
+        st = batch_capture(b, 1, ncluster, nmetro, &b->g_one);
+        if (!st && K > 1) st = batch_capture(b, K, ncluster, nmetro, &b->g_many);
+        if (st) {
+            free_graphs(b);
+            return st;
+        }
+        b->g_ncluster = ncluster;
+        b->g_nmetro = nmetro;
+        b->g_steps = K;
+    }
+    const uint64_t per_emcs = batch_launches_per_emcs(b->L, ncluster, nmetro);
+    std::vector<int32_t> csz;
+    int done = 0;
+    while (done < n_emcs) {
+        const int ch = std::min(n_emcs - done, CH);
+        MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
+        MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
+        b->launches++;
+        int k = 0;
+        if (K > 1)
+            for (; k + K <= ch; k += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
+        for (; k < ch; ++k) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
+        b->launches += per_emcs * (uint64_t)ch;
+        if (d_samples) {
+            MQV_CK(batch_launch_samples(b->L, b->stream, ch, done, n_emcs, d_samples));
+            b->launches++;
+        }
+        if (obs) {
+            MQV_CK(batch_launch_finalize(b->L, b->stream, ch, b->d_obs));
+            b->launches++;
+            MQV_CK(cudaMemcpyAsync(obs + (size_t)done * b->nrep, b->d_obs, sizeof(double) * 4 * (size_t)ch * b->nrep,
+                                   cudaMemcpyDeviceToHost, b->stream));
+        }
+        if (mean_cluster && ncluster > 0) {
+            csz.resize((size_t)ch * ncluster * b->nrep);
+            MQV_CK(cudaMemcpyAsync(csz.data(), b->d_csize, sizeof(int32_t) * csz.size(), cudaMemcpyDeviceToHost,
+                                   b->stream));
+        }
+        MQV_CK(cudaStreamSynchronize(b->stream));
+        if (mean_cluster) {
+            for (int e = 0; e < ch; ++e)
+                for (int r = 0; r < b->nrep; ++r) {
+                    double a = 0;
+                    for (int c = 0; c < ncluster; ++c) a += (double)csz[((size_t)e * ncluster + c) * b->nrep + r];
+                    mean_cluster[(size_t)(done + e) * b->nrep + r] = ncluster > 0 ? a / ncluster : 0.0;
+                }
+        }
+        done += ch;
+    }
+    MQV_CK(cudaStreamSynchronize(b->stream));
+    for (Sim* s : b->sims) {
+        s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
+        s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
+    }
     return MQV_OK;
 }
 
@@ -936,13 +1054,18 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     *out = nullptr;
     const int device = specs[0].params.device;
     for (int i = 0; i < n; ++i) {
-        const int k = specs[i].model.kind;
-        if (!(k == MQV_MODEL_ISING || k == MQV_MODEL_ISING_EMBED || k == MQV_MODEL_POTTS || k == MQV_MODEL_BLUME_CAPEL))
-            return fail(MQV_ERR_UNSUPPORTED_TERM, "batches take int8 models (Ising, embedded Ising, Potts, Blume-Capel)");
-        if (specs[i].lattice.kind != MQV_LATTICE_HYPERCUBIC)
-            return fail(MQV_ERR_UNSUPPORTED_TERM, "batches take hypercubic lattices");
+        if (!batch_kind_ok(specs[i].model.kind))
+            return fail(MQV_ERR_UNSUPPORTED_TERM, "unsupported model kind in batch member " + std::to_string(i));
+        if (is_f32_kind(specs[i].model.kind) != is_f32_kind(specs[0].model.kind))
+            return fail(MQV_ERR_UNSUPPORTED_TERM, "a batch holds int8 members or float members, not both");
         if (specs[i].params.device != device) return fail(MQV_ERR_INVALID_ARG, "all members of a batch share one device");
     }
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return fail(MQV_ERR_NO_DEVICE, "no CUDA device available");
+    }
+    if (device < 0 || device >= ndev) return fail(MQV_ERR_INVALID_ARG, "device ordinal out of range");
     Batch* b = new (std::nothrow) Batch();
     if (!b) return fail(MQV_ERR_OUT_OF_MEMORY, "host allocation failed");
     b->device = device;
@@ -950,16 +1073,6 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         free_batch(b);
         return st;
     };
-    int ndev = 0;
-    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
-        cudaGetLastError();
-        delete b;
-        return fail(MQV_ERR_NO_DEVICE, "no CUDA device available");
-    }
-    if (device < 0 || device >= ndev) {
-        delete b;
-        return fail(MQV_ERR_INVALID_ARG, "device ordinal out of range");
-    }
     DeviceGuard g(device);
     if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) {
         set_error("cudaStreamCreate failed");
@@ -968,6 +1081,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     // members: ordinary handles on the batch's stream, one launch per colour
     // class (reference site order, no fused two-colour layout)
     b->nrep = n;
+    b->f32 = is_f32_kind(specs[0].model.kind);
     b->sims.reserve((size_t)n);
     for (int i = 0; i < n; ++i) {
         mqv_run_params p = specs[i].params;
@@ -982,29 +1096,49 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         st = mqv_set_stream(h, b->stream);
         if (st) return bail(st);
     }
-    // flattened half-site work of the colour launches
-    std::vector<int64_t> prefix((size_t)n + 1, 0);
+    // per-colour work: colour c concatenates every member's colour-c sites
+    int ncol = 0;
     int64_t nmax = 0;
-    for (int i = 0; i < n; ++i) {
-        prefix[i + 1] = prefix[i] + b->sims[i]->n / 2;
-        nmax = std::max(nmax, b->sims[i]->n);
+    for (Sim* s : b->sims) {
+        ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
+        nmax = std::max(nmax, s->n);
     }
-    const int64_t total = prefix[n];
-    const int64_t blocks = (total + kBatchMetroThreads - 1) / kBatchMetroThreads;
-    if (blocks >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
-    std::vector<int32_t> brep((size_t)blocks);
-    for (int64_t k = 0, r = 0; k < blocks; ++k) {
-        const int64_t first = k * kBatchMetroThreads;
-        while (first >= prefix[r + 1]) ++r;
-        brep[(size_t)k] = (int32_t)r;
+    std::vector<int64_t> prefix((size_t)ncol * (n + 1), 0);
+    std::vector<int32_t> cbegin((size_t)n * ncol, 0), brep;
+    b->block_off.assign((size_t)ncol, 0);
+    b->blocks.assign((size_t)ncol, 0);
+    b->total.assign((size_t)ncol, 0);
+    for (int c = 0; c < ncol; ++c) {
+        int64_t* pf = prefix.data() + (size_t)c * (n + 1);
+        for (int r = 0; r < n; ++r) {
+            const Sim* s = b->sims[(size_t)r];
+            int64_t cnt = 0;
+            if (c + 1 < (int)s->colour_ptr.size()) {
+                cnt = s->colour_ptr[(size_t)c + 1] - s->colour_ptr[(size_t)c];
+                cbegin[(size_t)r * ncol + c] = s->colour_ptr[(size_t)c];
+            }
+            pf[r + 1] = pf[r] + cnt;
+        }
+        const int64_t tot = pf[n];
+        const int64_t nb = (tot + kBatchMetroThreads - 1) / kBatchMetroThreads;
+        if ((int64_t)brep.size() + nb >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
+        b->block_off[(size_t)c] = (int)brep.size();
+        b->blocks[(size_t)c] = (int)nb;
+        b->total[(size_t)c] = tot;
+        for (int64_t k = 0, r = 0; k < nb; ++k) {
+            while (k * kBatchMetroThreads >= pf[r + 1]) ++r;
+            brep.push_back((int32_t)r);
+        }
     }
+    if (brep.empty()) brep.push_back(0);
     auto dcopy = [&](void** dst, const void* src, size_t bytes) -> mqv_status {
         MQV_CK(cudaMalloc(dst, bytes));
         MQV_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
         return MQV_OK;
     };
-    mqv_status st = dcopy((void**)&b->d_half_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
+    mqv_status st = dcopy((void**)&b->d_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
     if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
+    if (!st) st = dcopy((void**)&b->d_cbegin, cbegin.data(), sizeof(int32_t) * std::max<size_t>(cbegin.size(), 1));
     if (st) return bail(st);
     if (cudaMalloc(&b->d_reps, sizeof(BatchRep) * (size_t)n) != cudaSuccess ||
         cudaMalloc(&b->d_ctr, sizeof(BatchCtr)) != cudaSuccess) {
@@ -1013,12 +1147,16 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         return bail(MQV_ERR_OUT_OF_MEMORY);
     }
     b->L.reps = b->d_reps;
-    b->L.half_prefix = b->d_half_prefix;
-    b->L.block_rep = b->d_block_rep;
-    b->L.total_half = total;
-    b->L.metro_blocks = (int)blocks;
-    b->L.meas_parts = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 4095) / 4096));
     b->L.nrep = n;
+    b->L.f32 = b->f32 ? 1 : 0;
+    b->L.ncol = ncol;
+    b->L.prefix = b->d_prefix;
+    b->L.block_rep = b->d_block_rep;
+    b->L.cbegin = b->d_cbegin;
+    b->L.block_off = b->block_off.data();
+    b->L.blocks = b->blocks.data();
+    b->L.total = b->total.data();
+    b->L.meas_parts = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 4095) / 4096));
     b->L.ctr = b->d_ctr;
     *out = reinterpret_cast<mqv_batch*>(b);
     return MQV_OK;
@@ -1064,100 +1202,16 @@ MQV_API mqv_status mqv_batch_emcs(mqv_batch* h, int32_t n_emcs, int32_t ncluster
 {
     Batch* b = reinterpret_cast<Batch*>(h);
     if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
-    DeviceGuard guard_(b->device);
-    if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
-    if (ncluster > 64 || nmetro > 64) return fail(MQV_ERR_INVALID_ARG, "at most 64 clusters and 64 sweeps per EMCS");
-    for (Sim* s : b->sims) {
-        if (!s->initialised) return fail(MQV_ERR_STATE, "state of a batch member not initialised");
-        MQV_CK(ensure_cuts(s));
-        if (ncluster > 0) {
-            mqv_status st = check_wolff_supported(s);
-            if (st) return st;
-            st = ensure_wolff(s);
-            if (st) return st;
-        }
-    }
-    // replica table at the start of the run
-    b->reps.assign((size_t)b->nrep, BatchRep{});
-    for (int i = 0; i < b->nrep; ++i) {
-        const Sim* s = b->sims[(size_t)i];
-        BatchRep& r = b->reps[(size_t)i];
-        r.md = s->md;
-        r.st = s->sten;
-        r.w = wolff_int8_params(s->md);
-        r.key = make_key(s->seed);
-        r.replica = s->replica;
-        r.sweep0 = (uint32_t)s->sweep;
-        r.cluster0 = (uint32_t)s->cluster;
-        r.s = (int8_t*)s->state[s->cur];
-        r.visited = s->d_visited;
-        r.queue = s->d_queue;
-        r.cuts = s->d_cuts;
-        r.D = s->max_degree;
-    }
-    MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
-                           b->stream));
-    const int CH = 256;  // EMCS per chunk of measurements
-    const int slots = std::min(CH, std::max(n_emcs, 1));
-    const long long* acc0 = b->d_acc;
-    const int32_t* csize0 = b->d_csize;
-    mqv_status st = batch_capacity(b, slots, slots * std::max(ncluster, 1));
-    if (st) return st;
-    if (b->d_acc != acc0 || b->d_csize != csize0) free_graphs(b);  // graphs hold the old pointers
-    const int K = std::max(1, std::min(b->graph_steps, CH));
-    if (b->g_ncluster != ncluster || b->g_nmetro != nmetro || b->g_steps != K || !b->g_one) {
-        free_graphs(b);
-        MQV_CK(cudaStreamSynchronize(b->stream));
-        st = batch_capture(b, 1, ncluster, nmetro, &b->g_one);
-        if (!st && K > 1) st = batch_capture(b, K, ncluster, nmetro, &b->g_many);
-        if (st) {
-            free_graphs(b);
-            return st;
-        }
-        b->g_ncluster = ncluster;
-        b->g_nmetro = nmetro;
-        b->g_steps = K;
-    }
-    const uint64_t per_emcs = (uint64_t)ncluster + 2ull * (uint64_t)nmetro + 2ull;
-    std::vector<int32_t> csz;
-    int done = 0;
-    while (done < n_emcs) {
-        const int ch = std::min(n_emcs - done, CH);
-        MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
-        MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
-        b->launches++;
-        int k = 0;
-        if (K > 1)
-            for (; k + K <= ch; k += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
-        for (; k < ch; ++k) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
-        b->launches += per_emcs * (uint64_t)ch;
-        MQV_CK(batch_launch_finalize(b->L, b->stream, ch, b->d_obs));
-        b->launches++;
-        if (obs)
-            MQV_CK(cudaMemcpyAsync(obs + (size_t)done * b->nrep, b->d_obs, sizeof(double) * 4 * (size_t)ch * b->nrep,
-                                   cudaMemcpyDeviceToHost, b->stream));
-        if (mean_cluster && ncluster > 0) {
-            csz.resize((size_t)ch * ncluster * b->nrep);
-            MQV_CK(cudaMemcpyAsync(csz.data(), b->d_csize, sizeof(int32_t) * csz.size(), cudaMemcpyDeviceToHost,
-                                   b->stream));
-        }
-        MQV_CK(cudaStreamSynchronize(b->stream));
-        if (mean_cluster) {
-            for (int e = 0; e < ch; ++e)
-                for (int r = 0; r < b->nrep; ++r) {
-                    double a = 0;
-                    for (int c = 0; c < ncluster; ++c) a += (double)csz[((size_t)e * ncluster + c) * b->nrep + r];
-                    mean_cluster[(size_t)(done + e) * b->nrep + r] = ncluster > 0 ? a / ncluster : 0.0;
-                }
-        }
-        done += ch;
-    }
-    MQV_CK(cudaStreamSynchronize(b->stream));
-    for (Sim* s : b->sims) {
-        s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
-        s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
-    }
-    return MQV_OK;
+    return batch_run(b, n_emcs, ncluster, nmetro, obs, mean_cluster, nullptr);
+}
+
+MQV_API mqv_status mqv_batch_emcs_samples(mqv_batch* h, int32_t n_emcs, int32_t ncluster, int32_t nmetro,
+                                          double* d_samples)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (n_emcs > 0 && !d_samples) return fail(MQV_ERR_INVALID_ARG, "null sample buffer");
+    return batch_run(b, n_emcs, ncluster, nmetro, nullptr, nullptr, d_samples);
 }
 
 MQV_API mqv_status mqv_batch_launch_count(mqv_batch* h, uint64_t* count)

@@ -8,104 +8,11 @@
 // lattice-wide reductions accumulate in FP64.
 #include <cuda_runtime.h>
 
-#include "engine.h"
+#include "f32_site.cuh"
 
 namespace mqv {
 
 unsigned long long accept_cut(int pref, double dE, double beta);
-
-// set_to_rnddir for SymD = 3 (src/hamiltonian/util/randomdir.h:45-64): two
-// reals -> (1 - a0, sqrt(a0 (2 - a0)) sin(pi a1), sqrt(a0 (2 - a0)) cos(pi a1)).
-__device__ __forceinline__ void rnddir3(SubStream& rng, double v[3])
-{
-    const double a0 = 2.0 * rng.real(), a1 = 2.0 * rng.real();
-    const double r1 = sqrt(a0 * (2.0 - a0));
-    double sn, cs;
-    sincospi(a1, &sn, &cs);
-    v[0] = 1.0 - a0;
-    v[1] = r1 * sn;
-    v[2] = r1 * cs;
-}
-
-// Small-cap proposal: uniform on the cap cos(angle to old) >= cap, built in
-// the frame that rotates +z onto the old spin (mirrored in z on the southern
-// hemisphere), then normalised.
-__device__ __forceinline__ void smallcap3(SubStream& rng, const float o[3], double cap, double v[3])
-{
-    const double u0 = rng.real(), u1 = rng.real();
-    const double ca = 1.0 - u0 * (1.0 - cap);
-    const double sa = sqrt(fmax(0.0, 1.0 - ca * ca));
-    double sn, cs;
-    sincospi(2.0 * u1, &sn, &cs);
-    const double dx = sa * cs, dy = sa * sn, dz = ca;
-    const double x = o[0], y = o[1], z = o[2];
-    const double sg = z < 0 ? -1.0 : 1.0;
-    const double a = 1.0 / (1.0 + sg * z);
-    const double bxy = -x * y * a;
-    const double e1[3] = {1.0 - x * x * a, bxy, -x * sg};
-    const double e2[3] = {bxy, 1.0 - y * y * a, -y * sg};
-    double nv[3];
-#pragma unroll
-    for (int c = 0; c < 3; ++c) nv[c] = dx * e1[c] + dy * e2[c] + dz * (double)o[c];
-    const double nn = sqrt(nv[0] * nv[0] + nv[1] * nv[1] + nv[2] * nv[2]);
-#pragma unroll
-    for (int c = 0; c < 3; ++c) v[c] = nv[c] / nn;
-}
-
-template <class Lat>
-__device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, float* __restrict__ s, int64_t i,
-                                         Key key, uint32_t sweep, uint32_t replica)
-{
-    SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
-    const int deg = lat.degree(i);
-    if (m.symd == 1) {
-        // shift proposal old + amp * real(-1, 1) (Phi4_Initializer_Cartesian,
-        // src/hamiltonian/Phi4.h:44-57); interaction + Onsite_Quadratic +
-        // Onsite_Fourth_Minus_One (src/hamiltonian/Phi4.h:63-74,103-121)
-        const double r = 1.0 + (-1.0 - 1.0) * real01(rng.next());
-        const double old = s[i];
-        const float nwf = (float)(old + m.cap * r);
-        const double nw = nwf;
-        double sum = 0;
-        for (int t = 0; t < deg; ++t) sum += (double)s[lat.nbr(i, t)];
-        const double o2 = old * old, n2 = nw * nw;
-        const double dE = m.J * (nw - old) * sum + m.h * (n2 - o2) +
-                          m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
-        if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) s[i] = nwf;
-        return;
-    }
-    float* so = s + 3 * i;
-    const float o[3] = {so[0], so[1], so[2]};
-    double v[3];
-    if (m.proposal == MQV_PROPOSAL_SMALL_CAP) smallcap3(rng, o, m.cap, v);
-    else rnddir3(rng, v);  // SVInitializer for float vectors (initializers.h:74-80)
-    const float nf[3] = {(float)v[0], (float)v[1], (float)v[2]};
-    double nb[3] = {0, 0, 0};
-    for (int t = 0; t < deg; ++t) {
-        const float* sj = s + 3 * lat.nbr(i, t);
-        nb[0] += (double)sj[0];
-        nb[1] += (double)sj[1];
-        nb[2] += (double)sj[2];
-    }
-    const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
-    double dE = ((double)nf[0] - (double)o[0]) * nb[0];
-    dE += ((double)nf[1] - (double)o[1]) * nb[1];
-    dE += wz * ((double)nf[2] - (double)o[2]) * nb[2];
-    dE *= m.J;
-    if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) {
-        so[0] = nf[0];
-        so[1] = nf[1];
-        so[2] = nf[2];
-    }
-}
-
-__device__ __forceinline__ int64_t parity_site_f(const StencilDev& st, int64_t t, int colour)
-{
-    const int64_t i0 = 2 * t;
-    int par = 0;
-    for (int j = 1; j < st.dim; ++j) par += st.coord(i0, j);
-    return i0 + (((par & 1) != colour) ? 1 : 0);
-}
 
 __global__ void metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s, int colour, Key key,
                                   uint32_t sweep, uint32_t replica)
@@ -122,80 +29,16 @@ __global__ void metro_f32_csr(ModelDev m, CSRDev g, float* __restrict__ s, const
         f32_site(m, g, s, order[begin + t], key, sweep, replica);
 }
 
-// ---- measurement (FP64) ---------------------------------------------------------
-
-__device__ __forceinline__ double warp_sum_d(double v)
-{
-#pragma unroll
-    for (int o = 16; o; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
-
 template <class Lat>
 __global__ void measure_f32(ModelDev m, Lat lat, const float* __restrict__ s, double* __restrict__ acc)
 {
-    __shared__ double red[6][32];
-    double e = 0, mx = 0, my = 0, mz = 0, q2 = 0, q4 = 0;
-    const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < lat.n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int deg = lat.degree(i);
-        if (m.symd == 1) {
-            const double si = s[i];
-            double nb = 0;
-            for (int t = 0; t < deg; ++t) nb += (double)s[lat.nbr(i, t)];
-            e += si * nb;
-            mx += si;
-            const double p2 = si * si;
-            q2 += p2;
-            q4 += (p2 - 1.0) * (p2 - 1.0);
-        } else {
-            const double a = s[3 * i], b = s[3 * i + 1], c = s[3 * i + 2];
-            double na = 0, nb = 0, nc = 0;
-            for (int t = 0; t < deg; ++t) {
-                const float* sj = s + 3 * lat.nbr(i, t);
-                na += (double)sj[0];
-                nb += (double)sj[1];
-                nc += (double)sj[2];
-            }
-            e += a * na + b * nb + wz * c * nc;
-            mx += a;
-            my += b;
-            mz += c;
-            const double p2 = a * a + b * b + c * c;
-            q2 += p2;
-            q4 += (p2 - 1.0) * (p2 - 1.0);
-        }
-    }
-    double v[6] = {e, mx, my, mz, q2, q4};
-    const int wid = threadIdx.x >> 5;
-#pragma unroll
-    for (int k = 0; k < 6; ++k) {
-        v[k] = warp_sum_d(v[k]);
-        if ((threadIdx.x & 31) == 0) red[k][wid] = v[k];
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        double a = 0;
-        for (int k = 0; k < (int)(blockDim.x >> 5); ++k) a += red[threadIdx.x][k];
-        const int idx[6] = {kAccEne, kAccMag, kAccMagY, kAccMagZ, kAccSq, kAccQ4};
-        atomicAdd(acc + idx[threadIdx.x], a);
-    }
+    measure_f32_part(m, lat, s, acc, blockIdx.x, gridDim.x);
 }
 
 __global__ void finalize_f32(ModelDev m, int64_t n, const double* __restrict__ acc, int nslots, double* __restrict__ out)
 {
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nslots) return;
-    const double* a = acc + (size_t)k * kAccStride;
-    const double mag = a[kAccMag] * a[kAccMag] + a[kAccMagY] * a[kAccMagY] + a[kAccMagZ] * a[kAccMagZ];
-    const double mm = sqrt(mag) / (double)n;
-    double e = m.J * a[kAccEne] / (double)(2 * n);
-    if (m.kind == MQV_MODEL_PHI4) e += (m.h * a[kAccSq] + m.h2 * a[kAccQ4]) / (double)n;
-    const double m2 = mm * mm;
-    out[4 * k + 0] = e;
-    out[4 * k + 1] = mm;
-    out[4 * k + 2] = m2;
-    out[4 * k + 3] = m2 * m2;
+    if (k < nslots) finalize_f32_one(m, n, acc + (size_t)k * kAccStride, out + 4 * (size_t)k);
 }
 
 // ---- initial state --------------------------------------------------------------
@@ -218,108 +61,13 @@ __global__ void init_f32(ModelDev m, int64_t n, float* __restrict__ s, Key key, 
     }
 }
 
-// ---- embedded Wolff for float states ----------------------------------------------
-// Generic Wolff (src/libmarqov/wolff.h:72-126) with Embedder<Heisenberg>
-// (src/hamiltonian/Heisenberg.h:158-185: random unit r, reflection about the
-// plane normal to r) or Embedder<Phi4> for one component
-// (src/hamiltonian/Phi4.h:217-243: r = +-1, phi -> -phi).  A neighbour joins
-// when cpl = J (-a_cur) a_nbr > 0 (a = s.r before any flip) and
-// !update_accepted<2>(cpl) on the bond's keyed word.
-
 template <class Lat>
 __global__ void __launch_bounds__(1024) wolff_f32(ModelDev m, Lat lat, float* __restrict__ s,
                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
                                                   uint32_t tg_seed, uint32_t tg_bond)
 {
-    __shared__ int s_head, s_tail, s_next;
-    __shared__ float s_r[3];
-    const int64_t n = lat.n;
-    const int symd = m.symd;
-    if (threadIdx.x == 0) {
-        SubStream rng(key, 0u, serial, tg_seed);
-        const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
-        double r[3] = {1.0, 0.0, 0.0};
-        if (symd == 3) rnddir3(rng, r);
-        else if (rng.real() < 0.5) r[0] = -1.0;
-        s_r[0] = (float)r[0];
-        s_r[1] = (float)r[1];
-        s_r[2] = (float)r[2];
-        queue[0] = (int32_t)rsite;
-        atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
-        s_head = 0;
-        s_tail = 1;
-        s_next = 1;
-    }
-    __syncthreads();
-    const float r0 = s_r[0], r1 = s_r[1], r2 = s_r[2];
-    auto proj = [&](int64_t i) -> double {
-        if (symd == 3)
-            return (double)s[3 * i] * r0 + (double)s[3 * i + 1] * r1 + (double)s[3 * i + 2] * r2;
-        return (double)s[i] * r0;
-    };
-    const unsigned lane = threadIdx.x & 31;
-    while (true) {
-        const int head = s_head, tail = s_tail;
-        if (head >= tail) break;
-        for (int base = head; base < tail; base += blockDim.x) {
-            const int idx = base + threadIdx.x;
-            const bool live = idx < tail;
-            const int64_t cur = live ? queue[idx] : 0;
-            const int deg = live ? lat.degree(cur) : 0;
-            const double ac = live ? proj(cur) : 0.0;
-            const int maxdeg = __reduce_max_sync(0xffffffffu, deg);
-            for (int t = 0; t < maxdeg; ++t) {
-                bool add = false;
-                int64_t j = 0;
-                if (t < deg) {
-                    j = lat.nbr(cur, t);
-                    if (!(visited[j >> 5] & (1u << (j & 31)))) {
-                        const double cpl = m.J * (-ac) * proj(j);
-                        if (cpl > 0) {
-                            const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
-                            const uint64_t wd = lo64(philox(lo, serial, hi, tg_bond, key));
-                            if (!update_accepted(2, cpl, m.beta, wd)) {
-                                const uint32_t old = atomicOr(&visited[j >> 5], 1u << (j & 31));
-                                add = !(old & (1u << (j & 31)));
-                            }
-                        }
-                    }
-                }
-                const unsigned mask = __ballot_sync(0xffffffffu, add);
-                if (mask) {
-                    int pos = 0;
-                    if (lane == 0) pos = atomicAdd(&s_next, __popc(mask));
-                    pos = __shfl_sync(0xffffffffu, pos, 0);
-                    if (add) queue[pos + __popc(mask & ((1u << lane) - 1))] = (int32_t)j;
-                }
-            }
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            s_head = tail;
-            s_tail = s_next;
-        }
-        __syncthreads();
-    }
-    const int size = s_tail;
-    for (int k = threadIdx.x; k < size; k += blockDim.x) {
-        const int32_t i = queue[k];
-        if (symd == 3) {
-            float* v = s + 3 * (int64_t)i;
-            const double d = (double)v[0] * r0 + (double)v[1] * r1 + (double)v[2] * r2;
-            const double w0 = (double)v[0] - 2.0 * d * r0, w1 = (double)v[1] - 2.0 * d * r1,
-                         w2 = (double)v[2] - 2.0 * d * r2;
-            const double nn = sqrt(w0 * w0 + w1 * w1 + w2 * w2);
-            v[0] = (float)(w0 / nn);
-            v[1] = (float)(w1 / nn);
-            v[2] = (float)(w2 / nn);
-        } else {
-            s[i] = -s[i];
-        }
-        atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
-    }
-    if (threadIdx.x == 0) *out_size = size;
+    wolff_f32_cluster(m, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond);
 }
 
 // ---- launchers ------------------------------------------------------------------

@@ -75,12 +75,87 @@ def test_batch_blume_capel_metropolis_only():
             c.close()
 
 
-def test_batch_rejects_unsupported_members():
+def test_batch_csr_members_equal_single_handles():
+    """int8 members on CSR lattices (EA disorder realisations, a random
+    geometric graph) beside hypercubic ones."""
+    import marqov_b200 as M
+    ms = [(M.RegularRandomBond(6, 3, 0.5, seed=s), M.Config(seed=300 + s, repid=s), M.EdwardsAndersonIsing(-1.0), 0.9)
+          for s in range(3)]
+    ms.append((M.RandomGeometricGraph2D(500, 8.0, seed=4), M.Config(seed=9, repid=9), M.Ising(-1.0, "int8"), 0.5))
+    ms.append((M.RegularHypercubic(16, 2), M.Config(seed=8, repid=8), M.Potts(3, -1.0), 1.0))
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms, graph_steps=4) as b:
+            b.init()
+            for c in singles:
+                c.init()
+            obs, _ = b.emcs(9, ncluster=0, nmetro=2)
+            for i, c in enumerate(singles):
+                o, _ = c.emcs(9, ncluster=0, nmetro=2)
+                assert (obs[:, i, :] == o).all(), f"member {i}"
+                assert (b.member(i).state == c.state).all(), f"member {i}"
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_float_members_equal_single_handles():
+    """phi^4 at several couplings and small-cap Heisenberg, Metropolis + Wolff."""
+    import marqov_b200 as M
+    ms = [(M.RegularHypercubic(L, 3), M.Config(seed=70 + i, repid=i), M.Phi4(b, 1.1), b)
+          for i, (L, b) in enumerate(((6, 0.36), (8, 0.37), (4, 0.38)))]
+    ms.append((M.RegularHypercubic(8, 3), M.Config(seed=80, repid=7), M.Heisenberg(-1.0, "smallcap", 0.3), 0.693))
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms, graph_steps=3) as b:
+            b.init()
+            for c in singles:
+                c.init()
+            for call in range(2):
+                obs, mc = b.emcs(5, ncluster=1, nmetro=2)
+                for i, c in enumerate(singles):
+                    o, m = c.emcs(5, ncluster=1, nmetro=2)
+                    np.testing.assert_allclose(obs[:, i, :], o, rtol=1e-5, atol=1e-7)
+                    np.testing.assert_array_equal(mc[:, i], m)
+                    np.testing.assert_allclose(b.member(i).state, c.state, rtol=1e-5, atol=1e-6)
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_samples_match_member_samples():
+    import ctypes as C
+    import torch
+    import marqov_b200 as M
+    ms = [(M.RegularHypercubic(4, 3), M.Config(seed=5, repid=i), M.Phi4(b, 1.1), b) for i, b in enumerate((0.36, 0.38))]
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms) as b:
+            b.init()
+            for c in singles:
+                c.init()
+            d = torch.zeros((2, 7, 4), dtype=torch.float64, device="cuda")
+            M._lib.check(M._lib.load().mqv_batch_emcs_samples(b._h, 7, 1, 1, C.c_void_p(d.data_ptr())))
+            for i, c in enumerate(singles):
+                ds = torch.zeros((7, 4), dtype=torch.float64, device="cuda")
+                M._lib.check(M._lib.load().mqv_emcs_samples(c.handle, 7, 1, 1, C.c_void_p(ds.data_ptr())))
+                c.synchronize()
+                np.testing.assert_allclose(d[i].cpu().numpy(), ds.cpu().numpy(), rtol=1e-9)
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_rejects_mixed_or_unsupported_members():
     import marqov_b200 as M
     with pytest.raises(M.MarqovError) as ei:
-        M.Batch([(M.RegularHypercubic(8, 3), M.Config(), M.Heisenberg(-1.0), 0.7)])
+        M.Batch([(M.RegularHypercubic(8, 3), M.Config(), M.Heisenberg(-1.0), 0.7),
+                 (M.RegularHypercubic(8, 2), M.Config(), M.Ising(-1.0), 0.4)])
     assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
-    lat = M.RegularRandomBond(8, 2, seed=1)
-    with pytest.raises(M.MarqovError) as ei:
-        M.Batch([(lat, M.Config(), M.EdwardsAndersonIsing(-1.0), 0.7)])
-    assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
+    with M.Batch([(M.RegularHypercubic(8, 3), M.Config(), M.XXZAntiferro(1.0, 0.5), 0.7)]) as b:
+        b.init()
+        with pytest.raises(M.MarqovError) as ei:
+            b.emcs(1, ncluster=1, nmetro=1)
+        assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
+        obs, _ = b.emcs(2, ncluster=0, nmetro=1)
+        assert np.isfinite(obs).all()
