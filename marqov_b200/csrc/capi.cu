@@ -408,6 +408,7 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         s->sten.lg = -1;
         for (int b = 0; b < 31; ++b)
             if ((1 << b) == lattice->len) s->sten.lg = b;
+        s->sten.mlen = s->sten.lg >= 0 ? 0 : UINT64_MAX / (uint64_t)lattice->len + 1;
         s->max_degree = 2 * lattice->dim;
         s->colour_ptr = {0, (int32_t)(n / 2), (int32_t)n};
     } else if (lattice->kind == MQV_LATTICE_CSR) {

@@ -98,6 +98,20 @@ MQV_HD bool accept_below(uint64_t cut, Key key, uint32_t site, uint32_t sweep, u
     return (((uint64_t)top << 45) | (accept_fine56(key, site, sweep, replica) >> 11)) < cut;
 }
 
+// x % q for the small ranges of state draws (q <= 65535): constant divisors
+// for the common q, else three 32-bit remainders of x = hi 2^32 + lo.
+MQV_HD uint32_t mod_small(uint64_t x, uint32_t q)
+{
+    switch (q) {
+        case 2: return (uint32_t)(x % 2ull);
+        case 3: return (uint32_t)(x % 3ull);
+        case 4: return (uint32_t)(x % 4ull);
+        default: break;
+    }
+    const uint32_t p32 = (0xFFFFFFFFu % q + 1u) % q;  // 2^32 mod q
+    return ((((uint32_t)(x >> 32)) % q) * p32 + ((uint32_t)x) % q) % q;
+}
+
 // real() of RNGCache: (word >> 11) * 2^-53 (src/libmarqov/rngcache.h:202-206).
 MQV_HD double real01(uint64_t w) { return (double)(w >> 11) * 0x1.0p-53; }
 

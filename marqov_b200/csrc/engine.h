@@ -44,14 +44,25 @@ struct StencilDev {
     int len;
     int64_t n;  // < 2^31: site indices fit 32 bits
     int64_t pows[4];
-    int split;  // 2D state stored in split rows (see split_addr)
-    int lg;     // log2(len) when len is a power of two, else -1
-    // coordinate j of site i (32-bit arithmetic; shifts for power-of-two sides)
+    int split;      // 2D state stored in split rows (see split_addr)
+    int lg;         // log2(len) when len is a power of two, else -1
+    uint64_t mlen;  // ceil(2^64 / len) otherwise: u / len = mulhi64(u, mlen), exact for 32-bit u
+    MQV_HD uint32_t divlen(uint32_t u) const
+    {
+#ifdef __CUDA_ARCH__
+        return (uint32_t)__umul64hi((unsigned long long)u, (unsigned long long)mlen);
+#else
+        return (uint32_t)(((unsigned __int128)u * mlen) >> 64);
+#endif
+    }
+    // coordinate j of site i (shifts for power-of-two sides, multiply-high
+    // division otherwise)
     MQV_HD int coord(int64_t i, int j) const
     {
-        const uint32_t u = (uint32_t)i;
+        uint32_t u = (uint32_t)i;
         if (lg >= 0) return (int)((u >> (lg * j)) & (uint32_t)(len - 1));
-        return (int)((u / (uint32_t)pows[j]) % (uint32_t)len);
+        for (int k = 0; k < j; ++k) u = divlen(u);
+        return (int)(u - divlen(u) * (uint32_t)len);
     }
     // device address of site i
     MQV_HD int64_t addr(int64_t i) const

@@ -26,7 +26,7 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int
     if (m.kind == MQV_MODEL_POTTS) {
         // Initializer<Potts<Q>>::newsv (src/hamiltonian/Potts.h:170-177) and
         // PottsInteraction::diff (src/hamiltonian/Potts.h:86-107)
-        nw = (int)(rng.next() % (uint64_t)m.q);
+        nw = (int)mod_small(rng.next(), (uint32_t)m.q);
         int eo = 0, en = 0;
         for (int t = 0; t < deg; ++t) {
             const int v = s[lat.addr(lat.nbr(i, t))];
