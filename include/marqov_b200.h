@@ -241,6 +241,13 @@ MQV_API mqv_status mqv_batch_destroy(mqv_batch* batch);
  * the batch and bound to its stream. */
 MQV_API mqv_status mqv_batch_member(mqv_batch* batch, int32_t i, mqv_sim** sim);
 MQV_API mqv_status mqv_batch_init_state(mqv_batch* batch);
+/* Cluster algorithms of a batch (same clusters either way): growth by one
+ * CTA per member, breadth first; or labelling of the activated-bond
+ * components of all members in a fixed number of whole-lattice passes
+ * (cost independent of cluster depth; pays for percolating clusters on large
+ * lattices).  The default is breadth first. */
+enum { MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
+MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* batch, int32_t algorithm);
 /* EMCS per graph launch (1 .. 256; default 8). */
 MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* batch, int32_t steps);
 /* n_emcs EMCS of every member (ncluster clusters, then nmetro sweeps, then a

@@ -305,6 +305,13 @@ class Batch:
     def init(self):
         L.check(self._lib.mqv_batch_init_state(self._h))
 
+    def set_wolff(self, algorithm: str):
+        """Cluster algorithm, "bfs" (one CTA per member grows its cluster) or
+        "label" (connected-component labelling of all members); both give the
+        same clusters."""
+        code = {"bfs": L.WOLFF_BFS, "label": L.WOLFF_LABEL}[algorithm]
+        L.check(self._lib.mqv_batch_set_wolff(self._h, code))
+
     def emcs(self, n: int, ncluster: int = 1, nmetro: int = 1):
         """n EMCS of every member; returns (obs [n, members, 4], mean cluster [n, members])."""
         obs = np.zeros((n, self.n, 4), np.float64)

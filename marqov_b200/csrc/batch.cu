@@ -23,6 +23,7 @@
 #include "batch.h"
 #include "f32_site.cuh"
 #include "int8_site.cuh"
+#include "wolff_ccl.cuh"
 #include "wolff_int8.cuh"
 
 namespace mqv {
@@ -143,8 +144,22 @@ __global__ void batch_samples(const long long* __restrict__ acc, int nslots, int
 template <bool F32>
 static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro)
 {
-    for (int c = 0; c < ncluster; ++c)
-        batch_wolff<F32><<<b.nrep, 1024, 0, st>>>(b.reps, b.ctr, ncluster, c, b.csize, b.nrep);
+    for (int c = 0; c < ncluster; ++c) {
+        if (b.wolff_ccl) {
+            CclSeed* sd = (CclSeed*)b.ccl_seeds;
+            const unsigned gb = (unsigned)b.site_blocks;
+            ccl_seed<F32><<<(b.nrep + 127) / 128, 128, 0, st>>>(b.reps, b.ctr, ncluster, c, sd, b.csize, b.nrep);
+            ccl_init<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
+                                                             sd);
+            ccl_hook<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
+                                                             sd, b.ctr, ncluster, c);
+            ccl_compress<<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites);
+            ccl_flip<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
+                                                             sd, b.ctr, ncluster, c, b.csize, b.nrep);
+        } else {
+            batch_wolff<F32><<<b.nrep, 1024, 0, st>>>(b.reps, b.ctr, ncluster, c, b.csize, b.nrep);
+        }
+    }
     for (int j = 0; j < nmetro; ++j)
         for (int colour = 0; colour < b.ncol; ++colour) {
             if (b.total[colour] == 0) continue;

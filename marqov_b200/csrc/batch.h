@@ -47,6 +47,13 @@ struct BatchLaunch {
     const int* blocks;           // host: [ncol] blocks of each colour
     const int64_t* total;        // host: [ncol] work items of each colour
     int meas_parts;              // measurement CTAs per member
+    // site-level work (every site of every member) for the labelling Wolff
+    const int64_t* site_prefix;  // [nrep + 1]
+    const int32_t* site_block_rep;
+    int64_t total_sites;
+    int site_blocks;
+    void* ccl_seeds;             // [nrep] seeds of the labelling Wolff
+    int wolff_ccl;               // clusters by labelling (1) or by one CTA's breadth-first growth (0)
     BatchCtr* ctr;
     long long* acc;              // slot-major accumulators (int64, or FP64 in the same words)
     int32_t* csize;              // cluster sizes: (slot * ncluster + c) * nrep + r
@@ -63,7 +70,7 @@ inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int 
 {
     int live = 0;
     for (int c = 0; c < b.ncol; ++c) live += b.total[c] > 0;
-    return (uint64_t)ncluster + (uint64_t)nmetro * (uint64_t)live + 2ull;
+    return (uint64_t)ncluster * (b.wolff_ccl ? 5ull : 1ull) + (uint64_t)nmetro * (uint64_t)live + 2ull;
 }
 
 }  // namespace mqv

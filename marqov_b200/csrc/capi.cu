@@ -841,6 +841,13 @@ MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, 
 
 namespace mqv {
 
+// host mirror of the labelling Wolff's per-member seed (wolff_ccl.cuh)
+struct CclSeedHost {
+    int64_t rsite;
+    int val, newq;
+    float r[3];
+};
+
 struct Batch {
     int device = 0;
     cudaStream_t stream = nullptr;
@@ -852,6 +859,10 @@ struct Batch {
     int64_t* d_prefix = nullptr;
     int32_t* d_block_rep = nullptr;
     int32_t* d_cbegin = nullptr;
+    int64_t* d_site_prefix = nullptr;
+    int32_t* d_site_block_rep = nullptr;
+    void* d_ccl_seeds = nullptr;
+    int wolff_mode = 0;  // MQV_WOLFF_*
     std::vector<int> block_off, blocks;
     std::vector<int64_t> total;
     BatchCtr* d_ctr = nullptr;
@@ -883,7 +894,8 @@ static void free_batch(Batch* b)
     free_graphs(b);
     for (Sim* s : b->sims) free_sim(s);
     for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin, (void*)b->d_ctr,
-                    (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize})
+                    (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize, (void*)b->d_site_prefix,
+                    (void*)b->d_site_block_rep, b->d_ccl_seeds})
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1132,6 +1144,16 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         }
     }
     if (brep.empty()) brep.push_back(0);
+    // site-level work of the labelling Wolff
+    std::vector<int64_t> sprefix((size_t)n + 1, 0);
+    for (int r = 0; r < n; ++r) sprefix[r + 1] = sprefix[r] + b->sims[(size_t)r]->n;
+    const int64_t sblocks = (sprefix[n] + kBatchMetroThreads - 1) / kBatchMetroThreads;
+    if (sblocks >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
+    std::vector<int32_t> sbrep((size_t)std::max<int64_t>(sblocks, 1), 0);
+    for (int64_t k = 0, r = 0; k < sblocks; ++k) {
+        while (k * kBatchMetroThreads >= sprefix[r + 1]) ++r;
+        sbrep[(size_t)k] = (int32_t)r;
+    }
     auto dcopy = [&](void** dst, const void* src, size_t bytes) -> mqv_status {
         MQV_CK(cudaMalloc(dst, bytes));
         MQV_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
@@ -1140,7 +1162,14 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     mqv_status st = dcopy((void**)&b->d_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
     if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
     if (!st) st = dcopy((void**)&b->d_cbegin, cbegin.data(), sizeof(int32_t) * std::max<size_t>(cbegin.size(), 1));
+    if (!st) st = dcopy((void**)&b->d_site_prefix, sprefix.data(), sizeof(int64_t) * sprefix.size());
+    if (!st) st = dcopy((void**)&b->d_site_block_rep, sbrep.data(), sizeof(int32_t) * sbrep.size());
     if (st) return bail(st);
+    if (cudaMalloc(&b->d_ccl_seeds, sizeof(CclSeedHost) * (size_t)n) != cudaSuccess) {
+        cudaGetLastError();
+        set_error("device allocation of the batch tables failed");
+        return bail(MQV_ERR_OUT_OF_MEMORY);
+    }
     if (cudaMalloc(&b->d_reps, sizeof(BatchRep) * (size_t)n) != cudaSuccess ||
         cudaMalloc(&b->d_ctr, sizeof(BatchCtr)) != cudaSuccess) {
         cudaGetLastError();
@@ -1158,6 +1187,12 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     b->L.blocks = b->blocks.data();
     b->L.total = b->total.data();
     b->L.meas_parts = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 4095) / 4096));
+    b->L.site_prefix = b->d_site_prefix;
+    b->L.site_block_rep = b->d_site_block_rep;
+    b->L.total_sites = sprefix[n];
+    b->L.site_blocks = (int)sblocks;
+    b->L.ccl_seeds = b->d_ccl_seeds;
+    b->L.wolff_ccl = 0;  // breadth-first clusters unless mqv_batch_set_wolff asks for labelling
     b->L.ctr = b->d_ctr;
     *out = reinterpret_cast<mqv_batch*>(b);
     return MQV_OK;
@@ -1195,6 +1230,20 @@ MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* h, int32_t steps)
     if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
     if (steps < 1 || steps > 256) return fail(MQV_ERR_INVALID_ARG, "graph steps must be in [1, 256]");
     b->graph_steps = steps;
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* h, int32_t algorithm)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (algorithm != MQV_WOLFF_BFS && algorithm != MQV_WOLFF_LABEL)
+        return fail(MQV_ERR_INVALID_ARG, "unknown cluster algorithm");
+    const int v = algorithm == MQV_WOLFF_LABEL ? 1 : 0;
+    if (v != b->L.wolff_ccl) {
+        b->L.wolff_ccl = v;
+        free_graphs(b);
+    }
     return MQV_OK;
 }
 

@@ -190,6 +190,54 @@ __device__ __forceinline__ void finalize_f32_one(const ModelDev& m, int64_t n, c
 
 // One cluster grown and reflected by the calling CTA (block size a multiple of
 // 32); the visited bits of its members are cleared before return.
+// The embedding arithmetic shared by the breadth-first and the labelling
+// cluster kernels, rounded as written (no contraction), as the reference's
+// double code: a = s . r, cpl = J (-a_i) a_j, and the reflection
+// s -> (s - 2 (s.r) r) / |s - 2 (s.r) r|.
+__device__ __forceinline__ double embed_proj(int symd, const float* __restrict__ s, int64_t i, float r0, float r1,
+                                             float r2)
+{
+    if (symd == 3)
+        return __dadd_rn(__dadd_rn(__dmul_rn((double)s[3 * i], (double)r0), __dmul_rn((double)s[3 * i + 1], (double)r1)),
+                         __dmul_rn((double)s[3 * i + 2], (double)r2));
+    return __dmul_rn((double)s[i], (double)r0);
+}
+__device__ __forceinline__ double embed_cpl(double J, double ai, double aj) { return __dmul_rn(__dmul_rn(J, -ai), aj); }
+__device__ __forceinline__ void embed_reflect(int symd, float* __restrict__ s, int64_t i, float r0, float r1, float r2)
+{
+    if (symd != 3) {
+        s[i] = -s[i];
+        return;
+    }
+    float* v = s + 3 * i;
+    const double x = v[0], y = v[1], z = v[2];
+    const double d = __dadd_rn(__dadd_rn(__dmul_rn(x, (double)r0), __dmul_rn(y, (double)r1)), __dmul_rn(z, (double)r2));
+    const double d2 = __dmul_rn(2.0, d);
+    const double w0 = __dsub_rn(x, __dmul_rn(d2, (double)r0)), w1 = __dsub_rn(y, __dmul_rn(d2, (double)r1)),
+                 w2 = __dsub_rn(z, __dmul_rn(d2, (double)r2));
+    const double nn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(w0, w0), __dmul_rn(w1, w1)), __dmul_rn(w2, w2)));
+    v[0] = (float)__ddiv_rn(w0, nn);
+    v[1] = (float)__ddiv_rn(w1, nn);
+    v[2] = (float)__ddiv_rn(w2, nn);
+}
+
+// The embedding of a cluster: seed site and reflection vector r (plane
+// reflections of O(3) spins, sign flips of scalars) from the WOLFF_SEED
+// substream.
+__device__ __forceinline__ int64_t embed_seed(const ModelDev& m, int64_t n, Key key, uint32_t serial, uint32_t tg_seed,
+                                              float r[3])
+{
+    SubStream rng(key, 0u, serial, tg_seed);
+    const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
+    double v[3] = {1.0, 0.0, 0.0};
+    if (m.symd == 3) rnddir3(rng, v);
+    else if (rng.real() < 0.5) v[0] = -1.0;
+    r[0] = (float)v[0];
+    r[1] = (float)v[1];
+    r[2] = (float)v[2];
+    return rsite;
+}
+
 template <class Lat>
 __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& lat, float* __restrict__ s,
                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
@@ -201,14 +249,11 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     const int64_t n = lat.n;
     const int symd = m.symd;
     if (threadIdx.x == 0) {
-        SubStream rng(key, 0u, serial, tg_seed);
-        const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
-        double r[3] = {1.0, 0.0, 0.0};
-        if (symd == 3) rnddir3(rng, r);
-        else if (rng.real() < 0.5) r[0] = -1.0;
-        s_r[0] = (float)r[0];
-        s_r[1] = (float)r[1];
-        s_r[2] = (float)r[2];
+        float r[3];
+        const int64_t rsite = embed_seed(m, n, key, serial, tg_seed, r);
+        s_r[0] = r[0];
+        s_r[1] = r[1];
+        s_r[2] = r[2];
         queue[0] = (int32_t)rsite;
         atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
         s_head = 0;
@@ -217,11 +262,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     }
     __syncthreads();
     const float r0 = s_r[0], r1 = s_r[1], r2 = s_r[2];
-    auto proj = [&](int64_t i) -> double {
-        if (symd == 3)
-            return (double)s[3 * i] * r0 + (double)s[3 * i + 1] * r1 + (double)s[3 * i + 2] * r2;
-        return (double)s[i] * r0;
-    };
+    auto proj = [&](int64_t i) -> double { return embed_proj(symd, s, i, r0, r1, r2); };
     const unsigned lane = threadIdx.x & 31;
     while (true) {
         const int head = s_head, tail = s_tail;
@@ -239,7 +280,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
                 if (t < deg) {
                     j = lat.nbr(cur, t);
                     if (!(visited[j >> 5] & (1u << (j & 31)))) {
-                        const double cpl = m.J * (-ac) * proj(j);
+                        const double cpl = embed_cpl(m.J, ac, proj(j));
                         if (cpl > 0) {
                             const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
                             const uint64_t wd = lo64(philox(lo, serial, hi, tg_bond, key));
@@ -269,18 +310,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     const int size = s_tail;
     for (int k = threadIdx.x; k < size; k += blockDim.x) {
         const int32_t i = queue[k];
-        if (symd == 3) {
-            float* v = s + 3 * (int64_t)i;
-            const double d = (double)v[0] * r0 + (double)v[1] * r1 + (double)v[2] * r2;
-            const double w0 = (double)v[0] - 2.0 * d * r0, w1 = (double)v[1] - 2.0 * d * r1,
-                         w2 = (double)v[2] - 2.0 * d * r2;
-            const double nn = sqrt(w0 * w0 + w1 * w1 + w2 * w2);
-            v[0] = (float)(w0 / nn);
-            v[1] = (float)(w1 / nn);
-            v[2] = (float)(w2 / nn);
-        } else {
-            s[i] = -s[i];
-        }
+        embed_reflect(symd, s, i, r0, r1, r2);
         atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
     }
     if (threadIdx.x == 0) *out_size = size;

@@ -1,0 +1,208 @@
+// Wolff clusters by connected-component labelling, for the batched path.
+//
+// With bond draws keyed by the undirected bond (lower id, cluster serial,
+// upper id), the Wolff cluster is the seed's connected component of the
+// activated bonds, whatever the visiting order.  A breadth-first growth from
+// one CTA needs one step per level of the cluster; this variant labels every
+// component of the activated-bond graph of every member in a fixed number of
+// whole-lattice passes -- lock-free union-find: each undirected bond once,
+// roots hooked by compare-and-swap, paths halved on the way -- and flips the
+// seed's component:
+//   ccl_seed      one thread per member: seed site, old/new state or the
+//                 reflection vector (the same substream draws as the BFS);
+//   ccl_init      label = own index for candidate sites (int8: state equal to
+//                 the seed's old state; float: every site), else -1;
+//   ccl_hook      activated bonds between candidates are united;
+//   ccl_compress  label = root (read-only walks: only roots are written);
+//   ccl_flip      members of the seed's component are flipped / reflected and
+//                 counted into the cluster size.
+// The label array is the member's BFS queue (n int32); the visited bitmap is
+// not touched.
+#pragma once
+#include "batch.h"
+#include "f32_site.cuh"
+#include "wolff_int8.cuh"
+
+namespace mqv {
+
+struct CclSeed {
+    int64_t rsite;
+    int val, newq;  // int8
+    float r[3];     // float
+};
+
+// member and local site of flattened site g
+__device__ __forceinline__ int ccl_member(int64_t g, const int64_t* __restrict__ prefix,
+                                          const int32_t* __restrict__ block_rep, int64_t& i)
+{
+    int r = block_rep[blockIdx.x];
+    while (g >= prefix[r + 1]) ++r;
+    i = g - prefix[r];
+    return r;
+}
+
+__device__ __forceinline__ int ccl_find(int* __restrict__ p, int x)
+{
+    while (true) {
+        const int px = __ldcg(p + x);
+        if (px == x) return x;
+        const int gp = __ldcg(p + px);
+        if (gp != px) p[x] = gp;  // path halving (races only shorten paths)
+        x = gp;
+    }
+}
+
+__device__ __forceinline__ void ccl_unite(int* __restrict__ p, int a, int b)
+{
+    while (true) {
+        a = ccl_find(p, a);
+        b = ccl_find(p, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS(p + a, a, b) == a) return;  // the larger root hangs below the smaller
+    }
+}
+
+__device__ __forceinline__ int64_t rep_n(const BatchRep& R)
+{
+    return R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.n : R.csr.n;
+}
+
+template <bool F32>
+__global__ void ccl_seed(const BatchRep* __restrict__ reps, const BatchCtr* __restrict__ ctr, int ncluster, int c,
+                         CclSeed* __restrict__ seeds, int32_t* __restrict__ csize, int nrep)
+{
+    const int r = blockIdx.x * blockDim.x + threadIdx.x;
+    if (r >= nrep) return;
+    const BatchRep& R = reps[r];
+    const uint32_t e = ctr->e, slot = e - ctr->ebase;
+    const uint32_t serial = R.cluster0 + e * (uint32_t)ncluster + (uint32_t)c;
+    const uint32_t tgs = tag(kWolffSeed, R.replica);
+    CclSeed sd{};
+    if (F32) {
+        sd.rsite = embed_seed(R.md, rep_n(R), R.key, serial, tgs, sd.r);
+    } else if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
+        sd.rsite = wolff_int8_seed(R.w, R.st, (const int8_t*)R.s, R.key, serial, tgs, sd.val, sd.newq);
+    } else {
+        sd.rsite = wolff_int8_seed(R.w, R.csr, (const int8_t*)R.s, R.key, serial, tgs, sd.val, sd.newq);
+    }
+    seeds[r] = sd;
+    csize[((size_t)slot * ncluster + c) * nrep + r] = 0;
+}
+
+template <bool F32>
+__global__ void ccl_init(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                         const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int64_t i;
+    const int r = ccl_member(g, prefix, block_rep, i);
+    const BatchRep& R = reps[r];
+    bool cand = true;
+    if (!F32) {
+        const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
+        cand = ((const int8_t*)R.s)[a] == seeds[r].val;
+    }
+    R.queue[i] = cand ? (int)i : -1;
+}
+
+template <bool F32, class Lat>
+__device__ __forceinline__ void ccl_bond(const BatchRep& R, const Lat& lat, const CclSeed& sd, uint32_t serial, int64_t i,
+                                         int64_t j)
+{
+    int* lab = R.queue;
+    if (__ldcg(lab + j) < 0) return;
+    const uint32_t tgb = tag(kWolffBond, R.replica);
+    bool act;
+    if (F32) {
+        const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
+        const float* s = (const float*)R.s;
+        const double cpl = embed_cpl(R.md.J, embed_proj(R.md.symd, s, lo, sd.r[0], sd.r[1], sd.r[2]),
+                                     embed_proj(R.md.symd, s, hi, sd.r[0], sd.r[1], sd.r[2]));
+        act = cpl > 0 &&
+              !update_accepted(2, cpl, R.md.beta, lo64(philox((uint32_t)lo, serial, (uint32_t)hi, tgb, R.key)));
+    } else {
+        act = wolff_int8_active(R.w, (uint32_t)i, (uint32_t)j, serial, tgb, R.key);
+    }
+    if (act) ccl_unite(lab, (int)i, (int)j);
+}
+
+template <bool F32>
+__global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                         const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds,
+                         const BatchCtr* __restrict__ ctr, int ncluster, int c)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int64_t i;
+    const int r = ccl_member(g, prefix, block_rep, i);
+    const BatchRep& R = reps[r];
+    if (__ldcg(R.queue + i) < 0) return;
+    const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
+    const CclSeed sd = seeds[r];
+    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
+        for (int d = 0; d < R.st.dim; ++d) ccl_bond<F32>(R, R.st, sd, serial, i, R.st.nbr(i, 2 * d));
+    } else {
+        for (int t = R.csr.rp[i]; t < R.csr.rp[i + 1]; ++t) {
+            const int64_t j = R.csr.ci[t];
+            if (j > i) ccl_bond<F32>(R, R.csr, sd, serial, i, j);
+        }
+    }
+}
+
+__global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                             const int32_t* __restrict__ block_rep, int64_t total)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int64_t i;
+    const int r = ccl_member(g, prefix, block_rep, i);
+    int* lab = reps[r].queue;
+    if (__ldcg(lab + i) < 0) return;
+    // read-only walk to the root: a halving write here could replace a label
+    // that another thread has just set to its root by a non-root ancestor
+    int x = (int)i, px;
+    while ((px = __ldcg(lab + x)) != x) x = px;
+    lab[i] = x;
+}
+
+template <bool F32>
+__global__ void ccl_flip(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                         const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds,
+                         const BatchCtr* __restrict__ ctr, int ncluster, int c, int32_t* __restrict__ csize, int nrep)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool in = false;
+    int r = 0;
+    if (g < total) {
+        int64_t i;
+        r = ccl_member(g, prefix, block_rep, i);
+        const BatchRep& R = reps[r];
+        const CclSeed& sd = seeds[r];
+        const int root = R.queue[sd.rsite];
+        in = root >= 0 && R.queue[i] == root;
+        if (in) {
+            if (F32) {
+                embed_reflect(R.md.symd, (float*)R.s, i, sd.r[0], sd.r[1], sd.r[2]);
+            } else {
+                const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
+                ((int8_t*)R.s)[a] = (int8_t)sd.newq;
+            }
+        }
+    }
+    // count per member: lanes of one member aggregate their adds
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned peers = __match_any_sync(0xffffffffu, r);
+    const unsigned cnt = __popc(__ballot_sync(0xffffffffu, in) & peers);
+    if (cnt && lane == (unsigned)(__ffs(peers) - 1)) {
+        const uint32_t slot = ctr->e - ctr->ebase;
+        atomicAdd(csize + ((size_t)slot * ncluster + c) * nrep + r, (int)cnt);
+    }
+}
+
+}  // namespace mqv

@@ -8,6 +8,36 @@
 namespace mqv {
 
 
+// Seed site, its state and the cluster's new state from the WOLFF_SEED
+// substream (Ising: the flipped spin; Potts: Embedder<Potts<Q>>::draw, a new
+// state different from the old one).
+template <class Lat>
+__device__ __forceinline__ int64_t wolff_int8_seed(const WolffDev& w, const Lat& lat, const int8_t* __restrict__ s,
+                                                   Key key, uint32_t serial, uint32_t tg_seed, int& val, int& newq)
+{
+    SubStream rng(key, 0u, serial, tg_seed);
+    const int64_t rsite = (int64_t)(rng.next() % (uint64_t)lat.n);
+    val = s[lat.addr(rsite)];
+    newq = -val;
+    if (w.mode == 2) {
+        int tries = 0;
+        do {
+            newq = (int)(rng.next() % (uint64_t)w.q);
+        } while (newq == val && ++tries < 256);
+        if (newq == val) newq = (val + 1) % w.q;
+    }
+    return rsite;
+}
+
+// Bond activation of the int8 rules on the bond's keyed word
+__device__ __forceinline__ bool wolff_int8_active(const WolffDev& w, uint32_t a, uint32_t b, uint32_t serial,
+                                                  uint32_t tg_bond, Key key)
+{
+    const uint32_t lo = a < b ? a : b, hi = a < b ? b : a;
+    const unsigned long long u53 = lo64(philox(lo, serial, hi, tg_bond, key)) >> 11;
+    return w.mode == 0 ? u53 < w.thr : u53 >= w.thr;
+}
+
 // One cluster grown and flipped by the calling CTA (any block size that is a
 // multiple of 32); the visited bits of its members are cleared before return.
 template <class Lat>
@@ -20,18 +50,8 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
     __shared__ int s_val, s_newq;
     const int64_t n = lat.n;
     if (threadIdx.x == 0) {
-        SubStream rng(key, 0u, serial, tg_seed);
-        const int64_t rsite = (int64_t)(rng.next() % (uint64_t)n);
-        const int val = s[lat.addr(rsite)];
-        int newq = -val;
-        if (w.mode == 2) {
-            // Embedder<Potts<Q>>::draw: new state different from the old one
-            int tries = 0;
-            do {
-                newq = (int)(rng.next() % (uint64_t)w.q);
-            } while (newq == val && ++tries < 256);
-            if (newq == val) newq = (val + 1) % w.q;
-        }
+        int val, newq;
+        const int64_t rsite = wolff_int8_seed(w, lat, s, key, serial, tg_seed, val, newq);
         s_val = val;
         s_newq = newq;
         queue[0] = (int32_t)rsite;
@@ -59,12 +79,7 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
                     j = lat.nbr(cur, t);
                     const int sj = s[lat.addr(j)];
                     if (sj == val && !(visited[j >> 5] & (1u << (j & 31)))) {
-                        const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
-                        const unsigned long long u53 = lo64(philox(lo, serial, hi, tg_bond, key)) >> 11;
-                        bool act;
-                        if (w.mode == 0) act = u53 < w.thr;
-                        else act = u53 >= w.thr;
-                        if (act) {
+                        if (wolff_int8_active(w, (uint32_t)cur, (uint32_t)j, serial, tg_bond, key)) {
                             const uint32_t old = atomicOr(&visited[j >> 5], 1u << (j & 31));
                             add = !(old & (1u << (j & 31)));
                         }

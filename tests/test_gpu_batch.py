@@ -123,6 +123,67 @@ def test_batch_float_members_equal_single_handles():
             c.close()
 
 
+@pytest.mark.parametrize("kind", ["int8", "float"])
+def test_batch_labelling_clusters_equal_single_handles(kind):
+    """Clusters by connected-component labelling equal the breadth-first
+    clusters of single handles (same bond draws), int8 and float members."""
+    import marqov_b200 as M
+    if kind == "int8":
+        ms = [(M.RegularHypercubic(L, 2), M.Config(seed=40 + i, repid=i), M.Potts(3, -1.0), b)
+              for i, (L, b) in enumerate(((16, 1.0), (24, 1.1), (256, 1.005)))]
+        ms.append((M.RegularHypercubic(32, 2), M.Config(seed=50, repid=50), M.Ising(-1.0), 0.44068679))
+        ms.append((M.RegularRandomBond(6, 3, 0.5, seed=2), M.Config(seed=51, repid=51), M.Ising(-1.0, "int8"), 0.3))
+    else:
+        ms = [(M.RegularHypercubic(L, 3), M.Config(seed=60 + i, repid=i), M.Phi4(b, 1.1), b)
+              for i, (L, b) in enumerate(((6, 0.36), (8, 0.38)))]
+        ms.append((M.RegularHypercubic(8, 3), M.Config(seed=70, repid=9), M.Heisenberg(-1.0), 0.693))
+    singles = [solo(M, m) for m in ms]
+    try:
+        with M.Batch(ms, graph_steps=2) as b:
+            b.set_wolff("label")
+            b.init()
+            for c in singles:
+                c.init()
+            for call in range(2):
+                obs, mc = b.emcs(4, ncluster=2, nmetro=1)
+                for i, c in enumerate(singles):
+                    o, m = c.emcs(4, ncluster=2, nmetro=1)
+                    np.testing.assert_array_equal(mc[:, i], m, err_msg=f"call {call} member {i}: cluster sizes")
+                    if kind == "int8":
+                        assert (obs[:, i, :] == o).all() and (b.member(i).state == c.state).all()
+                    else:
+                        np.testing.assert_allclose(obs[:, i, :], o, rtol=1e-5, atol=1e-7)
+                        np.testing.assert_allclose(b.member(i).state, c.state, rtol=1e-5, atol=1e-6)
+    finally:
+        for c in singles:
+            c.close()
+
+
+def test_batch_labelling_equals_bfs_on_a_potts_farm():
+    """The 256-member Potts farm (L up to 512, near Tc): both cluster
+    algorithms give the same clusters, observables and states."""
+    import marqov_b200 as M
+    sizes = [32, 48, 64, 96, 128, 192, 256, 384, 512]
+    rng = np.random.default_rng(3)
+    tc = 1.0 / np.log(1.0 + np.sqrt(3.0))
+    ms = []
+    for i in range(256):
+        L = int(rng.choice(sizes))
+        ms.append((M.RegularHypercubic(L, 2), M.Config(seed=9000 + i, repid=i), M.Potts(3, -1.0),
+                   1.0 / (tc * float(rng.uniform(0.9, 1.1)))))
+    out = {}
+    for alg in ("bfs", "label"):
+        with M.Batch(ms) as b:
+            b.set_wolff(alg)
+            b.init()
+            o1, m1 = b.emcs(12, 1, 1)
+            o2, m2 = b.emcs(8, 2, 0)
+            out[alg] = (m1, m2, o1, o2, [b.member(i).state for i in range(len(ms))])
+    for k in range(4):
+        np.testing.assert_array_equal(out["bfs"][k], out["label"][k])
+    assert all((x == y).all() for x, y in zip(out["bfs"][4], out["label"][4]))
+
+
 def test_batch_samples_match_member_samples():
     import ctypes as C
     import torch
