@@ -63,6 +63,7 @@ bool ising2d_supported(int L);
 const char* ising2d_config_name(Sim* s, char* buf, int len);
 cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split);
 cudaError_t launch_merge_rows(Sim* s, const void* split, void* rowmajor);
+cudaError_t launch_validate_int8(Sim* s, const void* rowmajor, int* flag);
 
 struct DeviceGuard {
     int prev = -1;
@@ -537,6 +538,21 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
     MQV_GUARD(s);
     if (!host || bytes != s->state_bytes)
         return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
+    if (s->fused_ising2d) {
+        // upload into the spare buffer, check every spin on the device, then
+        // convert into the current buffer (left untouched on an illegal spin)
+        int bad = 0;
+        MQV_CK(cudaMemcpyAsync(s->state[s->cur ^ 1], host, bytes, cudaMemcpyHostToDevice, s->stream));
+        MQV_CK(cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream));
+        MQV_CK(launch_validate_int8(s, s->state[s->cur ^ 1], s->d_counter));
+        MQV_CK(cudaMemcpyAsync(&bad, s->d_counter, sizeof(int), cudaMemcpyDeviceToHost, s->stream));
+        MQV_CK(cudaStreamSynchronize(s->stream));
+        if (bad) return fail(MQV_ERR_INVALID_ARG, "illegal spin value in the state");
+        MQV_CK(launch_split_rows(s, s->state[s->cur ^ 1], s->state[s->cur]));
+        MQV_CK(cudaStreamSynchronize(s->stream));
+        s->initialised = true;
+        return MQV_OK;
+    }
     if (!s->is_f32) {
         // integer states must be legal values of the model (branch-free scan)
         const int8_t* v = (const int8_t*)host;
@@ -550,12 +566,7 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
             for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] * v[i]) != 1;
         if (bad) return fail(MQV_ERR_INVALID_ARG, "illegal spin value in the state");
     }
-    if (s->fused_ising2d) {
-        MQV_CK(cudaMemcpyAsync(s->state[s->cur ^ 1], host, bytes, cudaMemcpyHostToDevice, s->stream));
-        MQV_CK(launch_split_rows(s, s->state[s->cur ^ 1], s->state[s->cur]));
-    } else {
-        MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
-    }
+    MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
     MQV_CK(cudaStreamSynchronize(s->stream));
     s->initialised = true;
     return MQV_OK;

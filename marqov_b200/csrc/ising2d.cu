@@ -750,25 +750,113 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
 }
 
 // ---- layout conversion: row-major <-> split rows -----------------------------
+// One thread moves a group of 64 consecutive sites of a row (x = 64w .. 64w+63):
+// its even sites become word w of the even half, its odd sites word w of the
+// odd half, each with the bytes transposed (split_addr): 16-byte loads and
+// stores, byte moves in registers.
+
+__device__ __forceinline__ void load64(const int8_t* __restrict__ p, uint8_t b[64])
+{
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const uint4 v = reinterpret_cast<const uint4*>(p)[k];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 16; ++j) b[16 * k + j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
+    }
+}
+
+__device__ __forceinline__ void load32(const int8_t* __restrict__ p, uint8_t b[32])
+{
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const uint4 v = reinterpret_cast<const uint4*>(p)[k];
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+#pragma unroll
+        for (int j = 0; j < 16; ++j) b[16 * k + j] = (uint8_t)(w[j >> 2] >> (8 * (j & 3)));
+    }
+}
+
+__device__ __forceinline__ void store32(int8_t* __restrict__ p, const uint8_t b[32])
+{
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        uint32_t w[4];
+#pragma unroll
+        for (int j = 0; j < 4; ++j)
+            w[j] = (uint32_t)b[16 * k + 4 * j] | ((uint32_t)b[16 * k + 4 * j + 1] << 8) |
+                   ((uint32_t)b[16 * k + 4 * j + 2] << 16) | ((uint32_t)b[16 * k + 4 * j + 3] << 24);
+        reinterpret_cast<uint4*>(p)[k] = make_uint4(w[0], w[1], w[2], w[3]);
+    }
+}
 
 __global__ void split_rows(const int8_t* __restrict__ in, int8_t* __restrict__ out, int L)
 {
-    const int64_t n = (int64_t)L * L;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t y = i / L;
-        const int x = (int)(i - y * L);
-        out[split_addr(y, x, L)] = in[i];
+    const int64_t groups = (int64_t)L * (L / 64);
+    const int gpr = L / 64;
+    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < groups;
+         gi += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t y = gi / gpr;
+        const int w = (int)(gi - y * gpr);
+        uint8_t b[64], e[32], o[32];
+        load64(in + y * L + 64 * w, b);
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            e[4 * (s & 7) + (s >> 3)] = b[2 * s];
+            o[4 * (s & 7) + (s >> 3)] = b[2 * s + 1];
+        }
+        store32(out + y * L + 32 * w, e);
+        store32(out + y * L + L / 2 + 32 * w, o);
     }
 }
 
 __global__ void merge_rows(const int8_t* __restrict__ in, int8_t* __restrict__ out, int L)
 {
-    const int64_t n = (int64_t)L * L;
-    for (int64_t i = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const int64_t y = i / L;
-        const int x = (int)(i - y * L);
-        out[i] = in[split_addr(y, x, L)];
+    const int64_t groups = (int64_t)L * (L / 64);
+    const int gpr = L / 64;
+    for (int64_t gi = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; gi < groups;
+         gi += (int64_t)gridDim.x * blockDim.x) {
+        const int64_t y = gi / gpr;
+        const int w = (int)(gi - y * gpr);
+        uint8_t e[32], o[32], b[64];
+        load32(in + y * L + 32 * w, e);
+        load32(in + y * L + L / 2 + 32 * w, o);
+#pragma unroll
+        for (int s = 0; s < 32; ++s) {
+            b[2 * s] = e[4 * (s & 7) + (s >> 3)];
+            b[2 * s + 1] = o[4 * (s & 7) + (s >> 3)];
+        }
+        store32(out + y * L + 64 * w, b);
+        store32(out + y * L + 64 * w + 32, b + 32);
     }
+}
+
+// Nonzero *flag when a byte of the row-major state is not a legal spin of
+// the model (Ising: +-1; Potts: 0 .. q-1; Blume-Capel: -1, 0, 1).
+__global__ void validate_int8(const int8_t* __restrict__ v, int64_t n, int kind, int q, int* __restrict__ flag)
+{
+    const int64_t n16 = n / 16;
+    uint32_t bad = 0;
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < n16; k += (int64_t)gridDim.x * blockDim.x) {
+        const uint4 x = reinterpret_cast<const uint4*>(v)[k];
+        const uint32_t w[4] = {x.x, x.y, x.z, x.w};
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+            uint32_t ok;
+            if (kind == MQV_MODEL_POTTS) ok = __vcmpltu4(w[j], 0x01010101u * (uint32_t)q);
+            else if (kind == MQV_MODEL_BLUME_CAPEL) ok = __vcmpltu4(__vadd4(w[j], 0x01010101u), 0x03030303u);
+            else ok = __vcmpeq4(w[j], 0x01010101u) | __vcmpeq4(w[j], 0xFFFFFFFFu);
+            bad |= ~ok;
+        }
+    }
+    for (int64_t i = 16 * n16 + blockIdx.x * (int64_t)blockDim.x + threadIdx.x; i < n;
+         i += (int64_t)gridDim.x * blockDim.x) {
+        const int x = v[i];
+        if (kind == MQV_MODEL_POTTS) bad |= (x < 0 || x >= q);
+        else if (kind == MQV_MODEL_BLUME_CAPEL) bad |= (x < -1 || x > 1);
+        else bad |= (x * x != 1);
+    }
+    if (__any_sync(0xffffffffu, bad != 0) && (threadIdx.x & 31) == 0) atomicOr(flag, 1);
 }
 
 // ---- host side ------------------------------------------------------------------
@@ -981,6 +1069,13 @@ cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split)
 cudaError_t launch_merge_rows(Sim* s, const void* split, void* rowmajor)
 {
     merge_rows<<<148 * 8, 256, 0, s->stream>>>((const int8_t*)split, (int8_t*)rowmajor, s->len);
+    s->launches++;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_validate_int8(Sim* s, const void* rowmajor, int* flag)
+{
+    validate_int8<<<148 * 8, 256, 0, s->stream>>>((const int8_t*)rowmajor, s->n, s->md.kind, s->md.q, flag);
     s->launches++;
     return cudaGetLastError();
 }

@@ -277,3 +277,22 @@ def test_error_statuses():
         with pytest.raises(E) as ei:
             c.wolff(1)
         assert ei.value.status == M._lib.ERR_UNSUPPORTED_TERM
+
+
+@pytest.mark.parametrize("L", [64, 192])
+def test_set_state_rejects_illegal_spins_and_keeps_the_state(L):
+    """The fused 2D path checks uploaded spins on the device; an illegal value
+    is refused and the current state is kept."""
+    M = mb()
+    with M.makeCore(M.RegularHypercubic(L, 2), M.Config(seed=3), M.Ising(-1.0), 0.4) as c:
+        c.init()
+        before = c.state
+        bad = before.copy()
+        bad[L * L - 5] = 0
+        with pytest.raises(M.MarqovError) as ei:
+            c.state = bad
+        assert ei.value.status == M._lib.ERR_INVALID_ARG
+        assert (c.state == before).all()
+        good = np.where(np.random.default_rng(L).random(L * L) < 0.5, 1, -1).astype(np.int8)
+        c.state = good
+        assert (c.state == good).all()
