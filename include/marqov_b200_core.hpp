@@ -1,0 +1,257 @@
+/*
+ * marqov_b200 -- header-only C++ host layer over the C ABI.
+ *
+ * Mirrors the public face of MARQOV's Core so that a program built on the
+ * reference switches by replacing makeCore with makeGPUCore:
+ *   makeCore<L,H>(std::tuple<L&, Config, std::tuple<beta, HArgs...>>)
+ *                                            src/libmarqov/core.h:1223-1229
+ *   Core::init / wrmploop / gameloop / elementaryMCstep
+ *                                            src/libmarqov/core.h:829-834,1001-1050
+ *   CXX11Scheduler::createSimfromParameter / start
+ *                                            src/libmarqov/marqovscheduler.h:75-144,223-273
+ * A Hamiltonian reaches the engine through ModelLowering<H> and a lattice
+ * through LatticeLowering<L>: hypercubic lattices (HypercubicShape<L>) take
+ * the stencil path, any other lattice with nbrs() is lowered to CSR once (with
+ * its bnds() when it has them).  marqov_b200_marqov.hpp provides the
+ * specialisations for MARQOV's own classes; user classes add their own.
+ * The Config type is any type with MARQOV::Config's fields (seed, repid,
+ * ncluster, nmetro, warmupsteps, gameloopsteps).
+ */
+#ifndef MARQOV_B200_CORE_HPP
+#define MARQOV_B200_CORE_HPP
+
+#include <cstddef>
+#include <cstdint>
+#include <memory>
+#include <stdexcept>
+#include <string>
+#include <tuple>
+#include <type_traits>
+#include <utility>
+#include <vector>
+
+#include "marqov_b200.h"
+
+namespace marqov_b200 {
+
+// Every failing C-ABI call becomes this exception (status + message).
+struct Error : std::runtime_error {
+    mqv_status status;
+    Error(mqv_status s, const std::string& m) : std::runtime_error(m), status(s) {}
+};
+
+inline void check(mqv_status s)
+{
+    if (s == MQV_OK) return;
+    char m[512];
+    mqv_last_error(m, sizeof m);
+    throw Error(s, std::string("[marqov_b200] ") + m);
+}
+
+// Hamiltonian -> model descriptor; specialise lower(const H&, double beta).
+template <class H, class Enable = void>
+struct ModelLowering;
+
+// Hypercubic lattices: specialise get() to return true with (dim, len).
+template <class L, class Enable = void>
+struct HypercubicShape {
+    static bool get(const L&, int&, int&) { return false; }
+};
+
+template <class L, class = void>
+struct has_bnds : std::false_type {};
+template <class L>
+struct has_bnds<L, decltype((void)std::declval<const L&>().bnds(0, 0), void())> : std::true_type {};
+
+// Lattice -> lattice descriptor; the CSR arrays live as long as this object.
+template <class L>
+class LatticeLowering {
+public:
+    mqv_lattice_desc lower(const L& g)
+    {
+        mqv_lattice_desc d{};
+        int dim = 0, len = 0;
+        if (HypercubicShape<L>::get(g, dim, len)) {
+            d.kind = MQV_LATTICE_HYPERCUBIC;
+            d.dim = dim;
+            d.len = len;
+            return d;
+        }
+        const std::size_t n = g.size();
+        rp_.assign(1, 0);
+        ci_.clear();
+        bd_.clear();
+        for (std::size_t i = 0; i < n; ++i) {
+            const auto nb = g.nbrs(0, (int)i);
+            for (std::size_t k = 0; k < nb.size(); ++k) ci_.push_back((int32_t)nb[k]);
+            add_bonds(g, (int)i, nb.size(), has_bnds<L>{});
+            rp_.push_back((int32_t)ci_.size());
+        }
+        d.kind = MQV_LATTICE_CSR;
+        d.n = (int32_t)n;
+        d.row_ptr = rp_.data();
+        d.col_idx = ci_.data();
+        d.bonds = bd_.empty() ? nullptr : bd_.data();
+        return d;
+    }
+
+private:
+    void add_bonds(const L&, int, std::size_t, std::false_type) {}
+    void add_bonds(const L& g, int i, std::size_t deg, std::true_type)
+    {
+        const auto b = g.bnds(0, i);
+        for (std::size_t k = 0; k < deg; ++k) bd_.push_back((int8_t)b[k]);
+    }
+    std::vector<int32_t> rp_, ci_;
+    std::vector<int8_t> bd_;
+};
+
+// One simulation on the GPU with Core's public face.  H is constructed from
+// the Hamiltonian arguments, as Core does (core.h:469).
+template <class L, class H, class ConfigT>
+class GPUCore {
+public:
+    template <class... HArgs>
+    GPUCore(L& lat, const ConfigT& c, double beta, HArgs&&... hargs)
+        : ham_(std::forward<HArgs>(hargs)...), beta_(beta), ncluster_(c.ncluster), nmetro_(c.nmetro),
+          warmup_(c.warmupsteps), gameloop_(c.gameloopsteps)
+    {
+        const mqv_model_desc md = ModelLowering<H>::lower(ham_, beta);
+        const mqv_lattice_desc ld = lowering_.lower(lat);
+        mqv_run_params rp{};
+        rp.beta = beta;
+        rp.seed = (uint64_t)(int64_t)c.seed;
+        rp.replica = (uint32_t)c.repid;
+        check(mqv_create(&md, &ld, &rp, &sim_));
+    }
+    ~GPUCore()
+    {
+        if (sim_) mqv_destroy(sim_);
+    }
+    GPUCore(const GPUCore&) = delete;
+    GPUCore& operator=(const GPUCore&) = delete;
+
+    void init() { check(mqv_init_state(sim_)); }  // Core::init (core.h:829-834)
+    double elementaryMCstep()                      // core.h:1001-1028, emcs.h:69-109
+    {
+        double mc = 0;
+        check(mqv_emcs(sim_, 1, ncluster_, nmetro_, nullptr, &mc));
+        return mc;
+    }
+    void wrmploop() { check(mqv_emcs(sim_, warmup_, ncluster_, nmetro_, nullptr, nullptr)); }
+    void gameloop()
+    {
+        const std::size_t old = obs_.size();
+        obs_.resize(old + (std::size_t)gameloop_);
+        cluster_.resize(old + (std::size_t)gameloop_);
+        check(mqv_emcs(sim_, gameloop_, ncluster_, nmetro_, obs_.data() + old, cluster_.data() + old));
+    }
+    // per-EMCS energy per site, |m|, m^2, m^4 of the game loops so far
+    const std::vector<mqv_obs>& observables() const { return obs_; }
+    const std::vector<double>& cluster_sizes() const { return cluster_; }
+    // state in the reference layout: int8 for integer models, float otherwise
+    template <class T>
+    std::vector<T> state() const
+    {
+        size_t b = 0;
+        check(mqv_state_bytes(sim_, &b));
+        std::vector<T> v(b / sizeof(T));
+        check(mqv_get_state(sim_, v.data(), b));
+        return v;
+    }
+    const H& hamiltonian() const { return ham_; }
+    mqv_sim* handle() const { return sim_; }
+
+private:
+    H ham_;
+    double beta_;
+    int ncluster_, nmetro_, warmup_, gameloop_;
+    LatticeLowering<L> lowering_;
+    mqv_sim* sim_ = nullptr;
+    std::vector<mqv_obs> obs_;
+    std::vector<double> cluster_;
+};
+
+namespace detail {
+template <class L, class H, class ConfigT, class Tuple, std::size_t... I>
+std::unique_ptr<GPUCore<L, H, ConfigT>> make(L& lat, const ConfigT& c, const Tuple& h, std::index_sequence<I...>)
+{
+    return std::unique_ptr<GPUCore<L, H, ConfigT>>(
+        new GPUCore<L, H, ConfigT>(lat, c, (double)std::get<0>(h), std::get<I + 1>(h)...));
+}
+}  // namespace detail
+
+// makeCore's tuple convention: (lattice&, Config, (beta, hamiltonian args...))
+template <class L, class H, class ConfigT, class... HArgs>
+std::unique_ptr<GPUCore<L, H, ConfigT>> makeGPUCore(const std::tuple<L&, ConfigT, std::tuple<HArgs...>>& t)
+{
+    static_assert(sizeof...(HArgs) >= 1, "the Hamiltonian arguments start with beta");
+    return detail::make<L, H, ConfigT>(std::get<0>(t), std::get<1>(t), std::get<2>(t),
+                                       std::make_index_sequence<sizeof...(HArgs) - 1>());
+}
+
+// The farm: parameter sets collected with createSimfromParameter (the
+// CXX11Scheduler's interface), run together by start() as one batch on the
+// GPU -- warm-up, then game loop with per-EMCS observables.
+template <class L, class H, class ConfigT>
+class GPUScheduler {
+public:
+    template <class... HArgs>
+    void createSimfromParameter(const std::tuple<L&, ConfigT, std::tuple<HArgs...>>& t)
+    {
+        Member m;
+        m.lowering.reset(new LatticeLowering<L>());
+        create(m, std::get<0>(t), std::get<1>(t), std::get<2>(t), std::make_index_sequence<sizeof...(HArgs) - 1>());
+        members_.push_back(std::move(m));
+    }
+    void start()
+    {
+        if (members_.empty()) return;
+        std::vector<mqv_sim_spec> specs;
+        for (auto& m : members_) specs.push_back(m.spec);
+        if (batch_) mqv_batch_destroy(batch_);
+        batch_ = nullptr;
+        check(mqv_batch_create(specs.data(), (int32_t)specs.size(), &batch_));
+        check(mqv_batch_init_state(batch_));
+        const Member& f = members_.front();
+        check(mqv_batch_emcs(batch_, f.warmup, f.ncluster, f.nmetro, nullptr, nullptr));
+        obs_.resize((std::size_t)f.gameloop * members_.size());
+        check(mqv_batch_emcs(batch_, f.gameloop, f.ncluster, f.nmetro, obs_.data(), nullptr));
+    }
+    // record e * size() + i: member i after game-loop EMCS e
+    const std::vector<mqv_obs>& observables() const { return obs_; }
+    std::size_t size() const { return members_.size(); }
+    ~GPUScheduler()
+    {
+        if (batch_) mqv_batch_destroy(batch_);
+    }
+
+private:
+    struct Member {
+        mqv_sim_spec spec{};
+        std::unique_ptr<LatticeLowering<L>> lowering;
+        int ncluster = 0, nmetro = 0, warmup = 0, gameloop = 0;
+    };
+    template <class Tuple, std::size_t... I>
+    void create(Member& m, L& lat, const ConfigT& c, const Tuple& h, std::index_sequence<I...>)
+    {
+        const double beta = (double)std::get<0>(h);
+        const H ham(std::get<I + 1>(h)...);
+        m.spec.model = ModelLowering<H>::lower(ham, beta);
+        m.spec.lattice = m.lowering->lower(lat);
+        m.spec.params.beta = beta;
+        m.spec.params.seed = (uint64_t)(int64_t)c.seed;
+        m.spec.params.replica = (uint32_t)c.repid;
+        m.ncluster = c.ncluster;
+        m.nmetro = c.nmetro;
+        m.warmup = c.warmupsteps;
+        m.gameloop = c.gameloopsteps;
+    }
+    std::vector<Member> members_;
+    mqv_batch* batch_ = nullptr;
+    std::vector<mqv_obs> obs_;
+};
+
+}  // namespace marqov_b200
+
+#endif /* MARQOV_B200_CORE_HPP */

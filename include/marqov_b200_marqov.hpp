@@ -1,0 +1,117 @@
+/*
+ * marqov_b200 -- lowering of MARQOV's own Hamiltonian and lattice classes.
+ *
+ * Include after the MARQOV headers of the classes you use; each block is
+ * compiled only when its MARQOV header (by its include guard) is present.
+ *   Ising<int>            Wolff<Ising<int>> specialisation   src/hamiltonian/Ising.h:62-169
+ *   Ising<other spin>     generic Wolff + Embedder           src/libmarqov/wolff.h:72-126
+ *   Potts<Q>              flex term k                         src/hamiltonian/Potts.h:80-156
+ *   BlumeCapel<S>         J, onsite D                         src/hamiltonian/BlumeCapel.h:46-80
+ *   Heisenberg<S, C>      J                                   src/hamiltonian/Heisenberg.h:62-105
+ *   EdwardsAndersonIsing  J with the lattice's bnds()         src/hamiltonian/EdwardsAndersonIsing.h:286-310
+ *   RegularHypercubic, FixedDimRegularHypercubic<d>: stencil  src/lattice/regular_hypercubic.h
+ * Other lattices (RegularRandomBond, GraphFromCSV, ...) are lowered to CSR
+ * from nbrs() / bnds() by LatticeLowering.  MARQOV's Phi4 is a three-
+ * component field; the engine's phi^4 is the scalar form and has no
+ * lowering from that class.
+ */
+#ifndef MARQOV_B200_MARQOV_HPP
+#define MARQOV_B200_MARQOV_HPP
+
+#include <type_traits>
+
+#include "marqov_b200_core.hpp"
+
+namespace marqov_b200 {
+
+#ifdef ISING_H
+template <class S>
+struct ModelLowering<Ising<S>> {
+    static mqv_model_desc lower(const Ising<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = std::is_same<S, int>::value ? MQV_MODEL_ISING : MQV_MODEL_ISING_EMBED;
+        d.J = h.J;
+        return d;
+    }
+};
+#endif
+
+#ifdef POTTS_H
+template <int Q>
+struct ModelLowering<Potts<Q>> {
+    static mqv_model_desc lower(const Potts<Q>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_POTTS;
+        d.q = Q;
+        d.k = h.potts_interaction.k;
+        return d;
+    }
+};
+#endif
+
+#ifdef BLUMECAPEL_H
+template <class S>
+struct ModelLowering<BlumeCapel<S>> {
+    static mqv_model_desc lower(const BlumeCapel<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_BLUME_CAPEL;
+        d.J = h.J;
+        d.h = h.D;
+        return d;
+    }
+};
+#endif
+
+#ifdef HEISENBERG_H
+template <class S, class C>
+struct ModelLowering<Heisenberg<S, C>> {
+    static mqv_model_desc lower(const Heisenberg<S, C>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_HEISENBERG;
+        d.J = h.J;
+        return d;
+    }
+};
+#endif
+
+#ifdef EDWARDSANDERSONISING_H
+template <class S>
+struct ModelLowering<EdwardsAndersonIsing<S>> {
+    static mqv_model_desc lower(const EdwardsAndersonIsing<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_EA;
+        d.J = h.J;
+        return d;
+    }
+};
+#endif
+
+#ifdef REGULAR_HYPERCUBIC_H
+template <>
+struct HypercubicShape<RegularHypercubic> {
+    static bool get(const RegularHypercubic& g, int& dim, int& len)
+    {
+        dim = g.dim;
+        len = g.len;
+        return true;
+    }
+};
+template <int D>
+struct HypercubicShape<FixedDimRegularHypercubic<D>> {
+    static bool get(const FixedDimRegularHypercubic<D>& g, int& dim, int& len)
+    {
+        dim = D;
+        len = g.len;
+        return true;
+    }
+};
+#endif
+
+}  // namespace marqov_b200
+
+#endif /* MARQOV_B200_MARQOV_HPP */

@@ -1,0 +1,115 @@
+// The C++ drop-in, as a MARQOV program uses it -- TEST PROGRAM.
+//
+// Built against the reference's own Hamiltonian and lattice headers and the
+// engine's headers, linked against libmarqov_b200.so.  It runs, through
+// makeGPUCore and GPUScheduler, what the reference's libshowcase.cpp runs
+// through makeCore (src/libshowcase.cpp:40-58): init, wrmploop, gameloop.
+// Output (one line each): "core <e> <|m|>" per game-loop EMCS of a 2D Ising
+// run, then "farm <i> <e> <|m|>" for the last EMCS of each member of a
+// three-member Potts farm and "ea <e> <|m|>" for a random-bond lattice.  With
+// no GPU it prints "no device: <message>" and exits 0.
+#define CACHECONTAINER_H 1
+#include <cstdio>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include <algorithm>
+#include <numeric>
+#include <random>
+#include <vector>
+
+namespace H5 { struct Group {}; }
+template <class... T> inline void dumpscalartoH5(T&&...) {}
+namespace MARQOV {
+// the state-space type the Hamiltonian headers name (src/libmarqov/core.h:249-330)
+template <class SV, class Grid>
+struct Space {
+    typedef Grid Lattice;
+    typedef SV StateVector;
+    using value_type = SV;
+    std::vector<SV> v;
+    SV& operator[](int j) { return v[j]; }
+    const SV& operator[](int j) const { return v[j]; }
+};
+}  // namespace MARQOV
+
+// the Hamiltonian headers specialise MARQOV's update templates: those first
+#include "libmarqov/rngcache.h"
+#include "libmarqov/util/svmath.h"
+#include "libmarqov/metropolis.h"
+#include "libmarqov/wolff.h"
+#include "hamiltonian/EdwardsAndersonIsing.h"
+#include "hamiltonian/Ising.h"
+#include "hamiltonian/Potts.h"
+#include "lattice/regular_hypercubic.h"
+#include "lattice/regular_random_bond.h"
+
+#include "marqov_b200_marqov.hpp"
+
+// MARQOV::Config's fields (src/libmarqov/core.h:74-192); core.h itself needs HDF5
+struct Config {
+    std::string outpath;
+    int id = 0, repid = 0, seed = 0, nsteps = 250, warmupsteps = 100, gameloopsteps = 200, ncluster = 20, nmetro = 10;
+    explicit Config(std::string p) : outpath(std::move(p)) {}
+};
+
+int main()
+{
+    try {
+        RegularHypercubic latt(32, 2);
+        Config cfg("out");
+        cfg.seed = 17;
+        cfg.ncluster = 1;
+        cfg.nmetro = 1;
+        cfg.warmupsteps = 50;
+        cfg.gameloopsteps = 5;
+        auto sim = marqov_b200::makeGPUCore<RegularHypercubic, Ising<int>>(
+            std::make_tuple(std::ref(latt), cfg, std::make_tuple(0.44068679, -1.0)));
+        sim->init();
+        sim->wrmploop();
+        sim->gameloop();
+        for (const auto& o : sim->observables()) std::printf("core %.17g %.17g\n", o.e, o.m);
+
+        marqov_b200::GPUScheduler<RegularHypercubic, Potts<3>, Config> farm;
+        std::vector<RegularHypercubic> lats{RegularHypercubic(16, 2), RegularHypercubic(24, 2), RegularHypercubic(32, 2)};
+        for (int i = 0; i < 3; ++i) {
+            Config c("out");
+            c.seed = 5;
+            c.repid = i;
+            c.ncluster = 1;
+            c.nmetro = 2;
+            c.warmupsteps = 20;
+            c.gameloopsteps = 4;
+            farm.createSimfromParameter(std::make_tuple(std::ref(lats[i]), c, std::make_tuple(1.0 + 0.05 * i, -1.0)));
+        }
+        farm.start();
+        const auto& fo = farm.observables();
+        for (std::size_t i = 0; i < farm.size(); ++i) {
+            const auto& o = fo[3 * farm.size() + i];
+            std::printf("farm %zu %.17g %.17g\n", i, o.e, o.m);
+        }
+
+        RegularRandomBond<BimodalPDF> rb(6, 3);
+        Config ce("out");
+        ce.seed = 9;
+        ce.ncluster = 0;
+        ce.nmetro = 1;
+        ce.warmupsteps = 10;
+        ce.gameloopsteps = 1;
+        auto ea = marqov_b200::makeGPUCore<RegularRandomBond<BimodalPDF>, EdwardsAndersonIsing<int>>(
+            std::make_tuple(std::ref(rb), ce, std::make_tuple(0.9, -1.0)));
+        ea->init();
+        ea->wrmploop();
+        ea->gameloop();
+        std::printf("ea %.17g %.17g\n", ea->observables().back().e, ea->observables().back().m);
+    } catch (const marqov_b200::Error& e) {
+        if (e.status == MQV_ERR_NO_DEVICE) {
+            std::printf("no device: %s\n", e.what());
+            return 0;
+        }
+        std::fprintf(stderr, "%s\n", e.what());
+        return 1;
+    }
+    return 0;
+}

@@ -1,0 +1,60 @@
+"""The header-only C++ layer (include/marqov_b200_core.hpp with the MARQOV
+lowerings of include/marqov_b200_marqov.hpp) used the way a MARQOV program
+uses makeCore: tests/cpp/dropin_demo.cpp is compiled against the reference's
+own Hamiltonian and lattice headers.  Without a GPU it must build and report
+the missing device; on a GPU its results must equal the Python API's."""
+import os
+import subprocess
+import sys
+
+import numpy as np
+import pytest
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+sys.path.insert(0, os.path.join(ROOT, "tests", "cpp"))
+
+
+def demo_binary(build: bool):
+    import build as B
+    path = B.build_demo() if build else (B.OUT if os.path.exists(B.OUT) else None)
+    if path is None:
+        pytest.skip("C++ drop-in program not built (reference headers absent)")
+    return path
+
+
+def test_dropin_builds_and_runs_without_a_device():
+    import marqov_b200 as M
+    path = demo_binary(build=True)
+    if M._lib.device_count() > 0:
+        pytest.skip("a GPU is present: see the gpu test")
+    out = subprocess.run([path], capture_output=True, text=True, timeout=120)
+    assert out.returncode == 0, out.stderr
+    assert out.stdout.startswith("no device:")
+
+
+@pytest.mark.gpu
+def test_dropin_equals_python_api():
+    import marqov_b200 as M
+    path = demo_binary(build=False)
+    out = subprocess.run([path], capture_output=True, text=True, timeout=300)
+    assert out.returncode == 0, out.stderr
+    lines = [l.split() for l in out.stdout.strip().splitlines()]
+    core = np.array([[float(a), float(b)] for t, a, b in (l for l in lines if l[0] == "core")])
+    farm = {int(l[1]): (float(l[2]), float(l[3])) for l in lines if l[0] == "farm"}
+    ea = [l for l in lines if l[0] == "ea"]
+    # the same runs through the Python API
+    cfg = M.Config(seed=17, repid=0, ncluster=1, nmetro=1)
+    with M.makeCore(M.RegularHypercubic(32, 2), cfg, M.Ising(-1.0), 0.44068679) as c:
+        c.init()
+        c.emcs(50, measure=False)
+        obs, _ = c.emcs(5)
+    np.testing.assert_array_equal(core, obs[:, :2])
+    ms = [(M.RegularHypercubic(L, 2), M.Config(seed=5, repid=i), M.Potts(3, -1.0), 1.0 + 0.05 * i)
+          for i, L in enumerate((16, 24, 32))]
+    with M.Batch(ms) as b:
+        b.init()
+        b.emcs(20, 1, 2)
+        fo, _ = b.emcs(4, 1, 2)
+    for i in range(3):
+        assert farm[i] == (fo[3, i, 0], fo[3, i, 1])
+    assert len(ea) == 1 and np.isfinite([float(ea[0][1]), float(ea[0][2])]).all()
