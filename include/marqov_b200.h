@@ -260,6 +260,26 @@ MQV_API mqv_status mqv_batch_emcs(mqv_batch* batch, int32_t n_emcs, int32_t nclu
  * DEVICE pointer to [n][n_emcs][4] doubles. */
 MQV_API mqv_status mqv_batch_emcs_samples(mqv_batch* batch, int32_t n_emcs, int32_t ncluster, int32_t nmetro,
                                           double* d_samples);
+/* Replica exchange (parallel tempering) between batch members; replaces the
+ * scheduler's PT loop, CXX11Scheduler::start / ptstep / calcprob /
+ * exchange_statespace (src/libmarqov/marqovscheduler.h:44-57,223-273,374-470).
+ * n_steps steps, each emcs_per_step EMCS of every member (one Core::gameloop)
+ * followed by exchange attempts between the step's pairs:
+ * plan[(t * pairs_per_step + k) * 2 + {0, 1}] are member ids; a pair (a, a)
+ * is skipped (the reference's self swap), the other pairs of one step are
+ * disjoint, and partners share model descriptor and lattice (they differ in
+ * beta).  A pair exchanges its members' states with probability
+ * min(1, exp(b_a E_a - b_a E_b + b_b E_b - b_b E_a)), E the total energy
+ * after the step's last EMCS, the uniform drawn from the TEMPER stream keyed
+ * by (seed, the batch's exchange-step counter, pair index).  Members keep
+ * beta, seed and counters; member i's state is the one it holds after the
+ * exchanges.  obs (optional): [n_steps * emcs_per_step][n]; accepted
+ * (optional): [n_steps][pairs_per_step], 1 exchanged, 0 rejected, -1 self
+ * pair.  No counterpart to the reference's plan generator: the caller passes
+ * the pairs (the reference draws maxpt random pairs, marqovscheduler.h:203-210). */
+MQV_API mqv_status mqv_batch_tempering(mqv_batch* batch, int32_t n_steps, int32_t emcs_per_step, int32_t ncluster,
+                                      int32_t nmetro, const int32_t* plan, int32_t pairs_per_step, uint64_t seed,
+                                      mqv_obs* obs, int32_t* accepted);
 MQV_API mqv_status mqv_batch_launch_count(mqv_batch* batch, uint64_t* count);
 
 /* Self test: Philox blocks for n counters (c0 = i, other words given) computed

@@ -5,7 +5,7 @@ behind a C ABI (include/marqov_b200.h, libmarqov_b200.so in this package);
 this package is the host side that mirrors MARQOV's Hamiltonian / lattice /
 Core interface.  Importing it loads the engine library; there is no CPU path.
 """
-from . import _lib
+from . import _lib, tempering
 from ._lib import MarqovError
 from .core import Batch, Config, Core, makeCore, tune_small_cap
 from .hamiltonians import (BlumeCapel, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising, Phi4, Potts,
@@ -15,7 +15,7 @@ from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGra
 
 _lib.load()
 
-__all__ = ["Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
+__all__ = ["tempering", "Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
            "Potts", "BlumeCapel", "Heisenberg", "XXZAntiferro", "Phi4", "CSRLattice",
            "FixedDimRegularHypercubic", "RegularHypercubic", "RegularRandomBond", "RandomGeometricGraph2D",
            "read_graph_csv"]

@@ -106,6 +106,8 @@ SIGNATURES = {
     "mqv_batch_set_wolff": (C.c_int32, [_vp, C.c_int32]),
     "mqv_batch_emcs": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp]),
     "mqv_batch_emcs_samples": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
+    "mqv_batch_tempering": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32,
+                                        C.c_uint64, _vp, _vp]),
     "mqv_batch_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
     "mqv_selftest_philox": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                         _vp, _vp]),

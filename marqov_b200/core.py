@@ -271,6 +271,7 @@ class Batch:
         L.check(lib.mqv_batch_create(specs, len(members), C.byref(self._h)))
         L.check(lib.mqv_batch_set_graph_steps(self._h, int(graph_steps)))
         self.n = len(members)
+        self._pt_steps = 0
         self._views = []
         for i, (lat, cfg, ham, beta) in enumerate(members):
             m = C.c_void_p()
@@ -318,6 +319,28 @@ class Batch:
         mc = np.zeros((n, self.n), np.float64)
         L.check(self._lib.mqv_batch_emcs(self._h, int(n), int(ncluster), int(nmetro), obs.ctypes.data, mc.ctypes.data))
         return obs, mc
+
+    def tempering(self, n_steps: int, emcs_per_step: int = 1, ncluster: int = 1, nmetro: int = 1, plan=None,
+                  seed: int = 0):
+        """Replica exchange: n_steps x (emcs_per_step EMCS of every member,
+        then exchange attempts between the step's member pairs).  plan: int
+        [n_steps, pairs, 2] (default: alternating neighbours in member order,
+        ``tempering.neighbour_plan``).  Returns (obs [n_steps * emcs_per_step,
+        members, 4], accepted [n_steps, pairs]: 1 exchanged, 0 rejected, -1
+        self pair)."""
+        from .tempering import neighbour_plan
+        if plan is None:
+            plan = neighbour_plan(self.n, n_steps, first=self._pt_steps)
+        plan = np.ascontiguousarray(plan, np.int32)
+        if plan.ndim != 3 or plan.shape[0] != n_steps or plan.shape[2] != 2:
+            raise ValueError("plan must have shape [n_steps, pairs, 2]")
+        obs = np.zeros((n_steps * emcs_per_step, self.n, 4), np.float64)
+        acc = np.zeros((n_steps, plan.shape[1]), np.int32)
+        L.check(self._lib.mqv_batch_tempering(self._h, int(n_steps), int(emcs_per_step), int(ncluster), int(nmetro),
+                                              plan.ctypes.data, int(plan.shape[1]), int(seed) & (2 ** 64 - 1),
+                                              obs.ctypes.data, acc.ctypes.data))
+        self._pt_steps += n_steps
+        return obs, acc
 
     @property
     def launches(self) -> int:

@@ -139,6 +139,62 @@ __global__ void batch_samples(const long long* __restrict__ acc, int nslots, int
     }
 }
 
+// Replica exchange after the EMCS just done: one thread per pair of the step's
+// plan, the pairs of a step disjoint (host-checked), a self pair skipped.
+// CXX11Scheduler::calcprob / calcMHratio / exchange_statespace
+// (src/libmarqov/marqovscheduler.h:44-57,445-470): action = beta * E_total
+// (Core::calcAction, src/libmarqov/core.h:1145-1151) with E_total the
+// measured energy per site times the sites; the two members share their
+// Hamiltonian and lattice (host-checked), so each member's action of the
+// partner's state is its beta times the partner's energy.  The exchange
+// swaps the members' state pointers in the member table (the graphs read
+// them there) and in the permutation the host applies to its handles.
+template <bool F32>
+__global__ void batch_temper(BatchRep* __restrict__ reps, const BatchCtr* __restrict__ ctr,
+                             const long long* __restrict__ acc, int nrep, const int32_t* __restrict__ pairs,
+                             int npairs, uint32_t step, Key key, double en_min, double en_max,
+                             int32_t* __restrict__ perm, int32_t* __restrict__ flags)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= npairs) return;
+    const int a = pairs[2 * p], b = pairs[2 * p + 1];
+    if (a == b) {
+        flags[p] = -1;
+        return;
+    }
+    const uint32_t slot = ctr->e - 1u - ctr->ebase;
+    double oa[4], ob[4];
+    BatchRep& Ra = reps[a];
+    BatchRep& Rb = reps[b];
+    const int64_t n = Ra.lat_kind == MQV_LATTICE_HYPERCUBIC ? Ra.st.n : Ra.csr.n;
+    const long long* acc_a = acc + ((size_t)slot * nrep + a) * kAccStride;
+    const long long* acc_b = acc + ((size_t)slot * nrep + b) * kAccStride;
+    if (F32) {
+        finalize_f32_one(Ra.md, n, (const double*)acc_a, oa);
+        finalize_f32_one(Rb.md, n, (const double*)acc_b, ob);
+    } else {
+        finalize_int8_one(Ra.md, n, acc_a, oa);
+        finalize_int8_one(Rb.md, n, acc_b, ob);
+    }
+    const double Ea = MQV_DMUL(oa[0], (double)n), Eb = MQV_DMUL(ob[0], (double)n);
+    const double aa = MQV_DMUL(Ra.md.beta, Ea), ab = MQV_DMUL(Ra.md.beta, Eb);
+    const double bb = MQV_DMUL(Rb.md.beta, Eb), ba = MQV_DMUL(Rb.md.beta, Ea);
+    const double en = MQV_DSUB(MQV_DADD(MQV_DSUB(aa, ab), bb), ba);
+    double ratio = 0.0;
+    if (en > en_min) ratio = en > en_max ? 1.7976931348623157e308 : exp(en);
+    const double u = (double)(lo64(philox(step, (uint32_t)p, 0u, tag(kTemper, 0u), key)) >> 11) * 0x1.0p-53;
+    const bool acc_ok = u < fmin(1.0, ratio);
+    flags[p] = acc_ok ? 1 : 0;
+    if (acc_ok) {
+        void* t = Ra.s;
+        Ra.s = Rb.s;
+        Rb.s = t;
+        const int32_t q = perm[a];
+        perm[a] = perm[b];
+        perm[b] = q;
+    }
+}
+
 // ---- launchers (stream-ordered; all capturable) ------------------------------------
 
 template <bool F32>
@@ -188,6 +244,20 @@ cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nsl
 {
     const int64_t n = (int64_t)nslots * b.nrep;
     batch_finalize<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(b.reps, b.acc, nslots, b.nrep, b.f32, out);
+    return cudaGetLastError();
+}
+
+cudaError_t batch_launch_temper(const BatchLaunch& b, cudaStream_t st, const int32_t* pairs, int npairs, uint32_t step,
+                                uint64_t seed, double en_min, double en_max, int32_t* perm, int32_t* flags)
+{
+    if (npairs <= 0) return cudaSuccess;
+    const unsigned g = (unsigned)((npairs + 127) / 128);
+    if (b.f32)
+        batch_temper<true><<<g, 128, 0, st>>>(const_cast<BatchRep*>(b.reps), b.ctr, b.acc, b.nrep, pairs, npairs, step,
+                                               make_key(seed), en_min, en_max, perm, flags);
+    else
+        batch_temper<false><<<g, 128, 0, st>>>(const_cast<BatchRep*>(b.reps), b.ctr, b.acc, b.nrep, pairs, npairs,
+                                                step, make_key(seed), en_min, en_max, perm, flags);
     return cudaGetLastError();
 }
 

@@ -65,6 +65,10 @@ cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nsl
 // raw sums of the chunk's slots -> samples[r][e0 + slot][4] (n_total EMCS per member)
 cudaError_t batch_launch_samples(const BatchLaunch& b, cudaStream_t st, int nslots, int e0, int n_total,
                                  double* samples);
+// replica exchange of the step's disjoint pairs ([npairs][2] member ids) from
+// the energies of the EMCS just done; perm/flags as batch_temper describes
+cudaError_t batch_launch_temper(const BatchLaunch& b, cudaStream_t st, const int32_t* pairs, int npairs, uint32_t step,
+                                uint64_t seed, double en_min, double en_max, int32_t* perm, int32_t* flags);
 // kernel launches of one EMCS
 inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int nmetro)
 {

@@ -8,6 +8,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <new>
 #include <string>
 #include <vector>
@@ -253,6 +254,15 @@ static mqv_status lower_csr(Sim* s, const mqv_lattice_desc* L)
     s->n = n;
     s->max_degree = maxdeg;
     s->csr = CSRDev{n, s->d_rp, s->d_ci, s->d_bonds};
+    uint64_t h = 1469598103934665603ull;
+    auto mix = [&h](const void* p, size_t bytes) {
+        const unsigned char* c = (const unsigned char*)p;
+        for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ull;
+    };
+    mix(rp, sizeof(int32_t) * (size_t)(n + 1));
+    mix(ci, sizeof(int32_t) * (size_t)nnz);
+    if (L->bonds) mix(L->bonds, (size_t)nnz);
+    s->lat_hash = h;
     return MQV_OK;
 }
 
@@ -887,6 +897,7 @@ struct Batch {
     int g_ncluster = -1, g_nmetro = -1, g_steps = 0;
     int graph_steps = 8;  // EMCS per graph launch
     uint64_t launches = 0;
+    uint32_t temper_steps = 0;  // replica-exchange steps done (part of their draws' counters)
 };
 
 static void free_graphs(Batch* b)
@@ -958,10 +969,27 @@ static bool batch_kind_ok(int k)
            k == MQV_MODEL_EA || k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ;
 }
 
+// calcMHratio's under/overflow guards (src/libmarqov/marqovscheduler.h:44-57)
+static const double kTemperEnMin = std::log(std::numeric_limits<double>::min());
+static const double kTemperEnMax = std::log(std::numeric_limits<double>::max());
+
+// Replica exchange inside a run: after every `interval` EMCS the step's
+// pairs (d_plan + 2 * npairs * step) attempt an exchange; d_perm tracks which
+// member's state buffers each member holds, d_flags the outcomes.
+struct TemperRun {
+    int interval = 0;  // EMCS per step; 0 = no exchanges
+    int npairs = 0;
+    const int32_t* d_plan = nullptr;
+    uint32_t step0 = 0;  // the batch's step counter when the run started
+    uint64_t seed = 0;
+    int32_t* d_perm = nullptr;
+    int32_t* d_flags = nullptr;
+};
+
 // n_emcs EMCS of every member; observables / cluster means to the host, raw
 // sums to the device samples buffer ([member][n_emcs][4]), each when given.
 static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_obs* obs, double* mean_cluster,
-                            double* d_samples)
+                            double* d_samples, const TemperRun* pt = nullptr)
 {
     DeviceGuard guard_(b->device);
     if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
@@ -1028,10 +1056,23 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
         MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
         b->launches++;
-        int k = 0;
-        if (K > 1)
-            for (; k + K <= ch; k += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
-        for (; k < ch; ++k) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
+        for (int k = 0; k < ch;) {
+            // EMCS up to the end of the chunk or the next exchange step
+            int run = ch - k;
+            if (pt) run = std::min(run, pt->interval - (done + k) % pt->interval);
+            int j = 0;
+            if (K > 1)
+                for (; j + K <= run; j += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
+            for (; j < run; ++j) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
+            k += run;
+            if (pt && (done + k) % pt->interval == 0) {
+                const int t = (done + k) / pt->interval - 1;
+                MQV_CK(batch_launch_temper(b->L, b->stream, pt->d_plan + (size_t)2 * pt->npairs * t, pt->npairs,
+                                           pt->step0 + (uint32_t)t, pt->seed, kTemperEnMin, kTemperEnMax, pt->d_perm,
+                                           pt->d_flags + (size_t)pt->npairs * t));
+                b->launches++;
+            }
+        }
         b->launches += per_emcs * (uint64_t)ch;
         if (d_samples) {
             MQV_CK(batch_launch_samples(b->L, b->stream, ch, done, n_emcs, d_samples));
@@ -1065,6 +1106,38 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
     }
     return MQV_OK;
+}
+
+// Partners of a replica exchange differ in beta only: the same model
+// descriptor and the same lattice.
+static bool temper_compatible(const Sim* a, const Sim* b)
+{
+    const mqv_model_desc &x = a->model, &y = b->model;
+    if (x.kind != y.kind || x.q != y.q || x.proposal != y.proposal || x.J != y.J || x.h != y.h || x.h2 != y.h2 ||
+        x.k != y.k || x.delta != y.delta || x.cap != y.cap)
+        return false;
+    if (a->lat_kind != b->lat_kind || a->n != b->n) return false;
+    if (a->lat_kind == MQV_LATTICE_HYPERCUBIC) return a->dim == b->dim && a->len == b->len;
+    return a->lat_hash == b->lat_hash;
+}
+
+// Member r takes the state buffers member perm[r] held when the run started.
+static void apply_state_permutation(Batch* b, const std::vector<int32_t>& perm)
+{
+    struct Bufs {
+        void* s0;
+        void* s1;
+        int cur;
+    };
+    std::vector<Bufs> old;
+    for (Sim* s : b->sims) old.push_back(Bufs{s->state[0], s->state[1], s->cur});
+    for (int r = 0; r < b->nrep; ++r) {
+        const Bufs& o = old[(size_t)perm[(size_t)r]];
+        Sim* s = b->sims[(size_t)r];
+        s->state[0] = o.s0;
+        s->state[1] = o.s1;
+        s->cur = o.cur;
+    }
 }
 
 }  // namespace mqv
@@ -1273,6 +1346,90 @@ MQV_API mqv_status mqv_batch_emcs_samples(mqv_batch* h, int32_t n_emcs, int32_t 
     if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
     if (n_emcs > 0 && !d_samples) return fail(MQV_ERR_INVALID_ARG, "null sample buffer");
     return batch_run(b, n_emcs, ncluster, nmetro, nullptr, nullptr, d_samples);
+}
+
+MQV_API mqv_status mqv_batch_tempering(mqv_batch* h, int32_t n_steps, int32_t emcs_per_step, int32_t ncluster,
+                                      int32_t nmetro, const int32_t* plan, int32_t pairs_per_step, uint64_t seed,
+                                      mqv_obs* obs, int32_t* accepted)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b || (!plan && n_steps > 0 && pairs_per_step > 0)) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    if (n_steps < 0 || emcs_per_step < 1 || pairs_per_step < 0)
+        return fail(MQV_ERR_INVALID_ARG, "need n_steps >= 0, emcs_per_step >= 1, pairs_per_step >= 0");
+    if ((int64_t)n_steps * emcs_per_step > INT32_MAX) return fail(MQV_ERR_INVALID_ARG, "too many EMCS");
+    if (pairs_per_step > b->nrep) return fail(MQV_ERR_INVALID_ARG, "more pairs per step than members");
+    DeviceGuard guard_(b->device);
+    // the plan: member ids in range, pairs of a step disjoint, partners alike
+    std::vector<int> seen((size_t)b->nrep, -1);
+    for (int t = 0; t < n_steps; ++t)
+        for (int k = 0; k < pairs_per_step; ++k) {
+            const int32_t* pr = plan + ((size_t)t * pairs_per_step + k) * 2;
+            const int a = pr[0], c = pr[1];
+            if (a < 0 || a >= b->nrep || c < 0 || c >= b->nrep)
+                return fail(MQV_ERR_INVALID_ARG, "plan step " + std::to_string(t) + ": member id out of range");
+            if (a == c) continue;
+            if (seen[(size_t)a] == t || seen[(size_t)c] == t)
+                return fail(MQV_ERR_INVALID_ARG, "plan step " + std::to_string(t) + ": pairs share a member");
+            seen[(size_t)a] = seen[(size_t)c] = t;
+            if (!temper_compatible(b->sims[(size_t)a], b->sims[(size_t)c]))
+                return fail(MQV_ERR_INVALID_ARG, "members " + std::to_string(a) + " and " + std::to_string(c) +
+                                                     " differ in more than beta (model or lattice)");
+        }
+    const int n_emcs = n_steps * emcs_per_step;
+    if (n_emcs == 0) return MQV_OK;
+    const size_t nflags = (size_t)n_steps * pairs_per_step;
+    int32_t *d_plan = nullptr, *d_perm = nullptr, *d_flags = nullptr;
+    auto release = [&]() {
+        for (void* p : {(void*)d_plan, (void*)d_perm, (void*)d_flags})
+            if (p) cudaFree(p);
+    };
+    std::vector<int32_t> ident((size_t)b->nrep);
+    for (int i = 0; i < b->nrep; ++i) ident[(size_t)i] = i;
+    if (cudaMalloc(&d_plan, sizeof(int32_t) * std::max<size_t>(2 * nflags, 1)) != cudaSuccess ||
+        cudaMalloc(&d_perm, sizeof(int32_t) * (size_t)b->nrep) != cudaSuccess ||
+        cudaMalloc(&d_flags, sizeof(int32_t) * std::max<size_t>(nflags, 1)) != cudaSuccess) {
+        cudaGetLastError();
+        release();
+        return fail(MQV_ERR_OUT_OF_MEMORY, "device allocation of the exchange plan failed");
+    }
+    cudaError_t ce = cudaSuccess;
+    if (nflags) ce = cudaMemcpy(d_plan, plan, sizeof(int32_t) * 2 * nflags, cudaMemcpyHostToDevice);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(d_perm, ident.data(), sizeof(int32_t) * ident.size(), cudaMemcpyHostToDevice);
+    if (ce != cudaSuccess) {
+        release();
+        return fail(MQV_ERR_CUDA, std::string("upload of the exchange plan failed: ") + cudaGetErrorString(ce));
+    }
+    TemperRun pt;
+    pt.interval = emcs_per_step;
+    pt.npairs = pairs_per_step;
+    pt.d_plan = d_plan;
+    pt.step0 = b->temper_steps;
+    pt.seed = seed;
+    pt.d_perm = d_perm;
+    pt.d_flags = d_flags;
+    mqv_status st = batch_run(b, n_emcs, ncluster, nmetro, obs, nullptr, nullptr, &pt);
+    // the handles take the state buffers the exchanges left them (also after a failed run)
+    std::vector<int32_t> perm((size_t)b->nrep);
+    std::vector<int32_t> flags(nflags);
+    ce = cudaStreamSynchronize(b->stream);
+    if (ce == cudaSuccess)
+        ce = cudaMemcpy(perm.data(), d_perm, sizeof(int32_t) * perm.size(), cudaMemcpyDeviceToHost);
+    if (ce == cudaSuccess && accepted && nflags)
+        ce = cudaMemcpy(flags.data(), d_flags, sizeof(int32_t) * nflags, cudaMemcpyDeviceToHost);
+    release();
+    if (ce != cudaSuccess)
+        return fail(MQV_ERR_CUDA, std::string("download of the exchange outcome failed: ") + cudaGetErrorString(ce));
+    std::vector<char> hit((size_t)b->nrep, 0);
+    for (int32_t q : perm) {
+        if (q < 0 || q >= b->nrep || hit[(size_t)q]) return fail(MQV_ERR_CUDA, "exchange permutation corrupted");
+        hit[(size_t)q] = 1;
+    }
+    apply_state_permutation(b, perm);
+    if (st) return st;
+    b->temper_steps += (uint32_t)n_steps;
+    if (accepted && nflags) std::memcpy(accepted, flags.data(), sizeof(int32_t) * nflags);
+    return MQV_OK;
 }
 
 MQV_API mqv_status mqv_batch_launch_count(mqv_batch* h, uint64_t* count)

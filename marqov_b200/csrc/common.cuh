@@ -15,7 +15,7 @@
 namespace mqv {
 
 // Stream tags, counter word 3 bits 24..31 (replica id in bits 0..23).
-enum Stream : uint32_t { kMetro = 1, kInit = 2, kWolffSeed = 3, kWolffBond = 4, kAccept = 5, kAcceptFine = 6 };
+enum Stream : uint32_t { kMetro = 1, kInit = 2, kWolffSeed = 3, kWolffBond = 4, kAccept = 5, kAcceptFine = 6, kTemper = 7 };
 
 struct Key {
     uint32_t k0, k1;

@@ -134,6 +134,7 @@ struct Sim {
     int32_t* d_ci = nullptr;
     int8_t* d_bonds = nullptr;
     int max_degree = 0;
+    uint64_t lat_hash = 0;            // CSR: FNV-1a of row_ptr, col_idx and bonds
     std::vector<int32_t> colour_ptr;  // host
     int32_t* d_order = nullptr;       // sites grouped by colour
     // random numbers

@@ -240,7 +240,23 @@ class RefHarness:
         lib.ref_emcs_ising2d.restype = C.c_int
         lib.ref_emcs_ising2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int,
                                          C.c_int, _f64p, _f64p]
+        lib.ref_calc_mh_ratio.restype = C.c_double
+        lib.ref_calc_mh_ratio.argtypes = [C.c_double]
+        lib.ref_pt_calcprob.restype = C.c_int
+        lib.ref_pt_calcprob.argtypes = [C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
         self.lib = lib
+
+    def calc_mh_ratio(self, en):
+        return float(self.lib.ref_calc_mh_ratio(en))
+
+    def pt_calcprob(self, beta_a, e_a, beta_b, e_b):
+        """The reference scheduler's calcprob for arrays of (beta, total energy) pairs."""
+        arrs = [np.ascontiguousarray(x, np.float64) for x in (beta_a, e_a, beta_b, e_b)]
+        out = np.zeros(arrs[0].size, np.float64)
+        rc = self.lib.ref_pt_calcprob(out.size, *arrs, out)
+        if rc:
+            raise RuntimeError(f"ref_pt_calcprob failed ({rc})")
+        return out
 
     def sweeps_int(self, kind, g: Graph, s, J, D, beta, seed, replica, sweep0, nsweeps, want_obs=True):
         obs = np.zeros(2 * nsweeps, np.float64) if want_obs else None
