@@ -378,6 +378,49 @@ def workload_ea(M, torch, sweeps=20, realisations=32):
             "roofline": {"bytes_per_update": 5, "frac_of_hbm": hbm_frac(5, rate), "note": "L2-resident"}}
 
 
+def workload_tempering(M, torch, emcs=200, replicas=64, L=128):
+    """Replica exchange: 64 2D Ising replicas L=128 on a beta ladder from 0.40
+    to 0.48, EMCS = 1 Wolff cluster + 1 sweep, an exchange step between
+    neighbouring betas after every EMCS, against the same batch without
+    exchanges."""
+    betas = np.linspace(0.40, 0.48, replicas)
+    members = [(M.RegularHypercubic(L, 2), M.Config(seed=700 + i, repid=i), M.Ising(-1.0), float(b))
+               for i, b in enumerate(betas)]
+    with M.Batch(members, graph_steps=8) as b:
+        b.init()
+        b.emcs(20, 1, 1)
+        st = torch.cuda.ExternalStream(stream_of(b.member(0)))
+        t_plain = timed(torch, st, lambda: b.emcs(emcs, 1, 1))
+        res = []
+        t_pt = timed(torch, st, lambda: res.append(b.tempering(emcs, emcs_per_step=1, ncluster=1, nmetro=1,
+                                                               seed=11)))
+        wolff_auto = "automatic choice: " + b.wolff
+        b.set_wolff("label")
+        b.emcs(2, 1, 1)
+        t_label = timed(torch, st, lambda: b.tempering(emcs, emcs_per_step=1, ncluster=1, nmetro=1, seed=12))
+        b.set_wolff("bfs")
+        b.emcs(2, 1, 1)
+        t_bfs = timed(torch, st, lambda: b.tempering(emcs, emcs_per_step=1, ncluster=1, nmetro=1, seed=13))
+    acc = res[0][1]
+    plan = M.tempering.neighbour_plan(replicas, emcs, first=0)
+    per_pair = np.zeros(replicas - 1)
+    tries = np.zeros(replicas - 1)
+    for t in range(emcs):
+        for p, (a, c) in enumerate(plan[t]):
+            if a != c:
+                per_pair[a] += acc[t, p] == 1
+                tries[a] += 1
+    rate_pair = per_pair / np.maximum(tries, 1)
+    n = replicas * L * L * emcs
+    return {"workload": "64 2D Ising replicas L=128, beta in [0.40, 0.48], EMCS = 1 Wolff + 1 sweep, "
+                        "an exchange step after every EMCS (neighbour pairs)",
+            "unit": UNIT, "value": n / (t_pt * 1e9), "without_exchanges": n / (t_plain * 1e9),
+            "exchange_overhead": t_pt / t_plain - 1.0, "clusters": wolff_auto,
+            "value_label_clusters": n / (t_label * 1e9), "value_bfs_clusters": n / (t_bfs * 1e9),
+            "acceptance_mean": float(rate_pair.mean()), "acceptance_min": float(rate_pair.min()),
+            "includes": "host copies of the observables and exchange outcomes at the end of the call"}
+
+
 def workload_phi4_autograd(M, torch, n_therm=10, n_meas=40):
     """Config 4: 3D phi^4 L=64 for 64 beta values uniform in [0.36, 0.38],
     lambda = 1.1: forward (chains + device samples) and backward (the FDT
@@ -406,7 +449,7 @@ def secondary(M, torch):
     out = {}
     for name, fn in (("potts_batch", workload_potts_batch), ("heisenberg3d_L128", workload_heisenberg),
                      ("phi4_autograd_64xL64", workload_phi4_autograd), ("rgg_ising_N1M", workload_rgg),
-                     ("ea_3d_L32x32", workload_ea)):
+                     ("ea_3d_L32x32", workload_ea), ("tempering_ising2d_64xL128", workload_tempering)):
         try:
             out[name] = fn(M, torch)
         except Exception as exc:  # a secondary line never hides the headline

@@ -245,9 +245,13 @@ MQV_API mqv_status mqv_batch_init_state(mqv_batch* batch);
  * CTA per member, breadth first; or labelling of the activated-bond
  * components of all members in a fixed number of whole-lattice passes
  * (cost independent of cluster depth; pays for percolating clusters on large
- * lattices).  The default is breadth first. */
-enum { MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
+ * lattices).  The default, MQV_WOLFF_AUTO, times both on EMCS 1 and 3 of the
+ * first run with clusters and at least 4 EMCS, then keeps the faster. */
+enum { MQV_WOLFF_AUTO = 0, MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
 MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* batch, int32_t algorithm);
+/* The algorithm in use: MQV_WOLFF_BFS or MQV_WOLFF_LABEL, or MQV_WOLFF_AUTO
+ * while the automatic choice has not been timed yet. */
+MQV_API mqv_status mqv_batch_get_wolff(mqv_batch* batch, int32_t* algorithm);
 /* EMCS per graph launch (1 .. 256; default 8). */
 MQV_API mqv_status mqv_batch_set_graph_steps(mqv_batch* batch, int32_t steps);
 /* n_emcs EMCS of every member (ncluster clusters, then nmetro sweeps, then a

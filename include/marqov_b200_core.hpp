@@ -23,6 +23,7 @@
 #include <cstddef>
 #include <cstdint>
 #include <memory>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -192,10 +193,26 @@ std::unique_ptr<GPUCore<L, H, ConfigT>> makeGPUCore(const std::tuple<L&, ConfigT
 
 // The farm: parameter sets collected with createSimfromParameter (the
 // CXX11Scheduler's interface), run together by start() as one batch on the
-// GPU -- warm-up, then game loop with per-EMCS observables.
+// GPU -- warm-up, then maxptsteps game loops with per-EMCS observables.
+// With maxptsteps > 1 the members exchange states between game loops as the
+// reference's parallel tempering does (CXX11Scheduler::start / ptstep,
+// src/libmarqov/marqovscheduler.h:223-273,374-413): a plan of maxptsteps
+// random pairs (x % len, y % len) from a 64-bit Mersenne twister
+// (createPTplan, :203-210), the pair of step t >= 1 attempting its exchange
+// after the t-th game loop, self pairs skipped.  The reference seeds that
+// generator from the clock; here it is ptseed.  The exchanges run on the
+// device (mqv_batch_tempering).  Partners must differ in beta only.
 template <class L, class H, class ConfigT>
 class GPUScheduler {
 public:
+    // CXX11Scheduler(int maxptsteps = 1, uint nthreads = 0, int mid = 0)
+    // (marqovscheduler.h:280-284); nthreads and mid have no meaning here.
+    explicit GPUScheduler(int maxptsteps = 1, unsigned nthreads = 0, int mid = 0, uint64_t ptseed = 0)
+        : maxpt_(maxptsteps < 1 ? 1 : maxptsteps), ptseed_(ptseed)
+    {
+        (void)nthreads;
+        (void)mid;
+    }
     template <class... HArgs>
     void createSimfromParameter(const std::tuple<L&, ConfigT, std::tuple<HArgs...>>& t)
     {
@@ -215,12 +232,32 @@ public:
         check(mqv_batch_init_state(batch_));
         const Member& f = members_.front();
         check(mqv_batch_emcs(batch_, f.warmup, f.ncluster, f.nmetro, nullptr, nullptr));
-        obs_.resize((std::size_t)f.gameloop * members_.size());
-        check(mqv_batch_emcs(batch_, f.gameloop, f.ncluster, f.nmetro, obs_.data(), nullptr));
+        obs_.resize((std::size_t)f.gameloop * (std::size_t)maxpt_ * members_.size());
+        if (maxpt_ == 1) {
+            check(mqv_batch_emcs(batch_, f.gameloop, f.ncluster, f.nmetro, obs_.data(), nullptr));
+            return;
+        }
+        const uint64_t len = members_.size();
+        std::mt19937_64 rng(ptseed_);
+        std::vector<int32_t> plan(2 * (std::size_t)maxpt_, 0);  // the last step has no exchange
+        for (int t = 0; t < maxpt_; ++t) {
+            const int32_t a = (int32_t)(rng() % len), b = (int32_t)(rng() % len);
+            if (t > 0) {
+                plan[2 * (std::size_t)(t - 1)] = a;
+                plan[2 * (std::size_t)(t - 1) + 1] = b;
+            }
+        }
+        std::vector<int32_t> acc((std::size_t)maxpt_, 0);
+        check(mqv_batch_tempering(batch_, maxpt_, f.gameloop, f.ncluster, f.nmetro, plan.data(), 1, ptseed_,
+                                  obs_.data(), acc.data()));
+        for (int32_t x : acc) acceptedmoves_ += x == 1;
     }
     // record e * size() + i: member i after game-loop EMCS e
     const std::vector<mqv_obs>& observables() const { return obs_; }
     std::size_t size() const { return members_.size(); }
+    // accepted exchanges / maxptsteps, the figure the reference logs
+    // ("PT acceptance", marqovscheduler.h:300)
+    double pt_acceptance() const { return (double)acceptedmoves_ / (double)maxpt_; }
     ~GPUScheduler()
     {
         if (batch_) mqv_batch_destroy(batch_);
@@ -250,6 +287,9 @@ private:
     std::vector<Member> members_;
     mqv_batch* batch_ = nullptr;
     std::vector<mqv_obs> obs_;
+    int maxpt_ = 1;
+    uint64_t ptseed_ = 0;
+    int acceptedmoves_ = 0;
 };
 
 }  // namespace marqov_b200

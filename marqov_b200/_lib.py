@@ -32,7 +32,7 @@ MODEL_ISING, MODEL_ISING_EMBED, MODEL_POTTS, MODEL_BLUME_CAPEL, MODEL_EA, MODEL_
 PROPOSAL_DEFAULT, PROPOSAL_SMALL_CAP = 0, 1
 LATTICE_HYPERCUBIC, LATTICE_CSR = 1, 2
 FLAG_PER_COLOUR = 1
-WOLFF_BFS, WOLFF_LABEL = 1, 2
+WOLFF_AUTO, WOLFF_BFS, WOLFF_LABEL = 0, 1, 2
 
 
 class ModelDesc(C.Structure):
@@ -104,6 +104,7 @@ SIGNATURES = {
     "mqv_batch_init_state": (C.c_int32, [_vp]),
     "mqv_batch_set_graph_steps": (C.c_int32, [_vp, C.c_int32]),
     "mqv_batch_set_wolff": (C.c_int32, [_vp, C.c_int32]),
+    "mqv_batch_get_wolff": (C.c_int32, [_vp, C.POINTER(C.c_int32)]),
     "mqv_batch_emcs": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp, _vp]),
     "mqv_batch_emcs_samples": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, _vp]),
     "mqv_batch_tempering": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32,

@@ -307,11 +307,19 @@ class Batch:
         L.check(self._lib.mqv_batch_init_state(self._h))
 
     def set_wolff(self, algorithm: str):
-        """Cluster algorithm, "bfs" (one CTA per member grows its cluster) or
-        "label" (connected-component labelling of all members); both give the
-        same clusters."""
-        code = {"bfs": L.WOLFF_BFS, "label": L.WOLFF_LABEL}[algorithm]
+        """Cluster algorithm, "bfs" (one CTA per member grows its cluster),
+        "label" (connected-component labelling of all members) or "auto" (the
+        default: the faster of the two, timed on the first run with
+        clusters); all give the same clusters."""
+        code = {"auto": L.WOLFF_AUTO, "bfs": L.WOLFF_BFS, "label": L.WOLFF_LABEL}[algorithm]
         L.check(self._lib.mqv_batch_set_wolff(self._h, code))
+
+    @property
+    def wolff(self) -> str:
+        """The cluster algorithm in use ("auto" until it has been timed)."""
+        v = C.c_int32()
+        L.check(self._lib.mqv_batch_get_wolff(self._h, C.byref(v)))
+        return {L.WOLFF_AUTO: "auto", L.WOLFF_BFS: "bfs", L.WOLFF_LABEL: "label"}[v.value]
 
     def emcs(self, n: int, ncluster: int = 1, nmetro: int = 1):
         """n EMCS of every member; returns (obs [n, members, 4], mean cluster [n, members])."""

@@ -883,7 +883,13 @@ struct Batch {
     int64_t* d_site_prefix = nullptr;
     int32_t* d_site_block_rep = nullptr;
     void* d_ccl_seeds = nullptr;
-    int wolff_mode = 0;  // MQV_WOLFF_*
+    int wolff_mode = MQV_WOLFF_AUTO;
+    // MQV_WOLFF_AUTO: ms per EMCS of breadth first [0] and labelling [1] when
+    // last timed (-1: never), the one in use, EMCS since the other was tried
+    double wolff_est[2] = {-1.0, -1.0};
+    int wolff_best = 0;
+    int64_t wolff_since_try = 0;
+    cudaEvent_t ev[4] = {};
     std::vector<int> block_off, blocks;
     std::vector<int64_t> total;
     BatchCtr* d_ctr = nullptr;
@@ -893,7 +899,7 @@ struct Batch {
     int cap_slots = 0;   // measurement slots in d_acc / d_obs (per member)
     int cap_cslots = 0;  // cluster-size slots in d_csize (per member)
     BatchLaunch L{};
-    cudaGraphExec_t g_one = nullptr, g_many = nullptr;
+    cudaGraphExec_t g_one[2] = {nullptr, nullptr}, g_many[2] = {nullptr, nullptr};  // [labelling clusters]
     int g_ncluster = -1, g_nmetro = -1, g_steps = 0;
     int graph_steps = 8;  // EMCS per graph launch
     uint64_t launches = 0;
@@ -902,9 +908,11 @@ struct Batch {
 
 static void free_graphs(Batch* b)
 {
-    if (b->g_one) cudaGraphExecDestroy(b->g_one);
-    if (b->g_many) cudaGraphExecDestroy(b->g_many);
-    b->g_one = b->g_many = nullptr;
+    for (int w = 0; w < 2; ++w) {
+        if (b->g_one[w]) cudaGraphExecDestroy(b->g_one[w]);
+        if (b->g_many[w]) cudaGraphExecDestroy(b->g_many[w]);
+        b->g_one[w] = b->g_many[w] = nullptr;
+    }
     b->g_ncluster = b->g_nmetro = -1;
 }
 
@@ -914,6 +922,8 @@ static void free_batch(Batch* b)
     DeviceGuard g(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     free_graphs(b);
+    for (cudaEvent_t e : b->ev)
+        if (e) cudaEventDestroy(e);
     for (Sim* s : b->sims) free_sim(s);
     for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin, (void*)b->d_ctr,
                     (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize, (void*)b->d_site_prefix,
@@ -1035,20 +1045,66 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
     if (st) return st;
     if (b->d_acc != acc0 || b->d_csize != csize0) free_graphs(b);  // graphs hold the old pointers
     const int K = std::max(1, std::min(b->graph_steps, CH));
-    if (b->g_ncluster != ncluster || b->g_nmetro != nmetro || b->g_steps != K || !b->g_one) {
+    // Cluster algorithm: fixed, or (MQV_WOLFF_AUTO) chosen by measurement.
+    // Both give the same clusters, so switching never changes the chain; the
+    // cost of breadth-first growth follows the clusters (it rises as a farm
+    // orders), labelling costs the same every EMCS.  Each chunk is timed; the
+    // algorithm not in use is tried on a few EMCS at the start of a chunk when
+    // it has no estimate or its estimate is old (256 EMCS, scaled by how
+    // much slower it was), and the faster estimate is used after that.
+    const bool adapt = b->wolff_mode == MQV_WOLFF_AUTO && ncluster > 0;
+    const int fixed = b->wolff_mode == MQV_WOLFF_LABEL ? 1 : 0;
+    if (b->g_ncluster != ncluster || b->g_nmetro != nmetro || b->g_steps != K) {
         free_graphs(b);
-        MQV_CK(cudaStreamSynchronize(b->stream));
-        st = batch_capture(b, 1, ncluster, nmetro, &b->g_one);
-        if (!st && K > 1) st = batch_capture(b, K, ncluster, nmetro, &b->g_many);
-        if (st) {
-            free_graphs(b);
-            return st;
-        }
         b->g_ncluster = ncluster;
         b->g_nmetro = nmetro;
         b->g_steps = K;
     }
-    const uint64_t per_emcs = batch_launches_per_emcs(b->L, ncluster, nmetro);
+    for (int w = 0; w < 2; ++w) {
+        if (!adapt && w != fixed) continue;
+        if (b->g_one[w] && (K == 1 || b->g_many[w])) continue;
+        MQV_CK(cudaStreamSynchronize(b->stream));
+        b->L.wolff_ccl = w;
+        if (!b->g_one[w]) st = batch_capture(b, 1, ncluster, nmetro, &b->g_one[w]);
+        if (!st && K > 1 && !b->g_many[w]) st = batch_capture(b, K, ncluster, nmetro, &b->g_many[w]);
+        if (!st) {
+            // upload now, so that the first timed launch is not the upload
+            if (cudaGraphUpload(b->g_one[w], b->stream) != cudaSuccess ||
+                (K > 1 && cudaGraphUpload(b->g_many[w], b->stream) != cudaSuccess))
+                st = fail(MQV_ERR_CUDA, "graph upload failed");
+        }
+        if (st) {
+            free_graphs(b);
+            return st;
+        }
+    }
+    if (adapt && !b->ev[0])
+        for (auto& e : b->ev) MQV_CK(cudaEventCreate(&e));
+    uint64_t per_emcs[2];
+    for (int w = 0; w < 2; ++w) {
+        BatchLaunch l = b->L;
+        l.wolff_ccl = w;
+        per_emcs[w] = batch_launches_per_emcs(l, ncluster, nmetro);
+    }
+    // `count` EMCS with the graphs of algorithm w
+    auto launch_emcs = [&](int w, int count) -> mqv_status {
+        int j = 0;
+        if (K > 1)
+            for (; j + K <= count; j += K) MQV_CK(cudaGraphLaunch(b->g_many[w], b->stream));
+        for (; j < count; ++j) MQV_CK(cudaGraphLaunch(b->g_one[w], b->stream));
+        b->launches += per_emcs[w] * (uint64_t)count;
+        return MQV_OK;
+    };
+    // the exchange step that ends after EMCS `e` of the run, if any
+    auto exchange_after = [&](int e) -> mqv_status {
+        if (!pt || e % pt->interval != 0) return MQV_OK;
+        const int t = e / pt->interval - 1;
+        MQV_CK(batch_launch_temper(b->L, b->stream, pt->d_plan + (size_t)2 * pt->npairs * t, pt->npairs,
+                                   pt->step0 + (uint32_t)t, pt->seed, kTemperEnMin, kTemperEnMax, pt->d_perm,
+                                   pt->d_flags + (size_t)pt->npairs * t));
+        b->launches++;
+        return MQV_OK;
+    };
     std::vector<int32_t> csz;
     int done = 0;
     while (done < n_emcs) {
@@ -1056,24 +1112,38 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
         MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
         b->launches++;
-        for (int k = 0; k < ch;) {
-            // EMCS up to the end of the chunk or the next exchange step
-            int run = ch - k;
-            if (pt) run = std::min(run, pt->interval - (done + k) % pt->interval);
-            int j = 0;
-            if (K > 1)
-                for (; j + K <= run; j += K) MQV_CK(cudaGraphLaunch(b->g_many, b->stream));
-            for (; j < run; ++j) MQV_CK(cudaGraphLaunch(b->g_one, b->stream));
-            k += run;
-            if (pt && (done + k) % pt->interval == 0) {
-                const int t = (done + k) / pt->interval - 1;
-                MQV_CK(batch_launch_temper(b->L, b->stream, pt->d_plan + (size_t)2 * pt->npairs * t, pt->npairs,
-                                           pt->step0 + (uint32_t)t, pt->seed, kTemperEnMin, kTemperEnMax, pt->d_perm,
-                                           pt->d_flags + (size_t)pt->npairs * t));
-                b->launches++;
-            }
+        const int w_main = adapt ? b->wolff_best : fixed, w_try = 1 - w_main;
+        int x = 0;  // EMCS of this chunk that try the other algorithm
+        if (adapt) {
+            const double* est = b->wolff_est;
+            const double r = est[w_try] > 0 && est[w_main] > 0 ? std::max(1.0, est[w_try] / est[w_main]) : 1.0;
+            if (est[w_try] < 0 || (double)b->wolff_since_try >= 256.0 * r) x = std::min(4, ch / 2);
         }
-        b->launches += per_emcs * (uint64_t)ch;
+        int k = 0;
+        // `count` EMCS from chunk position k, an exchange step where one ends
+        auto advance = [&](int w, int count) -> mqv_status {
+            const int stop = k + count;
+            while (k < stop) {
+                int run = stop - k;
+                if (pt) run = std::min(run, pt->interval - (done + k) % pt->interval);
+                mqv_status s2 = launch_emcs(w, run);
+                if (s2) return s2;
+                k += run;
+                s2 = exchange_after(done + k);
+                if (s2) return s2;
+            }
+            return MQV_OK;
+        };
+        if (x) {
+            MQV_CK(cudaEventRecord(b->ev[0], b->stream));
+            st = advance(w_try, x);
+            if (st) return st;
+            MQV_CK(cudaEventRecord(b->ev[1], b->stream));
+        }
+        if (adapt) MQV_CK(cudaEventRecord(b->ev[2], b->stream));
+        st = advance(w_main, ch - x);
+        if (st) return st;
+        if (adapt) MQV_CK(cudaEventRecord(b->ev[3], b->stream));
         if (d_samples) {
             MQV_CK(batch_launch_samples(b->L, b->stream, ch, done, n_emcs, d_samples));
             b->launches++;
@@ -1090,6 +1160,20 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
                                    b->stream));
         }
         MQV_CK(cudaStreamSynchronize(b->stream));
+        if (adapt) {
+            float ms = 0;
+            if (x) {
+                MQV_CK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+                b->wolff_est[w_try] = ms / x;
+                b->wolff_since_try = 0;
+            }
+            if (ch > x) {
+                MQV_CK(cudaEventElapsedTime(&ms, b->ev[2], b->ev[3]));
+                b->wolff_est[w_main] = ms / (ch - x);
+            }
+            b->wolff_since_try += ch - x;
+            if (b->wolff_est[0] > 0 && b->wolff_est[1] > 0) b->wolff_best = b->wolff_est[1] < b->wolff_est[0] ? 1 : 0;
+        }
         if (mean_cluster) {
             for (int e = 0; e < ch; ++e)
                 for (int r = 0; r < b->nrep; ++r) {
@@ -1276,7 +1360,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     b->L.total_sites = sprefix[n];
     b->L.site_blocks = (int)sblocks;
     b->L.ccl_seeds = b->d_ccl_seeds;
-    b->L.wolff_ccl = 0;  // breadth-first clusters unless mqv_batch_set_wolff asks for labelling
+    b->L.wolff_ccl = 0;  // set per captured graph (mqv_batch_set_wolff, or timed: MQV_WOLFF_AUTO)
     b->L.ctr = b->d_ctr;
     *out = reinterpret_cast<mqv_batch*>(b);
     return MQV_OK;
@@ -1321,13 +1405,26 @@ MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* h, int32_t algorithm)
 {
     Batch* b = reinterpret_cast<Batch*>(h);
     if (!b) return fail(MQV_ERR_INVALID_ARG, "null handle");
-    if (algorithm != MQV_WOLFF_BFS && algorithm != MQV_WOLFF_LABEL)
+    if (algorithm != MQV_WOLFF_AUTO && algorithm != MQV_WOLFF_BFS && algorithm != MQV_WOLFF_LABEL)
         return fail(MQV_ERR_INVALID_ARG, "unknown cluster algorithm");
-    const int v = algorithm == MQV_WOLFF_LABEL ? 1 : 0;
-    if (v != b->L.wolff_ccl) {
-        b->L.wolff_ccl = v;
-        free_graphs(b);
+    b->wolff_mode = algorithm;
+    if (algorithm == MQV_WOLFF_AUTO) {
+        b->wolff_est[0] = b->wolff_est[1] = -1.0;
+        b->wolff_best = 0;
+        b->wolff_since_try = 0;
     }
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_batch_get_wolff(mqv_batch* h, int32_t* algorithm)
+{
+    Batch* b = reinterpret_cast<Batch*>(h);
+    if (!b || !algorithm) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    const bool timed = b->wolff_est[0] > 0 && b->wolff_est[1] > 0;
+    *algorithm = b->wolff_mode != MQV_WOLFF_AUTO ? b->wolff_mode
+                 : !timed                       ? MQV_WOLFF_AUTO
+                 : b->wolff_best == 1           ? MQV_WOLFF_LABEL
+                                                : MQV_WOLFF_BFS;
     return MQV_OK;
 }
 

@@ -6,7 +6,9 @@
 // through makeCore (src/libshowcase.cpp:40-58): init, wrmploop, gameloop.
 // Output (one line each): "core <e> <|m|>" per game-loop EMCS of a 2D Ising
 // run, then "farm <i> <e> <|m|>" for the last EMCS of each member of a
-// three-member Potts farm and "ea <e> <|m|>" for a random-bond lattice.  With
+// three-member Potts farm, "pt <i> <e> <|m|>" for the last EMCS of each
+// member of a four-member Ising ladder with parallel tempering and "ptacc
+// <acceptance>", and "ea <e> <|m|>" for a random-bond lattice.  With
 // no GPU it prints "no device: <message>" and exits 0.
 #define CACHECONTAINER_H 1
 #include <cstdio>
@@ -90,6 +92,25 @@ int main()
             std::printf("farm %zu %.17g %.17g\n", i, o.e, o.m);
         }
 
+        // parallel tempering over an Ising ladder: CXX11Scheduler(maxptsteps)
+        marqov_b200::GPUScheduler<RegularHypercubic, Ising<int>, Config> pt(6, 0, 0, 3);
+        RegularHypercubic lpt(12, 2);
+        for (int i = 0; i < 4; ++i) {
+            Config c("out");
+            c.seed = 21 + i;
+            c.repid = i;
+            c.ncluster = 1;
+            c.nmetro = 1;
+            c.warmupsteps = 10;
+            c.gameloopsteps = 3;
+            pt.createSimfromParameter(std::make_tuple(std::ref(lpt), c, std::make_tuple(0.38 + 0.04 * i, -1.0)));
+        }
+        pt.start();
+        const auto& po = pt.observables();
+        const std::size_t last = po.size() / pt.size() - 1;
+        for (std::size_t i = 0; i < pt.size(); ++i)
+            std::printf("pt %zu %.17g %.17g\n", i, po[last * pt.size() + i].e, po[last * pt.size() + i].m);
+        std::printf("ptacc %.17g\n", pt.pt_acceptance());
         RegularRandomBond<BimodalPDF> rb(6, 3);
         Config ce("out");
         ce.seed = 9;

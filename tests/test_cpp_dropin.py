@@ -58,3 +58,16 @@ def test_dropin_equals_python_api():
     for i in range(3):
         assert farm[i] == (fo[3, i, 0], fo[3, i, 1])
     assert len(ea) == 1 and np.isfinite([float(ea[0][1]), float(ea[0][2])]).all()
+    # parallel tempering: GPUScheduler(maxptsteps=6, ptseed=3) vs Batch.tempering
+    pt = {int(l[1]): (float(l[2]), float(l[3])) for l in lines if l[0] == "pt"}
+    ptacc = [float(l[1]) for l in lines if l[0] == "ptacc"]
+    ms = [(M.RegularHypercubic(12, 2), M.Config(seed=21 + i, repid=i), M.Ising(-1.0), 0.38 + 0.04 * i)
+          for i in range(4)]
+    with M.Batch(ms) as b:
+        b.init()
+        b.emcs(10, 1, 1)
+        po, acc = b.tempering(6, emcs_per_step=3, ncluster=1, nmetro=1,
+                              plan=M.tempering.reference_plan(4, 6, seed=3), seed=3)
+    for i in range(4):
+        assert pt[i] == (po[-1, i, 0], po[-1, i, 1])
+    assert ptacc == [float((acc == 1).sum()) / 6.0]

@@ -172,16 +172,19 @@ def test_batch_labelling_equals_bfs_on_a_potts_farm():
         ms.append((M.RegularHypercubic(L, 2), M.Config(seed=9000 + i, repid=i), M.Potts(3, -1.0),
                    1.0 / (tc * float(rng.uniform(0.9, 1.1)))))
     out = {}
-    for alg in ("bfs", "label"):
+    for alg in ("bfs", "label", "auto"):
         with M.Batch(ms) as b:
             b.set_wolff(alg)
             b.init()
             o1, m1 = b.emcs(12, 1, 1)
             o2, m2 = b.emcs(8, 2, 0)
             out[alg] = (m1, m2, o1, o2, [b.member(i).state for i in range(len(ms))])
-    for k in range(4):
-        np.testing.assert_array_equal(out["bfs"][k], out["label"][k])
-    assert all((x == y).all() for x, y in zip(out["bfs"][4], out["label"][4]))
+            # auto: timed both on the first call, then kept one of them
+            assert b.wolff == (alg if alg != "auto" else b.wolff) and b.wolff in ("bfs", "label")
+    for alg in ("label", "auto"):
+        for k in range(4):
+            np.testing.assert_array_equal(out["bfs"][k], out[alg][k])
+        assert all((x == y).all() for x, y in zip(out["bfs"][4], out[alg][4]))
 
 
 def test_batch_samples_match_member_samples():
