@@ -11,11 +11,11 @@ from .core import Batch, Config, Core, makeCore, tune_small_cap
 from .hamiltonians import (BlumeCapel, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising, Phi4, Potts,
                            XXZAntiferro)
 from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
-                       RegularRandomBond, read_graph_csv)
+                       RegularRandomBond, read_graph_csv, save_geometry)
 
 _lib.load()
 
 __all__ = ["tempering", "Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
            "Potts", "BlumeCapel", "Heisenberg", "XXZAntiferro", "Phi4", "CSRLattice",
            "FixedDimRegularHypercubic", "RegularHypercubic", "RegularRandomBond", "RandomGeometricGraph2D",
-           "read_graph_csv"]
+           "read_graph_csv", "save_geometry"]

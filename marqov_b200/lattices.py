@@ -14,6 +14,8 @@
 """
 from __future__ import annotations
 
+import re
+
 import numpy as np
 
 from . import _lib as L
@@ -119,6 +121,10 @@ class CSRLattice(Lattice):
     def nbrs(self, alpha: int, i: int):
         return self.col_idx[self.row_ptr[i]:self.row_ptr[i + 1]].tolist()
 
+    def crds(self, i: int) -> list[float]:
+        """Site coordinates as given (none for a lattice built without)."""
+        return [] if self.coords is None else [float(c) for c in self.coords[i]]
+
     def bnds(self, alpha: int, i: int):
         if self.bonds is None:
             raise AttributeError("lattice has no bonds")
@@ -201,20 +207,64 @@ def RandomGeometricGraph2D(n: int, mean_degree: float = 8.0, seed: int = 0) -> C
     return CSRLattice(rp, dst.astype(np.int32), crds=pts)
 
 
-def read_graph_csv(path: str) -> CSRLattice:
-    """Read the reference's graph CSV format (src/lattice/util/io.h:34-126 as
-    used by GraphFromCSV, src/lattice/graph_from_csv.h:32-57): first line the
-    number of coordinates c; then one line per site with c tab-separated
-    coordinates followed by its neighbour ids."""
-    with open(path) as fh:
-        ncoords = int(fh.readline().strip())
-        rp, cols, crd = [0], [], []
-        for line in fh:
-            f = line.split()
-            if not f:
-                continue
-            crd.append([float(x) for x in f[:ncoords]])
-            nb = [int(x) for x in f[ncoords:]]
-            cols.extend(nb)
-            rp.append(rp[-1] + len(nb))
-    return CSRLattice(np.array(rp, np.int32), np.array(cols, np.int32), crds=np.array(crd))
+_STOI = re.compile(r"\s*([+-]?\d+)")
+_STOD = re.compile(r"\s*([+-]?(?:(?:\d+\.?\d*|\.\d+)(?:[eE][+-]?\d+)?|inf(?:inity)?|nan))", re.IGNORECASE)
+
+
+def _stoi(field: str) -> int:
+    """std::stoi: leading blanks, sign and digits; the rest is ignored."""
+    m = _STOI.match(field)
+    if not m:
+        raise ValueError(f"not an integer: {field!r}")
+    return int(m.group(1))
+
+
+def _stod(field: str) -> float:
+    """std::stod on a decimal field: the longest leading number."""
+    m = _STOD.match(field)
+    if not m:
+        raise ValueError(f"not a number: {field!r}")
+    return float(m.group(1))
+
+
+def read_graph_csv(path: str, idxoffs: int = 0) -> CSRLattice:
+    """GraphFromCSV(filename) (src/lattice/graph_from_csv.h:40-44) over
+    import_geometry_ncoords / import_geometry (src/lattice/util/io.h:60-126):
+    line 1 holds the number of coordinates c (std::stoi), line 2 is a header
+    and is skipped, every further line is one site: tab-separated fields, the
+    first c coordinates (std::stod), the rest neighbour ids (std::stoi, minus
+    idxoffs).  An empty line is a site without coordinates or neighbours,
+    except the empty remainder after the last newline; an empty field
+    between two tabs is an error, as std::stod / std::stoi of "" is there."""
+    with open(path, newline="") as fh:
+        rows = fh.read().split("\n")
+    ncoords = _stoi(rows[0])
+    body = rows[2:]
+    if body and body[-1] == "":
+        body = body[:-1]
+    rp, cols, crd = [0], [], []
+    for row in body:
+        fields = row.split("\t") if row else []
+        if fields and fields[-1] == "":
+            fields = fields[:-1]  # a trailing tab ends the line, it opens no field
+        crd.append([_stod(x) for x in fields[:ncoords]])
+        nb = [_stoi(x) - idxoffs for x in fields[ncoords:]]
+        cols.extend(nb)
+        rp.append(rp[-1] + len(nb))
+    rect = all(len(c) == len(crd[0]) for c in crd) if crd else True
+    return CSRLattice(np.array(rp, np.int32), np.array(cols, np.int32),
+                      crds=np.array(crd, np.float64) if rect else crd)
+
+
+def save_geometry(lattice, path: str) -> None:
+    """save_geometry(grid, path) (src/lattice/util/io.h:34-52): one line per
+    site, the count of neighbours plus coordinates, then tab-separated the
+    coordinates (fixed, 16 decimals) and the neighbour ids.  As in the
+    reference, the file has no header lines, so read_graph_csv does not read
+    it back."""
+    with open(path, "w", newline="") as fh:
+        for i in range(int(lattice.size())):
+            nb = list(lattice.nbrs(0, i))
+            cr = list(lattice.crds(i))
+            fh.write(str(len(nb) + len(cr)) + "".join("\t%.16f" % float(c) for c in cr)
+                     + "".join("\t%d" % int(j) for j in nb) + "\n")

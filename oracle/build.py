@@ -46,12 +46,12 @@ def build_ref(force: bool = False) -> str | None:
         return out if os.path.exists(out) else None
     os.makedirs(out_dir, exist_ok=True)
     srcs = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "oracle.c"),
-            os.path.join(HERE, "ref_scheduler.cpp")]
+            os.path.join(HERE, "ref_scheduler.cpp"), os.path.join(HERE, "ref_io.cpp")]
     if force or not _newer(out, srcs):
         obj = os.path.join(out_dir, "oracle_c.o")
         subprocess.check_call(["gcc", "-std=gnu11", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-c",
                                "-o", obj, srcs[1]])
-        cmd = ["g++", "-std=gnu++14", *ARCH, "-w", "-I", src_root, "-o", out, srcs[0], srcs[2], obj,
+        cmd = ["g++", "-std=gnu++14", *ARCH, "-w", "-I", src_root, "-o", out, srcs[0], srcs[2], srcs[3], obj,
                "-lm", "-lpthread"]
         subprocess.check_call(cmd)
     return out

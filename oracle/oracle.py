@@ -244,7 +244,39 @@ class RefHarness:
         lib.ref_calc_mh_ratio.argtypes = [C.c_double]
         lib.ref_pt_calcprob.restype = C.c_int
         lib.ref_pt_calcprob.argtypes = [C.c_int, _f64p, _f64p, _f64p, _f64p, _f64p]
+        lib.ref_save_geometry.restype = C.c_int
+        lib.ref_save_geometry.argtypes = [C.c_int, _i32p, _i32p, C.c_int, _f64p, C.c_char_p]
+        lib.ref_import_geometry.restype = C.c_int
+        lib.ref_import_geometry.argtypes = [C.c_char_p, C.c_int] + [C.POINTER(C.c_int)] * 4 + [C.c_void_p] * 4
         self.lib = lib
+
+    def save_geometry(self, row_ptr, col_idx, coords, path):
+        """The reference's save_geometry over CSR arrays and [n, c] coordinates."""
+        crd = np.ascontiguousarray(coords, np.float64)
+        n = len(row_ptr) - 1
+        nc = crd.shape[1] if crd.ndim == 2 else 0
+        self.lib.ref_save_geometry(n, np.ascontiguousarray(row_ptr, np.int32), np.ascontiguousarray(col_idx, np.int32),
+                                   nc, crd.reshape(-1) if crd.size else np.zeros(1), str(path).encode())
+
+    def import_geometry(self, path, idxoffs=0):
+        """GraphFromCSV / import_geometry: (row_ptr, col_idx, per-site coordinate
+        lists, ncoords), or None where the reference throws."""
+        n, nnz, nv, nc = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        p = str(path).encode()
+        if self.lib.ref_import_geometry(p, idxoffs, C.byref(n), C.byref(nnz), C.byref(nv), C.byref(nc),
+                                        None, None, None, None):
+            return None
+        rp = np.zeros(n.value + 1, np.int32)
+        ci = np.zeros(max(nnz.value, 1), np.int32)
+        cnt = np.zeros(max(n.value, 1), np.int32)
+        crd = np.zeros(max(nv.value, 1), np.float64)
+        self.lib.ref_import_geometry(p, idxoffs, C.byref(n), C.byref(nnz), C.byref(nv), C.byref(nc),
+                                     rp.ctypes.data, ci.ctypes.data, cnt.ctypes.data, crd.ctypes.data)
+        lists, o = [], 0
+        for k in cnt[:n.value]:
+            lists.append(crd[o:o + k].tolist())
+            o += k
+        return rp, ci[:nnz.value], lists, nc.value
 
     def calc_mh_ratio(self, en):
         return float(self.lib.ref_calc_mh_ratio(en))

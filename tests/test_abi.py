@@ -123,6 +123,6 @@ def test_random_geometric_graph():
 def test_graph_csv_roundtrip(tmp_path):
     from marqov_b200 import read_graph_csv
     p = tmp_path / "g.csv"
-    p.write_text("2\n0.1\t0.2\t1\t2\n0.3\t0.4\t0\n0.5\t0.6\t0\n")
+    p.write_text("2\nx y neighbours\n0.1\t0.2\t1\t2\n0.3\t0.4\t0\n0.5\t0.6\t0\n")
     g = read_graph_csv(str(p))
     assert g.n == 3 and g.nbrs(0, 0) == [1, 2] and g.nbrs(0, 2) == [0]
