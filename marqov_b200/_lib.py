@@ -134,6 +134,10 @@ def load() -> C.CDLL:
     return lib
 
 
+def version() -> str:
+    return load().mqv_version().decode()
+
+
 def device_count() -> int:
     n = C.c_int32(0)
     load().mqv_device_count(C.byref(n))

@@ -21,7 +21,8 @@ from .lattices import Lattice
 @dataclass
 class Config:
     """``MARQOV::Config`` (core.h:74-192): method parameters."""
-    outpath: str = ""
+    outpath: str = ""   # with outname: the dump container outpath + outname + ".mqv" (none if empty)
+    outname: str = ""
     id: int = 0
     repid: int = 0
     seed: int = 0
@@ -84,16 +85,36 @@ class Core:
         self.beta = float(beta)
         self._lib = lib
         self._h = C.c_void_p()
-        md = ham.desc(self.beta)
-        ld = lattice.desc()
-        rp = L.RunParams(beta=self.beta, seed=int(config.seed) & (2 ** 64 - 1),
-                         replica=int(config.repid), device=int(config.device),
-                         flags=L.FLAG_PER_COLOUR if config.per_colour else 0)
-        L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
         self._owner = None
         self._setup(lattice, ham)
+        # the dump container (Core's constructor, src/libmarqov/core.h:469-488):
+        # a new step, continuing from the previous step's final state and RNG
+        seed, replica, restore = int(config.seed), int(config.repid), None
+        if config.outpath:
+            from . import checkpoint as CP
+            path = CP.container_path(config)
+            prev = CP.last_step(path)
+            if prev >= 0:
+                last = CP.Step(path, prev)
+                if not last.complete:
+                    raise RuntimeError(f"{last.path} holds no final state (its run did not end)")
+                restore = last.read_state()
+                seed, replica = restore[1][0], restore[1][1]
+            self._step = CP.Step(path, prev + 1).create(self.beta, config, lattice, ham, L.version())
+        md = ham.desc(self.beta)
+        ld = lattice.desc()
+        rp = L.RunParams(beta=self.beta, seed=seed & (2 ** 64 - 1), replica=replica, device=int(config.device),
+                         flags=L.FLAG_PER_COLOUR if config.per_colour else 0)
+        L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
+        self._seed, self._replica = seed, replica
+        if restore is not None:
+            self.state = restore[0]
+            self.counters = restore[1][2:]
+            self._restored = True
 
     def _setup(self, lattice: Lattice, ham: Hamiltonian):
+        self._step = None
+        self._restored = False
         self.n = int(lattice.size())
         self.symd = ham.SymD
         self.dtype = ham.dtype
@@ -113,9 +134,21 @@ class Core:
         return c
 
     # -- lifecycle
+    def dump(self):
+        """Write the step's observable time series and final state (what
+        ~Core writes, src/libmarqov/core.h:876-902); close() calls it."""
+        if self._step is None or not self._h:
+            return
+        self._step.write_observables(self.obs.arrays())
+        sweep, cluster = self.counters
+        self._step.write_state(self.state, self._seed, self._replica, sweep, cluster)
+
     def close(self):
         if self._h and self._owner is None:
-            self._lib.mqv_destroy(self._h)
+            try:
+                self.dump()
+            finally:
+                self._lib.mqv_destroy(self._h)
         self._h = C.c_void_p()
 
     def __del__(self):
@@ -136,7 +169,10 @@ class Core:
 
     # -- reference Core API
     def init(self):
-        """Random initial state (Core::init -> initstatespace)."""
+        """Random initial state (Core::init -> initstatespace); a Core that
+        continues a dump keeps the state it read (core.h:829-834)."""
+        if self._restored:
+            return
         L.check(self._lib.mqv_init_state(self._h))
 
     def elementaryMCstep(self) -> float:
