@@ -65,14 +65,14 @@ __global__ void __launch_bounds__(1024) batch_wolff(const BatchRep* __restrict__
     const uint32_t tgs = tag(kWolffSeed, R.replica), tgb = tag(kWolffBond, R.replica);
     if (F32) {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            wolff_f32_cluster(R.md, R.st, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+            wolff_f32_cluster(R.md, R.st, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
         else
-            wolff_f32_cluster(R.md, R.csr, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+            wolff_f32_cluster(R.md, R.csr, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
     } else {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            wolff_int8_cluster(R.w, R.st, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+            wolff_int8_cluster(R.w, R.st, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
         else
-            wolff_int8_cluster(R.w, R.csr, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb);
+            wolff_int8_cluster(R.w, R.csr, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
     }
 }
 

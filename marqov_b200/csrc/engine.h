@@ -99,6 +99,12 @@ struct WolffDev {
     unsigned long long thr; // Ising exact: u53 < thr adds; embedded/Potts: u53 >= thr adds
     int q;
 };
+// Threads given to one frontier site in a breadth-first cluster level: one
+// per neighbour on stencils; on CSR graphs up to 8, a site of higher degree
+// looping over its neighbours t0, t0 + lanes, ...
+MQV_HD int wolff_lanes(const StencilDev& st, int) { return 2 * st.dim; }
+MQV_HD int wolff_lanes(const CSRDev&, int max_degree) { return max_degree < 1 ? 1 : max_degree > 8 ? 8 : max_degree; }
+
 // u53 cuts of an int8 model's Metropolis moves for lattices of maximum degree
 // D, indexed as int8_site computes its dE index (host side).
 std::vector<unsigned long long> int8_cut_table(const ModelDev& md, int D);

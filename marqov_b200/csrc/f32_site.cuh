@@ -242,7 +242,7 @@ template <class Lat>
 __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& lat, float* __restrict__ s,
                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                  uint32_t tg_seed, uint32_t tg_bond)
+                                                  uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
     __shared__ int s_head, s_tail, s_next;
     __shared__ float s_r[3];
@@ -263,24 +263,37 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     __syncthreads();
     const float r0 = s_r[0], r1 = s_r[1], r2 = s_r[2];
     auto proj = [&](int64_t i) -> double { return embed_proj(symd, s, i, r0, r1, r2); };
+    const int lanes = wolff_lanes(lat, max_degree);
     const unsigned lane = threadIdx.x & 31;
     while (true) {
         const int head = s_head, tail = s_tail;
         if (head >= tail) break;
-        for (int base = head; base < tail; base += blockDim.x) {
-            const int idx = base + threadIdx.x;
-            const bool live = idx < tail;
-            const int64_t cur = live ? queue[idx] : 0;
-            const int deg = live ? lat.degree(cur) : 0;
-            const double ac = live ? proj(cur) : 0.0;
-            const int maxdeg = __reduce_max_sync(0xffffffffu, deg);
-            for (int t = 0; t < maxdeg; ++t) {
+        // (frontier site, neighbour lane) items, as in wolff_int8_cluster
+        const int64_t items = (int64_t)(tail - head) * lanes;
+        for (int64_t base = 0; base < items; base += blockDim.x) {
+            const int64_t k = base + threadIdx.x;
+            int64_t cur = 0;
+            int t0 = 0, deg = 0;
+            double ac = 0.0;
+            if (k < items) {
+                const int64_t q = k / lanes;
+                t0 = (int)(k - q * lanes);
+                cur = queue[head + q];
+                deg = lat.degree(cur);
+                ac = proj(cur);
+            }
+            const int rounds = __reduce_max_sync(0xffffffffu, deg > t0 ? (deg - t0 + lanes - 1) / lanes : 0);
+            for (int rr = 0; rr < rounds; ++rr) {
+                const int t = t0 + rr * lanes;
                 bool add = false;
                 int64_t j = 0;
                 if (t < deg) {
                     j = lat.nbr(cur, t);
-                    if (!(visited[j >> 5] & (1u << (j & 31)))) {
-                        const double cpl = embed_cpl(m.J, ac, proj(j));
+                    // both loads issued before either is tested
+                    const uint32_t vw = visited[j >> 5];
+                    const double aj = proj(j);
+                    if (!(vw & (1u << (j & 31)))) {
+                        const double cpl = embed_cpl(m.J, ac, aj);
                         if (cpl > 0) {
                             const uint32_t lo = (uint32_t)(cur < j ? cur : j), hi = (uint32_t)(cur < j ? j : cur);
                             const uint64_t wd = lo64(philox(lo, serial, hi, tg_bond, key));

@@ -65,9 +65,9 @@ template <class Lat>
 __global__ void __launch_bounds__(1024) wolff_f32(ModelDev m, Lat lat, float* __restrict__ s,
                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                  uint32_t tg_seed, uint32_t tg_bond)
+                                                  uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
-    wolff_f32_cluster(m, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond);
+    wolff_f32_cluster(m, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree);
 }
 
 // ---- launchers ------------------------------------------------------------------
@@ -141,10 +141,10 @@ cudaError_t launch_wolff_f32(Sim* s, int slot)
     int32_t* out = s->d_csize + slot;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC)
         wolff_f32<<<1, 1024, 0, s->stream>>>(s->md, s->sten, st, s->d_visited, s->d_queue, out, key, serial,
-                                             tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                             tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     else
         wolff_f32<<<1, 1024, 0, s->stream>>>(s->md, s->csr, st, s->d_visited, s->d_queue, out, key, serial,
-                                             tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                             tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     s->launches++;
     s->cluster++;
     return cudaGetLastError();

@@ -27,9 +27,9 @@ template <class Lat>
 __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* __restrict__ s,
                                                    uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                    int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                   uint32_t tg_seed, uint32_t tg_bond)
+                                                   uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
-    wolff_int8_cluster(w, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond);
+    wolff_int8_cluster(w, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree);
 }
 
 unsigned long long accept_cut(int pref, double dE, double beta);
@@ -74,10 +74,10 @@ cudaError_t launch_wolff_int8(Sim* s, int slot)
     int32_t* out = s->d_csize + slot;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC)
         wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->sten, st, s->d_visited, s->d_queue, out, key, serial,
-                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     else
         wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->csr, st, s->d_visited, s->d_queue, out, key, serial,
-                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     s->launches++;
     s->cluster++;
     return cudaGetLastError();
@@ -150,10 +150,10 @@ cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot)
     const uint32_t serial = (uint32_t)s->cluster;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC)
         wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->sten, st, visited, queue, sizes + slot, key, serial,
-                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     else
         wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->csr, st, visited, queue, sizes + slot, key, serial,
-                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica));
+                                              tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     s->launches++;
     s->cluster++;
     return cudaGetLastError();

@@ -40,15 +40,17 @@ __device__ __forceinline__ bool wolff_int8_active(const WolffDev& w, uint32_t a,
 
 // One cluster grown and flipped by the calling CTA (any block size that is a
 // multiple of 32); the visited bits of its members are cleared before return.
+// A level's work items are (frontier site, neighbour lane) pairs, so the
+// neighbours of a site are examined side by side rather than one after the
+// other (the cluster is the same in any visiting order).
 template <class Lat>
 __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat& lat, int8_t* __restrict__ s,
                                                    uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                    int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                   uint32_t tg_seed, uint32_t tg_bond)
+                                                   uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
     __shared__ int s_head, s_tail, s_next;
     __shared__ int s_val, s_newq;
-    const int64_t n = lat.n;
     if (threadIdx.x == 0) {
         int val, newq;
         const int64_t rsite = wolff_int8_seed(w, lat, s, key, serial, tg_seed, val, newq);
@@ -62,23 +64,33 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
     }
     __syncthreads();
     const int val = s_val;
+    const int lanes = wolff_lanes(lat, max_degree);
     const unsigned lane = threadIdx.x & 31;
     while (true) {
         const int head = s_head, tail = s_tail;
         if (head >= tail) break;
-        for (int base = head; base < tail; base += blockDim.x) {
-            const int idx = base + threadIdx.x;
-            const bool live = idx < tail;
-            const int64_t cur = live ? queue[idx] : 0;
-            const int deg = live ? lat.degree(cur) : 0;
-            int maxdeg = __reduce_max_sync(0xffffffffu, deg);
-            for (int t = 0; t < maxdeg; ++t) {
+        const int64_t items = (int64_t)(tail - head) * lanes;
+        for (int64_t base = 0; base < items; base += blockDim.x) {
+            const int64_t k = base + threadIdx.x;
+            int64_t cur = 0;
+            int t0 = 0, deg = 0;
+            if (k < items) {
+                const int64_t q = k / lanes;
+                t0 = (int)(k - q * lanes);
+                cur = queue[head + q];
+                deg = lat.degree(cur);
+            }
+            const int rounds = __reduce_max_sync(0xffffffffu, deg > t0 ? (deg - t0 + lanes - 1) / lanes : 0);
+            for (int rr = 0; rr < rounds; ++rr) {
+                const int t = t0 + rr * lanes;
                 bool add = false;
                 int64_t j = 0;
                 if (t < deg) {
                     j = lat.nbr(cur, t);
+                    // both loads issued before either is tested
                     const int sj = s[lat.addr(j)];
-                    if (sj == val && !(visited[j >> 5] & (1u << (j & 31)))) {
+                    const uint32_t vw = visited[j >> 5];
+                    if (sj == val && !(vw & (1u << (j & 31)))) {
                         if (wolff_int8_active(w, (uint32_t)cur, (uint32_t)j, serial, tg_bond, key)) {
                             const uint32_t old = atomicOr(&visited[j >> 5], 1u << (j & 31));
                             add = !(old & (1u << (j & 31)));
