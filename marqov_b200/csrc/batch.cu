@@ -63,16 +63,22 @@ __global__ void __launch_bounds__(1024) batch_wolff(const BatchRep* __restrict__
     const uint32_t serial = R.cluster0 + e * (uint32_t)ncluster + (uint32_t)c;
     int32_t* out = csize + ((size_t)slot * ncluster + c) * nrep + blockIdx.x;
     const uint32_t tgs = tag(kWolffSeed, R.replica), tgb = tag(kWolffBond, R.replica);
+    // frontier buffers: int8 ids, or float ids followed by their projections
+    __shared__ __align__(16) unsigned char wbuf[kWolffSmem];
+    int32_t* fbuf = reinterpret_cast<int32_t*>(wbuf);
+    double* fproj = reinterpret_cast<double*>(wbuf + 2 * kWolffCapF * sizeof(int32_t));
     if (F32) {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            wolff_f32_cluster(R.md, R.st, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
+            wolff_f32_cluster(R.md, R.st, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D, fbuf,
+                              fproj);
         else
-            wolff_f32_cluster(R.md, R.csr, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
+            wolff_f32_cluster(R.md, R.csr, (float*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D, fbuf,
+                              fproj);
     } else {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            wolff_int8_cluster(R.w, R.st, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
+            wolff_int8_cluster(R.w, R.st, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D, fbuf);
         else
-            wolff_int8_cluster(R.w, R.csr, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D);
+            wolff_int8_cluster(R.w, R.csr, (int8_t*)R.s, R.visited, R.queue, out, R.key, serial, tgs, tgb, R.D, fbuf);
     }
 }
 

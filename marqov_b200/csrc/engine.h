@@ -99,6 +99,15 @@ struct WolffDev {
     unsigned long long thr; // Ising exact: u53 < thr adds; embedded/Potts: u53 >= thr adds
     int q;
 };
+// Shared memory of a breadth-first cluster kernel for the frontier of the
+// current and of the next level (site ids; float models also the site's
+// projection on the embedding direction), so that a level reads its sites
+// from shared memory; a level larger than the buffer is read from the
+// global queue.  int8: 2 x 4608 ids; float: 2 x 1536 (id, projection).
+constexpr int kWolffSmem = 36864;
+constexpr int kWolffCap8 = kWolffSmem / 8;
+constexpr int kWolffCapF = kWolffSmem / 24;
+
 // Threads given to one frontier site in a breadth-first cluster level: one
 // per neighbour on stencils; on CSR graphs up to 8, a site of higher degree
 // looping over its neighbours t0, t0 + lanes, ...

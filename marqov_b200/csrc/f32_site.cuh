@@ -242,10 +242,12 @@ template <class Lat>
 __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& lat, float* __restrict__ s,
                                                   uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                  uint32_t tg_seed, uint32_t tg_bond, int max_degree)
+                                                  uint32_t tg_seed, uint32_t tg_bond, int max_degree,
+                                                  int32_t* __restrict__ fbuf, double* __restrict__ fproj)
 {
     __shared__ int s_head, s_tail, s_next;
     __shared__ float s_r[3];
+    constexpr int CAP = kWolffCapF;
     const int64_t n = lat.n;
     const int symd = m.symd;
     if (threadIdx.x == 0) {
@@ -255,6 +257,8 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
         s_r[1] = r[1];
         s_r[2] = r[2];
         queue[0] = (int32_t)rsite;
+        fbuf[0] = (int32_t)rsite;
+        fproj[0] = embed_proj(symd, s, rsite, r[0], r[1], r[2]);
         atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
         s_head = 0;
         s_tail = 1;
@@ -265,10 +269,16 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     auto proj = [&](int64_t i) -> double { return embed_proj(symd, s, i, r0, r1, r2); };
     const int lanes = wolff_lanes(lat, max_degree);
     const unsigned lane = threadIdx.x & 31;
-    while (true) {
+    for (int lvl = 0;; ++lvl) {
         const int head = s_head, tail = s_tail;
         if (head >= tail) break;
-        // (frontier site, neighbour lane) items, as in wolff_int8_cluster
+        // (frontier site, neighbour lane) items, as in wolff_int8_cluster; the
+        // level's sites and projections from shared memory when they fit
+        const bool fits = tail - head <= CAP;
+        const int32_t* fcur = fbuf + (lvl & 1) * CAP;
+        const double* pcur = fproj + (lvl & 1) * CAP;
+        int32_t* fnext = fbuf + ((lvl + 1) & 1) * CAP;
+        double* pnext = fproj + ((lvl + 1) & 1) * CAP;
         const int64_t items = (int64_t)(tail - head) * lanes;
         for (int64_t base = 0; base < items; base += blockDim.x) {
             const int64_t k = base + threadIdx.x;
@@ -278,20 +288,26 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
             if (k < items) {
                 const int64_t q = k / lanes;
                 t0 = (int)(k - q * lanes);
-                cur = queue[head + q];
+                if (fits) {
+                    cur = fcur[q];
+                    ac = pcur[q];
+                } else {
+                    cur = queue[head + q];
+                    ac = proj(cur);
+                }
                 deg = lat.degree(cur);
-                ac = proj(cur);
             }
             const int rounds = __reduce_max_sync(0xffffffffu, deg > t0 ? (deg - t0 + lanes - 1) / lanes : 0);
             for (int rr = 0; rr < rounds; ++rr) {
                 const int t = t0 + rr * lanes;
                 bool add = false;
                 int64_t j = 0;
+                double aj = 0.0;
                 if (t < deg) {
                     j = lat.nbr(cur, t);
                     // both loads issued before either is tested
                     const uint32_t vw = visited[j >> 5];
-                    const double aj = proj(j);
+                    aj = proj(j);
                     if (!(vw & (1u << (j & 31)))) {
                         const double cpl = embed_cpl(m.J, ac, aj);
                         if (cpl > 0) {
@@ -309,7 +325,14 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
                     int pos = 0;
                     if (lane == 0) pos = atomicAdd(&s_next, __popc(mask));
                     pos = __shfl_sync(0xffffffffu, pos, 0);
-                    if (add) queue[pos + __popc(mask & ((1u << lane) - 1))] = (int32_t)j;
+                    if (add) {
+                        const int at = pos + __popc(mask & ((1u << lane) - 1));
+                        queue[at] = (int32_t)j;
+                        if (at - tail < CAP) {
+                            fnext[at - tail] = (int32_t)j;
+                            pnext[at - tail] = aj;
+                        }
+                    }
                 }
             }
         }

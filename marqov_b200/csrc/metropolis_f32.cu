@@ -67,7 +67,9 @@ __global__ void __launch_bounds__(1024) wolff_f32(ModelDev m, Lat lat, float* __
                                                   int32_t* __restrict__ out_size, Key key, uint32_t serial,
                                                   uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
-    wolff_f32_cluster(m, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree);
+    __shared__ int32_t fbuf[2 * kWolffCapF];
+    __shared__ double fproj[2 * kWolffCapF];
+    wolff_f32_cluster(m, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree, fbuf, fproj);
 }
 
 // ---- launchers ------------------------------------------------------------------

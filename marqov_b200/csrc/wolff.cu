@@ -29,7 +29,8 @@ __global__ void __launch_bounds__(1024) wolff_int8(WolffDev w, Lat lat, int8_t* 
                                                    int32_t* __restrict__ out_size, Key key, uint32_t serial,
                                                    uint32_t tg_seed, uint32_t tg_bond, int max_degree)
 {
-    wolff_int8_cluster(w, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree);
+    __shared__ int32_t fbuf[2 * kWolffCap8];
+    wolff_int8_cluster(w, lat, s, visited, queue, out_size, key, serial, tg_seed, tg_bond, max_degree, fbuf);
 }
 
 unsigned long long accept_cut(int pref, double dE, double beta);

@@ -47,16 +47,19 @@ template <class Lat>
 __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat& lat, int8_t* __restrict__ s,
                                                    uint32_t* __restrict__ visited, int32_t* __restrict__ queue,
                                                    int32_t* __restrict__ out_size, Key key, uint32_t serial,
-                                                   uint32_t tg_seed, uint32_t tg_bond, int max_degree)
+                                                   uint32_t tg_seed, uint32_t tg_bond, int max_degree,
+                                                   int32_t* __restrict__ fbuf)
 {
     __shared__ int s_head, s_tail, s_next;
     __shared__ int s_val, s_newq;
+    constexpr int CAP = kWolffCap8;
     if (threadIdx.x == 0) {
         int val, newq;
         const int64_t rsite = wolff_int8_seed(w, lat, s, key, serial, tg_seed, val, newq);
         s_val = val;
         s_newq = newq;
         queue[0] = (int32_t)rsite;
+        fbuf[0] = (int32_t)rsite;
         atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
         s_head = 0;
         s_tail = 1;
@@ -66,9 +69,13 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
     const int val = s_val;
     const int lanes = wolff_lanes(lat, max_degree);
     const unsigned lane = threadIdx.x & 31;
-    while (true) {
+    for (int lvl = 0;; ++lvl) {
         const int head = s_head, tail = s_tail;
         if (head >= tail) break;
+        // the level's sites: fbuf[(lvl & 1) * CAP ...] when they fit, else the queue
+        const bool fits = tail - head <= CAP;
+        const int32_t* fcur = fbuf + (lvl & 1) * CAP;
+        int32_t* fnext = fbuf + ((lvl + 1) & 1) * CAP;
         const int64_t items = (int64_t)(tail - head) * lanes;
         for (int64_t base = 0; base < items; base += blockDim.x) {
             const int64_t k = base + threadIdx.x;
@@ -77,7 +84,7 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
             if (k < items) {
                 const int64_t q = k / lanes;
                 t0 = (int)(k - q * lanes);
-                cur = queue[head + q];
+                cur = fits ? fcur[q] : queue[head + q];
                 deg = lat.degree(cur);
             }
             const int rounds = __reduce_max_sync(0xffffffffu, deg > t0 ? (deg - t0 + lanes - 1) / lanes : 0);
@@ -102,7 +109,11 @@ __device__ __forceinline__ void wolff_int8_cluster(const WolffDev& w, const Lat&
                     int pos = 0;
                     if (lane == 0) pos = atomicAdd(&s_next, __popc(mask));
                     pos = __shfl_sync(0xffffffffu, pos, 0);
-                    if (add) queue[pos + __popc(mask & ((1u << lane) - 1))] = (int32_t)j;
+                    if (add) {
+                        const int at = pos + __popc(mask & ((1u << lane) - 1));
+                        queue[at] = (int32_t)j;
+                        if (at - tail < CAP) fnext[at - tail] = (int32_t)j;
+                    }
                 }
             }
         }
