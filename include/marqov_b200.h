@@ -289,6 +289,11 @@ MQV_API mqv_status mqv_batch_launch_count(mqv_batch* batch, uint64_t* count);
 /* Self test: Philox blocks for n counters (c0 = i, other words given) computed
  * on the device by the engine and by cuRAND's Philox4_32_10; out_engine and
  * out_curand receive 4n words each (host). */
+/* Self test (host only, no device needed): the closed-form acceptance cut
+ * the sweep kernels use, cut[i] = the smallest word >> 11 that
+ * update_accepted<pref>(dE[i], beta[i], word) rejects (2^53: none). */
+MQV_API mqv_status mqv_selftest_accept_cut(int32_t pref, int32_t n, const double* dE, const double* beta,
+                                           uint64_t* cut);
 MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3,
                                        int32_t n, uint32_t* out_engine, uint32_t* out_curand);
 

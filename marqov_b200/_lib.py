@@ -110,6 +110,7 @@ SIGNATURES = {
     "mqv_batch_tempering": (C.c_int32, [_vp, C.c_int32, C.c_int32, C.c_int32, C.c_int32, _vp, C.c_int32,
                                         C.c_uint64, _vp, _vp]),
     "mqv_batch_launch_count": (C.c_int32, [_vp, C.POINTER(C.c_uint64)]),
+    "mqv_selftest_accept_cut": (C.c_int32, [C.c_int32, C.c_int32, _vp, _vp, _vp]),
     "mqv_selftest_philox": (C.c_int32, [C.c_uint64, C.c_uint32, C.c_uint32, C.c_uint32, C.c_int32,
                                         _vp, _vp]),
 }

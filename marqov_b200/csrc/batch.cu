@@ -29,28 +29,30 @@
 namespace mqv {
 
 template <bool F32, class Lat>
-__device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep)
+__device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep, bool live)
 {
-    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica);
-    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D);
+    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica, live);
+    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live);
 }
 
+// Lanes past the end of the colour's work take no part (live == false).
 template <bool F32>
 __global__ void batch_metro(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
                             const int32_t* __restrict__ block_rep, const int32_t* __restrict__ cbegin, int ncol,
                             int64_t total, int colour, const BatchCtr* __restrict__ ctr, int nmetro, int j)
 {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
+    const bool live = g < total;
     int r = block_rep[blockIdx.x];
-    while (g >= prefix[r + 1]) ++r;
+    if (live)
+        while (g >= prefix[r + 1]) ++r;
     const BatchRep& R = reps[r];
-    const int64_t t = g - prefix[r];
+    const int64_t t = live ? g - prefix[r] : 0;
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
     if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep);
+        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep, live);
     else
-        batch_site<F32>(R, R.csr, (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t], sweep);
+        batch_site<F32>(R, R.csr, live ? (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t] : 0, sweep, live);
 }
 
 template <bool F32>
@@ -82,23 +84,27 @@ __global__ void __launch_bounds__(1024) batch_wolff(const BatchRep* __restrict__
     }
 }
 
+// One CTA per (member, part): member sizes set their number of parts.
 template <bool F32>
 __global__ void batch_measure(const BatchRep* __restrict__ reps, const BatchCtr* __restrict__ ctr,
-                              long long* __restrict__ acc, int nrep)
+                              long long* __restrict__ acc, int nrep, const int32_t* __restrict__ meas_prefix,
+                              const int32_t* __restrict__ meas_rep)
 {
-    const BatchRep& R = reps[blockIdx.y];
+    const int r = meas_rep[blockIdx.x];
+    const int part = (int)blockIdx.x - meas_prefix[r], nparts = meas_prefix[r + 1] - meas_prefix[r];
+    const BatchRep& R = reps[r];
     const uint32_t slot = ctr->e - ctr->ebase;
-    long long* a = acc + ((size_t)slot * nrep + blockIdx.y) * kAccStride;
+    long long* a = acc + ((size_t)slot * nrep + r) * kAccStride;
     if (F32) {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            measure_f32_part(R.md, R.st, (const float*)R.s, (double*)a, blockIdx.x, gridDim.x);
+            measure_f32_part(R.md, R.st, (const float*)R.s, (double*)a, part, nparts);
         else
-            measure_f32_part(R.md, R.csr, (const float*)R.s, (double*)a, blockIdx.x, gridDim.x);
+            measure_f32_part(R.md, R.csr, (const float*)R.s, (double*)a, part, nparts);
     } else {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            measure_int8_part(R.md, R.st, (const int8_t*)R.s, a, blockIdx.x, gridDim.x);
+            measure_int8_part(R.md, R.st, (const int8_t*)R.s, a, part, nparts);
         else
-            measure_int8_part(R.md, R.csr, (const int8_t*)R.s, a, blockIdx.x, gridDim.x);
+            measure_int8_part(R.md, R.csr, (const int8_t*)R.s, a, part, nparts);
     }
 }
 
@@ -229,7 +235,7 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
                 b.reps, b.prefix + (size_t)colour * (b.nrep + 1), b.block_rep + b.block_off[colour], b.cbegin, b.ncol,
                 b.total[colour], colour, b.ctr, nmetro, j);
         }
-    batch_measure<F32><<<dim3(b.meas_parts, b.nrep), 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep);
+    batch_measure<F32><<<b.meas_blocks, 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep, b.meas_prefix, b.meas_rep);
     batch_tick<<<1, 1, 0, st>>>(b.ctr);
 }
 

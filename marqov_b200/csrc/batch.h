@@ -46,7 +46,11 @@ struct BatchLaunch {
     const int* block_off;        // host: [ncol] offsets into block_rep
     const int* blocks;           // host: [ncol] blocks of each colour
     const int64_t* total;        // host: [ncol] work items of each colour
-    int meas_parts;              // measurement CTAs per member
+    // measurement: member r's sites are split over meas_prefix[r + 1] -
+    // meas_prefix[r] CTAs (about 4096 sites each); meas_rep[c] is CTA c's member
+    const int32_t* meas_prefix;  // [nrep + 1]
+    const int32_t* meas_rep;     // [meas_blocks]
+    int meas_blocks;
     // site-level work (every site of every member) for the labelling Wolff
     const int64_t* site_prefix;  // [nrep + 1]
     const int32_t* site_block_rep;

@@ -840,6 +840,15 @@ MQV_API mqv_status mqv_launch_count(mqv_sim* h, uint64_t* count)
     return MQV_OK;
 }
 
+MQV_API mqv_status mqv_selftest_accept_cut(int32_t pref, int32_t n, const double* dE, const double* beta,
+                                           uint64_t* cut)
+{
+    if (n < 0 || (n > 0 && (!dE || !beta || !cut)) || (pref != 1 && pref != 2))
+        return fail(MQV_ERR_INVALID_ARG, "bad arguments");
+    for (int32_t i = 0; i < n; ++i) cut[i] = accept_cut_direct(pref, dE[i], beta[i]);
+    return MQV_OK;
+}
+
 MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3, int32_t n,
                                        uint32_t* out_engine, uint32_t* out_curand)
 {
@@ -882,6 +891,8 @@ struct Batch {
     int32_t* d_cbegin = nullptr;
     int64_t* d_site_prefix = nullptr;
     int32_t* d_site_block_rep = nullptr;
+    int32_t* d_meas_prefix = nullptr;
+    int32_t* d_meas_rep = nullptr;
     void* d_ccl_seeds = nullptr;
     int wolff_mode = MQV_WOLFF_AUTO;
     // MQV_WOLFF_AUTO: ms per EMCS of breadth first [0] and labelling [1] when
@@ -927,7 +938,7 @@ static void free_batch(Batch* b)
     for (Sim* s : b->sims) free_sim(s);
     for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin, (void*)b->d_ctr,
                     (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize, (void*)b->d_site_prefix,
-                    (void*)b->d_site_block_rep, b->d_ccl_seeds})
+                    (void*)b->d_site_block_rep, (void*)b->d_meas_prefix, (void*)b->d_meas_rep, b->d_ccl_seeds})
         if (p) cudaFree(p);
     if (b->stream) cudaStreamDestroy(b->stream);
     delete b;
@@ -1279,11 +1290,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     }
     // per-colour work: colour c concatenates every member's colour-c sites
     int ncol = 0;
-    int64_t nmax = 0;
-    for (Sim* s : b->sims) {
-        ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
-        nmax = std::max(nmax, s->n);
-    }
+    for (Sim* s : b->sims) ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
     std::vector<int64_t> prefix((size_t)ncol * (n + 1), 0);
     std::vector<int32_t> cbegin((size_t)n * ncol, 0), brep;
     b->block_off.assign((size_t)ncol, 0);
@@ -1327,7 +1334,17 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         MQV_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
         return MQV_OK;
     };
+    // measurement CTAs: about 4096 sites each, at least one per member
+    std::vector<int32_t> mprefix((size_t)n + 1, 0), mrep;
+    for (int r = 0; r < n; ++r) {
+        const int64_t parts = std::max<int64_t>(1, (b->sims[(size_t)r]->n + 4095) / 4096);
+        if (mprefix[(size_t)r] + parts >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
+        mprefix[(size_t)r + 1] = mprefix[(size_t)r] + (int32_t)parts;
+        for (int64_t k = 0; k < parts; ++k) mrep.push_back(r);
+    }
     mqv_status st = dcopy((void**)&b->d_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
+    if (!st) st = dcopy((void**)&b->d_meas_prefix, mprefix.data(), sizeof(int32_t) * mprefix.size());
+    if (!st) st = dcopy((void**)&b->d_meas_rep, mrep.data(), sizeof(int32_t) * mrep.size());
     if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
     if (!st) st = dcopy((void**)&b->d_cbegin, cbegin.data(), sizeof(int32_t) * std::max<size_t>(cbegin.size(), 1));
     if (!st) st = dcopy((void**)&b->d_site_prefix, sprefix.data(), sizeof(int64_t) * sprefix.size());
@@ -1354,7 +1371,9 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     b->L.block_off = b->block_off.data();
     b->L.blocks = b->blocks.data();
     b->L.total = b->total.data();
-    b->L.meas_parts = (int)std::min<int64_t>(64, std::max<int64_t>(1, (nmax + 4095) / 4096));
+    b->L.meas_prefix = b->d_meas_prefix;
+    b->L.meas_rep = b->d_meas_rep;
+    b->L.meas_blocks = (int)mprefix[(size_t)n];
     b->L.site_prefix = b->d_site_prefix;
     b->L.site_block_rep = b->d_site_block_rep;
     b->L.total_sites = sprefix[n];

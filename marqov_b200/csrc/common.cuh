@@ -87,16 +87,23 @@ MQV_HD uint64_t accept_word(Key key, uint32_t site, uint32_t sweep, uint32_t rep
 {
     return ((uint64_t)accept_top8(key, site, sweep, replica) << 56) | accept_fine56(key, site, sweep, replica);
 }
-// u53 < cut on the site's acceptance word (cut = accept_cut of the move's dE):
-// the fine half is drawn only when the top byte ties the cut's
-MQV_HD bool accept_below(uint64_t cut, Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+// u53 < cut on the site's acceptance word given its top byte: the fine half
+// is drawn only when the top byte ties the cut's
+MQV_HD bool accept_with_top(uint64_t cut, uint32_t top, Key key, uint32_t site, uint32_t sweep, uint32_t replica)
 {
     if (cut >= (1ull << 53)) return true;
     if (cut == 0) return false;
-    const uint32_t top = accept_top8(key, site, sweep, replica), t8 = (uint32_t)(cut >> 45);
+    const uint32_t t8 = (uint32_t)(cut >> 45);
     if (top != t8) return top < t8;
     return (((uint64_t)top << 45) | (accept_fine56(key, site, sweep, replica) >> 11)) < cut;
 }
+// u53 < cut on the site's acceptance word (cut = accept_cut of the move's dE)
+MQV_HD bool accept_below(uint64_t cut, Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    if (cut >= (1ull << 53) || cut == 0) return cut != 0;
+    return accept_with_top(cut, accept_top8(key, site, sweep, replica), key, site, sweep, replica);
+}
+
 
 // x % q for the small ranges of state draws (q <= 65535): constant divisors
 // for the common q, else three 32-bit remainders of x = hi 2^32 + lo.
@@ -206,6 +213,30 @@ MQV_HD bool update_accepted(int pref, double dE, double beta, uint64_t word)
     i64 = (i64 & ~(int64_t)0xFFF0000000000000LL) | 0x3FE0000000000000LL;
     double remainder = MQV_DSUB(action2, trunc(action2));
     return double_of(i64) < exp2app6(remainder);
+}
+
+// The cut of update_accepted<pref>(dE, beta, .) in closed form: the smallest
+// u53 = word >> 11 it rejects (2^53: it accepts every word), so that the rule
+// is u53 < cut.  With t = trunc(pref log2(e) (-beta dE)) and X the exp2app6
+// of the fractional part: u = u53 2^-53 lies in binade e (u53 in
+// [2^(52+e), 2^(53+e)); u53 = 0 has e = -1022); a smaller binade than t is
+// accepted, binade t when its mantissa u53 / 2^(53+t) < X, that is
+// u53 < X 2^(53+t) (a power-of-two scaling, exact).
+MQV_HD uint64_t accept_cut_direct(int pref, double dE, double beta)
+{
+    if (dE <= 0) return 1ull << 53;
+    const double plog2e = (double)pref * 1.4426950408889634074;
+    const double action2 = MQV_DMUL(plog2e, MQV_DMUL(-beta, dE));
+    const int64_t t = trunc_i64(action2);
+    if (t > 0) return 1ull << 53;  // every binade of u is below t
+    if (t < -1022) return 0;       // even u53 = 0 lies above t (also NaN)
+    const double x = exp2app6(MQV_DSUB(action2, trunc(action2)));
+    if (t == -1022) return 0.5 < x ? 1 : 0;  // only u53 = 0 ties; its mantissa reads 0.5
+    if (t < -52) return 1;                    // only u53 = 0 lies below t
+    const uint64_t lo = 1ull << (52 + t);
+    const double p2 = double_of((int64_t)(1023 + 53 + t) << 52);  // 2^(53 + t), t in [-52, 0]
+    const uint64_t c = (uint64_t)ceil(MQV_DMUL(x, p2));
+    return c < lo ? lo : c;
 }
 
 // ---- Blackwell async copies (bulk copy engine) and mbarriers -----------------

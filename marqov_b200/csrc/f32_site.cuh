@@ -47,50 +47,65 @@ __device__ __forceinline__ void smallcap3(SubStream& rng, const float o[3], doub
     for (int c = 0; c < 3; ++c) v[c] = nv[c] / nn;
 }
 
+// Lanes with live == false touch no memory.  The decision
+// is u53 < accept_cut_direct(1, dE, beta), which equals update_accepted<1> on
+// the site's acceptance word.
 template <class Lat>
 __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, float* __restrict__ s, int64_t i,
-                                         Key key, uint32_t sweep, uint32_t replica)
+                                         Key key, uint32_t sweep, uint32_t replica, bool live)
 {
-    SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
-    const int deg = lat.degree(i);
-    if (m.symd == 1) {
-        // shift proposal old + amp * real(-1, 1) (Phi4_Initializer_Cartesian,
-        // src/hamiltonian/Phi4.h:44-57); interaction + Onsite_Quadratic +
-        // Onsite_Fourth_Minus_One (src/hamiltonian/Phi4.h:63-74,103-121)
-        const double r = 1.0 + (-1.0 - 1.0) * real01(rng.next());
-        const double old = s[i];
-        const float nwf = (float)(old + m.cap * r);
-        const double nw = nwf;
-        double sum = 0;
-        for (int t = 0; t < deg; ++t) sum += (double)s[lat.nbr(i, t)];
-        const double o2 = old * old, n2 = nw * nw;
-        const double dE = m.J * (nw - old) * sum + m.h * (n2 - o2) +
-                          m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
-        if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) s[i] = nwf;
-        return;
+    uint64_t cut = 0;
+    float nf[3] = {0.f, 0.f, 0.f};
+    if (live) {
+        SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
+        const int deg = lat.degree(i);
+        double dE;
+        if (m.symd == 1) {
+            // shift proposal old + amp * real(-1, 1) (Phi4_Initializer_Cartesian,
+            // src/hamiltonian/Phi4.h:44-57); interaction + Onsite_Quadratic +
+            // Onsite_Fourth_Minus_One (src/hamiltonian/Phi4.h:63-74,103-121)
+            const double r = 1.0 + (-1.0 - 1.0) * real01(rng.next());
+            const double old = s[i];
+            nf[0] = (float)(old + m.cap * r);
+            const double nw = nf[0];
+            double sum = 0;
+            for (int t = 0; t < deg; ++t) sum += (double)s[lat.nbr(i, t)];
+            const double o2 = old * old, n2 = nw * nw;
+            dE = m.J * (nw - old) * sum + m.h * (n2 - o2) +
+                 m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
+        } else {
+            const float* so = s + 3 * i;
+            const float o[3] = {so[0], so[1], so[2]};
+            double v[3];
+            if (m.proposal == MQV_PROPOSAL_SMALL_CAP) smallcap3(rng, o, m.cap, v);
+            else rnddir3(rng, v);  // SVInitializer for float vectors (initializers.h:74-80)
+            nf[0] = (float)v[0];
+            nf[1] = (float)v[1];
+            nf[2] = (float)v[2];
+            double nb[3] = {0, 0, 0};
+            for (int t = 0; t < deg; ++t) {
+                const float* sj = s + 3 * lat.nbr(i, t);
+                nb[0] += (double)sj[0];
+                nb[1] += (double)sj[1];
+                nb[2] += (double)sj[2];
+            }
+            const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
+            dE = ((double)nf[0] - (double)o[0]) * nb[0];
+            dE += ((double)nf[1] - (double)o[1]) * nb[1];
+            dE += wz * ((double)nf[2] - (double)o[2]) * nb[2];
+            dE *= m.J;
+        }
+        cut = accept_cut_direct(1, dE, m.beta);
     }
-    float* so = s + 3 * i;
-    const float o[3] = {so[0], so[1], so[2]};
-    double v[3];
-    if (m.proposal == MQV_PROPOSAL_SMALL_CAP) smallcap3(rng, o, m.cap, v);
-    else rnddir3(rng, v);  // SVInitializer for float vectors (initializers.h:74-80)
-    const float nf[3] = {(float)v[0], (float)v[1], (float)v[2]};
-    double nb[3] = {0, 0, 0};
-    for (int t = 0; t < deg; ++t) {
-        const float* sj = s + 3 * lat.nbr(i, t);
-        nb[0] += (double)sj[0];
-        nb[1] += (double)sj[1];
-        nb[2] += (double)sj[2];
-    }
-    const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
-    double dE = ((double)nf[0] - (double)o[0]) * nb[0];
-    dE += ((double)nf[1] - (double)o[1]) * nb[1];
-    dE += wz * ((double)nf[2] - (double)o[2]) * nb[2];
-    dE *= m.J;
-    if (dE <= 0 || update_accepted(1, dE, m.beta, accept_word(key, (uint32_t)i, sweep, replica))) {
-        so[0] = nf[0];
-        so[1] = nf[1];
-        so[2] = nf[2];
+    if (live && accept_below(cut, key, (uint32_t)i, sweep, replica)) {
+        if (m.symd == 1) {
+            s[i] = nf[0];
+        } else {
+            float* so = s + 3 * i;
+            so[0] = nf[0];
+            so[1] = nf[1];
+            so[2] = nf[2];
+        }
     }
 }
 

@@ -13,47 +13,54 @@ namespace mqv {
 // `cuts`: the u53 cut of every dE the model can produce, indexed as
 // int8_cut_index (host table int8_cut_table); the decision equals
 // update_accepted<1>(dE, beta, word) on the site's acceptance word.
+// Lanes with live == false touch no memory.
 template <class Lat>
 __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int8_t* __restrict__ s, int64_t i,
                                           Key key, uint32_t sweep, uint32_t replica,
-                                          const unsigned long long* __restrict__ cuts, int D)
+                                          const unsigned long long* __restrict__ cuts, int D, bool live)
 {
-    SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
-    const int64_t ai = lat.addr(i);
-    const int old = s[ai];
-    const int deg = lat.degree(i);
-    int nw, k;
-    if (m.kind == MQV_MODEL_POTTS) {
-        // Initializer<Potts<Q>>::newsv (src/hamiltonian/Potts.h:170-177) and
-        // PottsInteraction::diff (src/hamiltonian/Potts.h:86-107)
-        nw = (int)mod_small(rng.next(), (uint32_t)m.q);
-        int eo = 0, en = 0;
-        for (int t = 0; t < deg; ++t) {
-            const int v = s[lat.addr(lat.nbr(i, t))];
-            eo += (v == old);
-            en += (v == nw);
+    int64_t ai = 0;
+    int nw = 0;
+    uint64_t cut = 0;
+    if (live) {
+        SubStream rng(key, (uint32_t)i, sweep, tag(kMetro, replica));
+        ai = lat.addr(i);
+        const int old = s[ai];
+        const int deg = lat.degree(i);
+        int k;
+        if (m.kind == MQV_MODEL_POTTS) {
+            // Initializer<Potts<Q>>::newsv (src/hamiltonian/Potts.h:170-177) and
+            // PottsInteraction::diff (src/hamiltonian/Potts.h:86-107)
+            nw = (int)mod_small(rng.next(), (uint32_t)m.q);
+            int eo = 0, en = 0;
+            for (int t = 0; t < deg; ++t) {
+                const int v = s[lat.addr(lat.nbr(i, t))];
+                eo += (v == old);
+                en += (v == nw);
+            }
+            k = en - eo + D;
+        } else if (m.kind == MQV_MODEL_BLUME_CAPEL) {
+            // Spin1_Initializer::newsv (src/hamiltonian/util/initializers.h:99-118)
+            int st = old;
+            if (st == 0) st = rng.real() < 0.5 ? -1 : 1;
+            else st = rng.real() < 0.5 ? -st : 0;
+            nw = st;
+            int sum = 0;
+            for (int t = 0; t < deg; ++t) sum += s[lat.addr(lat.nbr(i, t))];
+            k = (((nw - old) + 2) * (2 * D + 1) + (sum + D)) * 3 + (nw * nw - old * old + 1);
+        } else {
+            // spin flip (src/hamiltonian/util/initializers.h:52-58), neighbourhood
+            // sum with optional bonds (src/libmarqov/metropolishelpers.h:456-537)
+            nw = -old;
+            int sum = 0;
+            for (int t = 0; t < deg; ++t) sum += lat.bond(i, t) * s[lat.addr(lat.nbr(i, t))];
+            k = old * sum + D;
         }
-        k = en - eo + D;
-    } else if (m.kind == MQV_MODEL_BLUME_CAPEL) {
-        // Spin1_Initializer::newsv (src/hamiltonian/util/initializers.h:99-118)
-        int st = old;
-        if (st == 0) st = rng.real() < 0.5 ? -1 : 1;
-        else st = rng.real() < 0.5 ? -st : 0;
-        nw = st;
-        int sum = 0;
-        for (int t = 0; t < deg; ++t) sum += s[lat.addr(lat.nbr(i, t))];
-        k = (((nw - old) + 2) * (2 * D + 1) + (sum + D)) * 3 + (nw * nw - old * old + 1);
-    } else {
-        // spin flip (src/hamiltonian/util/initializers.h:52-58), neighbourhood
-        // sum with optional bonds (src/libmarqov/metropolishelpers.h:456-537)
-        nw = -old;
-        int sum = 0;
-        for (int t = 0; t < deg; ++t) sum += lat.bond(i, t) * s[lat.addr(lat.nbr(i, t))];
-        k = old * sum + D;
+        cut = cuts[k];
     }
     // metro_update_accepted (src/libmarqov/metropolis.h:61-64,120-124) on the
     // site's acceptance word
-    if (accept_below(cuts[k], key, (uint32_t)i, sweep, replica)) s[ai] = (int8_t)nw;
+    if (live && accept_below(cut, key, (uint32_t)i, sweep, replica)) s[ai] = (int8_t)nw;
 }
 
 // Site of colour `colour` in pair t of a parity-coloured hypercubic lattice
@@ -79,8 +86,39 @@ __device__ __forceinline__ long long warp_sum_ll(long long v)
 // accumulators (src/hamiltonian/util/observables.h:47-65,186-217,251-268,
 // src/hamiltonian/Potts.h:46-61), exact in int64.
 
+// Neighbour sum of the interaction energy of site i: sum over nbrs(i) of
+// s_i s_j (bonds) or [s_i == s_j] (Potts).  On stencils, where every bond
+// appears in both endpoints' lists, twice the sum over the forward
+// neighbours (+x, +y, ...) gives the same total with half the loads.
+template <class Lat>
+__device__ __forceinline__ int int8_bond_sum(const ModelDev& m, const Lat& lat, const int8_t* __restrict__ s,
+                                             int64_t i, int si, bool potts)
+{
+    const int deg = lat.degree(i);
+    int loc = 0;
+    if (potts)
+        for (int t = 0; t < deg; ++t) loc += (s[lat.addr(lat.nbr(i, t))] == si);
+    else {
+        for (int t = 0; t < deg; ++t) loc += lat.bond(i, t) * s[lat.addr(lat.nbr(i, t))];
+        loc *= si;
+    }
+    return loc;
+}
+__device__ __forceinline__ int int8_bond_sum(const ModelDev&, const StencilDev& st, const int8_t* __restrict__ s,
+                                             int64_t i, int si, bool potts)
+{
+    int loc = 0;
+    for (int d = 0; d < st.dim; ++d) {
+        const int v = s[st.addr(st.nbr(i, 2 * d))];
+        loc += potts ? (v == si) : v;
+    }
+    return 2 * (potts ? loc : loc * si);
+}
+
 // Part `part` of `nparts` of the accumulation (a grid-stride share per CTA;
-// the CTA's totals go to acc with atomics).
+// the CTA's totals go to acc with atomics).  Potts state counts are
+// aggregated per warp (lanes with equal states add once) before the shared
+// histogram.
 template <class Lat>
 __device__ __forceinline__ void measure_int8_part(const ModelDev& m, const Lat& lat, const int8_t* __restrict__ s,
                                                   long long* __restrict__ acc, int64_t part, int64_t nparts)
@@ -92,20 +130,23 @@ __device__ __forceinline__ void measure_int8_part(const ModelDev& m, const Lat& 
         for (int k = threadIdx.x; k < 64; k += blockDim.x) hist[k] = 0;
     __syncthreads();
     long long e = 0, mg = 0, sq = 0;
-    for (int64_t i = part * (int64_t)blockDim.x + threadIdx.x; i < lat.n; i += nparts * blockDim.x) {
-        const int si = s[lat.addr(i)];
-        const int deg = lat.degree(i);
-        int loc = 0;
-        if (potts) {
-            for (int t = 0; t < deg; ++t) loc += (s[lat.addr(lat.nbr(i, t))] == si);
-            atomicAdd(&hist[si & 63], 1);
-        } else {
-            for (int t = 0; t < deg; ++t) loc += lat.bond(i, t) * s[lat.addr(lat.nbr(i, t))];
-            loc *= si;
+    const unsigned lane = threadIdx.x & 31;
+    // warp-uniform trip count: every lane takes part in the warp's votes
+    const int64_t stride = nparts * blockDim.x;
+    for (int64_t i0 = part * (int64_t)blockDim.x + (threadIdx.x & ~31u); i0 < lat.n; i0 += stride) {
+        const int64_t i = i0 + lane;
+        const bool live = i < lat.n;
+        int si = 0;
+        if (live) {
+            si = s[lat.addr(i)];
+            e += int8_bond_sum(m, lat, s, i, si, potts);
+            mg += si;
+            sq += si * si;
         }
-        e += loc;
-        mg += si;
-        sq += si * si;
+        if (potts) {
+            const unsigned peers = __match_any_sync(0xffffffffu, live ? (si & 63) : 64);
+            if (live && lane == (unsigned)(__ffs(peers) - 1)) atomicAdd(&hist[si & 63], __popc(peers));
+        }
     }
     e = warp_sum_ll(e);
     mg = warp_sum_ll(mg);

@@ -17,16 +17,24 @@ unsigned long long accept_cut(int pref, double dE, double beta);
 __global__ void metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s, int colour, Key key,
                                   uint32_t sweep, uint32_t replica)
 {
-    const int64_t half = st.n / 2;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < half; t += (int64_t)gridDim.x * blockDim.x)
-        f32_site(m, st, s, parity_site_f(st, t, colour), key, sweep, replica);
+    // warp-uniform trips: the lanes of a warp update their sites together
+    const int64_t half = st.n / 2, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
+        const int64_t t = t0 + (threadIdx.x & 31u);
+        const bool live = t < half;
+        f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live);
+    }
 }
 
 __global__ void metro_f32_csr(ModelDev m, CSRDev g, float* __restrict__ s, const int32_t* __restrict__ order,
                               int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t replica)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
-        f32_site(m, g, s, order[begin + t], key, sweep, replica);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < count; t0 += stride) {
+        const int64_t t = t0 + (threadIdx.x & 31u);
+        const bool live = t < count;
+        f32_site(m, g, s, live ? (int64_t)order[begin + t] : 0, key, sweep, replica, live);
+    }
 }
 
 template <class Lat>

@@ -22,17 +22,25 @@ __global__ void metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict
                                    uint32_t sweep, uint32_t replica, const unsigned long long* __restrict__ cuts,
                                    int D)
 {
-    const int64_t half = st.n / 2;
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < half; t += (int64_t)gridDim.x * blockDim.x)
-        int8_site(m, st, s, parity_site(st, t, colour), key, sweep, replica, cuts, D);
+    // warp-uniform trips: the lanes of a warp update their sites together
+    const int64_t half = st.n / 2, stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
+        const int64_t t = t0 + (threadIdx.x & 31u);
+        const bool live = t < half;
+        int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live);
+    }
 }
 
 __global__ void metro_int8_csr(ModelDev m, CSRDev g, int8_t* __restrict__ s, const int32_t* __restrict__ order,
                                int64_t begin, int64_t count, Key key, uint32_t sweep, uint32_t replica,
                                const unsigned long long* __restrict__ cuts, int D)
 {
-    for (int64_t t = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; t < count; t += (int64_t)gridDim.x * blockDim.x)
-        int8_site(m, g, s, order[begin + t], key, sweep, replica, cuts, D);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < count; t0 += stride) {
+        const int64_t t = t0 + (threadIdx.x & 31u);
+        const bool live = t < count;
+        int8_site(m, g, s, live ? (int64_t)order[begin + t] : 0, key, sweep, replica, cuts, D, live);
+    }
 }
 
 // dE of every move index of int8_site, with the kernel's own FP64 operations
