@@ -504,9 +504,9 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
 
 // ---- band kernel: one CTA spans the lattice width --------------------------------
 //
-// Thread t owns word column t of both halves of every row (64 sites: 32 even-x
-// and 32 odd-x), so a CTA of L/64 threads covers whole rows and needs no
-// horizontal halo.  CTA c streams down its band of rows [y0, y1) (bands split
+// Thread t owns word columns t, t + NT, ..., t + (W - 1) NT of both halves of
+// every row (64 sites each: 32 even-x and 32 odd-x), so a CTA of L / (64 W)
+// threads covers whole rows and needs no horizontal halo.  CTA c streams down its band of rows [y0, y1) (bands split
 // the L rows evenly over the grid) with two halo rows above and below: staged
 // row r is lattice row y0 - 2 + r, r = 0 .. H + 3.  Step k of the pipeline
 //   packs staged row k (one bulk copy per row, ring of NSB slots) into the bit
@@ -515,34 +515,36 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
 // Top-byte ties of both colours are resolved in bulk every S steps, so a word
 // is final at most S - 1 steps after its update: colour 1 lags colour 0 by S
 // rows and the output lags colour 1 by S rows, which keeps every neighbour a
-// word reads final.  The bit ring keeps the last RB = 2S + 4 rows.
+// word reads final.  The bit ring keeps the last RB = 2S + 4 rows.  With
+// W > 1 a thread carries W independent words through every stage of a step.
 
-template <int NT, int S, int NSB_>  // NT = L / 64 threads; ties every S steps; NSB_ staged rows
+template <int NT, int S, int NSB_, int W = 1>  // NT threads of W columns; ties every S steps; NSB_ staged rows
 struct BandGeom {
     static constexpr int NW = NT / 32;
+    static constexpr int NC = NT * W;            // word columns
     static constexpr int NSB = NSB_;             // staged row slots
     static constexpr int RB = 2 * S + 4;         // bit ring rows
-    static constexpr int L = NT * 64;
+    static constexpr int L = NC * 64;
     static constexpr int STAGE = NSB * L;
-    static constexpr int BITS = RB * 2 * NT * 4;
-    static constexpr int TIECAP = 96;            // tie entries per warp
+    static constexpr int BITS = RB * 2 * NC * 4;
+    static constexpr int TIECAP = 32 + 64 * W;   // tie entries per warp: a step adds at most 64 W
     static constexpr int TIES = NW * TIECAP * 16;
     static constexpr int SMEM = STAGE + BITS + TIES + NSB * 8;
-    static_assert(NT % 32 == 0 && S >= 1, "band shape");
+    static_assert(NT % 32 == 0 && S >= 1 && W >= 1, "band shape");
 };
 
 struct BandTie {
-    uint32_t pos;  // word position in the bit ring: (slot * 2 + half) * NT + t
+    uint32_t pos;  // word position in the bit ring: (slot * 2 + half) * NC + column
     uint32_t tie;  // undecided sites of the word
     uint32_t inA;  // those of class A
     int32_t y;     // lattice row
 };
 
-template <int NT, int S, int NSB_, bool MEAS>
+template <int NT, int S, int NSB_, bool MEAS, int W = 1>
 __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising2DArgs a)
 {
-    using G = BandGeom<NT, S, NSB_>;
-    constexpr int RB = G::RB, NSB = G::NSB, L = G::L, Lh = L / 2;
+    using G = BandGeom<NT, S, NSB_, W>;
+    constexpr int RB = G::RB, NSB = G::NSB, L = G::L, Lh = L / 2, NC = G::NC;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* stage = smem;
     uint32_t* bits = reinterpret_cast<uint32_t*>(smem + G::STAGE);
@@ -554,7 +556,10 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     const int NR = y1 - y0 + 4;  // staged rows
     const uint32_t tg_acc = tag(kAccept, a.replica);
     const Thr th = make_thr(a);
-    const int tl_ = t == 0 ? NT - 1 : t - 1, tr_ = t == NT - 1 ? 0 : t + 1;
+    // column of word j of this thread, and the left / right neighbour columns
+    auto col = [&](int j) { return t + j * NT; };
+    auto coll = [&](int c) { return c == 0 ? NC - 1 : c - 1; };
+    auto colr = [&](int c) { return c == NC - 1 ? 0 : c + 1; };
 
     if (t == 0) {
         for (int k = 0; k < NSB; ++k) mbar_init(smem_addr(&bars[k]), 1);
@@ -582,7 +587,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         __syncwarp();
         for (int e = lane; e < ntie; e += 32) {
             const BandTie te = tl[e];
-            const uint32_t w = te.pos % NT, h = (te.pos / NT) & 1u;
+            const uint32_t w = te.pos % NC, h = (te.pos / NC) & 1u;
             const uint32_t site0 = (uint32_t)te.y * (uint32_t)L + 64u * w + h;
             uint32_t m = te.tie, flips = 0u;
             while (m) {
@@ -598,28 +603,32 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         __syncwarp();
         ntie = 0;
     };
-    // inputs of the word of column t in half p of staged row r
+    // inputs of the word of column c in half p of staged row r
     struct WordIn {
         uint32_t A, U, D, Lb, Rb, pos;
     };
-    auto word_in = [&](int sl, int su, int sd, int p) {
+    auto word_in = [&](int sl, int su, int sd, int p, int c) {
         WordIn w;
-        w.pos = (uint32_t)((sl * 2 + p) * NT + t);
-        const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NT;
-        const uint32_t Gw = Gr[t];
-        w.Lb = p ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
-        w.Rb = p ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
+        w.pos = (uint32_t)((sl * 2 + p) * NC + c);
+        const uint32_t* Gr = bits + (sl * 2 + (1 - p)) * NC;
+        const uint32_t Gw = Gr[c];
+        w.Lb = p ? Gw : __funnelshift_l(Gr[coll(c)], Gw, 1);
+        w.Rb = p ? __funnelshift_r(Gw, Gr[colr(c)], 1) : Gw;
         w.A = bits[w.pos];
-        w.U = bits[(su * 2 + p) * NT + t];
-        w.D = bits[(sd * 2 + p) * NT + t];
+        w.U = bits[(su * 2 + p) * NC + c];
+        w.D = bits[(sd * 2 + p) * NC + c];
         return w;
     };
-    // update the word of column t in half p of staged row r (lattice row y)
+    // update this thread's words in half p of staged row r (lattice row y)
     auto update = [&](int sl, int su, int sd, int p, int y) {
-        const WordIn w = word_in(sl, su, sd, p);
-        uint32_t tie, inA;
-        bits[w.pos] = update_word(w.A, w.U, w.D, w.Lb, w.Rb, 64 * t + p, y, tg_acc, a, th, tie, inA);
-        record(tie, inA, w.pos, y);
+#pragma unroll
+        for (int j = 0; j < W; ++j) {
+            const int c = col(j);
+            const WordIn w = word_in(sl, su, sd, p, c);
+            uint32_t tie, inA;
+            bits[w.pos] = update_word(w.A, w.U, w.D, w.Lb, w.Rb, 64 * c + p, y, tg_acc, a, th, tie, inA);
+            record(tie, inA, w.pos, y);
+        }
     };
 
     int esum = 0, msum = 0;
@@ -661,11 +670,15 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         }
         if (k < NR) {
             const uint8_t* row = stage + (k % NSB) * L;
-            uint32_t* brow = bits + sk * 2 * NT;
+            uint32_t* brow = bits + sk * 2 * NC;
 #pragma unroll
-            for (int h = 0; h < 2; ++h) {
-                const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * t);
-                brow[h * NT + t] = pack_word(q[0], q[1]);
+            for (int j = 0; j < W; ++j) {
+                const int c = col(j);
+#pragma unroll
+                for (int h = 0; h < 2; ++h) {
+                    const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * c);
+                    brow[h * NC + c] = pack_word(q[0], q[1]);
+                }
             }
         }
         // row k's bits are read in this step only by their own thread (the D
@@ -679,45 +692,55 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         const int ya = wrapi(y0 - 3 + k, L), yb = y0 - 2 + r1;
         if (do0 && do1) {
             const int pa = ya & 1, pb = 1 - (yb & 1);
-            const WordIn wa = word_in(back(1), back(2), sk, pa);
-            const WordIn wb = word_in(back(2 + S), back(3 + S), back(1 + S), pb);
-            uint32_t ta, ia, tb, ib;
-            const uint32_t na = update_word(wa.A, wa.U, wa.D, wa.Lb, wa.Rb, 64 * t + pa, ya, tg_acc, a, th, ta, ia);
-            const uint32_t nb = update_word(wb.A, wb.U, wb.D, wb.Lb, wb.Rb, 64 * t + pb, yb, tg_acc, a, th, tb, ib);
-            bits[wa.pos] = na;
-            bits[wb.pos] = nb;
-            record(ta, ia, wa.pos, ya);
-            record(tb, ib, wb.pos, yb);
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                const int c = col(j);
+                const WordIn wa = word_in(back(1), back(2), sk, pa, c);
+                const WordIn wb = word_in(back(2 + S), back(3 + S), back(1 + S), pb, c);
+                uint32_t ta, ia, tb, ib;
+                const uint32_t na =
+                    update_word(wa.A, wa.U, wa.D, wa.Lb, wa.Rb, 64 * c + pa, ya, tg_acc, a, th, ta, ia);
+                const uint32_t nb =
+                    update_word(wb.A, wb.U, wb.D, wb.Lb, wb.Rb, 64 * c + pb, yb, tg_acc, a, th, tb, ib);
+                bits[wa.pos] = na;
+                bits[wb.pos] = nb;
+                record(ta, ia, wa.pos, ya);
+                record(tb, ib, wb.pos, yb);
+            }
         } else if (do0) {
             update(back(1), back(2), sk, ya & 1, ya);
         } else if (do1) {
             update(back(2 + S), back(3 + S), back(1 + S), 1 - (yb & 1), yb);
         }
-        if (k % S == S - 1 || ntie > G::TIECAP - 64) flush();
+        if (k % S == S - 1 || ntie > G::TIECAP - 64 * W) flush();
         // row k - 2 - 2S out
         const int r2 = k - 2 - 2 * S;
         if (r2 >= 2 && r2 <= NR - 3) {
             const int y = y0 - 2 + r2;
             const int sl = back(2 + 2 * S);
-            const uint32_t w0 = bits[(sl * 2) * NT + t], w1 = bits[(sl * 2 + 1) * NT + t];
-            int8_t* drow = a.dst + (size_t)y * L + 32 * t;
-            uint4 lo, hi;
-            unpack_word(w0, lo, hi);
-            reinterpret_cast<uint4*>(drow)[0] = lo;
-            reinterpret_cast<uint4*>(drow)[1] = hi;
-            unpack_word(w1, lo, hi);
-            reinterpret_cast<uint4*>(drow + Lh)[0] = lo;
-            reinterpret_cast<uint4*>(drow + Lh)[1] = hi;
-            if (MEAS) {
-                const int p1 = 1 - (y & 1);
-                const uint32_t An = p1 ? w1 : w0, Gw = p1 ? w0 : w1;
-                const uint32_t* Gr = bits + (sl * 2 + (1 - p1)) * NT;
-                const uint32_t Lb = p1 ? Gw : __funnelshift_l(Gr[tl_], Gw, 1);
-                const uint32_t Rb = p1 ? __funnelshift_r(Gw, Gr[tr_], 1) : Gw;
-                const uint32_t U = bits[(back(3 + 2 * S) * 2 + p1) * NT + t];
-                const uint32_t D = bits[(back(1 + 2 * S) * 2 + p1) * NT + t];
-                esum += word_bonds(An, U, D, Lb, Rb);
-                msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+#pragma unroll
+            for (int j = 0; j < W; ++j) {
+                const int c = col(j);
+                const uint32_t w0 = bits[(sl * 2) * NC + c], w1 = bits[(sl * 2 + 1) * NC + c];
+                int8_t* drow = a.dst + (size_t)y * L + 32 * c;
+                uint4 lo, hi;
+                unpack_word(w0, lo, hi);
+                reinterpret_cast<uint4*>(drow)[0] = lo;
+                reinterpret_cast<uint4*>(drow)[1] = hi;
+                unpack_word(w1, lo, hi);
+                reinterpret_cast<uint4*>(drow + Lh)[0] = lo;
+                reinterpret_cast<uint4*>(drow + Lh)[1] = hi;
+                if (MEAS) {
+                    const int p1 = 1 - (y & 1);
+                    const uint32_t An = p1 ? w1 : w0, Gw = p1 ? w0 : w1;
+                    const uint32_t* Gr = bits + (sl * 2 + (1 - p1)) * NC;
+                    const uint32_t Lb = p1 ? Gw : __funnelshift_l(Gr[coll(c)], Gw, 1);
+                    const uint32_t Rb = p1 ? __funnelshift_r(Gw, Gr[colr(c)], 1) : Gw;
+                    const uint32_t U = bits[(back(3 + 2 * S) * 2 + p1) * NC + c];
+                    const uint32_t D = bits[(back(1 + 2 * S) * 2 + p1) * NC + c];
+                    esum += word_bonds(An, U, D, Lb, Rb);
+                    msum += 64 - 2 * __popc(An) - 2 * __popc(Gw);
+                }
             }
         }
     }
@@ -886,11 +909,11 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-template <int NT, int S, int NSB, bool MEAS>
+template <int NT, int S, int NSB, bool MEAS, int W = 1>
 static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
-    using G = BandGeom<NT, S, NSB>;
-    auto kern = ising2d_band<NT, S, NSB, MEAS>;
+    using G = BandGeom<NT, S, NSB, W>;
+    auto kern = ising2d_band<NT, S, NSB, MEAS, W>;
     static int cps = 0;  // resident CTAs per SM for this instantiation
     if (cps == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
@@ -916,18 +939,26 @@ struct SweepConfig {
     bool band;
     int nsb;            // band: staged row slots
     SweepLauncher plain, meas;
+    int w;              // band: word columns per thread
 };
 
 #define MQV_CFG(TX, TY, NW) \
-    SweepConfig{TX, TY, NW, false, 0, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>}
+    SweepConfig{TX, TY, NW, false, 0, launch_t<TX, TY, NW, false>, launch_t<TX, TY, NW, true>, 1}
 #define MQV_BAND(NT, S, NSB) \
-    SweepConfig{64 * NT, S, NT / 32, true, NSB, launch_band<NT, S, NSB, false>, launch_band<NT, S, NSB, true>}
+    SweepConfig{64 * NT, S, NT / 32, true, NSB, launch_band<NT, S, NSB, false>, launch_band<NT, S, NSB, true>, 1}
+#define MQV_BANDW(NT, S, NSB, W)                                                                         \
+    SweepConfig{64 * NT * W, S,                                                                          \
+                NT / 32,     true,                                                                       \
+                NSB,         launch_band<NT, S, NSB, false, W>,                                          \
+                launch_band<NT, S, NSB, true, W>, W}
 
 static const SweepConfig kConfigs[] = {
     MQV_CFG(512, 32, 4), MQV_CFG(256, 32, 4), MQV_CFG(512, 32, 2), MQV_CFG(256, 32, 8),
     MQV_CFG(1024, 32, 2), MQV_CFG(128, 32, 4), MQV_CFG(64, 32, 4),
     MQV_BAND(256, 4, 2), MQV_BAND(256, 2, 2), MQV_BAND(256, 4, 3), MQV_BAND(256, 4, 4),
     MQV_BAND(128, 4, 2), MQV_BAND(128, 4, 4),
+    MQV_BANDW(128, 4, 2, 2), MQV_BANDW(128, 2, 2, 2), MQV_BANDW(128, 1, 2, 2), MQV_BANDW(128, 3, 2, 2),
+    MQV_BANDW(64, 4, 2, 2),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
@@ -981,7 +1012,8 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
 // lattices take the first fitting candidate.
 static void config_name(const SweepConfig& c, char* buf, int len)
 {
-    if (c.band) snprintf(buf, len, "ising2d_band<%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb);
+    if (c.band && c.w > 1) snprintf(buf, len, "ising2d_band<%d,%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb, c.w);
+    else if (c.band) snprintf(buf, len, "ising2d_band<%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb);
     else snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
 }
 
