@@ -1007,8 +1007,8 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
     a.counter = s->d_counter;
 }
 
-// Time every fitting candidate on this lattice (two sweeps each into the
-// scratch buffer; the state is not modified) and keep the fastest.  Small
+// Time every fitting candidate on this lattice (sweeps into the scratch
+// buffer; the state is not modified) and keep the fastest.  Small
 // lattices take the first fitting candidate.
 static void config_name(const SweepConfig& c, char* buf, int len)
 {
@@ -1041,27 +1041,33 @@ static int pick_config(Sim* s)
         cudaEventDestroy(e0);
         return first;
     }
+    // two rounds over the candidates, four timed sweeps each, the best of
+    // the rounds per candidate: a candidate timed while the clocks still
+    // ramp up gets a second chance
     int best = first;
     float best_ms = 1e30f;
-    for (int k = 0; k < kNumConfigs; ++k) {
-        if (!config_fits(kConfigs[k], s->len)) continue;
-        Ising2DArgs a{};
-        fill_args(s, kConfigs[k], nullptr, a);
-        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
-        if (kConfigs[k].plain(a, s->num_sms, s->stream) != cudaSuccess) continue;  // warm-up
-        cudaEventRecord(e0, s->stream);
-        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
-        kConfigs[k].plain(a, s->num_sms, s->stream);
-        cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
-        kConfigs[k].plain(a, s->num_sms, s->stream);
-        cudaEventRecord(e1, s->stream);
-        s->launches += 3;
-        float ms = 0;
-        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
-            best_ms = ms;
-            best = k;
+    constexpr int kRounds = 2, kTimed = 4;
+    for (int round = 0; round < kRounds; ++round)
+        for (int k = 0; k < kNumConfigs; ++k) {
+            if (!config_fits(kConfigs[k], s->len)) continue;
+            Ising2DArgs a{};
+            fill_args(s, kConfigs[k], nullptr, a);
+            cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
+            if (kConfigs[k].plain(a, s->num_sms, s->stream) != cudaSuccess) continue;  // warm-up
+            cudaEventRecord(e0, s->stream);
+            for (int i = 0; i < kTimed; ++i) {
+                cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
+                kConfigs[k].plain(a, s->num_sms, s->stream);
+            }
+            cudaEventRecord(e1, s->stream);
+            s->launches += 1 + kTimed;
+            float ms = 0;
+            if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess &&
+                ms < best_ms) {
+                best_ms = ms;
+                best = k;
+            }
         }
-    }
     cudaGetLastError();
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
