@@ -89,7 +89,7 @@ class Core:
         self._setup(lattice, ham)
         # the dump container (Core's constructor, src/libmarqov/core.h:469-488):
         # a new step, continuing from the previous step's final state and RNG
-        seed, replica, restore = int(config.seed), int(config.repid), None
+        seed, replica, restore, prev = int(config.seed), int(config.repid), None, -1
         if config.outpath:
             from . import checkpoint as CP
             path = CP.container_path(config)
@@ -100,7 +100,6 @@ class Core:
                     raise RuntimeError(f"{last.path} holds no final state (its run did not end)")
                 restore = last.read_state()
                 seed, replica = restore[1][0], restore[1][1]
-            self._step = CP.Step(path, prev + 1).create(self.beta, config, lattice, ham, L.version())
         md = ham.desc(self.beta)
         ld = lattice.desc()
         rp = L.RunParams(beta=self.beta, seed=seed & (2 ** 64 - 1), replica=replica, device=int(config.device),
@@ -111,6 +110,9 @@ class Core:
             self.state = restore[0]
             self.counters = restore[1][2:]
             self._restored = True
+        # the step group exists only for a Core that could be set up
+        if config.outpath:
+            self._step = CP.Step(path, prev + 1).create(self.beta, config, lattice, ham, L.version())
 
     def _setup(self, lattice: Lattice, ham: Hamiltonian):
         self._step = None
