@@ -245,8 +245,10 @@ MQV_API mqv_status mqv_batch_init_state(mqv_batch* batch);
  * CTA per member, breadth first; or labelling of the activated-bond
  * components of all members in a fixed number of whole-lattice passes
  * (cost independent of cluster depth; pays for percolating clusters on large
- * lattices).  The default, MQV_WOLFF_AUTO, times both on EMCS 1 and 3 of the
- * first run with clusters and at least 4 EMCS, then keeps the faster. */
+ * lattices).  The default, MQV_WOLFF_AUTO, times every chunk of EMCS (up
+ * to 256 between host synchronisations), tries the algorithm not in use on a
+ * few EMCS at the start of a chunk when it has no estimate or an old one, and
+ * uses the faster estimate: the chain is the same whichever runs. */
 enum { MQV_WOLFF_AUTO = 0, MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
 MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* batch, int32_t algorithm);
 /* The algorithm in use: MQV_WOLFF_BFS or MQV_WOLFF_LABEL, or MQV_WOLFF_AUTO
