@@ -217,8 +217,8 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
             CclSeed* sd = (CclSeed*)b.ccl_seeds;
             const unsigned gb = (unsigned)b.site_blocks;
             ccl_seed<F32><<<(b.nrep + 127) / 128, 128, 0, st>>>(b.reps, b.ctr, ncluster, c, sd, b.csize, b.nrep);
-            ccl_init<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
-                                                             sd);
+            ccl_local<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
+                                                              sd, b.ctr, ncluster, c);
             ccl_hook<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
                                                              sd, b.ctr, ncluster, c);
             ccl_compress<<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites);

@@ -10,9 +10,12 @@
 // seed's component:
 //   ccl_seed      one thread per member: seed site, old/new state or the
 //                 reflection vector (the same substream draws as the BFS);
-//   ccl_init      label = own index for candidate sites (int8: state equal to
-//                 the seed's old state; float: every site), else -1;
-//   ccl_hook      activated bonds between candidates are united;
+//   ccl_local     per CTA of 256 consecutive sites: candidates (int8: state
+//                 equal to the seed's old state; float: every site) get
+//                 labels, and activated bonds with both ends in the CTA's
+//                 sites are united in shared memory first; each candidate's
+//                 label becomes its local root, non-candidates get -1;
+//   ccl_hook      the other activated bonds between candidates are united;
 //   ccl_compress  label = root (read-only walks: only roots are written);
 //   ccl_flip      members of the seed's component are flipped / reflected and
 //                 counted into the cluster size.
@@ -94,42 +97,118 @@ __global__ void ccl_seed(const BatchRep* __restrict__ reps, const BatchCtr* __re
     csize[((size_t)slot * ncluster + c) * nrep + r] = 0;
 }
 
+// activation of the bond (i, j) between two candidate sites of member R, on
+// the bond's keyed draw (the breadth-first growth's rule)
 template <bool F32>
-__global__ void ccl_init(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
-                         const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds)
+__device__ __forceinline__ bool ccl_active(const BatchRep& R, const CclSeed& sd, uint32_t serial, int64_t i, int64_t j)
 {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
-    int64_t i;
-    const int r = ccl_member(g, prefix, block_rep, i);
-    const BatchRep& R = reps[r];
-    bool cand = true;
-    if (!F32) {
-        const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
-        cand = ((const int8_t*)R.s)[a] == seeds[r].val;
-    }
-    R.queue[i] = cand ? (int)i : -1;
-}
-
-template <bool F32, class Lat>
-__device__ __forceinline__ void ccl_bond(const BatchRep& R, const Lat& lat, const CclSeed& sd, uint32_t serial, int64_t i,
-                                         int64_t j)
-{
-    int* lab = R.queue;
-    if (__ldcg(lab + j) < 0) return;
     const uint32_t tgb = tag(kWolffBond, R.replica);
-    bool act;
     if (F32) {
         const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
         const float* s = (const float*)R.s;
         const double cpl = embed_cpl(R.md.J, embed_proj(R.md.symd, s, lo, sd.r[0], sd.r[1], sd.r[2]),
                                      embed_proj(R.md.symd, s, hi, sd.r[0], sd.r[1], sd.r[2]));
-        act = cpl > 0 &&
-              !update_accepted(2, cpl, R.md.beta, lo64(philox((uint32_t)lo, serial, (uint32_t)hi, tgb, R.key)));
-    } else {
-        act = wolff_int8_active(R.w, (uint32_t)i, (uint32_t)j, serial, tgb, R.key);
+        return cpl > 0 &&
+               !update_accepted(2, cpl, R.md.beta, lo64(philox((uint32_t)lo, serial, (uint32_t)hi, tgb, R.key)));
     }
-    if (act) ccl_unite(lab, (int)i, (int)j);
+    return wolff_int8_active(R.w, (uint32_t)i, (uint32_t)j, serial, tgb, R.key);
+}
+
+// the forward bonds (i, j) of site i, each undirected bond once: +x, +y, ...
+// on stencils, j > i on CSR graphs
+template <class F>
+__device__ __forceinline__ void ccl_forward_bonds(const BatchRep& R, int64_t i, F&& f)
+{
+    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
+        for (int d = 0; d < R.st.dim; ++d) f(R.st.nbr(i, 2 * d));
+    } else {
+        for (int t = R.csr.rp[i]; t < R.csr.rp[i + 1]; ++t) {
+            const int64_t j = R.csr.ci[t];
+            if (j > i) f(j);
+        }
+    }
+}
+
+// union-find on the CTA's shared labels (the same scheme as ccl_find /
+// ccl_unite on shared memory)
+__device__ __forceinline__ int ccl_lfind(volatile int* p, int x)
+{
+    while (true) {
+        const int px = p[x];
+        if (px == x) return x;
+        const int gp = p[px];
+        if (gp != px) p[x] = gp;
+        x = gp;
+    }
+}
+__device__ __forceinline__ void ccl_lunite(volatile int* p, int a, int b)
+{
+    while (true) {
+        a = ccl_lfind(p, a);
+        b = ccl_lfind(p, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS((int*)p + a, a, b) == a) return;
+    }
+}
+
+// flattened site g and g2 in the same CTA block of kBatchMetroThreads sites
+__device__ __forceinline__ bool ccl_same_block(int64_t g, int64_t g2)
+{
+    return g / kBatchMetroThreads == g2 / kBatchMetroThreads;
+}
+
+template <bool F32>
+__global__ void __launch_bounds__(kBatchMetroThreads)
+    ccl_local(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+              const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds,
+              const BatchCtr* __restrict__ ctr, int ncluster, int c)
+{
+    __shared__ int slab[kBatchMetroThreads];
+    const int64_t base = (int64_t)blockIdx.x * kBatchMetroThreads;
+    const int64_t g = base + threadIdx.x;
+    int r = 0;
+    int64_t i = 0;
+    bool cand = false;
+    if (g < total) {
+        r = ccl_member(g, prefix, block_rep, i);
+        const BatchRep& R = reps[r];
+        cand = true;
+        if (!F32) {
+            const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
+            cand = ((const int8_t*)R.s)[a] == seeds[r].val;
+        }
+    }
+    slab[threadIdx.x] = cand ? (int)threadIdx.x : -1;
+    __syncthreads();
+    if (cand) {
+        const BatchRep& R = reps[r];
+        const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
+        const CclSeed sd = seeds[r];
+        const int64_t off = prefix[r];
+        volatile int* vl = slab;
+        ccl_forward_bonds(R, i, [&](int64_t j) {
+            const int64_t gj = off + j;
+            if (!ccl_same_block(g, gj)) return;
+            const int k = (int)(gj - base);
+            if (vl[k] >= 0 && ccl_active<F32>(R, sd, serial, i, j)) ccl_lunite(vl, (int)threadIdx.x, k);
+        });
+    }
+    __syncthreads();
+    if (g < total) {
+        int lab = -1;
+        if (cand) {
+            // read-only walk to the local root (same member: bonds join only its sites)
+            int x = (int)threadIdx.x, px;
+            while ((px = ((volatile int*)slab)[x]) != x) x = px;
+            lab = (int)(base + x - prefix[r]);
+        }
+        reps[r].queue[i] = lab;
+    }
 }
 
 template <bool F32>
@@ -142,17 +221,16 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
     int64_t i;
     const int r = ccl_member(g, prefix, block_rep, i);
     const BatchRep& R = reps[r];
-    if (__ldcg(R.queue + i) < 0) return;
+    int* lab = R.queue;
+    if (__ldcg(lab + i) < 0) return;
     const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
     const CclSeed sd = seeds[r];
-    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
-        for (int d = 0; d < R.st.dim; ++d) ccl_bond<F32>(R, R.st, sd, serial, i, R.st.nbr(i, 2 * d));
-    } else {
-        for (int t = R.csr.rp[i]; t < R.csr.rp[i + 1]; ++t) {
-            const int64_t j = R.csr.ci[t];
-            if (j > i) ccl_bond<F32>(R, R.csr, sd, serial, i, j);
-        }
-    }
+    const int64_t off = prefix[r];
+    // bonds within the CTA block were united by ccl_local
+    ccl_forward_bonds(R, i, [&](int64_t j) {
+        if (ccl_same_block(g, off + j) || __ldcg(lab + j) < 0) return;
+        if (ccl_active<F32>(R, sd, serial, i, j)) ccl_unite(lab, (int)i, (int)j);
+    });
 }
 
 __global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
