@@ -66,11 +66,14 @@ enum {
     MQV_MODEL_ISING = 1,        /* Ising<int>: int8 +-1, flip proposal, Wolff<Ising<int>> (exact -expm1) */
     MQV_MODEL_ISING_EMBED = 2,  /* Ising<int8_t>: generic Wolff + default Embedder */
     MQV_MODEL_POTTS = 3,        /* Potts<Q>: int8 0..Q-1, flex delta term k */
-    MQV_MODEL_BLUME_CAPEL = 4,  /* BlumeCapel: int8 -1/0/+1, Spin1 proposal, onsite h = D */
+    MQV_MODEL_BLUME_CAPEL = 4,  /* BlumeCapel / BlumeCapelBipartite: int8 -1/0/+1, Spin1 proposal,
+                                   onsite terms h s^2 (D or DA) and h2 s^2 (DB) */
     MQV_MODEL_EA = 5,           /* EdwardsAndersonIsing: Ising with lattice bonds */
     MQV_MODEL_HEISENBERG = 6,   /* Heisenberg: float 3-vectors */
     MQV_MODEL_PHI4 = 7,         /* scalar phi^4: float, onsite h = mass/beta, h2 = lambda/beta */
-    MQV_MODEL_XXZ = 8           /* XXZ: float 3-vectors, z coupling weighted by delta */
+    MQV_MODEL_XXZ = 8           /* XXZAntiferro / XXZAntiferroSingleAniso: float 3-vectors, interaction
+                                   get(s) = (delta s_x, delta s_y, s_z) with coefficient J (the
+                                   reference's J = +1), onsite terms h s_z (field H) and h2 s_z^2 (D) */
 };
 
 /* Metropolis proposal (Initializer<H>::newsv). */
@@ -85,8 +88,8 @@ typedef struct mqv_model_desc {
     int32_t proposal;  /* MQV_PROPOSAL_* */
     int32_t reserved;
     double J;          /* interaction coefficient, reference sign: dE = J dot(s_new - s_old, sum_nbrs) */
-    double h;          /* first onsite coefficient */
-    double h2;         /* second onsite coefficient */
+    double h;          /* coefficient of onsite term 0 */
+    double h2;         /* coefficient of onsite term 1 */
     double k;          /* flex (multisite) coefficient */
     double delta;      /* XXZ anisotropy */
     double cap;        /* proposal width: small-cap cos(half-angle), or phi^4 shift amplitude */
@@ -95,7 +98,10 @@ typedef struct mqv_model_desc {
 /* Lattice kinds. */
 enum {
     MQV_LATTICE_HYPERCUBIC = 1, /* FixedDimRegularHypercubic<d>: periodic, even len, stencil path */
-    MQV_LATTICE_CSR = 2         /* any lattice with nbrs(): CSR neighbours (+ optional bnds) */
+    MQV_LATTICE_CSR = 2,        /* any lattice with nbrs(): CSR neighbours (+ optional bnds) */
+    MQV_LATTICE_BIPARTITE = 3   /* SimpleBipartite (src/lattice/simple_bipartite.h): the hypercubic
+                                   stencil with a termselector -- a site whose coordinate sum is even
+                                   (sublattice A) takes onsite term 0 only, odd (B) term 1 only */
 };
 
 typedef struct mqv_lattice_desc {

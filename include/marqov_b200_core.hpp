@@ -59,6 +59,13 @@ struct HypercubicShape {
     static bool get(const L&, int&, int&) { return false; }
 };
 
+// Lattices with SimpleBipartite's termselector (sublattice by coordinate
+// parity): specialise get() to return true with (dim, len).
+template <class L, class Enable = void>
+struct BipartiteShape {
+    static bool get(const L&, int&, int&) { return false; }
+};
+
 template <class L, class = void>
 struct has_bnds : std::false_type {};
 template <class L>
@@ -72,6 +79,12 @@ public:
     {
         mqv_lattice_desc d{};
         int dim = 0, len = 0;
+        if (BipartiteShape<L>::get(g, dim, len)) {
+            d.kind = MQV_LATTICE_BIPARTITE;
+            d.dim = dim;
+            d.len = len;
+            return d;
+        }
         if (HypercubicShape<L>::get(g, dim, len)) {
             d.kind = MQV_LATTICE_HYPERCUBIC;
             d.dim = dim;

@@ -7,9 +7,13 @@
  *   Ising<other spin>     generic Wolff + Embedder           src/libmarqov/wolff.h:72-126
  *   Potts<Q>              flex term k                         src/hamiltonian/Potts.h:80-156
  *   BlumeCapel<S>         J, onsite D                         src/hamiltonian/BlumeCapel.h:46-80
+ *   BlumeCapelBipartite<S> J, onsite DA, DB                   src/hamiltonian/BlumeCapelBipartite.h:39-86
  *   Heisenberg<S, C>      J                                   src/hamiltonian/Heisenberg.h:62-105
+ *   XXZAntiferro<S>       J = +1, Delta, field H              src/hamiltonian/XXZAntiferro.h:135-205
+ *   XXZAntiferroSingleAniso<S>  ... and single-ion D          src/hamiltonian/XXZAntiferroSingleAniso.h:31-96
  *   EdwardsAndersonIsing  J with the lattice's bnds()         src/hamiltonian/EdwardsAndersonIsing.h:286-310
  *   RegularHypercubic, FixedDimRegularHypercubic<d>: stencil  src/lattice/regular_hypercubic.h
+ *   SimpleBipartite: stencil + termselector by sublattice     src/lattice/simple_bipartite.h:8-58
  * Other lattices (RegularRandomBond, GraphFromCSV, ...) are lowered to CSR
  * from nbrs() / bnds() by LatticeLowering.  MARQOV's Phi4 is a three-
  * component field; the engine's phi^4 is the scalar form and has no
@@ -65,6 +69,52 @@ struct ModelLowering<BlumeCapel<S>> {
 };
 #endif
 
+#ifdef BLUMECAPELBIPARTITE_H
+template <class S>
+struct ModelLowering<BlumeCapelBipartite<S>> {
+    static mqv_model_desc lower(const BlumeCapelBipartite<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_BLUME_CAPEL;
+        d.J = h.J;
+        d.h = h.DA;  // onsite term 0
+        d.h2 = h.DB; // onsite term 1
+        return d;
+    }
+};
+#endif
+
+#ifdef XXZANTIFERRO_H
+template <class S>
+struct ModelLowering<XXZAntiferro<S>> {
+    static mqv_model_desc lower(const XXZAntiferro<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_XXZ;
+        d.J = XXZAntiferro_interaction<typename XXZAntiferro<S>::StateVector>::J;
+        d.delta = h.Delta;
+        d.h = h.H;
+        return d;
+    }
+};
+#endif
+
+#ifdef XXZANTIFERROSINGLEANISO_H
+template <class S>
+struct ModelLowering<XXZAntiferroSingleAniso<S>> {
+    static mqv_model_desc lower(const XXZAntiferroSingleAniso<S>& h, double)
+    {
+        mqv_model_desc d{};
+        d.kind = MQV_MODEL_XXZ;
+        d.J = XXZAntiferro_interaction<typename XXZAntiferroSingleAniso<S>::StateVector>::J;
+        d.delta = h.Delta;
+        d.h = h.H;   // onsite term 0: XXZAntiferro_extfield
+        d.h2 = h.D;  // onsite term 1: XXZAntiferro_onsiteaniso
+        return d;
+    }
+};
+#endif
+
 #ifdef HEISENBERG_H
 template <class S, class C>
 struct ModelLowering<Heisenberg<S, C>> {
@@ -106,6 +156,18 @@ struct HypercubicShape<FixedDimRegularHypercubic<D>> {
     static bool get(const FixedDimRegularHypercubic<D>& g, int& dim, int& len)
     {
         dim = D;
+        len = g.len;
+        return true;
+    }
+};
+#endif
+
+#ifdef SIMPLE_BIPARTITE_H
+template <>
+struct BipartiteShape<SimpleBipartite> {
+    static bool get(const SimpleBipartite& g, int& dim, int& len)
+    {
+        dim = g.dim;
         len = g.len;
         return true;
     }

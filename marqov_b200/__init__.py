@@ -8,14 +8,15 @@ Core interface.  Importing it loads the engine library; there is no CPU path.
 from . import _lib, tempering
 from ._lib import MarqovError
 from .core import Batch, Config, Core, makeCore, tune_small_cap
-from .hamiltonians import (BlumeCapel, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising, Phi4, Potts,
-                           XXZAntiferro)
+from .hamiltonians import (BlumeCapel, BlumeCapelBipartite, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising,
+                           Phi4, Potts, XXZAntiferro, XXZAntiferroSingleAniso)
 from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
-                       RegularRandomBond, read_graph_csv, save_geometry)
+                       RegularRandomBond, SimpleBipartite, read_graph_csv, save_geometry)
 
 _lib.load()
 
 __all__ = ["tempering", "Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
-           "Potts", "BlumeCapel", "Heisenberg", "XXZAntiferro", "Phi4", "CSRLattice",
-           "FixedDimRegularHypercubic", "RegularHypercubic", "RegularRandomBond", "RandomGeometricGraph2D",
+           "Potts", "BlumeCapel", "BlumeCapelBipartite", "Heisenberg", "XXZAntiferro", "XXZAntiferroSingleAniso",
+           "Phi4", "CSRLattice", "FixedDimRegularHypercubic", "RegularHypercubic", "SimpleBipartite",
+           "RegularRandomBond", "RandomGeometricGraph2D",
            "read_graph_csv", "save_geometry"]

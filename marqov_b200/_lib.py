@@ -30,7 +30,7 @@ STATUS_NAMES = {0: "OK", 1: "INVALID_ARG", 2: "UNSUPPORTED_TERM", 3: "BAD_DESCRI
 MODEL_ISING, MODEL_ISING_EMBED, MODEL_POTTS, MODEL_BLUME_CAPEL, MODEL_EA, MODEL_HEISENBERG, \
     MODEL_PHI4, MODEL_XXZ = range(1, 9)
 PROPOSAL_DEFAULT, PROPOSAL_SMALL_CAP = 0, 1
-LATTICE_HYPERCUBIC, LATTICE_CSR = 1, 2
+LATTICE_HYPERCUBIC, LATTICE_CSR, LATTICE_BIPARTITE = 1, 2, 3
 FLAG_PER_COLOUR = 1
 WOLFF_AUTO, WOLFF_BFS, WOLFF_LABEL = 0, 1, 2
 

@@ -29,10 +29,11 @@
 namespace mqv {
 
 template <bool F32, class Lat>
-__device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep, bool live)
+__device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep, bool live,
+                                           int sub)
 {
-    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica, live);
-    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live);
+    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica, live, sub);
+    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live, sub);
 }
 
 // Lanes past the end of the colour's work take no part (live == false).
@@ -50,9 +51,11 @@ __global__ void batch_metro(const BatchRep* __restrict__ reps, const int64_t* __
     const int64_t t = live ? g - prefix[r] : 0;
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
     if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep, live);
+        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep, live,
+                        colour);
     else
-        batch_site<F32>(R, R.csr, live ? (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t] : 0, sweep, live);
+        batch_site<F32>(R, R.csr, live ? (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t] : 0, sweep, live,
+                        0);
 }
 
 template <bool F32>

@@ -293,6 +293,7 @@ static mqv_status lower_model(Sim* s, const mqv_model_desc* m, bool has_bonds)
     s->md.k = m->k;
     s->md.delta = m->delta;
     s->md.cap = m->cap;
+    s->md.termsel = s->termsel;
     s->is_f32 = is_f32_kind(m->kind);
     s->symd = (m->kind == MQV_MODEL_HEISENBERG || m->kind == MQV_MODEL_XXZ) ? 3 : 1;
     s->md.symd = s->symd;
@@ -387,6 +388,8 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         free_sim(s);
         return st;
     };
+    // SimpleBipartite: the hypercubic stencil plus its termselector
+    s->termsel = lattice->kind == MQV_LATTICE_BIPARTITE ? 1 : 0;
     mqv_status st = lower_model(s, model, lattice->bonds != nullptr);
     if (st) return bail(st);
     s->md.beta = params->beta;
@@ -397,7 +400,7 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         return bail(MQV_ERR_CUDA);
     }
     s->own_stream = true;
-    if (lattice->kind == MQV_LATTICE_HYPERCUBIC) {
+    if (lattice->kind == MQV_LATTICE_HYPERCUBIC || lattice->kind == MQV_LATTICE_BIPARTITE) {
         if (lattice->dim < 1 || lattice->dim > 4) return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "hypercubic dim must be 1..4"));
         if (lattice->len < 4 || (lattice->len & 1))
             return bail(fail(MQV_ERR_BAD_DESCRIPTOR,
@@ -826,7 +829,7 @@ MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
     char cfg[96] = "";
     if (s->fused_ising2d) ising2d_config_name(s, cfg, sizeof(cfg));
     std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s", s->md.kind,
-                  s->lat_kind == MQV_LATTICE_HYPERCUBIC ? "hypercubic" : "csr", (long long)s->n,
+                  s->lat_kind == MQV_LATTICE_HYPERCUBIC ? (s->termsel ? "bipartite" : "hypercubic") : "csr", (long long)s->n,
                   s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8"),
                   cfg[0] ? " kernel=" : "", cfg);
     return MQV_OK;
@@ -1211,7 +1214,7 @@ static bool temper_compatible(const Sim* a, const Sim* b)
     if (x.kind != y.kind || x.q != y.q || x.proposal != y.proposal || x.J != y.J || x.h != y.h || x.h2 != y.h2 ||
         x.k != y.k || x.delta != y.delta || x.cap != y.cap)
         return false;
-    if (a->lat_kind != b->lat_kind || a->n != b->n) return false;
+    if (a->lat_kind != b->lat_kind || a->n != b->n || a->termsel != b->termsel) return false;
     if (a->lat_kind == MQV_LATTICE_HYPERCUBIC) return a->dim == b->dim && a->len == b->len;
     return a->lat_hash == b->lat_hash;
 }

@@ -24,7 +24,16 @@ struct ModelDev {
     int symd;
     double J, h, h2, k, delta, cap;
     double beta;
+    // termselector of the lattice (src/libmarqov/metropolishelpers.h:402-430):
+    // 0 = every onsite term acts on every site; 1 = SimpleBipartite
+    // (src/lattice/simple_bipartite.h:22-41), onsite term p acts on the
+    // sites whose coordinate sum has parity p -- the checkerboard colour.
+    int termsel;
 };
+
+// Weights of onsite terms 0 and 1 at a site of sublattice (colour) `sub`.
+MQV_HD double onsite_w0(const ModelDev& m, int sub) { return (m.termsel && sub) ? 0.0 : 1.0; }
+MQV_HD double onsite_w1(const ModelDev& m, int sub) { return (m.termsel && !sub) ? 0.0 : 1.0; }
 
 // Layout of the fused 2D Ising path: row y holds its even-x sites, then its
 // odd-x sites (split rows); within each half, the 32 sites of a word (32
@@ -130,6 +139,7 @@ struct Sim {
     mqv_model_desc model{};
     ModelDev md{};
     int lat_kind = 0;
+    int termsel = 0;  // lattice termselector (ModelDev::termsel)
     int dim = 0, len = 0;
     int64_t n = 0;
     int symd = 1;
@@ -168,7 +178,7 @@ struct Sim {
     // int8 models: u53 cut of every possible dE (int8_cut_table), on the device
     unsigned long long* d_cuts = nullptr;
     int n_cuts = 0;
-    double cuts_for[5] = {0, 0, 0, -1, 0};  // (J, h, k, beta, kind) the table belongs to
+    double cuts_for[7] = {0, 0, 0, -1, 0, 0, 0};  // (J, h, k, beta, kind, h2, termsel) of the table
     // measurement
     int nslots = 0;
     long long* d_acc = nullptr;  // nslots * kAccStride

@@ -49,10 +49,11 @@ __device__ __forceinline__ void smallcap3(SubStream& rng, const float o[3], doub
 
 // Lanes with live == false touch no memory.  The decision
 // is u53 < accept_cut_direct(1, dE, beta), which equals update_accepted<1> on
-// the site's acceptance word.
+// the site's acceptance word.  `sub`: the site's sublattice (checkerboard
+// colour) where the lattice has a termselector.
 template <class Lat>
 __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, float* __restrict__ s, int64_t i,
-                                         Key key, uint32_t sweep, uint32_t replica, bool live)
+                                         Key key, uint32_t sweep, uint32_t replica, bool live, int sub = 0)
 {
     uint64_t cut = 0;
     float nf[3] = {0.f, 0.f, 0.f};
@@ -71,8 +72,8 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
             double sum = 0;
             for (int t = 0; t < deg; ++t) sum += (double)s[lat.nbr(i, t)];
             const double o2 = old * old, n2 = nw * nw;
-            dE = m.J * (nw - old) * sum + m.h * (n2 - o2) +
-                 m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
+            dE = m.J * (nw - old) * sum + onsite_w0(m, sub) * m.h * (n2 - o2) +
+                 onsite_w1(m, sub) * m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
         } else {
             const float* so = s + 3 * i;
             const float o[3] = {so[0], so[1], so[2]};
@@ -89,11 +90,19 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
                 nb[1] += (double)sj[1];
                 nb[2] += (double)sj[2];
             }
-            const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
-            dE = ((double)nf[0] - (double)o[0]) * nb[0];
-            dE += ((double)nf[1] - (double)o[1]) * nb[1];
-            dE += wz * ((double)nf[2] - (double)o[2]) * nb[2];
+            // XXZAntiferro_interaction::get (src/hamiltonian/XXZAntiferro.h:135-150)
+            // weights x and y by delta; Heisenberg's is the identity
+            const double wxy = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
+            dE = wxy * ((double)nf[0] - (double)o[0]) * nb[0];
+            dE += wxy * ((double)nf[1] - (double)o[1]) * nb[1];
+            dE += ((double)nf[2] - (double)o[2]) * nb[2];
             dE *= m.J;
+            if (m.kind == MQV_MODEL_XXZ) {
+                // XXZAntiferro_extfield H s_z and XXZAntiferro_onsiteaniso D s_z^2
+                // (XXZAntiferro.h:162-170, XXZAntiferroSingleAniso.h:31-44)
+                const double zn = nf[2], zo = o[2];
+                dE += onsite_w0(m, sub) * m.h * (zn - zo) + onsite_w1(m, sub) * m.h2 * (zn * zn - zo * zo);
+            }
         }
         cut = accept_cut_direct(1, dE, m.beta);
     }
@@ -134,7 +143,10 @@ __device__ __forceinline__ void measure_f32_part(const ModelDev& m, const Lat& l
 {
     __shared__ double red[6][32];
     double e = 0, mx = 0, my = 0, mz = 0, q2 = 0, q4 = 0;
-    const double wz = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
+    // InteractionEnergy applies the interaction's get() to both ends
+    // (observables.h:186-217): XXZ weights x x' and y y' by delta^2
+    const double wxy = m.kind == MQV_MODEL_XXZ ? m.delta * m.delta : 1.0;
+    const bool xxz = m.kind == MQV_MODEL_XXZ;
     for (int64_t i = part * (int64_t)blockDim.x + threadIdx.x; i < lat.n; i += nparts * blockDim.x) {
         const int deg = lat.degree(i);
         if (m.symd == 1) {
@@ -155,13 +167,17 @@ __device__ __forceinline__ void measure_f32_part(const ModelDev& m, const Lat& l
                 nb += (double)sj[1];
                 nc += (double)sj[2];
             }
-            e += a * na + b * nb + wz * c * nc;
+            e += wxy * (a * na + b * nb) + c * nc;
             mx += a;
             my += b;
             mz += c;
-            const double p2 = a * a + b * b + c * c;
-            q2 += p2;
-            q4 += (p2 - 1.0) * (p2 - 1.0);
+            if (xxz) {
+                q2 += c * c;  // the single-ion term's sum of s_z^2
+            } else {
+                const double p2 = a * a + b * b + c * c;
+                q2 += p2;
+                q4 += (p2 - 1.0) * (p2 - 1.0);
+            }
         }
     }
     double v[6] = {e, mx, my, mz, q2, q4};
@@ -187,7 +203,9 @@ __device__ __forceinline__ void finalize_f32_one(const ModelDev& m, int64_t n, c
     const double mag = a[kAccMag] * a[kAccMag] + a[kAccMagY] * a[kAccMagY] + a[kAccMagZ] * a[kAccMagZ];
     const double mm = sqrt(mag) / (double)n;
     double e = m.J * a[kAccEne] / (double)(2 * n);
+    // SelfEnergy: every onsite term over every site (observables.h:251-268)
     if (m.kind == MQV_MODEL_PHI4) e += (m.h * a[kAccSq] + m.h2 * a[kAccQ4]) / (double)n;
+    if (m.kind == MQV_MODEL_XXZ) e += (m.h * a[kAccMagZ] + m.h2 * a[kAccSq]) / (double)n;
     const double m2 = mm * mm;
     o[0] = e;
     o[1] = mm;

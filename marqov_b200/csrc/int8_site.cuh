@@ -12,12 +12,13 @@ namespace mqv {
 
 // `cuts`: the u53 cut of every dE the model can produce, indexed as
 // int8_cut_index (host table int8_cut_table); the decision equals
-// update_accepted<1>(dE, beta, word) on the site's acceptance word.
-// Lanes with live == false touch no memory.
+// update_accepted<1>(dE, beta, word) on the site's acceptance word.  `sub`:
+// the site's sublattice (checkerboard colour) where the lattice has a
+// termselector.  Lanes with live == false touch no memory.
 template <class Lat>
 __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int8_t* __restrict__ s, int64_t i,
                                           Key key, uint32_t sweep, uint32_t replica,
-                                          const unsigned long long* __restrict__ cuts, int D, bool live)
+                                          const unsigned long long* __restrict__ cuts, int D, bool live, int sub = 0)
 {
     int64_t ai = 0;
     int nw = 0;
@@ -48,6 +49,7 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int
             int sum = 0;
             for (int t = 0; t < deg; ++t) sum += s[lat.addr(lat.nbr(i, t))];
             k = (((nw - old) + 2) * (2 * D + 1) + (sum + D)) * 3 + (nw * nw - old * old + 1);
+            if (m.termsel && sub) k += 15 * (2 * D + 1);  // the sublattice-B table
         } else {
             // spin flip (src/hamiltonian/util/initializers.h:52-58), neighbourhood
             // sum with optional bonds (src/libmarqov/metropolishelpers.h:456-537)
@@ -189,7 +191,10 @@ __device__ __forceinline__ void finalize_int8_one(const ModelDev& m, int64_t n, 
         const double mag = (double)a[kAccMag];
         mm = sqrt(MQV_DMUL(mag, mag)) / (double)n;
         e = MQV_DMUL(m.J, (double)a[kAccEne]) / (double)(2 * n);
-        if (m.kind == MQV_MODEL_BLUME_CAPEL) e = MQV_DADD(e, MQV_DMUL(m.h, (double)a[kAccSq]) / (double)n);
+        // SelfEnergy sums every onsite term over every site, whatever the
+        // termselector (observables.h:251-268): (h + h2 terms) / N
+        if (m.kind == MQV_MODEL_BLUME_CAPEL)
+            e = MQV_DADD(e, MQV_DADD(MQV_DMUL(m.h, (double)a[kAccSq]), MQV_DMUL(m.h2, (double)a[kAccSq])) / (double)n);
     }
     const double m2 = MQV_DMUL(mm, mm);
     o[0] = e;

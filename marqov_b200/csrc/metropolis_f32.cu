@@ -22,7 +22,7 @@ __global__ void metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__
     for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
         const int64_t t = t0 + (threadIdx.x & 31u);
         const bool live = t < half;
-        f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live);
+        f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live, colour);
     }
 }
 

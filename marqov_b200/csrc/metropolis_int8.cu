@@ -27,7 +27,7 @@ __global__ void metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict
     for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
         const int64_t t = t0 + (threadIdx.x & 31u);
         const bool live = t < half;
-        int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live);
+        int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live, colour);
     }
 }
 
@@ -48,13 +48,23 @@ std::vector<unsigned long long> int8_cut_table(const ModelDev& m, int D)
 {
     std::vector<unsigned long long> t;
     if (m.kind == MQV_MODEL_BLUME_CAPEL) {
-        t.resize((size_t)5 * (2 * D + 1) * 3);
-        for (int dn = -2; dn <= 2; ++dn)
-            for (int sum = -D; sum <= D; ++sum)
-                for (int dq = -1; dq <= 1; ++dq) {
-                    const double dE = MQV_DADD(MQV_DMUL(m.J, (double)(dn * sum)), MQV_DMUL(m.h, (double)dq));
-                    t[(size_t)(((dn + 2) * (2 * D + 1) + (sum + D)) * 3 + (dq + 1))] = accept_cut(1, dE, m.beta);
-                }
+        // interaction J dn sum plus the onsite terms of the site, summed in
+        // the reference's order (compute_onsiteenergydiff,
+        // src/libmarqov/metropolishelpers.h:651-683): every term, or with a
+        // termselector term 0 on sublattice A (table 0) and term 1 on B (table 1)
+        const int per = 5 * (2 * D + 1) * 3;
+        t.resize((size_t)per * (m.termsel ? 2 : 1));
+        for (int sub = 0; sub < (m.termsel ? 2 : 1); ++sub)
+            for (int dn = -2; dn <= 2; ++dn)
+                for (int sum = -D; sum <= D; ++sum)
+                    for (int dq = -1; dq <= 1; ++dq) {
+                        double ons;
+                        if (!m.termsel) ons = MQV_DADD(MQV_DMUL(m.h, (double)dq), MQV_DMUL(m.h2, (double)dq));
+                        else ons = MQV_DMUL(sub ? m.h2 : m.h, (double)dq);
+                        const double dE = MQV_DADD(MQV_DMUL(m.J, (double)(dn * sum)), ons);
+                        t[(size_t)sub * per + (size_t)(((dn + 2) * (2 * D + 1) + (sum + D)) * 3 + (dq + 1))] =
+                            accept_cut(1, dE, m.beta);
+                    }
     } else {
         t.resize((size_t)2 * D + 1);
         for (int k = 0; k <= 2 * D; ++k) {
@@ -69,8 +79,8 @@ std::vector<unsigned long long> int8_cut_table(const ModelDev& m, int D)
 // the handle's cut table, rebuilt when the model or beta changed
 cudaError_t ensure_cuts(Sim* s)
 {
-    const double key[5] = {s->md.J, s->md.h, s->md.k, s->md.beta, (double)s->md.kind};
-    if (s->d_cuts && std::equal(key, key + 5, s->cuts_for)) return cudaSuccess;
+    const double key[7] = {s->md.J, s->md.h, s->md.k, s->md.beta, (double)s->md.kind, s->md.h2, (double)s->md.termsel};
+    if (s->d_cuts && std::equal(key, key + 7, s->cuts_for)) return cudaSuccess;
     const std::vector<unsigned long long> t = int8_cut_table(s->md, s->max_degree);
     if ((int)t.size() > s->n_cuts) {
         if (s->d_cuts) cudaFree(s->d_cuts);
@@ -84,7 +94,7 @@ cudaError_t ensure_cuts(Sim* s)
     const cudaError_t e = cudaMemcpyAsync(s->d_cuts, t.data(), sizeof(unsigned long long) * t.size(),
                                           cudaMemcpyHostToDevice, s->stream);
     if (e != cudaSuccess) return e;
-    std::copy(key, key + 5, s->cuts_for);
+    std::copy(key, key + 7, s->cuts_for);
     return cudaStreamSynchronize(s->stream);  // the host table goes out of scope
 }
 
@@ -102,7 +112,11 @@ __global__ void finalize_int8(ModelDev m, int64_t n, const long long* __restrict
 }
 
 // ---------------------------------------------------------------------------
-// initial state (Ising.h:99-107, Potts.h:149-156 rules on the INIT stream)
+// initial state on the INIT stream: Ising::initstatespace (Ising.h:99-107),
+// Potts<Q>::initstatespace (Potts.h:149-156); Blume-Capel has no
+// initstatespace and takes Core::init_hot's random direction of a one-
+// component integer state, +1 turned to -1 when real() < 0.5
+// (src/libmarqov/core.h:773-782, src/hamiltonian/util/randomdir.h:84-90)
 
 template <class Lat>
 __global__ void init_int8(ModelDev m, Lat lat, int64_t n, int8_t* __restrict__ s, Key key, uint32_t tg)
@@ -111,7 +125,7 @@ __global__ void init_int8(ModelDev m, Lat lat, int64_t n, int8_t* __restrict__ s
         const uint64_t w = lo64(philox((uint32_t)i, 0u, 0u, tg, key));
         int v;
         if (m.kind == MQV_MODEL_POTTS) v = (int)(w % (uint64_t)m.q);
-        else if (m.kind == MQV_MODEL_BLUME_CAPEL) v = (int)(w % 3ull) - 1;
+        else if (m.kind == MQV_MODEL_BLUME_CAPEL) v = real01(w) < 0.5 ? -1 : 1;
         else v = real01(w) > 0.5 ? 1 : -1;
         s[lat.addr(i)] = (int8_t)v;
     }

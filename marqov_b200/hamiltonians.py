@@ -90,7 +90,8 @@ class Potts(Hamiltonian):
 
 class BlumeCapel(Hamiltonian):
     """``BlumeCapel`` (src/hamiltonian/BlumeCapel.h:46-153): spin-1 states with
-    the Spin1 proposal and onsite D s^2."""
+    the Spin1 proposal and onsite D s^2.  It has no ``initstatespace``, so its
+    initial state is ``Core::init_hot``'s: +-1 (src/libmarqov/core.h:773-782)."""
 
     SymD = 1
     name = "BlumeCapel"
@@ -103,6 +104,26 @@ class BlumeCapel(Hamiltonian):
 
     def desc(self, beta):
         return L.ModelDesc(kind=L.MODEL_BLUME_CAPEL, J=self.J, h=self.D)
+
+
+class BlumeCapelBipartite(Hamiltonian):
+    """``BlumeCapelBipartite(J, DA, DB)`` (src/hamiltonian/BlumeCapelBipartite.h:39-86):
+    Blume-Capel with two onsite s^2 terms.  On a ``SimpleBipartite`` lattice the
+    termselector gives sublattice A the term DA and B the term DB; on any other
+    lattice both act on every site, as in the reference."""
+
+    SymD = 1
+    name = "BlumeCapelBipartite"
+    kind = L.MODEL_BLUME_CAPEL
+    wolff = False
+
+    def __init__(self, J: float = -1.0, DA: float = 0.0, DB: float = 0.0):
+        self.J = float(J)
+        self.DA = float(DA)
+        self.DB = float(DB)
+
+    def desc(self, beta):
+        return L.ModelDesc(kind=L.MODEL_BLUME_CAPEL, J=self.J, h=self.DA, h2=self.DB)
 
 
 class Heisenberg(Hamiltonian):
@@ -134,25 +155,59 @@ class Heisenberg(Hamiltonian):
 
 
 class XXZAntiferro(Hamiltonian):
-    """XXZ O(3) model (src/hamiltonian/XXZAntiferro.h:135-205): the z component of
-    the interaction weighted by ``delta``."""
+    """``XXZAntiferro(Delta, H)`` (src/hamiltonian/XXZAntiferro.h:135-205): O(3)
+    spins with the interaction ``get(s) = (Delta s_x, Delta s_y, s_z)`` and the
+    reference's fixed antiferromagnetic ``J = +1`` (XXZAntiferro.h:141-150),
+    plus the field ``H s_z`` (``XXZAntiferro_extfield``, :162-170).
+
+    As in the reference, the Metropolis energy difference is
+    ``J dot(s_new - s_old, sum_j get(s_j))`` (linear in Delta) while the
+    ``Energy`` observable applies ``get`` to both ends of a bond, so its x and y
+    parts carry Delta^2 (src/hamiltonian/util/observables.h:186-217).  No Wolff
+    embedding (the reference has none for this model).  ``proposal="smallcap"``
+    replaces the fresh-direction proposal by the small-cap one of
+    ``Heisenberg``."""
 
     SymD = 3
     name = "XXZAntiferro"
     kind = L.MODEL_XXZ
     dtype = np.float32
     wolff = False
+    J = 1.0
 
-    def __init__(self, J: float = 1.0, delta: float = 1.0, proposal: str = "fresh", cap: float = 0.5):
-        self.J = float(J)
-        self.delta = float(delta)
+    def __init__(self, Delta: float = 1.0, H: float = 0.0, proposal: str = "fresh", cap: float = 0.5):
+        if proposal not in ("fresh", "smallcap"):
+            raise ValueError("proposal must be 'fresh' or 'smallcap'")
+        self.Delta = float(Delta)
+        self.H = float(H)
         self.proposal = proposal
         self.cap = float(cap)
 
+    def _onsite(self):
+        return self.H, 0.0
+
     def desc(self, beta):
-        return L.ModelDesc(kind=L.MODEL_XXZ, J=self.J, delta=self.delta,
+        h, h2 = self._onsite()
+        return L.ModelDesc(kind=L.MODEL_XXZ, J=self.J, delta=self.Delta, h=h, h2=h2,
                            proposal=L.PROPOSAL_SMALL_CAP if self.proposal == "smallcap" else 0,
                            cap=self.cap)
+
+
+class XXZAntiferroSingleAniso(XXZAntiferro):
+    """``XXZAntiferroSingleAniso(H, Delta, D)`` (src/hamiltonian/XXZAntiferroSingleAniso.h:54-96;
+    note the reference's argument order): ``XXZAntiferro`` plus the single-ion
+    anisotropy ``D s_z^2`` as onsite term 1.  On a ``SimpleBipartite`` lattice
+    the termselector gives sublattice A the field and B the anisotropy."""
+
+    name = "XXZAntiferroSingleAniso"
+
+    def __init__(self, H: float = 0.0, Delta: float = 1.0, D: float = 0.0, proposal: str = "fresh",
+                 cap: float = 0.5):
+        super().__init__(Delta, H, proposal, cap)
+        self.D = float(D)
+
+    def _onsite(self):
+        return self.H, self.D
 
 
 class Phi4(Hamiltonian):

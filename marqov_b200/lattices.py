@@ -85,6 +85,32 @@ class RegularHypercubic(Lattice):
         return CSRLattice(rp, cols.reshape(-1), colours=(par & 1).astype(np.int32))
 
 
+class SimpleBipartite(RegularHypercubic):
+    """``SimpleBipartite(len, dim)`` (src/lattice/simple_bipartite.h:8-58): the
+    periodic hypercubic lattice with a ``termselector`` -- a site whose
+    coordinate sum is even (sublattice A) takes onsite term 0 only, an odd one
+    term 1 only (``identify``, simple_bipartite.h:22-36).  Runs on the stencil
+    path; the sublattice of a site is its checkerboard colour."""
+
+    def __init__(self, len: int, dim: int):  # noqa: A002 - reference argument name
+        if int(len) % 2:
+            raise ValueError("SimpleBipartite needs an even linear size")
+        super().__init__(len, dim)
+
+    def identify(self, k: int) -> int:
+        s = 0
+        for _ in range(self.dim):
+            s += k % self.len
+            k //= self.len
+        return s % 2
+
+    def termselector(self, rsite: int) -> list[int]:
+        return [self.identify(rsite)]
+
+    def desc(self) -> L.LatticeDesc:
+        return L.LatticeDesc(kind=L.LATTICE_BIPARTITE, dim=self.dim, len=self.len)
+
+
 def FixedDimRegularHypercubic(dim: int, len: int) -> RegularHypercubic:  # noqa: A002
     """``FixedDimRegularHypercubic<dim>(len)``."""
     return RegularHypercubic(len, dim)

@@ -209,9 +209,16 @@ void orc_parity_colours(int dim, int len, int32_t* colour_ptr, int32_t* order)
 
 /* ---- int8 models: Metropolis --------------------------------------------- */
 
+/* Weights of onsite terms 0 / 1 at a site of sublattice `sub` (the parity
+ * colour): every term acts unless the lattice has SimpleBipartite's
+ * termselector (src/lattice/simple_bipartite.h:22-41, read by get_terms,
+ * src/libmarqov/metropolishelpers.h:402-430), which gives sublattice p term p. */
+static int ons0(const orc_model* m, int sub) { return !(m->termsel && sub); }
+static int ons1(const orc_model* m, int sub) { return !(m->termsel && !sub); }
+
 /* One Metropolis::move (src/libmarqov/metropolis.h:88-126) at site i. */
 static void metro_int8_site(const orc_model* m, const orc_lattice* g, int8_t* s, double beta,
-                            orc_rng* rng, int32_t i)
+                            orc_rng* rng, int32_t i, int sub)
 {
     const int32_t b = g->row_ptr[i], e = g->row_ptr[i + 1];
     int old = s[i], nw;
@@ -238,7 +245,13 @@ static void metro_int8_site(const orc_model* m, const orc_lattice* g, int8_t* s,
         nw = st;
         int sum = 0;
         for (int32_t p = b; p < e; ++p) sum += s[g->col_idx[p]];
-        dE = m->J * (double)((nw - old) * sum) + m->h * (double)(nw * nw - old * old);
+        /* compute_onsiteenergydiff (metropolishelpers.h:651-683): the site's
+         * terms in order, each h_b (get(new) - get(old)), get = s^2 */
+        const double dq = (double)(nw * nw - old * old);
+        double ons = 0.0;
+        if (ons0(m, sub)) ons += m->h * dq;
+        if (ons1(m, sub) && (m->termsel || m->h2 != 0.0)) ons += m->h2 * dq;
+        dE = m->J * (double)((nw - old) * sum) + ons;
         break;
     }
     default: {
@@ -268,7 +281,7 @@ void orc_sweep_int8(const orc_model* m, const orc_lattice* g, int8_t* s, double 
         for (int32_t p = g->colour_ptr[c]; p < g->colour_ptr[c + 1]; ++p) {
             int32_t i = g->order[p];
             orc_rng rng = {seed, replica, ST_METRO, (uint32_t)i, sweep, 0};
-            metro_int8_site(m, g, s, beta, &rng, i);
+            metro_int8_site(m, g, s, beta, &rng, i, c);
         }
 }
 
@@ -295,14 +308,17 @@ void orc_ising2d_sweep(int32_t L, double J, int8_t* s, double beta, uint64_t see
 }
 
 /* Initial states: Ising::initstatespace (src/hamiltonian/Ising.h:99-107),
- * Potts::initstatespace (src/hamiltonian/Potts.h:149-156); Blume-Capel draws
- * uniformly from {-1,0,1}. One INIT substream per site. */
+ * Potts::initstatespace (src/hamiltonian/Potts.h:149-156); Blume-Capel has
+ * none and gets Core::init_hot (src/libmarqov/core.h:773-782): the
+ * one-component random direction of set_to_rnddir, +1 turned to -1 when
+ * real() < 0.5 (src/hamiltonian/util/randomdir.h:84-90,102-106).  One INIT
+ * substream per site. */
 void orc_init_int8(const orc_model* m, int32_t n, int8_t* s, uint64_t seed, uint32_t replica)
 {
     for (int32_t i = 0; i < n; ++i) {
         orc_rng rng = {seed, replica, ST_INIT, (uint32_t)i, 0, 0};
         if (m->kind == ORC_POTTS) s[i] = (int8_t)rng_integer_r(&rng, (uint64_t)m->q);
-        else if (m->kind == ORC_BLUME_CAPEL) s[i] = (int8_t)((int)rng_integer_r(&rng, 3) - 1);
+        else if (m->kind == ORC_BLUME_CAPEL) s[i] = rng_real(&rng) < 0.5 ? -1 : 1;
         else s[i] = rng_real(&rng) > 0.5 ? 1 : -1;
     }
 }
@@ -348,7 +364,7 @@ static void smallcap3(orc_rng* rng, const float* o, double cap, double v[3])
 }
 
 static void metro_f32_site(const orc_model* m, const orc_lattice* g, float* s, int symd,
-                           double beta, orc_rng* rng, int32_t i)
+                           double beta, orc_rng* rng, int32_t i, int sub)
 {
     const int32_t b = g->row_ptr[i], e = g->row_ptr[i + 1];
     float* so = s + (size_t)i * symd;
@@ -365,8 +381,8 @@ static void metro_f32_site(const orc_model* m, const orc_lattice* g, float* s, i
         double o2 = old * old, n2 = nw[0] * nw[0];
         /* interaction + Onsite_Quadratic + Onsite_Fourth_Minus_One,
          * src/hamiltonian/Phi4.h:63-74,103-121 */
-        dE = m->J * (nw[0] - old) * sum + m->h * (n2 - o2) +
-             m->h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
+        dE = m->J * (nw[0] - old) * sum + ons0(m, sub) * m->h * (n2 - o2) +
+             ons1(m, sub) * m->h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
     } else {
         double v[3];
         if (m->proposal == 1) smallcap3(rng, so, m->cap, v);
@@ -377,10 +393,18 @@ static void metro_f32_site(const orc_model* m, const orc_lattice* g, float* s, i
             const float* sj = s + (size_t)g->col_idx[p] * 3;
             for (int c = 0; c < 3; ++c) nb[c] += (double)sj[c];
         }
-        double w[3] = {1.0, 1.0, m->kind == ORC_XXZ ? m->delta : 1.0};
+        /* the interaction's get(): XXZAntiferro_interaction weights x and y
+         * by Delta (src/hamiltonian/XXZAntiferro.h:135-150), Heisenberg none */
+        double w[3] = {m->kind == ORC_XXZ ? m->delta : 1.0, m->kind == ORC_XXZ ? m->delta : 1.0, 1.0};
         dE = 0;
         for (int c = 0; c < 3; ++c) dE += w[c] * (nw[c] - (double)so[c]) * nb[c];
         dE *= m->J;
+        if (m->kind == ORC_XXZ) {
+            /* XXZAntiferro_extfield H s_z (XXZAntiferro.h:162-170) and
+             * XXZAntiferro_onsiteaniso D s_z^2 (XXZAntiferroSingleAniso.h:31-44) */
+            double zn = nw[2], zo = so[2];
+            dE += ons0(m, sub) * m->h * (zn - zo) + ons1(m, sub) * m->h2 * (zn * zn - zo * zo);
+        }
     }
     if (dE <= 0 || orc_update_accepted(1, dE, beta, orc_accept_word(rng->seed, rng->replica, rng->c0, rng->c1)))
         for (int c = 0; c < symd; ++c) so[c] = (float)nw[c];
@@ -393,7 +417,7 @@ void orc_sweep_f32(const orc_model* m, const orc_lattice* g, float* s, int symd,
         for (int32_t p = g->colour_ptr[c]; p < g->colour_ptr[c + 1]; ++p) {
             int32_t i = g->order[p];
             orc_rng rng = {seed, replica, ST_METRO, (uint32_t)i, sweep, 0};
-            metro_f32_site(m, g, s, symd, beta, &rng, i);
+            metro_f32_site(m, g, s, symd, beta, &rng, i, c);
         }
 }
 
@@ -583,9 +607,10 @@ void orc_measure_int8(const orc_model* m, const orc_lattice* g, const int8_t* s,
         }
         e = m->J * enepart / (double)(2 * (int64_t)n);
         if (m->kind == ORC_BLUME_CAPEL) {
+            /* SelfEnergy: every onsite term over every site (observables.h:251-268) */
             double sq = 0;
             for (int32_t i = 0; i < n; ++i) sq += (double)(s[i] * s[i]);
-            e += m->h * sq / (double)n;
+            e += (m->h * sq + m->h2 * sq) / (double)n;
         }
     }
     out->e = e; out->m = mm; out->m2 = mm * mm; out->m4 = out->m2 * out->m2;
@@ -601,8 +626,11 @@ void orc_measure_f32(const orc_model* m, const orc_lattice* g, const float* s, i
     double r = 0;
     for (int c = 0; c < symd; ++c) r += mag[c] * mag[c];
     double mm = sqrt(r) / (double)n;
-    double w[3] = {1.0, 1.0, m->kind == ORC_XXZ ? m->delta : 1.0};
-    double enepart = 0, q2 = 0, q4 = 0;
+    /* InteractionEnergy applies get() to both ends (observables.h:186-217):
+     * XXZ weights x x' and y y' by Delta^2 */
+    const double d2 = m->kind == ORC_XXZ ? m->delta * m->delta : 1.0;
+    double w[3] = {d2, d2, 1.0};
+    double enepart = 0, q2 = 0, q4 = 0, sz = 0, szz = 0;
     for (int32_t i = 0; i < n; ++i) {
         const float* si = s + (size_t)i * symd;
         for (int32_t p = g->row_ptr[i]; p < g->row_ptr[i + 1]; ++p) {
@@ -613,9 +641,15 @@ void orc_measure_f32(const orc_model* m, const orc_lattice* g, const float* s, i
         for (int c = 0; c < symd; ++c) p2 += (double)si[c] * (double)si[c];
         q2 += p2;
         q4 += (p2 - 1.0) * (p2 - 1.0);
+        if (symd == 3) {
+            sz += (double)si[2];
+            szz += (double)si[2] * (double)si[2];
+        }
     }
     double e = m->J * enepart / (double)(2 * (int64_t)n);
+    /* SelfEnergy: every onsite term over every site (observables.h:251-268) */
     if (m->kind == ORC_PHI4) e += (m->h * q2 + m->h2 * q4) / (double)n;
+    if (m->kind == ORC_XXZ) e += (m->h * sz + m->h2 * szz) / (double)n;
     out->e = e; out->m = mm; out->m2 = mm * mm; out->m4 = out->m2 * out->m2;
 }
 

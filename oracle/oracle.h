@@ -52,7 +52,7 @@ enum {
     ORC_EA = 5,           /* EdwardsAndersonIsing with lattice bonds */
     ORC_HEISENBERG = 6,   /* O(3), fresh-direction or small-cap proposals */
     ORC_PHI4 = 7,         /* scalar phi^4, Cartesian shift proposal */
-    ORC_XXZ = 8           /* XXZ anisotropic O(3) */
+    ORC_XXZ = 8           /* XXZAntiferro(SingleAniso): (Delta x, Delta y, z) interaction, H s_z, D s_z^2 */
 };
 
 typedef struct orc_model {
@@ -60,11 +60,13 @@ typedef struct orc_model {
     int q;           /* Potts states */
     int proposal;    /* 0 = model default, 1 = small-cap (Heisenberg/XXZ) */
     double J;        /* interaction prefactor, reference sign: dE = J dot(dS, sum nbrs) */
-    double h;        /* onsite prefactor (Blume-Capel D; phi^4 mass/beta) */
-    double h2;       /* second onsite prefactor (phi^4 lambda/beta) */
+    double h;        /* onsite term 0 (Blume-Capel D or DA; phi^4 mass/beta; XXZ field H) */
+    double h2;       /* onsite term 1 (Blume-Capel DB; phi^4 lambda/beta; XXZ single-ion D) */
     double k;        /* flex prefactor (Potts) */
-    double delta;    /* XXZ anisotropy (z component weight) */
+    double delta;    /* XXZ anisotropy (weight of the x and y components) */
     double cap;      /* proposal width: small-cap cos(theta_max) or phi^4 shift amplitude */
+    int termsel;     /* 1: SimpleBipartite termselector -- onsite term p only on the sites of
+                        colour p (the lattice's colouring must be the coordinate parity) */
 } orc_model;
 
 typedef struct orc_lattice {

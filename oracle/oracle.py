@@ -30,7 +30,7 @@ _u32p = np.ctypeslib.ndpointer(np.uint32, flags="C_CONTIGUOUS")
 class OrcModel(C.Structure):
     _fields_ = [("kind", C.c_int), ("q", C.c_int), ("proposal", C.c_int), ("J", C.c_double),
                 ("h", C.c_double), ("h2", C.c_double), ("k", C.c_double),
-                ("delta", C.c_double), ("cap", C.c_double)]
+                ("delta", C.c_double), ("cap", C.c_double), ("termsel", C.c_int)]
 
 
 class OrcLattice(C.Structure):
@@ -211,16 +211,19 @@ class RefHarness:
             raise FileNotFoundError(path)
         lib = C.CDLL(path)
         lib.ref_sweeps_int.restype = C.c_int
-        lib.ref_sweeps_int.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_void_p, C.c_int, _i32p,
-                                       _i32p, _i8p, C.c_double, C.c_double, C.c_double,
+        lib.ref_sweeps_int.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_void_p, C.c_void_p, C.c_int, _i32p,
+                                       _i32p, _i8p, C.c_double, C.c_double, C.c_double, C.c_double,
                                        C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]
         lib.ref_sweeps_f32.restype = C.c_int
-        lib.ref_sweeps_f32.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_int, _i32p, _i32p, _f32p,
-                                       C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
+        lib.ref_sweeps_f32.argtypes = [C.c_int, C.c_int, _i32p, _i32p, C.c_void_p, C.c_int, _i32p, _i32p, _f32p,
+                                       C.c_double, C.c_double, C.c_double, C.c_double, C.c_double, C.c_double,
                                        C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, C.c_void_p]
         lib.ref_wolff_int.restype = C.c_int
         lib.ref_wolff_int.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _i8p, C.c_double, C.c_double,
                                       C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, _i32p]
+        lib.ref_wolff_f32.restype = C.c_int
+        lib.ref_wolff_f32.argtypes = [C.c_int, C.c_int, _i32p, _i32p, _f32p, C.c_double, C.c_double, C.c_double,
+                                      C.c_double, C.c_uint64, C.c_uint32, C.c_uint32, C.c_int, _i32p]
         lib.ref_metro_exp.restype = C.c_longlong
         lib.ref_metro_exp.argtypes = [C.c_int, C.c_int, C.c_double, _f64p, C.c_void_p]
         lib.ref_metro_exp_plain.restype = C.c_longlong
@@ -290,28 +293,49 @@ class RefHarness:
             raise RuntimeError(f"ref_pt_calcprob failed ({rc})")
         return out
 
-    def sweeps_int(self, kind, g: Graph, s, J, D, beta, seed, replica, sweep0, nsweeps, want_obs=True):
-        obs = np.zeros(2 * nsweeps, np.float64) if want_obs else None
+    @staticmethod
+    def _sub(sub):
+        if sub is None:
+            return None, None
+        a = np.ascontiguousarray(sub, np.uint8)
+        return a, a.ctypes.data
+
+    def sweeps_int(self, kind, g: Graph, s, J, D, beta, seed, replica, sweep0, nsweeps, want_obs=True, D2=0.0,
+                   sub=None):
+        """Reference Metropolis sweeps in colour order; per sweep (e, m, e_obs):
+        the energy the moves see, the magnetization and Energy<H> (ref_harness.cpp)."""
+        obs = np.zeros(3 * nsweeps, np.float64) if want_obs else None
         bonds = None if g.bonds is None else g.bonds.ctypes.data
-        rc = self.lib.ref_sweeps_int(kind, g.n, g.row_ptr, g.col_idx, bonds, len(g.colour_ptr) - 1,
-                                     g.colour_ptr, g.order, s, J, D, beta, seed, replica, sweep0,
+        keep, subp = self._sub(sub)
+        rc = self.lib.ref_sweeps_int(kind, g.n, g.row_ptr, g.col_idx, bonds, subp, len(g.colour_ptr) - 1,
+                                     g.colour_ptr, g.order, s, J, D, D2, beta, seed, replica, sweep0,
                                      nsweeps, None if obs is None else obs.ctypes.data)
         assert rc == 0
-        return None if obs is None else obs.reshape(nsweeps, 2)
+        return None if obs is None else obs.reshape(nsweeps, 3)
 
     def sweeps_f32(self, kind, g: Graph, s, J, p0, p1, cap, beta, seed, replica, sweep0, nsweeps,
-                   want_obs=True):
-        obs = np.zeros(2 * nsweeps, np.float64) if want_obs else None
-        rc = self.lib.ref_sweeps_f32(kind, g.n, g.row_ptr, g.col_idx, len(g.colour_ptr) - 1,
-                                     g.colour_ptr, g.order, s, J, p0, p1, cap, beta, seed, replica,
+                   want_obs=True, p2=0.0, sub=None):
+        obs = np.zeros(3 * nsweeps, np.float64) if want_obs else None
+        keep, subp = self._sub(sub)
+        rc = self.lib.ref_sweeps_f32(kind, g.n, g.row_ptr, g.col_idx, subp, len(g.colour_ptr) - 1,
+                                     g.colour_ptr, g.order, s, J, p0, p1, p2, cap, beta, seed, replica,
                                      sweep0, nsweeps, None if obs is None else obs.ctypes.data)
         assert rc == 0
-        return None if obs is None else obs.reshape(nsweeps, 2)
+        return None if obs is None else obs.reshape(nsweeps, 3)
 
     def wolff_int(self, kind, g: Graph, s, J, beta, seed, replica, serial0, nclusters):
         sizes = np.zeros(nclusters, np.int32)
         rc = self.lib.ref_wolff_int(kind, g.n, g.row_ptr, g.col_idx, s, J, beta, seed, replica,
                                     serial0, nclusters, sizes)
+        assert rc == 0
+        return sizes
+
+    def wolff_f32(self, kind, g: Graph, s, J, p0, p1, beta, seed, replica, serial0, nclusters):
+        """The reference's generic Wolff with Embedder<Heisenberg> (kind 6) or the
+        scalar Embedder<Phi4> (kind 8), sequential draws; s updated in place."""
+        sizes = np.zeros(nclusters, np.int32)
+        rc = self.lib.ref_wolff_f32(kind, g.n, g.row_ptr, g.col_idx, s, J, p0, p1, beta, seed, replica, serial0,
+                                    nclusters, sizes)
         assert rc == 0
         return sizes
 

@@ -95,6 +95,9 @@ public:
 #include "hamiltonian/Heisenberg.h"
 #include "hamiltonian/Phi4.h"
 #include "hamiltonian/BlumeCapel.h"
+#include "hamiltonian/BlumeCapelBipartite.h"
+#include "hamiltonian/XXZAntiferro.h"
+#include "hamiltonian/XXZAntiferroSingleAniso.h"
 #include "lattice/regular_hypercubic.h"
 
 enum { ST_METRO = 1, ST_INIT = 2, ST_WOLFF_SEED = 3 };
@@ -181,6 +184,49 @@ public:
     }
 };
 
+// Heisenberg whose clusters are the reference's generic Wolff<H,L>::move
+// (src/libmarqov/wolff.h:72-126) driven by the reference's own
+// Embedder<Heisenberg> (src/hamiltonian/Heisenberg.h:123-186: random unit
+// rdir, coupling (s_i.r)(s_j.r), reflection about the plane normal to r,
+// normalised).  The derived type only keeps the reference's Wolff<Heisenberg>
+// specialisation (random Cartesian axis, Heisenberg.h:191-243) out of the
+// way, and forwards the two-argument draw() the generic Wolff calls to the
+// embedder's one-argument draw().
+struct HeisenbergPlane : public Heisenberg<float, double> {
+    explicit HeisenbergPlane(double J) : Heisenberg<float, double>(J) {}
+};
+namespace MARQOV {
+template <class Lattice>
+class Embedder<HeisenbergPlane, Lattice> : public Embedder<Heisenberg<float, double>, Lattice> {
+    typedef Embedder<Heisenberg<float, double>, Lattice> Base;
+
+public:
+    Embedder(const HeisenbergPlane& h, const Lattice& l, Space<std::array<float, 3>, Lattice>& s) : Base(h, l, s) {}
+    template <class RNG>
+    void draw(RNG& rng, std::array<float, 3>&) { Base::draw(rng); }
+};
+// The scalar field's embedder, Embedder<Phi4> (src/hamiltonian/Phi4.h:182-244)
+// for one component: rdir = set_to_rnddir of a one-component vector (+-1),
+// coupling (s_i r)(s_j r), flip s -> s - 2 (s r) r, no normalisation.
+template <class Lattice>
+class Embedder<Phi4Scalar, Lattice> {
+    typedef std::array<float, 1> SV;
+    const Space<SV, Lattice>& ss;
+    SV rdir;
+
+public:
+    Embedder(const Phi4Scalar&, const Lattice&, Space<SV, Lattice>& s) : ss(s) {}
+    template <class RNG>
+    void draw(RNG& rng, SV&) { set_to_rnddir(rng, rdir); }
+    double coupling(int a, int b) const { return dot(ss[a], rdir) * dot(ss[b], rdir); }
+    void flip(SV& sv)
+    {
+        const double d = dot(sv, rdir);
+        sv[0] -= 2 * d * rdir[0];
+    }
+};
+}  // namespace MARQOV
+
 // ---------------------------------------------------------------------------
 // Colour-order Metropolis through the reference templates.
 
@@ -203,84 +249,167 @@ static void colour_sweep(const H& ham, const L& grid, SS& ss, RNGCache<PhiloxSit
         }
 }
 
+// A lattice with SimpleBipartite's termselector (src/lattice/simple_bipartite.h:38-41):
+// site i takes only onsite term sub[i] (its sublattice).
+struct CSRTermLattice : CSRLattice {
+    const uint8_t* sub;
+    std::vector<int> termselector(int i) const { return {(int)sub[i]}; }
+};
+struct CSRBondTermLattice : CSRBondLattice {
+    const uint8_t* sub;
+    std::vector<int> termselector(int i) const { return {(int)sub[i]}; }
+};
+
+// Energy per site as the reference's Metropolis moves see it, through the
+// reference's own helpers: J/(2N) sum_i dot(get(s_i), nbrhoodloop(i)), with
+// the lattice's bonds when it has them (src/libmarqov/metropolishelpers.h:
+// 456-537), plus the SelfEnergy observable.  It equals Energy<H> on lattices
+// without bonds; Energy<H> itself never reads bnds() (observables.h:186-217).
+template <class H, class L, class SS>
+static double nbrhood_energy(const H& ham, const L& lat, const SS& ss)
+{
+    typedef typename MARQOV::has_bnds<L>::type HB;
+    const int n = (int)lat.size();
+    double part = 0.0;
+    for (int i = 0; i < n; ++i) {
+        auto nb = MARQOV::nbrhoodloop<L, H, SS>(lat, ham, ss, 0, i, std::true_type(), HB());
+        part += dot(ham.interactions[0]->get(ss[i]), nb);
+    }
+    SelfEnergy<H> se(ham);
+    return ham.interactions[0]->J * part / double(2 * n) + se.measure(ss, lat);
+}
+
+// Potts energy as its Metropolis moves see it: k/(2N) sum_i #{j in nbrs(i):
+// s_j = s_i}, each count taken from the reference's PottsInteraction::diff
+// with an old state no neighbour holds (src/hamiltonian/Potts.h:86-107).
+// Energy<Potts<Q>> reads 0: PottsInteraction::energy is a stub (Potts.h:108-109).
+template <class L, class SS>
+static double potts_energy(const Potts<3>& ham, const L& lat, SS& ss)
+{
+    const int n = (int)lat.size();
+    double cnt = 0.0;
+    std::array<int, 1> none{{-1}};
+    for (int i = 0; i < n; ++i)
+        cnt += const_cast<Potts<3>&>(ham).potts_interaction.diff(i, none, ss[i], lat.nbrs(0, i), ss);
+    return ham.potts_interaction.k * cnt / double(2 * n);
+}
+
+// Runs nsweeps colour-ordered sweeps of the reference Metropolis on ss and
+// writes per sweep (e, m, e_obs): e the energy per site the moves see, m the
+// model's magnetization observable, e_obs the reference's Energy<H> observable.
+template <class H, class L, class SS, class EFn, class MFn>
+static void run_sweeps(const H& ham, const L& lat, SS& ss, RNGCache<PhiloxSite>& rng, double beta, uint32_t sweep0,
+                       int nsweeps, int ncol, const int32_t* cptr, const int32_t* order, int nprop, EFn efn,
+                       MFn mfn, double* obs)
+{
+    for (int t = 0; t < nsweeps; ++t) {
+        colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, nprop);
+        if (obs) {
+            Energy<H> eo(ham);
+            obs[3 * t] = efn(ss);
+            obs[3 * t + 1] = mfn(ss);
+            obs[3 * t + 2] = eo.measure(ss, lat);
+        }
+    }
+}
+
+template <class SV, class L, class T>
+static void load_state(MARQOV::Space<SV, L>& ss, const T* s, int n)
+{
+    constexpr int D = std::tuple_size<SV>::value;
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < D; ++c) ss[i][c] = s[(size_t)i * D + c];
+}
+template <class SV, class L, class T>
+static void store_state(const MARQOV::Space<SV, L>& ss, T* s, int n)
+{
+    constexpr int D = std::tuple_size<SV>::value;
+    for (int i = 0; i < n; ++i)
+        for (int c = 0; c < D; ++c) s[(size_t)i * D + c] = (T)ss[i][c];
+}
+
+template <class H, class L>
+static void int_model(const H& ham, const L& lat, int8_t* spins, RNGCache<PhiloxSite>& rng, double beta,
+                      uint32_t sweep0, int nsweeps, int ncol, const int32_t* cptr, const int32_t* order, int nprop,
+                      double* obs)
+{
+    const int n = (int)lat.size();
+    MARQOV::Space<std::array<int, 1>, L> ss(n);
+    load_state(ss, spins, n);
+    auto ef = [&](const MARQOV::Space<std::array<int, 1>, L>& x) { return nbrhood_energy(ham, lat, x); };
+    auto mf = [&](const MARQOV::Space<std::array<int, 1>, L>& x) { return Magnetization().measure(x, lat); };
+    run_sweeps(ham, lat, ss, rng, beta, sweep0, nsweeps, ncol, cptr, order, nprop, ef, mf, obs);
+    store_state(ss, spins, n);
+}
+
+template <class H, class L>
+static void f32_model(const H& ham, const L& lat, float* s, RNGCache<PhiloxSite>& rng, double beta,
+                      uint32_t sweep0, int nsweeps, int ncol, const int32_t* cptr, const int32_t* order, int nprop,
+                      double* obs)
+{
+    typedef typename H::StateVector SV;
+    const int n = (int)lat.size();
+    MARQOV::Space<SV, L> ss(n);
+    load_state(ss, s, n);
+    auto ef = [&](const MARQOV::Space<SV, L>& x) { return nbrhood_energy(ham, lat, x); };
+    auto mf = [&](const MARQOV::Space<SV, L>& x) { return Magnetization().measure(x, lat); };
+    run_sweeps(ham, lat, ss, rng, beta, sweep0, nsweeps, ncol, cptr, order, nprop, ef, mf, obs);
+    store_state(ss, s, n);
+}
+
 extern "C" {
 
 // Metropolis sweeps for int8-state models.  kind: 1 Ising<int>, 3 Potts<3>,
-// 4 BlumeCapel, 5 Ising with bonds (EdwardsAnderson form).  Writes per-sweep
-// reference observables (e, m) when obs != NULL.
-int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const int8_t* bonds,
+// 4 BlumeCapel<int>(J, D), 5 Ising with bonds (EdwardsAndersonIsing form),
+// 11 BlumeCapelBipartite<int>(J, D, D2).  sub (optional): per-site
+// sublattice, giving the lattice SimpleBipartite's termselector.  obs
+// (optional): per sweep (e, m, e_obs) as run_sweeps.
+int ref_sweeps_int(int kind, int n, const int32_t* rp, const int32_t* ci, const int8_t* bonds, const uint8_t* sub,
                    int ncol, const int32_t* cptr, const int32_t* order, int8_t* spins,
-                   double J, double D, double beta, uint64_t seed, uint32_t replica,
+                   double J, double D, double D2, double beta, uint64_t seed, uint32_t replica,
                    uint32_t sweep0, int nsweeps, double* obs)
 {
     RNGCache<PhiloxSite> rng;
     rng.seed = seed;
     rng.replica = replica;
     CSRLattice lat{n, rp, ci};
+    CSRTermLattice tlat;
+    tlat.n = n; tlat.rp = rp; tlat.ci = ci; tlat.sub = sub;
     if (kind == 1) {
         Ising<int> ham(J);
-        MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
-        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
-        for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
-            if (obs) {
-                Magnetization mo;
-                Energy<Ising<int>> eo(ham);
-                obs[2 * t] = eo.measure(ss, lat);
-                obs[2 * t + 1] = mo.measure(ss, lat);
-            }
-        }
-        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+        int_model(ham, lat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 0, obs);
     } else if (kind == 3) {
         Potts<3> ham(J);
         MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
-        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
-        for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
-            if (obs) {
-                PottsMagnetization<3> mo;
-                obs[2 * t] = 0.0;
-                obs[2 * t + 1] = mo.measure(ss, lat);
-            }
-        }
-        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+        load_state(ss, spins, n);
+        auto ef = [&](MARQOV::Space<std::array<int, 1>, CSRLattice>& x) { return potts_energy(ham, lat, x); };
+        auto mf = [&](MARQOV::Space<std::array<int, 1>, CSRLattice>& x) { return PottsMagnetization<3>().measure(x, lat); };
+        run_sweeps(ham, lat, ss, rng, beta, sweep0, nsweeps, ncol, cptr, order, NProp<Potts<3>>::value, ef, mf, obs);
+        store_state(ss, spins, n);
     } else if (kind == 4) {
         BlumeCapel<int> ham(J, D);
-        MARQOV::Space<std::array<int, 1>, CSRLattice> ss(n);
-        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
-        for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
-            if (obs) {
-                Magnetization mo;
-                obs[2 * t] = 0.0;
-                obs[2 * t + 1] = mo.measure(ss, lat);
-            }
-        }
-        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+        if (sub) int_model(ham, tlat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
+        else int_model(ham, lat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
+    } else if (kind == 11) {
+        BlumeCapelBipartite<int> ham(J, D, D2);
+        if (sub) int_model(ham, tlat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
+        else int_model(ham, lat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
     } else if (kind == 5) {
         CSRBondLattice blat;
         blat.n = n; blat.rp = rp; blat.ci = ci; blat.bd = bonds;
         Ising<int> ham(J);
-        MARQOV::Space<std::array<int, 1>, CSRBondLattice> ss(n);
-        for (int i = 0; i < n; ++i) ss[i][0] = spins[i];
-        for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, blat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 0);
-            if (obs) {
-                Magnetization mo;
-                obs[2 * t] = 0.0;
-                obs[2 * t + 1] = mo.measure(ss, blat);
-            }
-        }
-        for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+        int_model(ham, blat, spins, rng, beta, sweep0, nsweeps, ncol, cptr, order, 0, obs);
     } else {
         return -1;
     }
     return 0;
 }
 
-// Initial state by the reference's own initstatespace rule, one INIT
-// substream per site: Ising::initstatespace (src/hamiltonian/Ising.h:99-107)
-// for kind 1, Potts<3>::initstatespace (src/hamiltonian/Potts.h:149-156) for 3.
+// Initial state by the reference's own rules, one INIT substream per site:
+// Ising::initstatespace (src/hamiltonian/Ising.h:99-107) for kind 1,
+// Potts<3>::initstatespace (src/hamiltonian/Potts.h:149-156) for 3, and for
+// 4 (BlumeCapel, which has no initstatespace) Core::init_hot's
+// set_to_rnddir of a one-component integer state (src/libmarqov/core.h:773-782).
 int ref_init_int(int kind, int n, uint64_t seed, uint32_t replica, int8_t* out)
 {
     RNGCache<PhiloxSite> rng;
@@ -292,6 +421,7 @@ int ref_init_int(int kind, int n, uint64_t seed, uint32_t replica, int8_t* out)
         MARQOV::Space<std::array<int, 1>, FixedDimRegularHypercubic<1>> ss(1);
         if (kind == 1) Ising<int>(-1.0).initstatespace(ss, one, rng);
         else if (kind == 3) Potts<3>(-1.0).initstatespace(ss, one, rng);
+        else if (kind == 4) set_to_rnddir(rng, ss[0]);
         else return -1;
         out[i] = (int8_t)ss[0][0];
     }
@@ -301,48 +431,41 @@ int ref_init_int(int kind, int n, uint64_t seed, uint32_t replica, int8_t* out)
 // Metropolis sweeps for float-state models. kind: 6 Heisenberg<float> with
 // the reference's fresh-direction proposal, 7 Heisenberg small-cap (cap =
 // cos of the cap half-angle), 8 scalar phi^4 (p0 = lambda, p1 = mass,
-// cap = shift amplitude).
-int ref_sweeps_f32(int kind, int n, const int32_t* rp, const int32_t* ci, int ncol,
+// cap = shift amplitude), 9 XXZAntiferro<float>(Delta = p0, H = p1),
+// 10 XXZAntiferroSingleAniso<float>(H = p1, Delta = p0, D = p2).  sub
+// (optional): per-site sublattice (SimpleBipartite's termselector).  obs
+// (optional): per sweep (e, m, e_obs) as run_sweeps.
+int ref_sweeps_f32(int kind, int n, const int32_t* rp, const int32_t* ci, const uint8_t* sub, int ncol,
                    const int32_t* cptr, const int32_t* order, float* s, double J, double p0,
-                   double p1, double cap, double beta, uint64_t seed, uint32_t replica,
+                   double p1, double p2, double cap, double beta, uint64_t seed, uint32_t replica,
                    uint32_t sweep0, int nsweeps, double* obs)
 {
     RNGCache<PhiloxSite> rng;
     rng.seed = seed;
     rng.replica = replica;
     CSRLattice lat{n, rp, ci};
-    if (kind == 6 || kind == 7) {
+    CSRTermLattice tlat;
+    tlat.n = n; tlat.rp = rp; tlat.ci = ci; tlat.sub = sub;
+    if (kind == 6) {
+        Heisenberg<float, double> ham(J);
+        f32_model(ham, lat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
+    } else if (kind == 7) {
         HeisenbergCap::cap = cap;
-        HeisenbergCap hc(J);
-        Heisenberg<float, double> hf(J);
-        MARQOV::Space<std::array<float, 3>, CSRLattice> ss(n);
-        for (int i = 0; i < n; ++i)
-            for (int c = 0; c < 3; ++c) ss[i][c] = s[3 * i + c];
-        for (int t = 0; t < nsweeps; ++t) {
-            if (kind == 6) colour_sweep(hf, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 2);
-            else colour_sweep(hc, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, 2);
-            if (obs) {
-                Magnetization mo;
-                obs[2 * t] = 0.0;
-                obs[2 * t + 1] = mo.measure(ss, lat);
-            }
-        }
-        for (int i = 0; i < n; ++i)
-            for (int c = 0; c < 3; ++c) s[3 * i + c] = ss[i][c];
+        HeisenbergCap ham(J);
+        f32_model(ham, lat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
     } else if (kind == 8) {
         Phi4Scalar::amp = cap;
         Phi4Scalar ham(beta, p0, p1);
-        MARQOV::Space<std::array<float, 1>, CSRLattice> ss(n);
-        for (int i = 0; i < n; ++i) ss[i][0] = s[i];
-        for (int t = 0; t < nsweeps; ++t) {
-            colour_sweep(ham, lat, ss, rng, beta, sweep0 + t, ncol, cptr, order, NProp<decltype(ham)>::value);
-            if (obs) {
-                Magnetization mo;
-                obs[2 * t] = 0.0;
-                obs[2 * t + 1] = mo.measure(ss, lat);
-            }
-        }
-        for (int i = 0; i < n; ++i) s[i] = ss[i][0];
+        if (sub) f32_model(ham, tlat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
+        else f32_model(ham, lat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 1, obs);
+    } else if (kind == 9) {
+        XXZAntiferro<float> ham(p0, p1);
+        if (sub) f32_model(ham, tlat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
+        else f32_model(ham, lat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
+    } else if (kind == 10) {
+        XXZAntiferroSingleAniso<float> ham(p1, p0, p2);
+        if (sub) f32_model(ham, tlat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
+        else f32_model(ham, lat, s, rng, beta, sweep0, nsweeps, ncol, cptr, order, 2, obs);
     } else {
         return -1;
     }
@@ -381,6 +504,46 @@ int ref_wolff_int(int kind, int n, const int32_t* rp, const int32_t* ci, int8_t*
         return -1;
     }
     for (int i = 0; i < n; ++i) spins[i] = (int8_t)ss[i][0];
+    return 0;
+}
+
+// Unmodified generic Wolff<H,L>::move (src/libmarqov/wolff.h:72-126) for the
+// float models on a sequential Philox substream per cluster: kind 6 with the
+// reference's Embedder<Heisenberg> (HeisenbergPlane), kind 8 with the scalar
+// Embedder<Phi4> (p0 = lambda, p1 = mass: they do not enter the clusters).
+// s: site-major float state, updated in place; sizes: the cluster sizes.
+int ref_wolff_f32(int kind, int n, const int32_t* rp, const int32_t* ci, float* s, double J, double p0, double p1,
+                  double beta, uint64_t seed, uint32_t replica, uint32_t serial0, int nclusters, int32_t* sizes)
+{
+    RNGCache<PhiloxSite> rng;
+    rng.seed = seed;
+    rng.replica = replica;
+    CSRLattice lat{n, rp, ci};
+    if (kind == 6) {
+        HeisenbergPlane ham(J);
+        MARQOV::Space<std::array<float, 3>, CSRLattice> ss(n);
+        load_state(ss, s, n);
+        MARQOV::Wolff<HeisenbergPlane, CSRLattice> w;
+        for (int c = 0; c < nclusters; ++c) {
+            rng.rekey(ST_WOLFF_SEED, 0, serial0 + c);
+            const int site = (int)rng.integer(n);
+            sizes[c] = w.move(ham, lat, ss, rng, beta, site);
+        }
+        store_state(ss, s, n);
+    } else if (kind == 8) {
+        Phi4Scalar ham(beta, p0, p1);
+        MARQOV::Space<std::array<float, 1>, CSRLattice> ss(n);
+        load_state(ss, s, n);
+        MARQOV::Wolff<Phi4Scalar, CSRLattice> w;
+        for (int c = 0; c < nclusters; ++c) {
+            rng.rekey(ST_WOLFF_SEED, 0, serial0 + c);
+            const int site = (int)rng.integer(n);
+            sizes[c] = w.move(ham, lat, ss, rng, beta, site);
+        }
+        store_state(ss, s, n);
+    } else {
+        return -1;
+    }
     return 0;
 }
 

@@ -8,7 +8,8 @@
 // run, then "farm <i> <e> <|m|>" for the last EMCS of each member of a
 // three-member Potts farm, "pt <i> <e> <|m|>" for the last EMCS of each
 // member of a four-member Ising ladder with parallel tempering and "ptacc
-// <acceptance>", and "ea <e> <|m|>" for a random-bond lattice.  With
+// <acceptance>", "ea <e> <|m|>" for a random-bond lattice, and "xxz <e>
+// <|m|>" per game-loop EMCS of an XXZ model on SimpleBipartite.  With
 // no GPU it prints "no device: <message>" and exits 0.
 #define CACHECONTAINER_H 1
 #include <cstdio>
@@ -44,8 +45,11 @@ struct Space {
 #include "hamiltonian/EdwardsAndersonIsing.h"
 #include "hamiltonian/Ising.h"
 #include "hamiltonian/Potts.h"
+#include "hamiltonian/XXZAntiferroSingleAniso.h"
 #include "lattice/regular_hypercubic.h"
 #include "lattice/regular_random_bond.h"
+#include "lattice/util/regular_lattice.h"
+#include "lattice/simple_bipartite.h"
 
 #include "marqov_b200_marqov.hpp"
 
@@ -124,6 +128,22 @@ int main()
         ea->wrmploop();
         ea->gameloop();
         std::printf("ea %.17g %.17g\n", ea->observables().back().e, ea->observables().back().m);
+
+        // XXZAntiferroSingleAniso(H, Delta, D) on SimpleBipartite: the
+        // termselector gives sublattice A the field and B the anisotropy
+        SimpleBipartite sb(6, 3);
+        Config cx("out");
+        cx.seed = 33;
+        cx.ncluster = 0;
+        cx.nmetro = 1;
+        cx.warmupsteps = 4;
+        cx.gameloopsteps = 3;
+        auto xxz = marqov_b200::makeGPUCore<SimpleBipartite, XXZAntiferroSingleAniso<double>>(
+            std::make_tuple(std::ref(sb), cx, std::make_tuple(0.8, 0.3, 1.2, 0.5)));
+        xxz->init();
+        xxz->wrmploop();
+        xxz->gameloop();
+        for (const auto& o : xxz->observables()) std::printf("xxz %.17g %.17g\n", o.e, o.m);
     } catch (const marqov_b200::Error& e) {
         if (e.status == MQV_ERR_NO_DEVICE) {
             std::printf("no device: %s\n", e.what());

@@ -17,10 +17,16 @@ Fixtures:
   <case>.npz      Metropolis runs through MARQOV::Metropolis<H,L>::move in
                   colour order on the keyed Philox stream: initial state (by
                   the reference initstatespace rule where it has one), final
-                  state, per-sweep reference observables (energy, |m|).
+                  state, per-sweep reference observables (e, |m|, e_obs): e is
+                  the energy per site the moves see (the reference's
+                  nbrhoodloop / PottsInteraction::diff plus SelfEnergy),
+                  e_obs the reference's Energy<H> observable, equal to e
+                  except for Potts (its flex energy() is a stub returning 0)
+                  and bond lattices (Energy ignores bnds()).
   wolff_*.npz     cluster-size statistics of the unmodified reference Wolff
                   updates (sequential draws), for a statistical comparison
-                  with the bond-keyed restatement.
+                  with the bond-keyed restatement; for the float models also
+                  the per-EMCS energy and |m|.
 """
 from __future__ import annotations
 
@@ -61,8 +67,14 @@ def main():
     save("mt19937_64_words", words=ref.mt_words(1024))
 
     # -- Metropolis cases through the reference templates
+    def sublattice(g):
+        """Per-site sublattice of a hypercubic graph: its parity colour."""
+        sub = np.zeros(g.n, np.uint8)
+        sub[g.order[g.colour_ptr[1]:]] = 1
+        return sub
+
     def int_case(name, kind, ref_kind, dim, L, J, D, beta, seed, replica, nsweeps, q=0, bonds=None,
-                 init_kind=None):
+                 init_kind=None, D2=0.0, bipartite=False):
         g = orc.hypercubic(dim, L, bonds)
         if init_kind is not None:
             s0 = ref.init_int(init_kind, g.n, seed, replica)
@@ -70,10 +82,12 @@ def main():
             m = O.OrcModel(kind=kind, q=q, J=J, h=D, k=J)
             s0 = orc.init_int8(m, g.n, seed, replica)
         s = s0.copy()
-        obs = ref.sweeps_int(ref_kind, g, s, J, D, beta, seed, replica, 0, nsweeps)
+        obs = ref.sweeps_int(ref_kind, g, s, J, D, beta, seed, replica, 0, nsweeps, D2=D2,
+                             sub=sublattice(g) if bipartite else None)
         arrs = dict(kind=np.int32(kind), dim=np.int32(dim), L=np.int32(L), J=np.float64(J), D=np.float64(D),
-                    q=np.int32(q), beta=np.float64(beta), seed=np.uint64(seed), replica=np.uint32(replica),
-                    nsweeps=np.int32(nsweeps), init=s0, final=s, obs=obs)
+                    D2=np.float64(D2), bipartite=np.int32(bipartite), q=np.int32(q), beta=np.float64(beta),
+                    seed=np.uint64(seed), replica=np.uint32(replica), nsweeps=np.int32(nsweeps), init=s0, final=s,
+                    obs=obs)
         if bonds is not None:
             arrs["bonds"] = bonds
         save(name, **arrs)
@@ -82,7 +96,10 @@ def main():
     int_case("ising2d_L64", O.ISING, 1, 2, 64, -1.0, 0.0, 0.44068679, 2024, 5, 40, init_kind=1)
     int_case("ising3d_L8", O.ISING, 1, 3, 8, -1.0, 0.0, 0.2216544, 7, 1, 40, init_kind=1)
     int_case("potts2d_L16", O.POTTS, 3, 2, 16, -1.0, 0.0, 1.0050525, 11, 2, 40, q=3, init_kind=3)
-    int_case("bc2d_L16", O.BLUME_CAPEL, 4, 2, 16, -1.0, 0.5, 0.6, 13, 0, 40)
+    int_case("bc2d_L16", O.BLUME_CAPEL, 4, 2, 16, -1.0, 0.5, 0.6, 13, 0, 40, init_kind=4)
+    # BlumeCapelBipartite(J, DA, DB) on SimpleBipartite: DA on sublattice A, DB on B
+    int_case("bcbip2d_L16", O.BLUME_CAPEL, 11, 2, 16, -1.0, 0.7, 0.6, 19, 1, 40, init_kind=4, D2=-0.4,
+             bipartite=True)
     # Edwards-Anderson +-J on 3D L=8 with symmetric bimodal bonds
     L = 8
     g = orc.hypercubic(3, L)
@@ -97,20 +114,26 @@ def main():
     int_case("ea3d_L8", O.EA, 5, 3, L, -1.0, 0.0, 0.9, 17, 3, 40, bonds=bonds.reshape(-1))
 
     # -- float cases
-    def f32_case(name, ref_kind, dim, L, J, p0, p1, cap, beta, seed, nsweeps, symd):
+    def f32_case(name, ref_kind, dim, L, J, p0, p1, cap, beta, seed, nsweeps, symd, p2=0.0, bipartite=False):
         g = orc.hypercubic(dim, L)
         kind = O.PHI4 if symd == 1 else O.HEISENBERG
         m = O.OrcModel(kind=kind, J=J)
         s0 = orc.init_f32(m, g.n, symd, seed, 0)
         s = s0.copy()
-        obs = ref.sweeps_f32(ref_kind, g, s, J, p0, p1, cap, beta, seed, 0, 0, nsweeps)
+        obs = ref.sweeps_f32(ref_kind, g, s, J, p0, p1, cap, beta, seed, 0, 0, nsweeps, p2=p2,
+                             sub=sublattice(g) if bipartite else None)
         save(name, dim=np.int32(dim), L=np.int32(L), J=np.float64(J), p0=np.float64(p0), p1=np.float64(p1),
-             cap=np.float64(cap), beta=np.float64(beta), seed=np.uint64(seed), nsweeps=np.int32(nsweeps),
-             symd=np.int32(symd), ref_kind=np.int32(ref_kind), init=s0, final=s, obs=obs)
+             p2=np.float64(p2), bipartite=np.int32(bipartite), cap=np.float64(cap), beta=np.float64(beta),
+             seed=np.uint64(seed), nsweeps=np.int32(nsweeps), symd=np.int32(symd), ref_kind=np.int32(ref_kind),
+             init=s0, final=s, obs=obs)
 
     f32_case("heis3d_L8_fresh", 6, 3, 8, -1.0, 0, 0, 0.0, 0.6930, 21, 10, 3)
     f32_case("heis3d_L8_cap", 7, 3, 8, -1.0, 0, 0, 0.6, 0.6930, 22, 10, 3)
     f32_case("phi4_3d_L8", 8, 3, 8, -1.0, 1.1, 1.0, 0.5, 0.37, 23, 10, 1)
+    # XXZAntiferro(Delta = 0.6, H = 0.35): J = +1, interaction (Delta x, Delta y, z), field on z
+    f32_case("xxz3d_L8", 9, 3, 8, 1.0, 0.6, 0.35, 0.0, 0.7, 31, 10, 3)
+    # XXZAntiferroSingleAniso(H = 0.25, Delta = 1.4, D = 0.5) on SimpleBipartite
+    f32_case("xxzsa3d_L8_bip", 10, 3, 8, 1.0, 1.4, 0.25, 0.0, 0.9, 32, 10, 3, p2=0.5, bipartite=True)
 
     # -- Wolff statistics: unmodified reference clusters on Ising L=16 and Potts L=16
     for name, kind, okind, beta, q in (("wolff_ising_L16", 1, O.ISING, 0.44068679, 0),
@@ -126,6 +149,27 @@ def main():
             orc.sweep_int8(m, g, s, beta, 99, 0, 1000 + t)
         sizes = np.array(sizes, np.int32)
         save(name, beta=np.float64(beta), q=np.int32(q), sizes=sizes)
+
+    # -- Wolff statistics of the float models: the reference's generic Wolff
+    # with Embedder<Heisenberg> / the scalar Embedder<Phi4>, one cluster then
+    # one colour-order Metropolis sweep per EMCS on a 3D L = 8 lattice
+    for name, rkind, okind, symd, beta, p0, p1, amp in (
+            ("wolff_heis_L8", 6, O.HEISENBERG, 3, 0.6930, 0.0, 0.0, 0.0),
+            ("wolff_phi4_L8", 8, O.PHI4, 1, 0.37, 1.1, 1.0, 0.5)):
+        g = orc.hypercubic(3, 8)
+        m = O.OrcModel(kind=okind, J=-1.0, h=p1 / beta, h2=p0 / beta, cap=amp)
+        s = orc.init_f32(m, g.n, symd, 77, 0)
+        for t in range(200):
+            orc.sweep_f32(m, g, s, symd, beta, 77, 0, t)
+        sizes, energies, mags = [], [], []
+        for t in range(6000):
+            sizes.append(int(ref.wolff_f32(rkind, g, s, -1.0, p0, p1, beta, 77, 0, t, 1)[0]))
+            orc.sweep_f32(m, g, s, symd, beta, 77, 0, 1000 + t)
+            e, mm, _, _ = orc.measure_f32(m, g, s, symd)
+            energies.append(e)
+            mags.append(mm)
+        save(name, beta=np.float64(beta), p0=np.float64(p0), p1=np.float64(p1), amp=np.float64(amp),
+             sizes=np.array(sizes, np.int32), e=np.array(energies), m=np.array(mags))
 
 
 if __name__ == "__main__":

@@ -71,3 +71,11 @@ def test_dropin_equals_python_api():
     for i in range(4):
         assert pt[i] == (po[-1, i, 0], po[-1, i, 1])
     assert ptacc == [float((acc == 1).sum()) / 6.0]
+    # XXZAntiferroSingleAniso(H=0.3, Delta=1.2, D=0.5) on SimpleBipartite(6, 3) at beta 0.8
+    xxz = np.array([[float(a), float(b)] for t, a, b in (l for l in lines if l[0] == "xxz")])
+    cfg = M.Config(seed=33, repid=0, ncluster=0, nmetro=1)
+    with M.makeCore(M.SimpleBipartite(6, 3), cfg, M.XXZAntiferroSingleAniso(0.3, 1.2, 0.5), 0.8) as c:
+        c.init()
+        c.emcs(4, ncluster=0, nmetro=1, measure=False)
+        xo, _ = c.emcs(3, ncluster=0, nmetro=1)
+    np.testing.assert_array_equal(xxz, xo[:, :2])

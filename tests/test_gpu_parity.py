@@ -11,8 +11,10 @@ from oracle import oracle as O
 
 pytestmark = pytest.mark.gpu
 
-INT_CASES = ["ising2d_L16", "ising2d_L64", "ising3d_L8", "potts2d_L16", "bc2d_L16", "ea3d_L8"]
-F32_CASES = ["heis3d_L8_fresh", "heis3d_L8_cap", "phi4_3d_L8"]
+INT_CASES = ["ising2d_L16", "ising2d_L64", "ising3d_L8", "potts2d_L16", "bc2d_L16", "bcbip2d_L16", "ea3d_L8"]
+F32_CASES = ["heis3d_L8_fresh", "heis3d_L8_cap", "phi4_3d_L8", "xxz3d_L8", "xxzsa3d_L8_bip"]
+# float models: per-sweep energy and |m| within this relative tolerance of the reference
+F32_RTOL = 1e-5
 
 
 def mb():
@@ -27,6 +29,8 @@ def ham_of(g):
         return M.Ising(float(g["J"]))
     if kind == O.POTTS:
         return M.Potts(int(g["q"]), float(g["J"]))
+    if kind == O.BLUME_CAPEL and int(g.get("bipartite", 0)):
+        return M.BlumeCapelBipartite(float(g["J"]), float(g["D"]), float(g["D2"]))
     if kind == O.BLUME_CAPEL:
         return M.BlumeCapel(float(g["J"]), float(g["D"]))
     if kind == O.EA:
@@ -40,6 +44,8 @@ def lattice_of(g):
     if "bonds" in g:
         base = M.RegularHypercubic(L, dim).to_csr()
         return M.CSRLattice(base.row_ptr, base.col_idx, g["bonds"], base.colours)
+    if int(g.get("bipartite", 0)):
+        return M.SimpleBipartite(L, dim)
     return M.RegularHypercubic(L, dim)
 
 
@@ -51,37 +57,51 @@ def core_for(lat, ham, beta, seed, replica=0, per_colour=False):
 
 @pytest.mark.parametrize("case", INT_CASES)
 def test_int_golden_bit_exact(golden, case):
+    """Initial state (the reference's init rule), final state and every
+    per-sweep energy and |m| equal the reference's, bit for bit."""
     g = golden(case)
     with core_for(lattice_of(g), ham_of(g), g["beta"], g["seed"], g["replica"]) as c:
-        if case.startswith(("ising", "potts")):
+        if "bonds" not in g:
             c.init()
             assert (c.state == g["init"]).all(), "initstatespace rule"
         c.state = g["init"]
         obs, _ = c.emcs(int(g["nsweeps"]), ncluster=0, nmetro=1)
         assert (obs[:, 1] == g["obs"][:, 1]).all()
-        if case.startswith("ising"):
-            assert (obs[:, 0] == g["obs"][:, 0]).all()
+        assert (obs[:, 0] == g["obs"][:, 0]).all()
         assert (c.state == g["final"]).all()
         assert c.launches > 0
 
 
+def f32_ham_of(g):
+    M = mb()
+    rk, beta = int(g["ref_kind"]), float(g["beta"])
+    if rk == 8:
+        return M.Phi4(beta, float(g["p0"]), float(g["p1"]), amp=float(g["cap"]))
+    if rk == 9:
+        return M.XXZAntiferro(float(g["p0"]), float(g["p1"]))
+    if rk == 10:
+        return M.XXZAntiferroSingleAniso(float(g["p1"]), float(g["p0"]), float(g["p2"]))
+    return M.Heisenberg(-1.0, proposal="smallcap" if rk == 7 else "fresh", cap=float(g["cap"]))
+
+
+def rel_close(a, b, rtol=F32_RTOL, floor=1e-3):
+    a, b = np.asarray(a, float), np.asarray(b, float)
+    return (np.abs(a - b) <= rtol * np.maximum(np.abs(b), floor)).all()
+
+
 @pytest.mark.parametrize("case", F32_CASES)
 def test_f32_golden_tolerance(golden, case):
-    M = mb()
+    """Float models against the reference: per-sweep energy and |m| within
+    F32_RTOL relative, final state within 1e-5."""
     g = golden(case)
-    rk = int(g["ref_kind"])
     beta = float(g["beta"])
-    if rk == 8:
-        ham = M.Phi4(beta, float(g["p0"]), float(g["p1"]), amp=float(g["cap"]))
-    else:
-        ham = M.Heisenberg(-1.0, proposal="smallcap" if rk == 7 else "fresh", cap=float(g["cap"]))
-    with core_for(M.RegularHypercubic(int(g["L"]), int(g["dim"])), ham, beta, g["seed"]) as c:
+    with core_for(lattice_of(g), f32_ham_of(g), beta, g["seed"]) as c:
         c.init()
         assert np.allclose(c.state, g["init"], rtol=0, atol=1e-6)
         c.state = g["init"]
         obs, _ = c.emcs(int(g["nsweeps"]), ncluster=0, nmetro=1)
-        ref = g["obs"][:, 1]
-        assert (np.abs(obs[:, 1] - ref) <= 1e-5 * np.maximum(np.abs(ref), 1e-3)).all()
+        assert rel_close(obs[:, 1], g["obs"][:, 1])
+        assert rel_close(obs[:, 0], g["obs"][:, 0])
         assert np.allclose(c.state, g["final"], rtol=0, atol=1e-5)
 
 
@@ -182,6 +202,30 @@ def test_wolff_emcs_bit_exact(orc, name, L, beta):
     assert (obs[:, 0] == oobs[:, 0]).all()
     assert (final == s).all()
     assert sizes.max() > 1
+
+
+def test_config1_eleven_thousand_emcs_bit_exact(orc):
+    """The parity configuration over its whole run: 2D Ising L = 64 at beta_c,
+    EMCS = one Wolff cluster + one checkerboard sweep, 10^3 thermalisation +
+    10^4 measured EMCS from the reference's initial-state rule -- every
+    cluster size, every per-EMCS energy and |m|, and the final state equal
+    the oracle's, bit for bit."""
+    M = mb()
+    L, beta, seed, replica, nsteps = 64, 0.44068679, 2024, 5, 11000
+    cfg = M.Config(seed=seed, repid=replica, ncluster=1, nmetro=1)
+    with M.makeCore(M.RegularHypercubic(L, 2), cfg, M.Ising(-1.0), beta) as c:
+        c.init()
+        s0 = c.state
+        obs, mc = c.emcs(nsteps)
+        final = c.state
+    g = orc.hypercubic(2, L)
+    m = O.OrcModel(kind=O.ISING, J=-1.0)
+    assert (orc.init_int8(m, g.n, seed, replica) == s0).all()
+    s = s0.copy()
+    sizes, oobs = run_oracle_emcs(orc, m, g, s, beta, seed, replica, nsteps, 1, 1)
+    assert (mc == sizes).all()
+    assert (obs[:, 0] == oobs[:, 0]).all() and (obs[:, 1] == oobs[:, 1]).all()
+    assert (final == s).all()
 
 
 @pytest.mark.parametrize("model", ["heisenberg", "phi4"])

@@ -9,13 +9,33 @@ import pytest
 
 from oracle import oracle as O
 
-INT_CASES = ["ising2d_L16", "ising2d_L64", "ising3d_L8", "potts2d_L16", "bc2d_L16", "ea3d_L8"]
-F32_CASES = ["heis3d_L8_fresh", "heis3d_L8_cap", "phi4_3d_L8"]
+INT_CASES = ["ising2d_L16", "ising2d_L64", "ising3d_L8", "potts2d_L16", "bc2d_L16", "bcbip2d_L16", "ea3d_L8"]
+F32_CASES = ["heis3d_L8_fresh", "heis3d_L8_cap", "phi4_3d_L8", "xxz3d_L8", "xxzsa3d_L8_bip"]
+# float cases: per-sweep e and |m| within this relative tolerance of the reference
+F32_RTOL = 1e-5
 
 
 def model_of(g):
     kind = int(g["kind"])
-    return O.OrcModel(kind=kind, q=int(g["q"]), J=float(g["J"]), h=float(g["D"]), k=float(g["J"]))
+    return O.OrcModel(kind=kind, q=int(g["q"]), J=float(g["J"]), h=float(g["D"]), h2=float(g.get("D2", 0.0)),
+                      k=float(g["J"]), termsel=int(g.get("bipartite", 0)))
+
+
+def f32_model_of(g):
+    """The oracle model of a float fixture (ref_kind as in ref_harness.cpp)."""
+    rk, beta = int(g["ref_kind"]), float(g["beta"])
+    ts = int(g.get("bipartite", 0))
+    if rk == 8:
+        return O.OrcModel(kind=O.PHI4, J=-1.0, h=float(g["p1"]) / beta, h2=float(g["p0"]) / beta,
+                          cap=float(g["cap"]), termsel=ts)
+    if rk in (9, 10):
+        return O.OrcModel(kind=O.XXZ, J=float(g["J"]), delta=float(g["p0"]), h=float(g["p1"]),
+                          h2=float(g["p2"]) if rk == 10 else 0.0, termsel=ts)
+    return O.OrcModel(kind=O.HEISENBERG, J=-1.0, proposal=1 if rk == 7 else 0, cap=float(g["cap"]))
+
+
+def close(a, b, rtol=F32_RTOL, floor=1e-3):
+    return abs(a - b) <= rtol * max(abs(b), floor)
 
 
 def test_philox_matches_curand_fixture(orc, golden):
@@ -65,39 +85,74 @@ def test_acceptance_edge_cases(orc):
 
 @pytest.mark.parametrize("case", INT_CASES)
 def test_int_case_bit_exact(orc, golden, case):
+    """Initial state, final state and every per-sweep energy and |m| equal the
+    reference's, bit for bit.  The energy is the one the reference's moves see
+    (column 0); it equals the reference's Energy observable (column 2) except
+    where that observable is a stub (Potts) or ignores bnds() (bond lattices)."""
     g = golden(case)
     dim, L = int(g["dim"]), int(g["L"])
     graph = orc.hypercubic(dim, L, g.get("bonds"))
     m = model_of(g)
-    if case.startswith(("ising", "potts")):
+    if "bonds" not in g:
         assert (orc.init_int8(m, graph.n, int(g["seed"]), int(g["replica"])) == g["init"]).all()
     s = g["init"].copy()
     for t in range(int(g["nsweeps"])):
         orc.sweep_int8(m, graph, s, float(g["beta"]), int(g["seed"]), int(g["replica"]), t)
         e, mm, _, _ = orc.measure_int8(m, graph, s)
         assert mm == g["obs"][t, 1]
-        if case.startswith("ising"):
-            assert e == g["obs"][t, 0]
+        assert e == g["obs"][t, 0]
+        if not (case.startswith("potts") or "bonds" in g):
+            assert g["obs"][t, 0] == g["obs"][t, 2]
     assert (s == g["final"]).all()
+
+
+def test_potts_and_bond_energies_differ_from_the_stub_observable(golden):
+    """The reference's Energy<Potts<3>> reads 0 (PottsInteraction::energy is a
+    stub) and Energy<Ising> on a bond lattice ignores the bonds; the fixtures
+    keep both readings, and the parity energy is the one the moves see."""
+    assert (golden("potts2d_L16")["obs"][:, 2] == 0).all()
+    g = golden("ea3d_L8")
+    assert (g["obs"][:, 0] != g["obs"][:, 2]).any()
 
 
 @pytest.mark.parametrize("case", F32_CASES)
 def test_f32_case_tolerance(orc, golden, case):
+    """Float models: per-sweep energy and |m| within F32_RTOL of the
+    reference's, final state within 1e-5."""
     g = golden(case)
     dim, L, symd = int(g["dim"]), int(g["L"]), int(g["symd"])
     graph = orc.hypercubic(dim, L)
-    rk = int(g["ref_kind"])
     beta = float(g["beta"])
-    if rk == 8:
-        m = O.OrcModel(kind=O.PHI4, J=-1.0, h=float(g["p1"]) / beta, h2=float(g["p0"]) / beta, cap=float(g["cap"]))
-    else:
-        m = O.OrcModel(kind=O.HEISENBERG, J=-1.0, proposal=1 if rk == 7 else 0, cap=float(g["cap"]))
+    m = f32_model_of(g)
     s = g["init"].copy()
     for t in range(int(g["nsweeps"])):
         orc.sweep_f32(m, graph, s, symd, beta, int(g["seed"]), 0, t)
-        _, mm, _, _ = orc.measure_f32(m, graph, s, symd)
-        assert abs(mm - g["obs"][t, 1]) <= 1e-5 * max(abs(g["obs"][t, 1]), 1e-3)
+        e, mm, _, _ = orc.measure_f32(m, graph, s, symd)
+        assert close(mm, g["obs"][t, 1]), (t, mm, g["obs"][t, 1])
+        assert close(e, g["obs"][t, 0]), (t, e, g["obs"][t, 0])
+        assert close(e, g["obs"][t, 2]), (t, e, g["obs"][t, 2])
     assert np.allclose(s, g["final"], rtol=0, atol=1e-5)
+
+
+def test_xxz_weights_delta_on_x_and_y(orc, golden):
+    """The restatement must fail the XXZ fixture if Delta weights z instead."""
+    g = golden("xxz3d_L8")
+    graph = orc.hypercubic(3, 8)
+    m = f32_model_of(g)
+    s = g["init"].copy()
+    orc.sweep_f32(m, graph, s, 3, float(g["beta"]), int(g["seed"]), 0, 0)
+    e_x, _, _, _ = orc.measure_f32(m, graph, s, 3)
+    assert close(e_x, g["obs"][0, 0])
+    # the same energy function with the anisotropy moved onto z misses
+    s3 = s.reshape(-1, 3)
+    d = float(g["p0"])
+    rp, ci = graph.row_ptr, graph.col_idx
+    wrong = 0.0
+    for i in range(graph.n):
+        nb = s3[ci[rp[i]:rp[i + 1]]].sum(axis=0, dtype=np.float64)
+        wrong += s3[i, 0] * nb[0] + s3[i, 1] * nb[1] + d * d * s3[i, 2] * nb[2]
+    wrong = wrong / (2 * graph.n) + float(g["p1"]) * s3[:, 2].astype(np.float64).sum() / graph.n
+    assert not close(wrong, g["obs"][0, 0])
 
 
 def _batch_err(x, nb=20):
@@ -123,6 +178,32 @@ def test_wolff_restatement_statistics(orc, golden, case, kind, q):
     a, b = np.asarray(sizes, float), g["sizes"].astype(float)
     err = np.hypot(_batch_err(a), _batch_err(b))
     assert abs(a.mean() - b.mean()) < 4 * err, (a.mean(), b.mean(), err)
+
+
+@pytest.mark.parametrize("case,kind,symd", [("wolff_heis_L8", O.HEISENBERG, 3), ("wolff_phi4_L8", O.PHI4, 1)])
+def test_wolff_f32_restatement_statistics(orc, golden, case, kind, symd):
+    """The bond-keyed float clusters (orc_wolff_f32: Embedder<Heisenberg> /
+    scalar Embedder<Phi4>) against the reference's generic Wolff driven by
+    those embedders with sequential draws: mean cluster size, <e> and <|m|>
+    within 3 sigma (batch-means errors), same Metropolis in between."""
+    g = golden(case)
+    beta, p0, p1, amp = float(g["beta"]), float(g["p0"]), float(g["p1"]), float(g["amp"])
+    graph = orc.hypercubic(3, 8)
+    m = O.OrcModel(kind=kind, J=-1.0, h=p1 / beta, h2=p0 / beta, cap=amp)
+    s = orc.init_f32(m, graph.n, symd, 77, 0)
+    for t in range(200):
+        orc.sweep_f32(m, graph, s, symd, beta, 77, 0, t)
+    sizes, es, ms = [], [], []
+    for t in range(len(g["sizes"])):
+        sizes.append(orc.wolff_f32(m, graph, s, symd, beta, 5, 0, t))
+        orc.sweep_f32(m, graph, s, symd, beta, 5, 0, 1000 + t)
+        e, mm, _, _ = orc.measure_f32(m, graph, s, symd)
+        es.append(e)
+        ms.append(mm)
+    for mine, theirs in ((sizes, g["sizes"]), (es, g["e"]), (ms, g["m"])):
+        a, b = np.asarray(mine, float), np.asarray(theirs, float)
+        err = np.hypot(_batch_err(a), _batch_err(b))
+        assert abs(a.mean() - b.mean()) < 3 * err, (case, a.mean(), b.mean(), err)
 
 
 def test_ref_harness_live_matches_oracle(orc):
