@@ -111,7 +111,9 @@ typedef struct mqv_lattice_desc {
     int32_t n;                 /* CSR: number of sites */
     const int32_t* row_ptr;    /* CSR: n+1 offsets (host memory, copied) */
     const int32_t* col_idx;    /* CSR: neighbour ids in nbrs(0,i) order (host, copied) */
-    const int8_t* bonds;       /* optional per-entry bond weights (bnds), symmetric */
+    const int8_t* bonds;       /* optional bond weights (bnds), symmetric: CSR, one per col_idx entry;
+                                  hypercubic, 2 dim per site in the nbrs(0,i) order +x,-x,+y,-y,...
+                                  (RegularRandomBond), kept on the stencil path */
     const int32_t* colours;    /* optional proper colouring; NULL = greedy colouring */
 } mqv_lattice_desc;
 
@@ -159,9 +161,11 @@ MQV_API mqv_status mqv_init_state(mqv_sim* sim);
 MQV_API mqv_status mqv_get_state(mqv_sim* sim, void* host, size_t bytes);
 MQV_API mqv_status mqv_set_state(mqv_sim* sim, const void* host, size_t bytes);
 /* Device pointer of the current state (valid until the next engine call).
- * Layout: the reference site order, except on the fused 2D Ising path, whose
- * rows hold the even-x sites, then the odd-x sites, with the 32 bytes of each
- * 32-site group transposed (site s of a group at byte 4 (s & 7) + (s >> 3));
+ * Layout: the reference site order, except (a) on the fused 2D Ising path,
+ * whose rows hold the even-x sites, then the odd-x sites, with the 32 bytes
+ * of each 32-site group transposed (site s of a group at byte 4 (s & 7) +
+ * (s >> 3)), and (b) for 3-vector models (Heisenberg, XXZ), stored as one
+ * float array per component (component c of site i at [c n + i]);
  * mqv_get_state / mqv_set_state convert. */
 MQV_API mqv_status mqv_state_device_ptr(mqv_sim* sim, void** dev, size_t* bytes);
 MQV_API mqv_status mqv_state_bytes(mqv_sim* sim, size_t* bytes);

@@ -10,13 +10,13 @@ from ._lib import MarqovError
 from .core import Batch, Config, Core, makeCore, tune_small_cap
 from .hamiltonians import (BlumeCapel, BlumeCapelBipartite, EdwardsAndersonIsing, Hamiltonian, Heisenberg, Ising,
                            Phi4, Potts, XXZAntiferro, XXZAntiferroSingleAniso)
-from .lattices import (CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
+from .lattices import (BondedHypercubic, CSRLattice, FixedDimRegularHypercubic, RandomGeometricGraph2D, RegularHypercubic,
                        RegularRandomBond, SimpleBipartite, read_graph_csv, save_geometry)
 
 _lib.load()
 
 __all__ = ["tempering", "Batch", "Config", "Core", "makeCore", "tune_small_cap", "MarqovError", "Hamiltonian", "Ising", "EdwardsAndersonIsing",
            "Potts", "BlumeCapel", "BlumeCapelBipartite", "Heisenberg", "XXZAntiferro", "XXZAntiferroSingleAniso",
-           "Phi4", "CSRLattice", "FixedDimRegularHypercubic", "RegularHypercubic", "SimpleBipartite",
+           "Phi4", "CSRLattice", "BondedHypercubic", "FixedDimRegularHypercubic", "RegularHypercubic", "SimpleBipartite",
            "RegularRandomBond", "RandomGeometricGraph2D",
            "read_graph_csv", "save_geometry"]

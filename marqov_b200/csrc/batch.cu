@@ -30,32 +30,53 @@ namespace mqv {
 
 template <bool F32, class Lat>
 __device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, int64_t i, uint32_t sweep, bool live,
-                                           int sub)
+                                           int sub, const uint4* tab, uint32_t run0)
 {
-    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica, live, sub);
-    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live, sub);
+    if (F32) f32_site(R.md, lat, (float*)R.s, i, R.key, sweep, R.replica, live, sub, tab, run0);
+    else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live, sub, tab, run0);
 }
 
-// Lanes past the end of the colour's work take no part (live == false).
+// One colour of a sweep over every member.  Each warp takes one block of
+// kAccSites consecutive positions of one member's colour-c sites (member
+// counts are padded to whole blocks, positions past a member's count are
+// idle lanes): on hypercubic members the block's sites fill kAccRuns
+// aligned 64-site runs, whose acceptance bytes the warp draws once
+// (accept_tab_fill); CSR members draw per site.
 template <bool F32>
-__global__ void batch_metro(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
-                            const int32_t* __restrict__ block_rep, const int32_t* __restrict__ cbegin, int ncol,
-                            int64_t total, int colour, const BatchCtr* __restrict__ ctr, int nmetro, int j)
+__global__ void __launch_bounds__(kBatchMetroThreads)
+    batch_metro(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                const int32_t* __restrict__ block_rep, const int32_t* __restrict__ cbegin,
+                const int32_t* __restrict__ ccount, int ncol, int64_t total, int colour,
+                const BatchCtr* __restrict__ ctr, int nmetro, int j)
 {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    const bool live = g < total;
+    __shared__ uint4 tabs[kBatchMetroThreads / 32][kAccTab];
+    uint4* tab = tabs[threadIdx.x >> 5];
+    const int64_t g0 = ((int64_t)blockIdx.x * (kBatchMetroThreads / 32) + (threadIdx.x >> 5)) * kAccSites;
+    if (g0 >= total) return;  // whole warps
     int r = block_rep[blockIdx.x];
-    if (live)
-        while (g >= prefix[r + 1]) ++r;
+    while (g0 >= prefix[r + 1]) ++r;
     const BatchRep& R = reps[r];
-    const int64_t t = live ? g - prefix[r] : 0;
+    const int64_t t0 = g0 - prefix[r];
+    const int64_t cnt = ccount[(size_t)r * ncol + colour];
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
-    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-        batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep, live,
-                        colour);
-    else
-        batch_site<F32>(R, R.csr, live ? (int64_t)R.order[cbegin[(size_t)r * ncol + colour] + t] : 0, sweep, live,
-                        0);
+    const unsigned lane = threadIdx.x & 31u;
+    if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
+        const uint32_t run0 = (uint32_t)(t0 / 32);  // sites [2 t0, 2 t0 + 2 kAccSites)
+        accept_tab_fill(tab, run0, R.key, sweep, R.replica);
+        for (int k = 0; k < kAccRuns; ++k) {
+            const int64_t t = t0 + k * 32 + lane;
+            const bool live = t < cnt;
+            batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep,
+                            live, colour, tab, run0);
+        }
+    } else {
+        const int32_t* ord = R.order + cbegin[(size_t)r * ncol + colour];
+        for (int k = 0; k < kAccRuns; ++k) {
+            const int64_t t = t0 + k * 32 + lane;
+            const bool live = t < cnt;
+            batch_site<F32>(R, R.csr, live ? (int64_t)ord[t] : 0, sweep, live, 0, nullptr, 0u);
+        }
+    }
 }
 
 template <bool F32>
@@ -235,8 +256,8 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
         for (int colour = 0; colour < b.ncol; ++colour) {
             if (b.total[colour] == 0) continue;
             batch_metro<F32><<<b.blocks[colour], kBatchMetroThreads, 0, st>>>(
-                b.reps, b.prefix + (size_t)colour * (b.nrep + 1), b.block_rep + b.block_off[colour], b.cbegin, b.ncol,
-                b.total[colour], colour, b.ctr, nmetro, j);
+                b.reps, b.prefix + (size_t)colour * (b.nrep + 1), b.block_rep + b.block_off[colour], b.cbegin,
+                b.ccount, b.ncol, b.total[colour], colour, b.ctr, nmetro, j);
         }
     batch_measure<F32><<<b.meas_blocks, 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep, b.meas_prefix, b.meas_rep);
     batch_tick<<<1, 1, 0, st>>>(b.ctr);

@@ -22,6 +22,12 @@ struct BatchRep {
     int D;                           // int8: its maximum degree
 };
 
+// Sites of a member's lattice.
+__host__ __device__ __forceinline__ int64_t rep_sites(const BatchRep& R)
+{
+    return R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.n : R.csr.n;
+}
+
 // Device counters of a run: EMCS done, first EMCS of the current chunk
 // (measurement slot = e - ebase).
 struct BatchCtr {
@@ -32,9 +38,11 @@ struct BatchCtr {
 constexpr int kBatchMetroThreads = 256;
 
 // Device tables and shapes the launchers need.  Colour c's work is the
-// concatenation over members of their colour-c sites: prefix + c * (nrep + 1)
-// holds its prefix sums, block_rep + block_off[c] the first member of each of
-// its blocks, cbegin[r * ncol + c] member r's offset into its colour order.
+// concatenation over members of their colour-c sites, each member's count
+// ccount[r * ncol + c] padded to whole warp blocks of kAccSites sites:
+// prefix + c * (nrep + 1) holds the padded prefix sums, block_rep +
+// block_off[c] the first member of each CTA's first warp block,
+// cbegin[r * ncol + c] member r's offset into its colour order.
 struct BatchLaunch {
     const BatchRep* reps;
     int nrep;
@@ -43,9 +51,10 @@ struct BatchLaunch {
     const int64_t* prefix;       // [ncol][nrep + 1]
     const int32_t* block_rep;    // [sum of blocks]
     const int32_t* cbegin;       // [nrep][ncol]
+    const int32_t* ccount;       // [nrep][ncol] sites of each colour
     const int* block_off;        // host: [ncol] offsets into block_rep
     const int* blocks;           // host: [ncol] blocks of each colour
-    const int64_t* total;        // host: [ncol] work items of each colour
+    const int64_t* total;        // host: [ncol] padded work items of each colour
     // measurement: member r's sites are split over meas_prefix[r + 1] -
     // meas_prefix[r] CTAs (about 4096 sites each); meas_rep[c] is CTA c's member
     const int32_t* meas_prefix;  // [nrep + 1]

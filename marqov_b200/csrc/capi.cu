@@ -266,6 +266,38 @@ static mqv_status lower_csr(Sim* s, const mqv_lattice_desc* L)
     return MQV_OK;
 }
 
+static uint64_t fnv1a(const void* p, size_t bytes, uint64_t h = 1469598103934665603ull)
+{
+    const unsigned char* c = (const unsigned char*)p;
+    for (size_t k = 0; k < bytes; ++k) h = (h ^ c[k]) * 1099511628211ull;
+    return h;
+}
+
+// Bonds of a hypercubic lattice, given per neighbour entry in nbrs(0, i)
+// order (+x, -x, +y, -y, ...; RegularRandomBond::bnds,
+// src/lattice/regular_random_bond.h:58-67): checked symmetric and stored as
+// one plane of +d bonds per dimension (StencilDev::fb), 1 byte per site and
+// dimension.
+static mqv_status lower_stencil_bonds(Sim* s, const int8_t* bonds)
+{
+    const int64_t n = s->n;
+    const int dim = s->dim, deg = 2 * dim;
+    std::vector<int8_t> fb((size_t)dim * (size_t)n);
+    for (int64_t i = 0; i < n; ++i)
+        for (int d = 0; d < dim; ++d) {
+            const int8_t w = bonds[(size_t)i * deg + 2 * d];
+            const int64_t j = s->sten.nbr(i, 2 * d);
+            if (bonds[(size_t)j * deg + 2 * d + 1] != w)
+                return fail(MQV_ERR_BAD_DESCRIPTOR, "hypercubic bonds are not symmetric at site " + std::to_string(i));
+            fb[(size_t)d * n + i] = w;
+        }
+    MQV_CK(cudaMalloc(&s->d_bonds, fb.size()));
+    MQV_CK(cudaMemcpy(s->d_bonds, fb.data(), fb.size(), cudaMemcpyHostToDevice));
+    s->sten.fb = s->d_bonds;
+    s->lat_hash = fnv1a(fb.data(), fb.size());
+    return MQV_OK;
+}
+
 static mqv_status lower_model(Sim* s, const mqv_model_desc* m, bool has_bonds)
 {
     if (m->kind < MQV_MODEL_ISING || m->kind > MQV_MODEL_XXZ)
@@ -405,7 +437,6 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         if (lattice->len < 4 || (lattice->len & 1))
             return bail(fail(MQV_ERR_BAD_DESCRIPTOR,
                              "hypercubic checkerboard needs an even side >= 4 (use a CSR lattice otherwise)"));
-        if (lattice->bonds) return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "bonds need a CSR lattice"));
         int64_t n = 1;
         for (int j = 0; j < lattice->dim; ++j) {
             s->sten.pows[j] = n;
@@ -425,6 +456,10 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         s->sten.mlen = s->sten.lg >= 0 ? 0 : UINT64_MAX / (uint64_t)lattice->len + 1;
         s->max_degree = 2 * lattice->dim;
         s->colour_ptr = {0, (int32_t)(n / 2), (int32_t)n};
+        if (lattice->bonds) {
+            st = lower_stencil_bonds(s, lattice->bonds);
+            if (st) return bail(st);
+        }
     } else if (lattice->kind == MQV_LATTICE_CSR) {
         s->lat_kind = MQV_LATTICE_CSR;
         st = lower_csr(s, lattice);
@@ -433,6 +468,7 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
         return bail(fail(MQV_ERR_BAD_DESCRIPTOR, "unknown lattice kind"));
     }
     s->fused_ising2d = !(params->flags & MQV_FLAG_PER_COLOUR) && !s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC &&
+                       !s->d_bonds &&
                        s->dim == 2 && ising2d_supported(s->len) &&
                        (s->md.kind == MQV_MODEL_ISING || s->md.kind == MQV_MODEL_ISING_EMBED);
     s->sten.split = s->fused_ising2d ? 1 : 0;
@@ -538,6 +574,14 @@ MQV_API mqv_status mqv_get_state(mqv_sim* h, void* host, size_t bytes)
         // the other buffer is free between sweeps: merge the split rows into it
         MQV_CK(launch_merge_rows(s, s->state[s->cur], s->state[s->cur ^ 1]));
         MQV_CK(cudaMemcpyAsync(host, s->state[s->cur ^ 1], bytes, cudaMemcpyDeviceToHost, s->stream));
+    } else if (s->is_f32 && s->symd > 1) {
+        // device: one array per component; host: the reference's site-major vectors
+        std::vector<float> soa((size_t)s->n * s->symd);
+        MQV_CK(cudaMemcpyAsync(soa.data(), s->state[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
+        MQV_CK(cudaStreamSynchronize(s->stream));
+        float* out = (float*)host;
+        for (int c = 0; c < s->symd; ++c)
+            for (int64_t i = 0; i < s->n; ++i) out[(size_t)i * s->symd + c] = soa[(size_t)c * s->n + i];
     } else {
         MQV_CK(cudaMemcpyAsync(host, s->state[s->cur], bytes, cudaMemcpyDeviceToHost, s->stream));
     }
@@ -578,6 +622,16 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
         else
             for (int64_t i = 0; i < s->n; ++i) bad |= (v[i] * v[i]) != 1;
         if (bad) return fail(MQV_ERR_INVALID_ARG, "illegal spin value in the state");
+    }
+    if (s->is_f32 && s->symd > 1) {
+        std::vector<float> soa((size_t)s->n * s->symd);
+        const float* in = (const float*)host;
+        for (int c = 0; c < s->symd; ++c)
+            for (int64_t i = 0; i < s->n; ++i) soa[(size_t)c * s->n + i] = in[(size_t)i * s->symd + c];
+        MQV_CK(cudaMemcpyAsync(s->state[s->cur], soa.data(), bytes, cudaMemcpyHostToDevice, s->stream));
+        MQV_CK(cudaStreamSynchronize(s->stream));
+        s->initialised = true;
+        return MQV_OK;
     }
     MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
     MQV_CK(cudaStreamSynchronize(s->stream));
@@ -892,6 +946,7 @@ struct Batch {
     int64_t* d_prefix = nullptr;
     int32_t* d_block_rep = nullptr;
     int32_t* d_cbegin = nullptr;
+    int32_t* d_ccount = nullptr;
     int64_t* d_site_prefix = nullptr;
     int32_t* d_site_block_rep = nullptr;
     int32_t* d_meas_prefix = nullptr;
@@ -939,7 +994,8 @@ static void free_batch(Batch* b)
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
     for (Sim* s : b->sims) free_sim(s);
-    for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin, (void*)b->d_ctr,
+    for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin,
+                    (void*)b->d_ccount, (void*)b->d_ctr,
                     (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize, (void*)b->d_site_prefix,
                     (void*)b->d_site_block_rep, (void*)b->d_meas_prefix, (void*)b->d_meas_rep, b->d_ccl_seeds})
         if (p) cudaFree(p);
@@ -1215,7 +1271,8 @@ static bool temper_compatible(const Sim* a, const Sim* b)
         x.k != y.k || x.delta != y.delta || x.cap != y.cap)
         return false;
     if (a->lat_kind != b->lat_kind || a->n != b->n || a->termsel != b->termsel) return false;
-    if (a->lat_kind == MQV_LATTICE_HYPERCUBIC) return a->dim == b->dim && a->len == b->len;
+    if (a->lat_kind == MQV_LATTICE_HYPERCUBIC)
+        return a->dim == b->dim && a->len == b->len && a->lat_hash == b->lat_hash;  // hash: bonds (0 without)
     return a->lat_hash == b->lat_hash;
 }
 
@@ -1291,14 +1348,17 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         st = mqv_set_stream(h, b->stream);
         if (st) return bail(st);
     }
-    // per-colour work: colour c concatenates every member's colour-c sites
+    // per-colour work: colour c concatenates every member's colour-c sites,
+    // each member's count padded to whole warp blocks of kAccSites, so that a
+    // warp's block lies in one member (batch_metro)
     int ncol = 0;
     for (Sim* s : b->sims) ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
     std::vector<int64_t> prefix((size_t)ncol * (n + 1), 0);
-    std::vector<int32_t> cbegin((size_t)n * ncol, 0), brep;
+    std::vector<int32_t> cbegin((size_t)n * ncol, 0), ccount((size_t)n * ncol, 0), brep;
     b->block_off.assign((size_t)ncol, 0);
     b->blocks.assign((size_t)ncol, 0);
     b->total.assign((size_t)ncol, 0);
+    const int64_t per_cta = (int64_t)kBatchMetroThreads / 32 * kAccSites;  // padded positions per CTA
     for (int c = 0; c < ncol; ++c) {
         int64_t* pf = prefix.data() + (size_t)c * (n + 1);
         for (int r = 0; r < n; ++r) {
@@ -1308,16 +1368,17 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
                 cnt = s->colour_ptr[(size_t)c + 1] - s->colour_ptr[(size_t)c];
                 cbegin[(size_t)r * ncol + c] = s->colour_ptr[(size_t)c];
             }
-            pf[r + 1] = pf[r] + cnt;
+            ccount[(size_t)r * ncol + c] = (int32_t)cnt;
+            pf[r + 1] = pf[r] + (cnt + kAccSites - 1) / kAccSites * kAccSites;
         }
         const int64_t tot = pf[n];
-        const int64_t nb = (tot + kBatchMetroThreads - 1) / kBatchMetroThreads;
+        const int64_t nb = (tot + per_cta - 1) / per_cta;
         if ((int64_t)brep.size() + nb >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
         b->block_off[(size_t)c] = (int)brep.size();
         b->blocks[(size_t)c] = (int)nb;
         b->total[(size_t)c] = tot;
         for (int64_t k = 0, r = 0; k < nb; ++k) {
-            while (k * kBatchMetroThreads >= pf[r + 1]) ++r;
+            while (k * per_cta >= pf[r + 1]) ++r;
             brep.push_back((int32_t)r);
         }
     }
@@ -1350,6 +1411,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     if (!st) st = dcopy((void**)&b->d_meas_rep, mrep.data(), sizeof(int32_t) * mrep.size());
     if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
     if (!st) st = dcopy((void**)&b->d_cbegin, cbegin.data(), sizeof(int32_t) * std::max<size_t>(cbegin.size(), 1));
+    if (!st) st = dcopy((void**)&b->d_ccount, ccount.data(), sizeof(int32_t) * std::max<size_t>(ccount.size(), 1));
     if (!st) st = dcopy((void**)&b->d_site_prefix, sprefix.data(), sizeof(int64_t) * sprefix.size());
     if (!st) st = dcopy((void**)&b->d_site_block_rep, sbrep.data(), sizeof(int32_t) * sbrep.size());
     if (st) return bail(st);
@@ -1371,6 +1433,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     b->L.prefix = b->d_prefix;
     b->L.block_rep = b->d_block_rep;
     b->L.cbegin = b->d_cbegin;
+    b->L.ccount = b->d_ccount;
     b->L.block_off = b->block_off.data();
     b->L.blocks = b->blocks.data();
     b->L.total = b->total.data();

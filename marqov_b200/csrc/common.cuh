@@ -104,6 +104,42 @@ MQV_HD bool accept_below(uint64_t cut, Key key, uint32_t site, uint32_t sweep, u
     return accept_with_top(cut, accept_top8(key, site, sweep, replica), key, site, sweep, replica);
 }
 
+// u53 < cut given the site's top byte, for per-site kernels that share the
+// ACCEPT blocks (accept_tab_fill): dE <= 0 cuts accept without a draw.
+MQV_HD bool accept_top_or_fine(uint64_t cut, uint32_t top, Key key, uint32_t site, uint32_t sweep, uint32_t replica)
+{
+    if (cut >= (1ull << 53) || cut == 0) return cut != 0;
+    return accept_with_top(cut, top, key, site, sweep, replica);
+}
+
+#ifdef __CUDACC__
+// Warp-shared acceptance bytes.  A warp that updates sites of an aligned
+// block of kAccRuns 64-site runs (sites [64 run0, 64 (run0 + kAccRuns)))
+// draws the two ACCEPT blocks of each of the block's 2 kAccRuns groups once,
+// one per lane -- lane L draws half (L & 1) of parity (L >> 1) & 1 of run
+// run0 + (L >> 2) into `tab` (kAccTab uint4 of warp-private shared memory) --
+// and every site of the block then reads its eight planes from there: one
+// Philox block per lane per 512 sites instead of two per site.  Same bits as
+// accept_top8.
+constexpr int kAccRuns = 8;
+constexpr int kAccTab = 4 * kAccRuns;  // uint4 per warp: [run][parity][half]
+constexpr int kAccSites = 32 * kAccRuns;  // sites of one colour in a block (checkerboard)
+__device__ __forceinline__ void accept_tab_fill(uint4* tab, uint32_t run0, Key key, uint32_t sweep, uint32_t replica)
+{
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t c3 = (kAccept << 24) | (replica & 0xFFFFFFu);
+    __syncwarp();  // the previous block's readers are done
+    tab[lane] = philox(((run0 + (lane >> 2)) << 1) | ((lane >> 1) & 1u), sweep, lane & 1u, c3, key);
+    __syncwarp();
+}
+__device__ __forceinline__ uint32_t accept_top8_tab(const uint4* tab, uint32_t run0, uint32_t site)
+{
+    const uint32_t k = (site >> 6) - run0, p = site & 1u, q = (site >> 1) & 31u;
+    const uint4 a = tab[(k * 2 + p) * 2], b = tab[(k * 2 + p) * 2 + 1];
+    return ((a.x >> q) & 1u) | (((a.y >> q) & 1u) << 1) | (((a.z >> q) & 1u) << 2) | (((a.w >> q) & 1u) << 3) |
+           (((b.x >> q) & 1u) << 4) | (((b.y >> q) & 1u) << 5) | (((b.z >> q) & 1u) << 6) | (((b.w >> q) & 1u) << 7);
+}
+#endif
 
 // x % q for the small ranges of state draws (q <= 65535): constant divisors
 // for the common q, else three 32-bit remainders of x = hi 2^32 + lo.

@@ -56,6 +56,10 @@ struct StencilDev {
     int split;      // 2D state stored in split rows (see split_addr)
     int lg;         // log2(len) when len is a power of two, else -1
     uint64_t mlen;  // ceil(2^64 / len) otherwise: u / len = mulhi64(u, mlen), exact for 32-bit u
+    // bond weights (bnds, e.g. RegularRandomBond): plane d holds the bond of
+    // every site to its +d neighbour, fb[d n + i]; the bond to the -d
+    // neighbour is that neighbour's +d bond.  NULL: every bond is 1.
+    const int8_t* fb;
     MQV_HD uint32_t divlen(uint32_t u) const
     {
 #ifdef __CUDA_ARCH__
@@ -88,7 +92,12 @@ struct StencilDev {
         if ((slot & 1) == 0) return x == len - 1 ? i - (int64_t)(len - 1) * p : i + p;
         return x == 0 ? i + (int64_t)(len - 1) * p : i - p;
     }
-    MQV_HD int bond(int64_t, int) const { return 1; }
+    MQV_HD int bond(int64_t i, int slot) const
+    {
+        if (!fb) return 1;
+        const int64_t j = (slot & 1) ? nbr(i, slot) : i;
+        return fb[(int64_t)(slot >> 1) * n + j];
+    }
 };
 
 struct CSRDev {

@@ -1,8 +1,9 @@
 // Device building blocks of the float models shared by the per-handle kernels
 // (metropolis_f32.cu) and the batched kernels (batch.cu): proposals, the
 // per-site Metropolis update, the embedded Wolff cluster, the observable
-// accumulation and its finalisation.  Storage is FP32; energy differences,
-// proposals and acceptance are FP64, like the reference's double arithmetic
+// accumulation and its finalisation.  Storage is FP32 in structure-of-arrays
+// layout (component c of site i at s[c n + i]); proposals, onsite terms and
+// acceptance are FP64, like the reference's double arithmetic
 // (src/libmarqov/metropolishelpers.h:598-738).
 #pragma once
 #include "engine.h"
@@ -47,14 +48,33 @@ __device__ __forceinline__ void smallcap3(SubStream& rng, const float o[3], doub
     for (int c = 0; c < 3; ++c) v[c] = nv[c] / nn;
 }
 
-// Lanes with live == false touch no memory.  The decision
-// is u53 < accept_cut_direct(1, dE, beta), which equals update_accepted<1> on
-// the site's acceptance word.  `sub`: the site's sublattice (checkerboard
-// colour) where the lattice has a termselector.
+// Component c of site i of a float state: structure of arrays, s[c n + i]
+// (n = the lattice's sites), so that the lanes of a warp, which update
+// neighbouring sites of one colour, read each component in one coalesced run.
+__device__ __forceinline__ float f32_get(const float* __restrict__ s, int64_t n, int c, int64_t i)
+{
+    return s[(int64_t)c * n + i];
+}
+
+// One Metropolis move (Metropolis<H,L>::move, src/libmarqov/metropolis.h:88-126)
+// of a float model.  The neighbourhood sums are FP32 like the reference's
+// float state vectors (nbrhoodloop, src/libmarqov/metropolishelpers.h:456-537:
+// neighbourhood = neighbourhood + get(s_j) in the state's type), the
+// interaction difference J dot(s_new - s_old, neighbourhood) takes FP32
+// products summed in FP64 (svmath.h dot: inner_product with a double
+// initial value), the onsite terms and the acceptance are FP64.  The
+// decision is u53 < accept_cut_direct(1, dE, beta), which equals
+// update_accepted<1> on the site's acceptance word; its top byte comes from
+// the warp's shared table when `tab` is given (accept_tab_fill), else from
+// the site's own two ACCEPT blocks.  `sub`: the site's sublattice
+// (checkerboard colour) where the lattice has a termselector.  Lanes with
+// live == false touch no memory.
 template <class Lat>
 __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, float* __restrict__ s, int64_t i,
-                                         Key key, uint32_t sweep, uint32_t replica, bool live, int sub = 0)
+                                         Key key, uint32_t sweep, uint32_t replica, bool live, int sub = 0,
+                                         const uint4* tab = nullptr, uint32_t run0 = 0)
 {
+    const int64_t n = lat.n;
     uint64_t cut = 0;
     float nf[3] = {0.f, 0.f, 0.f};
     if (live) {
@@ -66,37 +86,35 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
             // src/hamiltonian/Phi4.h:44-57); interaction + Onsite_Quadratic +
             // Onsite_Fourth_Minus_One (src/hamiltonian/Phi4.h:63-74,103-121)
             const double r = 1.0 + (-1.0 - 1.0) * real01(rng.next());
-            const double old = s[i];
+            const float of = s[i];
+            const double old = of;
             nf[0] = (float)(old + m.cap * r);
             const double nw = nf[0];
-            double sum = 0;
-            for (int t = 0; t < deg; ++t) sum += (double)s[lat.nbr(i, t)];
+            float sum = 0.f;
+            for (int t = 0; t < deg; ++t) sum += s[lat.nbr(i, t)];
             const double o2 = old * old, n2 = nw * nw;
-            dE = m.J * (nw - old) * sum + onsite_w0(m, sub) * m.h * (n2 - o2) +
+            dE = m.J * (double)((nf[0] - of) * sum) + onsite_w0(m, sub) * m.h * (n2 - o2) +
                  onsite_w1(m, sub) * m.h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
         } else {
-            const float* so = s + 3 * i;
-            const float o[3] = {so[0], so[1], so[2]};
+            const float o[3] = {f32_get(s, n, 0, i), f32_get(s, n, 1, i), f32_get(s, n, 2, i)};
             double v[3];
             if (m.proposal == MQV_PROPOSAL_SMALL_CAP) smallcap3(rng, o, m.cap, v);
             else rnddir3(rng, v);  // SVInitializer for float vectors (initializers.h:74-80)
             nf[0] = (float)v[0];
             nf[1] = (float)v[1];
             nf[2] = (float)v[2];
-            double nb[3] = {0, 0, 0};
+            float nb[3] = {0.f, 0.f, 0.f};
             for (int t = 0; t < deg; ++t) {
-                const float* sj = s + 3 * lat.nbr(i, t);
-                nb[0] += (double)sj[0];
-                nb[1] += (double)sj[1];
-                nb[2] += (double)sj[2];
+                const int64_t j = lat.nbr(i, t);
+                nb[0] += f32_get(s, n, 0, j);
+                nb[1] += f32_get(s, n, 1, j);
+                nb[2] += f32_get(s, n, 2, j);
             }
             // XXZAntiferro_interaction::get (src/hamiltonian/XXZAntiferro.h:135-150)
             // weights x and y by delta; Heisenberg's is the identity
-            const double wxy = m.kind == MQV_MODEL_XXZ ? m.delta : 1.0;
-            dE = wxy * ((double)nf[0] - (double)o[0]) * nb[0];
-            dE += wxy * ((double)nf[1] - (double)o[1]) * nb[1];
-            dE += ((double)nf[2] - (double)o[2]) * nb[2];
-            dE *= m.J;
+            const double dxy = (double)((nf[0] - o[0]) * nb[0]) + (double)((nf[1] - o[1]) * nb[1]);
+            const double dz = (double)((nf[2] - o[2]) * nb[2]);
+            dE = m.J * (m.kind == MQV_MODEL_XXZ ? m.delta * dxy + dz : dxy + dz);
             if (m.kind == MQV_MODEL_XXZ) {
                 // XXZAntiferro_extfield H s_z and XXZAntiferro_onsiteaniso D s_z^2
                 // (XXZAntiferro.h:162-170, XXZAntiferroSingleAniso.h:31-44)
@@ -106,14 +124,18 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
         }
         cut = accept_cut_direct(1, dE, m.beta);
     }
-    if (live && accept_below(cut, key, (uint32_t)i, sweep, replica)) {
-        if (m.symd == 1) {
-            s[i] = nf[0];
-        } else {
-            float* so = s + 3 * i;
-            so[0] = nf[0];
-            so[1] = nf[1];
-            so[2] = nf[2];
+    bool acc;
+    if (tab) {
+        const uint32_t top = live ? accept_top8_tab(tab, run0, (uint32_t)i) : 0u;
+        acc = live && accept_top_or_fine(cut, top, key, (uint32_t)i, sweep, replica);
+    } else {
+        acc = live && accept_below(cut, key, (uint32_t)i, sweep, replica);
+    }
+    if (acc) {
+        s[i] = nf[0];
+        if (m.symd != 1) {
+            s[n + i] = nf[1];
+            s[2 * n + i] = nf[2];
         }
     }
 }
@@ -159,13 +181,14 @@ __device__ __forceinline__ void measure_f32_part(const ModelDev& m, const Lat& l
             q2 += p2;
             q4 += (p2 - 1.0) * (p2 - 1.0);
         } else {
-            const double a = s[3 * i], b = s[3 * i + 1], c = s[3 * i + 2];
+            const int64_t n = lat.n;
+            const double a = f32_get(s, n, 0, i), b = f32_get(s, n, 1, i), c = f32_get(s, n, 2, i);
             double na = 0, nb = 0, nc = 0;
             for (int t = 0; t < deg; ++t) {
-                const float* sj = s + 3 * lat.nbr(i, t);
-                na += (double)sj[0];
-                nb += (double)sj[1];
-                nc += (double)sj[2];
+                const int64_t j = lat.nbr(i, t);
+                na += (double)f32_get(s, n, 0, j);
+                nb += (double)f32_get(s, n, 1, j);
+                nc += (double)f32_get(s, n, 2, j);
             }
             e += wxy * (a * na + b * nb) + c * nc;
             mx += a;
@@ -227,31 +250,32 @@ __device__ __forceinline__ void finalize_f32_one(const ModelDev& m, int64_t n, c
 // cluster kernels, rounded as written (no contraction), as the reference's
 // double code: a = s . r, cpl = J (-a_i) a_j, and the reflection
 // s -> (s - 2 (s.r) r) / |s - 2 (s.r) r|.
-__device__ __forceinline__ double embed_proj(int symd, const float* __restrict__ s, int64_t i, float r0, float r1,
-                                             float r2)
+__device__ __forceinline__ double embed_proj(int symd, const float* __restrict__ s, int64_t n, int64_t i, float r0,
+                                             float r1, float r2)
 {
     if (symd == 3)
-        return __dadd_rn(__dadd_rn(__dmul_rn((double)s[3 * i], (double)r0), __dmul_rn((double)s[3 * i + 1], (double)r1)),
-                         __dmul_rn((double)s[3 * i + 2], (double)r2));
+        return __dadd_rn(__dadd_rn(__dmul_rn((double)f32_get(s, n, 0, i), (double)r0),
+                                   __dmul_rn((double)f32_get(s, n, 1, i), (double)r1)),
+                         __dmul_rn((double)f32_get(s, n, 2, i), (double)r2));
     return __dmul_rn((double)s[i], (double)r0);
 }
 __device__ __forceinline__ double embed_cpl(double J, double ai, double aj) { return __dmul_rn(__dmul_rn(J, -ai), aj); }
-__device__ __forceinline__ void embed_reflect(int symd, float* __restrict__ s, int64_t i, float r0, float r1, float r2)
+__device__ __forceinline__ void embed_reflect(int symd, float* __restrict__ s, int64_t n, int64_t i, float r0, float r1,
+                                              float r2)
 {
     if (symd != 3) {
         s[i] = -s[i];
         return;
     }
-    float* v = s + 3 * i;
-    const double x = v[0], y = v[1], z = v[2];
+    const double x = f32_get(s, n, 0, i), y = f32_get(s, n, 1, i), z = f32_get(s, n, 2, i);
     const double d = __dadd_rn(__dadd_rn(__dmul_rn(x, (double)r0), __dmul_rn(y, (double)r1)), __dmul_rn(z, (double)r2));
     const double d2 = __dmul_rn(2.0, d);
     const double w0 = __dsub_rn(x, __dmul_rn(d2, (double)r0)), w1 = __dsub_rn(y, __dmul_rn(d2, (double)r1)),
                  w2 = __dsub_rn(z, __dmul_rn(d2, (double)r2));
     const double nn = __dsqrt_rn(__dadd_rn(__dadd_rn(__dmul_rn(w0, w0), __dmul_rn(w1, w1)), __dmul_rn(w2, w2)));
-    v[0] = (float)__ddiv_rn(w0, nn);
-    v[1] = (float)__ddiv_rn(w1, nn);
-    v[2] = (float)__ddiv_rn(w2, nn);
+    s[i] = (float)__ddiv_rn(w0, nn);
+    s[n + i] = (float)__ddiv_rn(w1, nn);
+    s[2 * n + i] = (float)__ddiv_rn(w2, nn);
 }
 
 // The embedding of a cluster: seed site and reflection vector r (plane
@@ -291,7 +315,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
         s_r[2] = r[2];
         queue[0] = (int32_t)rsite;
         fbuf[0] = (int32_t)rsite;
-        fproj[0] = embed_proj(symd, s, rsite, r[0], r[1], r[2]);
+        fproj[0] = embed_proj(symd, s, n, rsite, r[0], r[1], r[2]);
         atomicOr(&visited[rsite >> 5], 1u << (rsite & 31));
         s_head = 0;
         s_tail = 1;
@@ -299,7 +323,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     }
     __syncthreads();
     const float r0 = s_r[0], r1 = s_r[1], r2 = s_r[2];
-    auto proj = [&](int64_t i) -> double { return embed_proj(symd, s, i, r0, r1, r2); };
+    auto proj = [&](int64_t i) -> double { return embed_proj(symd, s, n, i, r0, r1, r2); };
     const int lanes = wolff_lanes(lat, max_degree);
     const unsigned lane = threadIdx.x & 31;
     for (int lvl = 0;; ++lvl) {
@@ -379,7 +403,7 @@ __device__ __forceinline__ void wolff_f32_cluster(const ModelDev& m, const Lat& 
     const int size = s_tail;
     for (int k = threadIdx.x; k < size; k += blockDim.x) {
         const int32_t i = queue[k];
-        embed_reflect(symd, s, i, r0, r1, r2);
+        embed_reflect(symd, s, n, i, r0, r1, r2);
         atomicAnd(&visited[i >> 5], ~(1u << (i & 31)));
     }
     if (threadIdx.x == 0) *out_size = size;

@@ -18,7 +18,8 @@ namespace mqv {
 template <class Lat>
 __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int8_t* __restrict__ s, int64_t i,
                                           Key key, uint32_t sweep, uint32_t replica,
-                                          const unsigned long long* __restrict__ cuts, int D, bool live, int sub = 0)
+                                          const unsigned long long* __restrict__ cuts, int D, bool live, int sub = 0,
+                                          const uint4* tab = nullptr, uint32_t run0 = 0)
 {
     int64_t ai = 0;
     int nw = 0;
@@ -61,8 +62,16 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int
         cut = cuts[k];
     }
     // metro_update_accepted (src/libmarqov/metropolis.h:61-64,120-124) on the
-    // site's acceptance word
-    if (live && accept_below(cut, key, (uint32_t)i, sweep, replica)) s[ai] = (int8_t)nw;
+    // site's acceptance word, its top byte from the warp's shared table when
+    // `tab` is given (accept_tab_fill)
+    bool acc;
+    if (tab) {
+        const uint32_t top = live ? accept_top8_tab(tab, run0, (uint32_t)i) : 0u;
+        acc = live && accept_top_or_fine(cut, top, key, (uint32_t)i, sweep, replica);
+    } else {
+        acc = live && accept_below(cut, key, (uint32_t)i, sweep, replica);
+    }
+    if (acc) s[ai] = (int8_t)nw;
 }
 
 // Site of colour `colour` in pair t of a parity-coloured hypercubic lattice
@@ -112,7 +121,7 @@ __device__ __forceinline__ int int8_bond_sum(const ModelDev&, const StencilDev& 
     int loc = 0;
     for (int d = 0; d < st.dim; ++d) {
         const int v = s[st.addr(st.nbr(i, 2 * d))];
-        loc += potts ? (v == si) : v;
+        loc += potts ? (v == si) : st.bond(i, 2 * d) * v;
     }
     return 2 * (potts ? loc : loc * si);
 }

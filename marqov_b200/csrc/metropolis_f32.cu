@@ -14,15 +14,26 @@ namespace mqv {
 
 unsigned long long accept_cut(int pref, double dE, double beta);
 
-__global__ void metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s, int colour, Key key,
-                                  uint32_t sweep, uint32_t replica)
+// One colour of a stencil sweep.  Warps take aligned blocks of kAccSites
+// sites of the colour (kAccRuns runs of 64 lattice sites): the warp draws the
+// block's acceptance bytes once (accept_tab_fill), then its lanes update
+// kAccRuns sites each, 32 neighbouring sites per step.
+constexpr int kMetroThreads = 256;
+__global__ void __launch_bounds__(kMetroThreads) metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s,
+                                                                   int colour, Key key, uint32_t sweep, uint32_t replica)
 {
-    // warp-uniform trips: the lanes of a warp update their sites together
-    const int64_t half = st.n / 2, stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
-        const int64_t t = t0 + (threadIdx.x & 31u);
-        const bool live = t < half;
-        f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live, colour);
+    __shared__ uint4 tabs[kMetroThreads / 32][kAccTab];
+    uint4* tab = tabs[threadIdx.x >> 5];
+    const int64_t half = st.n / 2, nblk = (half + kAccSites - 1) / kAccSites;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += nw) {
+        const uint32_t run0 = (uint32_t)(b * kAccRuns);
+        accept_tab_fill(tab, run0, key, sweep, replica);
+        for (int j = 0; j < kAccRuns; ++j) {
+            const int64_t t = b * kAccSites + j * 32 + (threadIdx.x & 31u);
+            const bool live = t < half;
+            f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live, colour, tab, run0);
+        }
     }
 }
 
@@ -58,9 +69,9 @@ __global__ void init_f32(ModelDev m, int64_t n, float* __restrict__ s, Key key, 
         if (m.symd == 3) {
             double v[3];
             rnddir3(rng, v);
-            s[3 * i] = (float)v[0];
-            s[3 * i + 1] = (float)v[1];
-            s[3 * i + 2] = (float)v[2];
+            s[i] = (float)v[0];
+            s[n + i] = (float)v[1];
+            s[2 * n + i] = (float)v[2];
         } else {
             // standard normal by Box-Muller
             const double u0 = rng.real(), u1 = rng.real();
@@ -123,9 +134,11 @@ cudaError_t launch_metropolis_f32(Sim* s, int slot)
     const Key key = make_key(s->seed);
     float* st = (float*)s->state[s->cur];
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
-        const int g = grid_for_f(s->n / 2, 256);
+        // one warp per block of kAccSites sites of a colour, up to 16 CTAs per SM
+        const int g = grid_for_f((s->n / 2 + kAccSites - 1) / kAccSites * 32, kMetroThreads);
         for (int c = 0; c < 2; ++c) {
-            metro_f32_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, s->replica);
+            metro_f32_stencil<<<g, kMetroThreads, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep,
+                                                                  s->replica);
             s->launches++;
         }
     } else {

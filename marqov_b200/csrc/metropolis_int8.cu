@@ -18,16 +18,29 @@
 
 namespace mqv {
 
-__global__ void metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict__ s, int colour, Key key,
-                                   uint32_t sweep, uint32_t replica, const unsigned long long* __restrict__ cuts,
-                                   int D)
+// One colour of a stencil sweep.  Warps take aligned blocks of kAccSites
+// sites of the colour (kAccRuns runs of 64 lattice sites): the warp draws the
+// block's acceptance bytes once (accept_tab_fill), then its lanes update
+// kAccRuns sites each, 32 neighbouring sites per step.
+constexpr int kMetroThreads = 256;
+__global__ void __launch_bounds__(kMetroThreads) metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict__ s,
+                                                                    int colour, Key key, uint32_t sweep,
+                                                                    uint32_t replica,
+                                                                    const unsigned long long* __restrict__ cuts, int D)
 {
-    // warp-uniform trips: the lanes of a warp update their sites together
-    const int64_t half = st.n / 2, stride = (int64_t)gridDim.x * blockDim.x;
-    for (int64_t t0 = blockIdx.x * (int64_t)blockDim.x + (threadIdx.x & ~31u); t0 < half; t0 += stride) {
-        const int64_t t = t0 + (threadIdx.x & 31u);
-        const bool live = t < half;
-        int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live, colour);
+    __shared__ uint4 tabs[kMetroThreads / 32][kAccTab];
+    uint4* tab = tabs[threadIdx.x >> 5];
+    const int64_t half = st.n / 2, nblk = (half + kAccSites - 1) / kAccSites;
+    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
+    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += nw) {
+        const uint32_t run0 = (uint32_t)(b * kAccRuns);
+        accept_tab_fill(tab, run0, key, sweep, replica);
+        for (int j = 0; j < kAccRuns; ++j) {
+            const int64_t t = b * kAccSites + j * 32 + (threadIdx.x & 31u);
+            const bool live = t < half;
+            int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live, colour, tab,
+                      run0);
+        }
     }
 }
 
@@ -194,10 +207,11 @@ cudaError_t launch_metropolis_int8(Sim* s, int slot)
     err = ensure_cuts(s);
     if (err != cudaSuccess) return err;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
-        const int g = grid_for(s->n / 2, 256);
+        // one warp per block of kAccSites sites of a colour, up to 16 CTAs per SM
+        const int g = grid_for((s->n / 2 + kAccSites - 1) / kAccSites * 32, kMetroThreads);
         for (int c = 0; c < 2; ++c) {
-            metro_int8_stencil<<<g, 256, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep, s->replica,
-                                                          s->d_cuts, s->max_degree);
+            metro_int8_stencil<<<g, kMetroThreads, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep,
+                                                                   s->replica, s->d_cuts, s->max_degree);
             s->launches++;
         }
     } else {

@@ -106,8 +106,9 @@ __device__ __forceinline__ bool ccl_active(const BatchRep& R, const CclSeed& sd,
     if (F32) {
         const int64_t lo = i < j ? i : j, hi = i < j ? j : i;
         const float* s = (const float*)R.s;
-        const double cpl = embed_cpl(R.md.J, embed_proj(R.md.symd, s, lo, sd.r[0], sd.r[1], sd.r[2]),
-                                     embed_proj(R.md.symd, s, hi, sd.r[0], sd.r[1], sd.r[2]));
+        const int64_t n = rep_sites(R);
+        const double cpl = embed_cpl(R.md.J, embed_proj(R.md.symd, s, n, lo, sd.r[0], sd.r[1], sd.r[2]),
+                                     embed_proj(R.md.symd, s, n, hi, sd.r[0], sd.r[1], sd.r[2]));
         return cpl > 0 &&
                !update_accepted(2, cpl, R.md.beta, lo64(philox((uint32_t)lo, serial, (uint32_t)hi, tgb, R.key)));
     }
@@ -266,7 +267,7 @@ __global__ void ccl_flip(const BatchRep* __restrict__ reps, const int64_t* __res
         in = root >= 0 && R.queue[i] == root;
         if (in) {
             if (F32) {
-                embed_reflect(R.md.symd, (float*)R.s, i, sd.r[0], sd.r[1], sd.r[2]);
+                embed_reflect(R.md.symd, (float*)R.s, rep_sites(R), i, sd.r[0], sd.r[1], sd.r[2]);
             } else {
                 const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
                 ((int8_t*)R.s)[a] = (int8_t)sd.newq;

@@ -8,6 +8,8 @@
   (``bnds``) and an optional proper colouring (else the engine colours
   greedily).  ``from_nbrs`` lowers any object with ``size()`` / ``nbrs()`` /
   optional ``bnds()``, the way a reference lattice plugs in.
+* ``BondedHypercubic``: a hypercubic lattice with bond weights, kept on the
+  stencil path.
 * Builders for the synthetic workloads: ``RegularRandomBond`` (bimodal +-1
   bonds on a hypercubic lattice, src/lattice/regular_random_bond.h:13-77 with a
   seeded generator) and ``RandomGeometricGraph2D`` (periodic unit square).
@@ -174,11 +176,32 @@ class CSRLattice(Lattice):
         return col
 
 
-def RegularRandomBond(len: int, dim: int, p: float = 0.5, seed: int = 0) -> CSRLattice:  # noqa: A002
+class BondedHypercubic(RegularHypercubic):
+    """A periodic hypercubic lattice with symmetric bond weights ``bnds``,
+    given per site in the ``nbrs(0, i)`` order +x,-x,+y,-y,... (an n x 2 dim
+    int8 array).  The engine keeps it on the stencil path and stores one plane
+    of +d bonds per dimension; ``to_csr()`` gives the same lattice as CSR."""
+
+    def __init__(self, len: int, dim: int, bonds):  # noqa: A002 - reference argument name
+        super().__init__(len, dim)
+        self.bonds = np.ascontiguousarray(bonds, np.int8).reshape(self.npoints, 2 * self.dim)
+
+    def bnds(self, alpha: int, i: int):
+        return self.bonds[i].tolist()
+
+    def desc(self) -> L.LatticeDesc:
+        return L.LatticeDesc(kind=L.LATTICE_HYPERCUBIC, dim=self.dim, len=self.len, bonds=self.bonds.ctypes.data)
+
+    def to_csr(self) -> "CSRLattice":
+        base = super().to_csr()
+        return CSRLattice(base.row_ptr, base.col_idx, self.bonds.reshape(-1), base.colours)
+
+
+def RegularRandomBond(len: int, dim: int, p: float = 0.5, seed: int = 0) -> BondedHypercubic:  # noqa: A002
     """Hypercubic lattice with symmetric bimodal +-1 bonds, P(+1) = p: the
     ``RegularRandomBond<BimodalPDF>`` lattice (regular_random_bond.h:26-55) with
     a seeded generator instead of ``random_device``.  Each undirected bond gets
-    one draw; both of its CSR entries carry it."""
+    one draw; both of its entries carry it."""
     base = RegularHypercubic(len, dim).to_csr()
     n = base.n
     rng = np.random.default_rng(seed)
@@ -189,7 +212,7 @@ def RegularRandomBond(len: int, dim: int, p: float = 0.5, seed: int = 0) -> CSRL
     for j in range(dim):
         bonds[:, 2 * j] = w[:, j]                        # +dir bond owned by the site
         bonds[:, 2 * j + 1] = w[cols[:, 2 * j + 1], j]   # -dir bond owned by the neighbour
-    return CSRLattice(base.row_ptr, base.col_idx, bonds.reshape(-1), base.colours)
+    return BondedHypercubic(len, dim, bonds)
 
 
 def RandomGeometricGraph2D(n: int, mean_degree: float = 8.0, seed: int = 0) -> CSRLattice:

@@ -376,29 +376,33 @@ static void metro_f32_site(const orc_model* m, const orc_lattice* g, float* s, i
         double r = real_of(rng_integer(rng), -1.0, 1.0);
         double old = so[0];
         nw[0] = (double)(float)(old + m->cap * r);
-        double sum = 0;
-        for (int32_t p = b; p < e; ++p) sum += (double)s[g->col_idx[p]];
+        /* the neighbourhood is summed in the state's float type (nbrhoodloop,
+         * metropolishelpers.h:456-537) and dot() multiplies float components */
+        float sum = 0.f;
+        for (int32_t p = b; p < e; ++p) sum += s[g->col_idx[p]];
         double o2 = old * old, n2 = nw[0] * nw[0];
         /* interaction + Onsite_Quadratic + Onsite_Fourth_Minus_One,
          * src/hamiltonian/Phi4.h:63-74,103-121 */
-        dE = m->J * (nw[0] - old) * sum + ons0(m, sub) * m->h * (n2 - o2) +
+        dE = m->J * (double)(((float)nw[0] - so[0]) * sum) + ons0(m, sub) * m->h * (n2 - o2) +
              ons1(m, sub) * m->h2 * ((n2 - 1.0) * (n2 - 1.0) - (o2 - 1.0) * (o2 - 1.0));
     } else {
         double v[3];
         if (m->proposal == 1) smallcap3(rng, so, m->cap, v);
         else rnddir3(rng, v); /* SVInitializer<float>, initializers.h:74-80 */
         for (int c = 0; c < 3; ++c) nw[c] = (double)(float)v[c];
-        double nb[3] = {0, 0, 0};
+        /* float neighbourhood sums and float component products summed in
+         * double (nbrhoodloop and svmath.h dot on float state vectors) */
+        float nb[3] = {0.f, 0.f, 0.f};
         for (int32_t p = b; p < e; ++p) {
             const float* sj = s + (size_t)g->col_idx[p] * 3;
-            for (int c = 0; c < 3; ++c) nb[c] += (double)sj[c];
+            for (int c = 0; c < 3; ++c) nb[c] += sj[c];
         }
+        double pr[3];
+        for (int c = 0; c < 3; ++c) pr[c] = (double)(((float)nw[c] - so[c]) * nb[c]);
         /* the interaction's get(): XXZAntiferro_interaction weights x and y
          * by Delta (src/hamiltonian/XXZAntiferro.h:135-150), Heisenberg none */
-        double w[3] = {m->kind == ORC_XXZ ? m->delta : 1.0, m->kind == ORC_XXZ ? m->delta : 1.0, 1.0};
-        dE = 0;
-        for (int c = 0; c < 3; ++c) dE += w[c] * (nw[c] - (double)so[c]) * nb[c];
-        dE *= m->J;
+        double dxy = pr[0] + pr[1];
+        dE = m->J * ((m->kind == ORC_XXZ ? m->delta * dxy : dxy) + pr[2]);
         if (m->kind == ORC_XXZ) {
             /* XXZAntiferro_extfield H s_z (XXZAntiferro.h:162-170) and
              * XXZAntiferro_onsiteaniso D s_z^2 (XXZAntiferroSingleAniso.h:31-44) */

@@ -243,6 +243,9 @@ class RefHarness:
         lib.ref_emcs_ising2d.restype = C.c_int
         lib.ref_emcs_ising2d.argtypes = [C.c_int, C.c_double, C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int,
                                          C.c_int, _f64p, _f64p]
+        lib.ref_emcs_generic.restype = C.c_int
+        lib.ref_emcs_generic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
+                                         C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p]
         lib.ref_calc_mh_ratio.restype = C.c_double
         lib.ref_calc_mh_ratio.argtypes = [C.c_double]
         lib.ref_pt_calcprob.restype = C.c_int
@@ -367,6 +370,16 @@ class RefHarness:
         obs = np.zeros(2 * nmeas, np.float64)
         mc = np.zeros(nmeas, np.float64)
         assert self.lib.ref_emcs_ising2d(L, J, beta, seed, ncluster, nmetro, ntherm, nmeas, obs, mc) == 0
+        return obs.reshape(nmeas, 2), mc
+
+    def emcs_generic(self, kind, L, dim, J, beta, seed, ncluster, nmetro, ntherm, nmeas, p0=0.0, p1=0.0, p2=0.0):
+        """The reference's own EMCS loop for Potts<3> (kind 3), Heisenberg with
+        the plane embedder (6) or scalar phi^4 (8): per measured EMCS (e, |m|)
+        and the mean cluster size."""
+        obs = np.zeros(2 * nmeas, np.float64)
+        mc = np.zeros(nmeas, np.float64)
+        assert self.lib.ref_emcs_generic(kind, L, dim, J, p0, p1, p2, beta, seed, ncluster, nmetro, ntherm, nmeas,
+                                         obs, mc) == 0
         return obs.reshape(nmeas, 2), mc
 
     def farm(self, length, beta, nthreads, seed=12345):

@@ -728,3 +728,81 @@ int ref_emcs_ising2d(int len, double J, double beta, uint64_t seed, int ncluster
 }
 
 }  // extern "C"
+
+// The reference's own EMCS loop (src/libmarqov/emcs.h:69-109: ncluster
+// Wolff clusters seeded at rng.integer(N), then nmetro x N random-site
+// Metropolis moves) on RegularHypercubic(len, dim) with
+// RNGCache<mt19937_64>, for the models other than Ising:
+//   kind 3: Potts<3>(J), Wolff<Potts<3>>, initstatespace of Potts<3>;
+//   kind 6: Heisenberg<float> (J) with fresh-direction proposals and the
+//           generic Wolff over Embedder<Heisenberg> (HeisenbergPlane),
+//           Heisenberg::initstatespace;
+//   kind 8: scalar phi^4 (p0 = lambda, p1 = mass, p2 = shift amplitude) with
+//           its embedder, phi_i started from N(0, 1) (Box-Muller on real()).
+// obs receives per measured EMCS (e, |m|): the energy the moves see
+// (potts_energy / nbrhood_energy) and the magnetization observable;
+// mean_cluster the mean cluster size per EMCS.
+template <class H, class G, class SS, class EFn, class MFn>
+static void generic_emcs(const H& ham, const G& grid, SS& ss, RNGCache<std::mt19937_64>& rng, double beta, int ncluster,
+                         int nmetro, int ntherm, int nmeas, EFn efn, MFn mfn, double* obs, double* mean_cluster)
+{
+    MARQOV::Wolff<H, G> wolff;
+    const int N = (int)grid.size();
+    for (int t = 0; t < ntherm + nmeas; ++t) {
+        double avg = 0;
+        for (int c = 0; c < ncluster; ++c) {
+            const int site = rng.integer(N);
+            avg += (double)wolff.move(ham, grid, ss, rng, beta, site);
+        }
+        for (int j = 0; j < nmetro; ++j)
+            for (int i = 0; i < N; ++i) {
+                const int rsite = rng.integer(N);
+                MARQOV::Metropolis<H, G>::move(ham, grid, ss, rng, beta, rsite);
+            }
+        if (t >= ntherm) {
+            const int k = t - ntherm;
+            obs[2 * k] = efn(ss);
+            obs[2 * k + 1] = mfn(ss);
+            if (mean_cluster) mean_cluster[k] = ncluster ? avg / ncluster : 0.0;
+        }
+    }
+}
+
+extern "C" int ref_emcs_generic(int kind, int len, int dim, double J, double p0, double p1, double p2, double beta,
+                                uint64_t seed, int ncluster, int nmetro, int ntherm, int nmeas, double* obs,
+                                double* mean_cluster)
+{
+    typedef RegularHypercubic G;
+    G grid(len, dim);
+    const int N = (int)grid.size();
+    RNGCache<std::mt19937_64> rng(seed);
+    if (kind == 3) {
+        Potts<3> ham(J);
+        MARQOV::Space<std::array<int, 1>, G> ss(N);
+        ham.initstatespace(ss, grid, rng);
+        auto ef = [&](MARQOV::Space<std::array<int, 1>, G>& x) { return potts_energy(ham, grid, x); };
+        auto mf = [&](MARQOV::Space<std::array<int, 1>, G>& x) { return PottsMagnetization<3>().measure(x, grid); };
+        generic_emcs(ham, grid, ss, rng, beta, ncluster, nmetro, ntherm, nmeas, ef, mf, obs, mean_cluster);
+    } else if (kind == 6) {
+        HeisenbergPlane ham(J);
+        MARQOV::Space<std::array<float, 3>, G> ss(N);
+        ham.initstatespace(ss, grid, rng);
+        auto ef = [&](MARQOV::Space<std::array<float, 3>, G>& x) { return nbrhood_energy(ham, grid, x); };
+        auto mf = [&](MARQOV::Space<std::array<float, 3>, G>& x) { return Magnetization().measure(x, grid); };
+        generic_emcs(ham, grid, ss, rng, beta, ncluster, nmetro, ntherm, nmeas, ef, mf, obs, mean_cluster);
+    } else if (kind == 8) {
+        Phi4Scalar::amp = p2;
+        Phi4Scalar ham(beta, p0, p1);
+        MARQOV::Space<std::array<float, 1>, G> ss(N);
+        for (int i = 0; i < N; ++i) {
+            const double u0 = rng.real(), u1 = rng.real();
+            ss[i][0] = (float)(std::sqrt(-2.0 * std::log(1.0 - u0)) * std::cos(2.0 * M_PI * u1));
+        }
+        auto ef = [&](MARQOV::Space<std::array<float, 1>, G>& x) { return nbrhood_energy(ham, grid, x); };
+        auto mf = [&](MARQOV::Space<std::array<float, 1>, G>& x) { return Magnetization().measure(x, grid); };
+        generic_emcs(ham, grid, ss, rng, beta, ncluster, nmetro, ntherm, nmeas, ef, mf, obs, mean_cluster);
+    } else {
+        return -1;
+    }
+    return 0;
+}

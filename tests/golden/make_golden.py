@@ -23,6 +23,10 @@ Fixtures:
                   e_obs the reference's Energy<H> observable, equal to e
                   except for Potts (its flex energy() is a stub returning 0)
                   and bond lattices (Energy ignores bnds()).
+  ref_emcs_*.npz  <e>, <|m|>, chi, U4 and the mean cluster size (each with its
+                  autocorrelation-corrected error) of the reference's own EMCS
+                  loop -- random-site order, mt19937_64, its Wolff -- for
+                  Potts, Heisenberg and phi^4.
   wolff_*.npz     cluster-size statistics of the unmodified reference Wolff
                   updates (sequential draws), for a statistical comparison
                   with the bond-keyed restatement; for the float models also
@@ -170,6 +174,22 @@ def main():
             mags.append(mm)
         save(name, beta=np.float64(beta), p0=np.float64(p0), p1=np.float64(p1), amp=np.float64(amp),
              sizes=np.array(sizes, np.int32), e=np.array(energies), m=np.array(mags))
+
+    # -- long-run statistics of the reference's own EMCS loop (random-site
+    # order, mt19937_64, reference Wolff): value and tau_int-corrected error
+    # of <e>, <|m|>, chi, U4 and the mean cluster size after 10^3 + 10^4 EMCS
+    from oracle import stats as S
+    for name, rk, dim, L, beta, ncl, nmet, kw in (
+            ("ref_emcs_potts2d_L16", 3, 2, 16, 1.0050525, 1, 1, {}),
+            ("ref_emcs_heis3d_L8", 6, 3, 8, 0.6930, 1, 5, {}),
+            ("ref_emcs_phi4_3d_L8", 8, 3, 8, 0.37, 1, 2, dict(p0=1.1, p1=1.0, p2=0.5))):
+        obs, mc = ref.emcs_generic(rk, L, dim, -1.0, beta, 11, ncl, nmet, 1000, 10000, **kw)
+        summ = S.summary(obs[:, 0], obs[:, 1], L ** dim, beta)
+        cm, ce = S.mean_err(mc)
+        save(name, kind=np.int32(rk), dim=np.int32(dim), L=np.int32(L), beta=np.float64(beta), ncluster=np.int32(ncl),
+             nmetro=np.int32(nmet), p0=np.float64(kw.get("p0", 0.0)), p1=np.float64(kw.get("p1", 0.0)),
+             p2=np.float64(kw.get("p2", 0.0)), ntherm=np.int32(1000), nmeas=np.int32(10000),
+             **{k: np.array(v) for k, v in summ.items()}, cluster=np.array([cm, ce]))
 
 
 if __name__ == "__main__":

@@ -101,7 +101,9 @@ def _symmetric(csr):
 def test_random_bond_lattice_symmetric():
     from marqov_b200 import RegularRandomBond
     lat = RegularRandomBond(6, 3, p=0.5, seed=3)
-    assert _symmetric(lat)
+    assert _symmetric(lat.to_csr())
+    for i in range(lat.size()):
+        assert lat.bnds(0, i) == lat.to_csr().bnds(0, i)
     assert set(np.unique(lat.bonds)) <= {-1, 1}
     frac = (lat.bonds == 1).mean()
     assert 0.35 < frac < 0.65

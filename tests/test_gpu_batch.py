@@ -81,6 +81,8 @@ def test_batch_csr_members_equal_single_handles():
     import marqov_b200 as M
     ms = [(M.RegularRandomBond(6, 3, 0.5, seed=s), M.Config(seed=300 + s, repid=s), M.EdwardsAndersonIsing(-1.0), 0.9)
           for s in range(3)]
+    ms.append((M.RegularRandomBond(6, 3, 0.5, seed=7).to_csr(), M.Config(seed=307, repid=7),
+               M.EdwardsAndersonIsing(-1.0), 0.9))
     ms.append((M.RandomGeometricGraph2D(500, 8.0, seed=4), M.Config(seed=9, repid=9), M.Ising(-1.0, "int8"), 0.5))
     ms.append((M.RegularHypercubic(16, 2), M.Config(seed=8, repid=8), M.Potts(3, -1.0), 1.0))
     singles = [solo(M, m) for m in ms]

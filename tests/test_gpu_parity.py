@@ -38,10 +38,12 @@ def ham_of(g):
     raise ValueError(kind)
 
 
-def lattice_of(g):
+def lattice_of(g, stencil_bonds=False):
     M = mb()
     dim, L = int(g["dim"]), int(g["L"])
     if "bonds" in g:
+        if stencil_bonds:
+            return M.BondedHypercubic(L, dim, g["bonds"])
         base = M.RegularHypercubic(L, dim).to_csr()
         return M.CSRLattice(base.row_ptr, base.col_idx, g["bonds"], base.colours)
     if int(g.get("bipartite", 0)):
@@ -70,6 +72,18 @@ def test_int_golden_bit_exact(golden, case):
         assert (obs[:, 0] == g["obs"][:, 0]).all()
         assert (c.state == g["final"]).all()
         assert c.launches > 0
+
+
+def test_ea_golden_on_the_stencil_path(golden):
+    """The EA fixture's bonds on the hypercubic stencil (one plane of +d bonds
+    per dimension) give the reference's states and energies, bit for bit."""
+    g = golden("ea3d_L8")
+    with core_for(lattice_of(g, stencil_bonds=True), ham_of(g), g["beta"], g["seed"], g["replica"]) as c:
+        assert "hypercubic" in c.describe()
+        c.state = g["init"]
+        obs, _ = c.emcs(int(g["nsweeps"]), ncluster=0, nmetro=1)
+        assert (obs[:, 0] == g["obs"][:, 0]).all() and (obs[:, 1] == g["obs"][:, 1]).all()
+        assert (c.state == g["final"]).all()
 
 
 def f32_ham_of(g):

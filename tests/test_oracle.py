@@ -220,3 +220,49 @@ def test_ref_harness_live_matches_oracle(orc):
         orc.sweep_int8(m, graph, s, 0.3, 1234, 9, 100 + t)
     ref.sweeps_int(1, graph, s2, -1.0, 0.0, 0.3, 1234, 9, 100, 25, want_obs=False)
     assert (s == s2).all()
+
+
+@pytest.mark.parametrize("case", ["ref_emcs_potts2d_L16", "ref_emcs_heis3d_L8", "ref_emcs_phi4_3d_L8"])
+def test_restatement_long_runs_match_reference(orc, golden, case):
+    """The restatement's EMCS (colour order, keyed Philox, bond-keyed clusters)
+    samples what the reference's own loop samples: <e>, <|m|>, chi, U4 and the
+    mean cluster size within 2 sigma (tau_int-corrected) over 10^4 EMCS."""
+    from oracle import stats as S
+    g = golden(case)
+    kind, dim, L, beta = int(g["kind"]), int(g["dim"]), int(g["L"]), float(g["beta"])
+    graph = orc.hypercubic(dim, L)
+    if kind == 3:
+        m, symd = O.OrcModel(kind=O.POTTS, q=3, k=-1.0), 0
+    elif kind == 6:
+        m, symd = O.OrcModel(kind=O.HEISENBERG, J=-1.0), 3
+    else:
+        m, symd = O.OrcModel(kind=O.PHI4, J=-1.0, h=float(g["p1"]) / beta, h2=float(g["p0"]) / beta,
+                             cap=float(g["p2"])), 1
+    ncl, nmet, nth, nmeas = int(g["ncluster"]), int(g["nmetro"]), int(g["ntherm"]), int(g["nmeas"])
+    s = orc.init_f32(m, graph.n, symd, 7, 0) if symd else orc.init_int8(m, graph.n, 7, 0)
+    obs, mc = [], []
+    sweep = cluster = 0
+    for t in range(nth + nmeas):
+        tot = 0
+        for _ in range(ncl):
+            tot += (orc.wolff_f32(m, graph, s, symd, beta, 7, 0, cluster) if symd
+                    else orc.wolff_int8(m, graph, s, beta, 7, 0, cluster))
+            cluster += 1
+        for _ in range(nmet):
+            if symd:
+                orc.sweep_f32(m, graph, s, symd, beta, 7, 0, sweep)
+            else:
+                orc.sweep_int8(m, graph, s, beta, 7, 0, sweep)
+            sweep += 1
+        if t >= nth:
+            obs.append(orc.measure_f32(m, graph, s, symd) if symd else orc.measure_int8(m, graph, s))
+            mc.append(tot / ncl)
+    obs = np.array(obs)
+    mine = S.summary(obs[:, 0], obs[:, 1], graph.n, beta)
+    for k in ("e", "m", "chi", "u4"):
+        a, da = mine[k]
+        b, db = g[k]
+        assert abs(a - b) < 2 * np.hypot(da, db), (case, k, a, da, b, db)
+    m1, s1 = S.mean_err(mc)
+    m2, s2 = g["cluster"]
+    assert abs(m1 - m2) < 2 * np.hypot(s1, s2), (case, m1, s1, m2, s2)
