@@ -119,7 +119,10 @@ typedef struct mqv_lattice_desc {
 
 /* Run flags. */
 enum {
-    MQV_FLAG_PER_COLOUR = 1  /* always use one launch per colour class (no fused two-colour tiles) */
+    MQV_FLAG_PER_COLOUR = 1,  /* always use one launch per colour class (no fused two-colour tiles) */
+    MQV_FLAG_NO_RESIDENT = 2  /* never run a small int8 lattice (<= 32768 sites) as one resident CTA that
+                                 keeps the state in shared memory for a whole chunk of EMCS; launch
+                                 per cluster, colour and measurement instead (same results) */
 };
 
 typedef struct mqv_run_params {
@@ -177,6 +180,16 @@ MQV_API mqv_status mqv_set_counters(mqv_sim* sim, uint64_t sweep, uint64_t clust
 
 /* nsweeps colour-ordered Metropolis sweeps (asynchronous on the handle's stream). */
 MQV_API mqv_status mqv_metropolis(mqv_sim* sim, int32_t nsweeps);
+/* Cluster algorithms (same clusters either way, the seed's component of the
+ * bonds activated on their keyed draws): growth by one CTA, breadth first
+ * (a barrier per level of the cluster's depth), or labelling of the
+ * activated-bond components in a fixed number of whole-lattice passes. */
+enum { MQV_WOLFF_AUTO = 0, MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
+/* No counterpart in the reference.  The cluster algorithm of a handle:
+ * MQV_WOLFF_AUTO (default) labels int8 lattices of at least 2^18 sites and
+ * grows the others breadth first; lattices on the resident path
+ * (MQV_FLAG_NO_RESIDENT unset, int8, <= 32768 sites) label in shared memory. */
+MQV_API mqv_status mqv_set_wolff(mqv_sim* sim, int32_t algorithm);
 /* nclusters Wolff clusters; sizes (host, may be NULL) receives each size
  * (synchronises when sizes != NULL). */
 MQV_API mqv_status mqv_wolff(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
@@ -251,15 +264,15 @@ MQV_API mqv_status mqv_batch_destroy(mqv_batch* batch);
  * the batch and bound to its stream. */
 MQV_API mqv_status mqv_batch_member(mqv_batch* batch, int32_t i, mqv_sim** sim);
 MQV_API mqv_status mqv_batch_init_state(mqv_batch* batch);
-/* Cluster algorithms of a batch (same clusters either way): growth by one
- * CTA per member, breadth first; or labelling of the activated-bond
- * components of all members in a fixed number of whole-lattice passes
- * (cost independent of cluster depth; pays for percolating clusters on large
- * lattices).  The default, MQV_WOLFF_AUTO, times every chunk of EMCS (up
+/* Cluster algorithms of a batch (MQV_WOLFF_*; same clusters either way):
+ * growth by one CTA per member, breadth first; or labelling of the
+ * activated-bond components of all members in a fixed number of
+ * whole-lattice passes (cost independent of cluster depth; pays for
+ * percolating clusters on large lattices).  The default, MQV_WOLFF_AUTO,
+ * times every chunk of EMCS (up
  * to 256 between host synchronisations), tries the algorithm not in use on a
  * few EMCS at the start of a chunk when it has no estimate or an old one, and
  * uses the faster estimate: the chain is the same whichever runs. */
-enum { MQV_WOLFF_AUTO = 0, MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
 MQV_API mqv_status mqv_batch_set_wolff(mqv_batch* batch, int32_t algorithm);
 /* The algorithm in use: MQV_WOLFF_BFS or MQV_WOLFF_LABEL, or MQV_WOLFF_AUTO
  * while the automatic choice has not been timed yet. */

@@ -32,6 +32,7 @@ MODEL_ISING, MODEL_ISING_EMBED, MODEL_POTTS, MODEL_BLUME_CAPEL, MODEL_EA, MODEL_
 PROPOSAL_DEFAULT, PROPOSAL_SMALL_CAP = 0, 1
 LATTICE_HYPERCUBIC, LATTICE_CSR, LATTICE_BIPARTITE = 1, 2, 3
 FLAG_PER_COLOUR = 1
+FLAG_NO_RESIDENT = 2
 WOLFF_AUTO, WOLFF_BFS, WOLFF_LABEL = 0, 1, 2
 
 
@@ -76,6 +77,7 @@ SIGNATURES = {
     "mqv_create": (C.c_int32, [C.POINTER(ModelDesc), C.POINTER(LatticeDesc), C.POINTER(RunParams),
                                C.POINTER(_vp)]),
     "mqv_destroy": (C.c_int32, [_vp]),
+    "mqv_set_wolff": (C.c_int32, [_vp, C.c_int32]),
     "mqv_set_stream": (C.c_int32, [_vp, _vp]),
     "mqv_get_stream": (C.c_int32, [_vp, C.POINTER(_vp)]),
     "mqv_set_beta": (C.c_int32, [_vp, C.c_double]),

@@ -34,6 +34,9 @@ class Config:
     device: int = 0
     # force one launch per colour class (no fused two-colour tiles)
     per_colour: bool = False
+    # small int8 lattices (<= 32768 sites) run whole chunks of EMCS in one
+    # CTA's shared memory; False forces the launch-per-step path (same results)
+    resident: bool = True
 
     def setid(self, i):
         self.id = i
@@ -103,7 +106,8 @@ class Core:
         md = ham.desc(self.beta)
         ld = lattice.desc()
         rp = L.RunParams(beta=self.beta, seed=seed & (2 ** 64 - 1), replica=replica, device=int(config.device),
-                         flags=L.FLAG_PER_COLOUR if config.per_colour else 0)
+                         flags=(L.FLAG_PER_COLOUR if config.per_colour else 0) |
+                         (0 if config.resident else L.FLAG_NO_RESIDENT))
         L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
         self._seed, self._replica = seed, replica
         if restore is not None:
@@ -219,6 +223,12 @@ class Core:
         L.check(self._lib.mqv_wolff(self._h, int(nclusters), sizes.ctypes.data))
         return sizes
 
+    def set_wolff(self, algorithm: str):
+        """Cluster algorithm of this lattice: "auto" (labelling for int8 lattices
+        of >= 2^18 sites), "bfs" or "label"; the clusters are the same."""
+        code = {"auto": L.WOLFF_AUTO, "bfs": L.WOLFF_BFS, "label": L.WOLFF_LABEL}[algorithm]
+        L.check(self._lib.mqv_set_wolff(self._h, code))
+
     def measure(self) -> tuple[float, float, float, float]:
         o = L.Obs()
         L.check(self._lib.mqv_measure(self._h, C.byref(o)))
@@ -305,7 +315,8 @@ class Batch:
             specs[i].model = ham.desc(float(beta))
             specs[i].lattice = lat.desc()
             specs[i].params = L.RunParams(beta=float(beta), seed=int(cfg.seed) & (2 ** 64 - 1),
-                                          replica=int(cfg.repid), device=int(cfg.device), flags=0)
+                                          replica=int(cfg.repid), device=int(cfg.device),
+                                          flags=0 if cfg.resident else L.FLAG_NO_RESIDENT)
         L.check(lib.mqv_batch_create(specs, len(members), C.byref(self._h)))
         L.check(lib.mqv_batch_set_graph_steps(self._h, int(graph_steps)))
         self.n = len(members)

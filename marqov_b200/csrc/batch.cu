@@ -85,6 +85,7 @@ __global__ void __launch_bounds__(1024) batch_wolff(const BatchRep* __restrict__
                                                     int32_t* __restrict__ csize, int nrep)
 {
     const BatchRep& R = reps[blockIdx.x];
+    if (R.resident) return;  // its clusters are grown by batch_resident
     const uint32_t e = ctr->e, slot = e - ctr->ebase;
     const uint32_t serial = R.cluster0 + e * (uint32_t)ncluster + (uint32_t)c;
     int32_t* out = csize + ((size_t)slot * ncluster + c) * nrep + blockIdx.x;
@@ -240,6 +241,7 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
         if (b.wolff_ccl) {
             CclSeed* sd = (CclSeed*)b.ccl_seeds;
             const unsigned gb = (unsigned)b.site_blocks;
+            if (b.site_blocks == 0) continue;  // every member is resident
             ccl_seed<F32><<<(b.nrep + 127) / 128, 128, 0, st>>>(b.reps, b.ctr, ncluster, c, sd, b.csize, b.nrep);
             ccl_local<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
                                                               sd, b.ctr, ncluster, c);
@@ -259,7 +261,8 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
                 b.reps, b.prefix + (size_t)colour * (b.nrep + 1), b.block_rep + b.block_off[colour], b.cbegin,
                 b.ccount, b.ncol, b.total[colour], colour, b.ctr, nmetro, j);
         }
-    batch_measure<F32><<<b.meas_blocks, 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep, b.meas_prefix, b.meas_rep);
+    if (b.meas_blocks > 0)
+        batch_measure<F32><<<b.meas_blocks, 256, 0, st>>>(b.reps, b.ctr, b.acc, b.nrep, b.meas_prefix, b.meas_rep);
     batch_tick<<<1, 1, 0, st>>>(b.ctr);
 }
 

@@ -20,6 +20,7 @@ struct BatchRep {
     int32_t* queue;
     const unsigned long long* cuts;  // int8: the member's Metropolis cut table
     int D;                           // int8: its maximum degree
+    int resident;                    // runs in one CTA's shared memory (batch_resident), not in the graphs
 };
 
 // Sites of a member's lattice.
@@ -73,6 +74,10 @@ struct BatchLaunch {
 };
 
 cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro);
+// EMCS e0 .. e0 + count - 1 of the resident members order[0 .. nres) (the
+// largest with max_n sites), measurement slots from slot0 (smem_emcs.cu)
+cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, int64_t max_n,
+                                  uint32_t e0, int slot0, int count, int ncluster, int nmetro, int device);
 cudaError_t batch_launch_chunk_start(const BatchLaunch& b, cudaStream_t st, uint32_t e);
 cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nslots, double* out);
 // raw sums of the chunk's slots -> samples[r][e0 + slot][4] (n_total EMCS per member)
@@ -87,7 +92,9 @@ inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int 
 {
     int live = 0;
     for (int c = 0; c < b.ncol; ++c) live += b.total[c] > 0;
-    return (uint64_t)ncluster * (b.wolff_ccl ? 5ull : 1ull) + (uint64_t)nmetro * (uint64_t)live + 2ull;
+    const uint64_t ccl = b.site_blocks > 0 ? 5ull : 1ull;
+    return (uint64_t)ncluster * (b.wolff_ccl ? ccl : 1ull) + (uint64_t)nmetro * (uint64_t)live +
+           (b.meas_blocks > 0 ? 2ull : 1ull);
 }
 
 }  // namespace mqv

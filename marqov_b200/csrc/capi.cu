@@ -33,11 +33,15 @@ cudaError_t launch_metropolis_f32(Sim* s, int slot);
 cudaError_t launch_measure_f32(Sim* s, int slot);
 cudaError_t launch_finalize_f32(Sim* s, int nslots, double* d_out);
 cudaError_t launch_wolff_f32(Sim* s, int slot);
+cudaError_t launch_wolff_label(Sim* s, int slot);
 int64_t wolff_noalloc_max_sites();
 int wolff_noalloc_max_clusters();
 cudaError_t wolff_noalloc_scratch(int device, uint32_t** out);
 cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot);
 const int32_t* wolff_noalloc_sizes(const uint32_t* scratch);
+bool resident_fits(const Sim* s);
+cudaError_t launch_emcs_resident(Sim* s, int n_emcs, int ncluster, int nmetro, bool measure, long long* acc,
+                                 int32_t* csize);
 cudaError_t launch_acc_to_samples(const long long* acc, int is_f32, int nslots, double* out, cudaStream_t st);
 cudaError_t launch_phi4_fdt(const double* samples, int nrep, int nsamp, double invN, const double* beta,
                             const double* lam, double mass, double* obs, double* jac, const double* gout,
@@ -103,7 +107,8 @@ static void free_sim(Sim* s)
     if (s->stream) cudaStreamSynchronize(s->stream);
     for (void* p : {s->state[0], s->state[1], (void*)s->d_rp, (void*)s->d_ci, (void*)s->d_bonds, (void*)s->d_order,
                     (void*)s->d_acc, (void*)s->d_obs, (void*)s->d_visited, (void*)s->d_queue, (void*)s->d_csize,
-                    (void*)s->d_status, (void*)s->d_counter, (void*)s->d_cuts})
+                    (void*)s->d_status, (void*)s->d_counter, (void*)s->d_cuts, (void*)s->d_rep1, (void*)s->d_ctr1,
+                    s->d_seed1, (void*)s->d_sprefix1, (void*)s->d_sbrep1})
         if (p) cudaFree(p);
     if (s->own_stream && s->stream) cudaStreamDestroy(s->stream);
     delete s;
@@ -347,11 +352,24 @@ static mqv_status launch_sweep(Sim* s, int slot)
     MQV_CK(s->is_f32 ? launch_metropolis_f32(s, slot) : launch_metropolis_int8(s, slot));
     return MQV_OK;
 }
+// Clusters by labelling (a fixed number of whole-lattice passes) or by one
+// CTA's breadth-first growth (one barrier per level of the cluster's depth):
+// MQV_WOLFF_AUTO labels int8 lattices of at least kLabelMinSites sites, where
+// critical clusters are thousands of levels deep; both give the same cluster.
+constexpr int64_t kLabelMinSites = (int64_t)1 << 18;
+static bool cluster_by_label(const Sim* s)
+{
+    if (s->wolff_algo == MQV_WOLFF_LABEL) return true;
+    if (s->wolff_algo == MQV_WOLFF_BFS) return false;
+    return !s->is_f32 && s->n >= kLabelMinSites;
+}
+
 static mqv_status launch_cluster(Sim* s, int slot)
 {
     mqv_status st = ensure_wolff(s);
     if (st) return st;
-    MQV_CK(s->is_f32 ? launch_wolff_f32(s, slot) : launch_wolff_int8(s, slot));
+    if (cluster_by_label(s)) MQV_CK(launch_wolff_label(s, slot));
+    else MQV_CK(s->is_f32 ? launch_wolff_f32(s, slot) : launch_wolff_int8(s, slot));
     return MQV_OK;
 }
 
@@ -367,6 +385,9 @@ static mqv_status check_wolff_supported(Sim* s)
         return fail(MQV_ERR_UNSUPPORTED_TERM, "no Wolff embedding for XXZ");
     return MQV_OK;
 }
+
+// EMCS of this handle run on the resident path (smem_emcs.cu)?
+static bool use_resident(const Sim* s) { return !(s->flags & MQV_FLAG_NO_RESIDENT) && resident_fits(s); }
 
 }  // namespace mqv
 
@@ -425,6 +446,7 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
     mqv_status st = lower_model(s, model, lattice->bonds != nullptr);
     if (st) return bail(st);
     s->md.beta = params->beta;
+    s->flags = params->flags;
     s->seed = params->seed;
     s->replica = params->replica;
     if (cudaStreamCreateWithFlags(&s->stream, cudaStreamNonBlocking) != cudaSuccess) {
@@ -692,9 +714,13 @@ MQV_API mqv_status mqv_wolff(mqv_sim* h, int32_t nclusters, int32_t* sizes)
         const int chunk = std::min(nclusters - done, 65536);
         st = ensure_cslots(s, chunk);
         if (st) return st;
-        for (int c = 0; c < chunk; ++c) {
-            st = launch_cluster(s, c);
-            if (st) return st;
+        if (use_resident(s)) {
+            MQV_CK(launch_emcs_resident(s, chunk, 1, 0, false, nullptr, s->d_csize));
+        } else {
+            for (int c = 0; c < chunk; ++c) {
+                st = launch_cluster(s, c);
+                if (st) return st;
+            }
         }
         if (sizes) {
             MQV_CK(cudaMemcpyAsync(sizes + done, s->d_csize, sizeof(int32_t) * chunk, cudaMemcpyDeviceToHost, s->stream));
@@ -760,18 +786,23 @@ MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_
             if (st) return st;
         }
         MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch, s->stream));
-        for (int e = 0; e < ch; ++e) {
-            for (int c = 0; c < ncluster; ++c) {
-                st = launch_cluster(s, e * ncluster + c);
-                if (st) return st;
-            }
-            for (int j = 0; j < nmetro; ++j) {
-                st = launch_sweep(s, j == nmetro - 1 ? e : -1);
-                if (st) return st;
-            }
-            if (nmetro == 0) {
-                st = launch_measure(s, e);
-                if (st) return st;
+        if (use_resident(s)) {
+            MQV_CK(ensure_cuts(s));
+            MQV_CK(launch_emcs_resident(s, ch, ncluster, nmetro, true, s->d_acc, s->d_csize));
+        } else {
+            for (int e = 0; e < ch; ++e) {
+                for (int c = 0; c < ncluster; ++c) {
+                    st = launch_cluster(s, e * ncluster + c);
+                    if (st) return st;
+                }
+                for (int j = 0; j < nmetro; ++j) {
+                    st = launch_sweep(s, j == nmetro - 1 ? e : -1);
+                    if (st) return st;
+                }
+                if (nmetro == 0) {
+                    st = launch_measure(s, e);
+                    if (st) return st;
+                }
             }
         }
         st = launch_finalize(s, ch);
@@ -819,18 +850,23 @@ MQV_API mqv_status mqv_emcs_samples(mqv_sim* h, int32_t n_emcs, int32_t ncluster
             if (st) return st;
         }
         MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch, s->stream));
-        for (int e = 0; e < ch; ++e) {
-            for (int c = 0; c < ncluster; ++c) {
-                st = launch_cluster(s, e * ncluster + c);
-                if (st) return st;
-            }
-            for (int j = 0; j < nmetro; ++j) {
-                st = launch_sweep(s, j == nmetro - 1 ? e : -1);
-                if (st) return st;
-            }
-            if (nmetro == 0) {
-                st = launch_measure(s, e);
-                if (st) return st;
+        if (use_resident(s)) {
+            MQV_CK(ensure_cuts(s));
+            MQV_CK(launch_emcs_resident(s, ch, ncluster, nmetro, true, s->d_acc, s->d_csize));
+        } else {
+            for (int e = 0; e < ch; ++e) {
+                for (int c = 0; c < ncluster; ++c) {
+                    st = launch_cluster(s, e * ncluster + c);
+                    if (st) return st;
+                }
+                for (int j = 0; j < nmetro; ++j) {
+                    st = launch_sweep(s, j == nmetro - 1 ? e : -1);
+                    if (st) return st;
+                }
+                if (nmetro == 0) {
+                    st = launch_measure(s, e);
+                    if (st) return st;
+                }
             }
         }
         MQV_CK(launch_acc_to_samples(s->d_acc, s->is_f32 ? 1 : 0, ch, d_samples + 4 * (size_t)done, s->stream));
@@ -882,10 +918,21 @@ MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
     if (!s || !buf || len == 0) return fail(MQV_ERR_INVALID_ARG, "bad arguments");
     char cfg[96] = "";
     if (s->fused_ising2d) ising2d_config_name(s, cfg, sizeof(cfg));
-    std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s", s->md.kind,
+    std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s clusters=%s", s->md.kind,
                   s->lat_kind == MQV_LATTICE_HYPERCUBIC ? (s->termsel ? "bipartite" : "hypercubic") : "csr", (long long)s->n,
-                  s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8"),
-                  cfg[0] ? " kernel=" : "", cfg);
+                  use_resident(s) ? "resident-smem"
+                                  : (s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8")),
+                  cfg[0] ? " kernel=" : "", cfg,
+                  use_resident(s) ? "label-smem" : (cluster_by_label(s) ? "label" : "bfs"));
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_wolff(mqv_sim* h, int32_t algorithm)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (algorithm < MQV_WOLFF_AUTO || algorithm > MQV_WOLFF_LABEL) return fail(MQV_ERR_INVALID_ARG, "unknown algorithm");
+    s->wolff_algo = algorithm;
     return MQV_OK;
 }
 
@@ -947,6 +994,13 @@ struct Batch {
     int32_t* d_block_rep = nullptr;
     int32_t* d_cbegin = nullptr;
     int32_t* d_ccount = nullptr;
+    // members run by batch_resident (one CTA each, state in shared memory):
+    // two classes by size (<= kResSmall sites: several CTAs per SM), each
+    // listed largest first; resident[r] marks them
+    std::vector<char> resident;
+    int32_t* d_res_order = nullptr;
+    int nres[2] = {0, 0};
+    int64_t res_maxn[2] = {0, 0};
     int64_t* d_site_prefix = nullptr;
     int32_t* d_site_block_rep = nullptr;
     int32_t* d_meas_prefix = nullptr;
@@ -995,7 +1049,7 @@ static void free_batch(Batch* b)
         if (e) cudaEventDestroy(e);
     for (Sim* s : b->sims) free_sim(s);
     for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin,
-                    (void*)b->d_ccount, (void*)b->d_ctr,
+                    (void*)b->d_ccount, (void*)b->d_res_order, (void*)b->d_ctr,
                     (void*)b->d_acc, (void*)b->d_obs, (void*)b->d_csize, (void*)b->d_site_prefix,
                     (void*)b->d_site_block_rep, (void*)b->d_meas_prefix, (void*)b->d_meas_rep, b->d_ccl_seeds})
         if (p) cudaFree(p);
@@ -1104,6 +1158,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         r.queue = s->d_queue;
         r.cuts = s->d_cuts;
         r.D = s->max_degree;
+        r.resident = b->resident[(size_t)i];
     }
     MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
                            b->stream));
@@ -1150,14 +1205,23 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
     }
     if (adapt && !b->ev[0])
         for (auto& e : b->ev) MQV_CK(cudaEventCreate(&e));
+    int done_run = 0;  // first EMCS of the chunk in progress
     uint64_t per_emcs[2];
     for (int w = 0; w < 2; ++w) {
         BatchLaunch l = b->L;
         l.wolff_ccl = w;
         per_emcs[w] = batch_launches_per_emcs(l, ncluster, nmetro);
     }
-    // `count` EMCS with the graphs of algorithm w
-    auto launch_emcs = [&](int w, int count) -> mqv_status {
+    // `count` EMCS with the graphs of algorithm w, after the same EMCS of the
+    // resident members (chunk positions from k0; members are independent)
+    auto launch_emcs = [&](int w, int count, int k0) -> mqv_status {
+        for (int cls = 0; cls < 2; ++cls) {
+            if (!b->nres[cls]) continue;
+            MQV_CK(batch_launch_resident(b->L, b->stream, b->d_res_order + (cls ? b->nres[0] : 0), b->nres[cls],
+                                         b->res_maxn[cls], (uint32_t)(done_run + k0), k0, count, ncluster, nmetro,
+                                         b->device));
+            b->launches++;
+        }
         int j = 0;
         if (K > 1)
             for (; j + K <= count; j += K) MQV_CK(cudaGraphLaunch(b->g_many[w], b->stream));
@@ -1179,6 +1243,8 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
     int done = 0;
     while (done < n_emcs) {
         const int ch = std::min(n_emcs - done, CH);
+        done_run = done;
+        done_run = done;
         MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
         MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
         b->launches++;
@@ -1196,7 +1262,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
             while (k < stop) {
                 int run = stop - k;
                 if (pt) run = std::min(run, pt->interval - (done + k) % pt->interval);
-                mqv_status s2 = launch_emcs(w, run);
+                mqv_status s2 = launch_emcs(w, run, k);
                 if (s2) return s2;
                 k += run;
                 s2 = exchange_after(done + k);
@@ -1348,9 +1414,29 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         st = mqv_set_stream(h, b->stream);
         if (st) return bail(st);
     }
-    // per-colour work: colour c concatenates every member's colour-c sites,
-    // each member's count padded to whole warp blocks of kAccSites, so that a
-    // warp's block lies in one member (batch_metro)
+    // resident members: int8 stencil lattices that fit one CTA's shared
+    // memory, unless their spec asks for the launch path
+    b->resident.assign((size_t)n, 0);
+    std::vector<int32_t> res_order[2];
+    for (int r = 0; r < n; ++r) {
+        const Sim* s = b->sims[(size_t)r];
+        if (!(specs[r].params.flags & MQV_FLAG_NO_RESIDENT) && resident_fits(s)) {
+            b->resident[(size_t)r] = 1;
+            res_order[s->n > kResSmall ? 1 : 0].push_back(r);
+        }
+    }
+    for (int k = 0; k < 2; ++k) {
+        std::stable_sort(res_order[k].begin(), res_order[k].end(),
+                         [&](int32_t x, int32_t y) { return b->sims[(size_t)x]->n > b->sims[(size_t)y]->n; });
+        b->nres[k] = (int)res_order[k].size();
+        b->res_maxn[k] = res_order[k].empty() ? 0 : b->sims[(size_t)res_order[k][0]]->n;
+    }
+    std::vector<int32_t> res_all(res_order[0]);
+    res_all.insert(res_all.end(), res_order[1].begin(), res_order[1].end());
+    // per-colour work: colour c concatenates every graph member's colour-c
+    // sites (resident members contribute none), each member's count padded
+    // to whole warp blocks of kAccSites, so that a warp's block lies in one
+    // member (batch_metro)
     int ncol = 0;
     for (Sim* s : b->sims) ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
     std::vector<int64_t> prefix((size_t)ncol * (n + 1), 0);
@@ -1368,6 +1454,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
                 cnt = s->colour_ptr[(size_t)c + 1] - s->colour_ptr[(size_t)c];
                 cbegin[(size_t)r * ncol + c] = s->colour_ptr[(size_t)c];
             }
+            if (b->resident[(size_t)r]) cnt = 0;
             ccount[(size_t)r * ncol + c] = (int32_t)cnt;
             pf[r + 1] = pf[r] + (cnt + kAccSites - 1) / kAccSites * kAccSites;
         }
@@ -1385,7 +1472,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     if (brep.empty()) brep.push_back(0);
     // site-level work of the labelling Wolff
     std::vector<int64_t> sprefix((size_t)n + 1, 0);
-    for (int r = 0; r < n; ++r) sprefix[r + 1] = sprefix[r] + b->sims[(size_t)r]->n;
+    for (int r = 0; r < n; ++r) sprefix[r + 1] = sprefix[r] + (b->resident[(size_t)r] ? 0 : b->sims[(size_t)r]->n);
     const int64_t sblocks = (sprefix[n] + kBatchMetroThreads - 1) / kBatchMetroThreads;
     if (sblocks >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
     std::vector<int32_t> sbrep((size_t)std::max<int64_t>(sblocks, 1), 0);
@@ -1401,14 +1488,18 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     // measurement CTAs: about 4096 sites each, at least one per member
     std::vector<int32_t> mprefix((size_t)n + 1, 0), mrep;
     for (int r = 0; r < n; ++r) {
-        const int64_t parts = std::max<int64_t>(1, (b->sims[(size_t)r]->n + 4095) / 4096);
+        const int64_t parts =
+            b->resident[(size_t)r] ? 0 : std::max<int64_t>(1, (b->sims[(size_t)r]->n + 4095) / 4096);
         if (mprefix[(size_t)r] + parts >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
         mprefix[(size_t)r + 1] = mprefix[(size_t)r] + (int32_t)parts;
         for (int64_t k = 0; k < parts; ++k) mrep.push_back(r);
     }
     mqv_status st = dcopy((void**)&b->d_prefix, prefix.data(), sizeof(int64_t) * prefix.size());
     if (!st) st = dcopy((void**)&b->d_meas_prefix, mprefix.data(), sizeof(int32_t) * mprefix.size());
+    if (mrep.empty()) mrep.push_back(0);
+    if (res_all.empty()) res_all.push_back(0);
     if (!st) st = dcopy((void**)&b->d_meas_rep, mrep.data(), sizeof(int32_t) * mrep.size());
+    if (!st) st = dcopy((void**)&b->d_res_order, res_all.data(), sizeof(int32_t) * res_all.size());
     if (!st) st = dcopy((void**)&b->d_block_rep, brep.data(), sizeof(int32_t) * brep.size());
     if (!st) st = dcopy((void**)&b->d_cbegin, cbegin.data(), sizeof(int32_t) * std::max<size_t>(cbegin.size(), 1));
     if (!st) st = dcopy((void**)&b->d_ccount, ccount.data(), sizeof(int32_t) * std::max<size_t>(ccount.size(), 1));

@@ -124,12 +124,15 @@ MQV_HD bool accept_top_or_fine(uint64_t cut, uint32_t top, Key key, uint32_t sit
 constexpr int kAccRuns = 8;
 constexpr int kAccTab = 4 * kAccRuns;  // uint4 per warp: [run][parity][half]
 constexpr int kAccSites = 32 * kAccRuns;  // sites of one colour in a block (checkerboard)
-__device__ __forceinline__ void accept_tab_fill(uint4* tab, uint32_t run0, Key key, uint32_t sweep, uint32_t replica)
+// (nruns < kAccRuns: a block of nruns runs, drawn by the first 4 nruns lanes.)
+__device__ __forceinline__ void accept_tab_fill(uint4* tab, uint32_t run0, Key key, uint32_t sweep, uint32_t replica,
+                                                uint32_t nruns = kAccRuns)
 {
     const uint32_t lane = threadIdx.x & 31u;
     const uint32_t c3 = (kAccept << 24) | (replica & 0xFFFFFFu);
     __syncwarp();  // the previous block's readers are done
-    tab[lane] = philox(((run0 + (lane >> 2)) << 1) | ((lane >> 1) & 1u), sweep, lane & 1u, c3, key);
+    if (lane < 4u * nruns)
+        tab[lane] = philox(((run0 + (lane >> 2)) << 1) | ((lane >> 1) & 1u), sweep, lane & 1u, c3, key);
     __syncwarp();
 }
 __device__ __forceinline__ uint32_t accept_top8_tab(const uint4* tab, uint32_t run0, uint32_t site)

@@ -138,6 +138,15 @@ std::vector<unsigned long long> int8_cut_table(const ModelDev& md, int D);
 // Activation rule of an int8 model (host side, wolff.cu).
 WolffDev wolff_int8_params(const ModelDev& md);
 
+// The resident path (smem_emcs.cu): int8 lattices of at most this many
+// sites run whole chunks of EMCS in the shared memory of one CTA.
+constexpr int64_t kResidentMaxSites = 65536;
+// batches launch their resident members in two classes, up to this many
+// sites (several CTAs per SM) and above
+constexpr int64_t kResSmall = 16384;
+struct Sim;
+bool resident_fits(const Sim* s);
+
 struct Sim;
 // Smallest u53 rejected by update_accepted<pref>(dE, beta, .) (2^53: all accepted).
 unsigned long long accept_cut(int pref, double dE, double beta);
@@ -184,6 +193,7 @@ struct Sim {
     double thr_J = 0, thr_beta = -1;  // (J, beta) the cached 2D thresholds belong to
     unsigned long long thr_cut[5] = {};
     int sweep_cfg = -1;  // autotuned fused-sweep configuration (-1: not chosen yet)
+    uint32_t flags = 0;  // MQV_FLAG_* of the run parameters
     // int8 models: u53 cut of every possible dE (int8_cut_table), on the device
     unsigned long long* d_cuts = nullptr;
     int n_cuts = 0;
@@ -197,6 +207,14 @@ struct Sim {
     int32_t* d_queue = nullptr;     // n entries
     int32_t* d_csize = nullptr;     // cluster sizes, nslots_c entries
     int nslots_c = 0;
+    // clusters of this lattice: MQV_WOLFF_AUTO (by size), _BFS or _LABEL, and
+    // the one-member tables of the labelling kernels (wolff.cu)
+    int wolff_algo = 0;
+    struct BatchRep* d_rep1 = nullptr;
+    struct BatchCtr* d_ctr1 = nullptr;
+    void* d_seed1 = nullptr;
+    int64_t* d_sprefix1 = nullptr;
+    int32_t* d_sbrep1 = nullptr;
     uint64_t launches = 0;
 };
 

@@ -1,0 +1,298 @@
+// Elementary Monte Carlo steps of small int8 lattices held in the shared
+// memory of one CTA each, for sm_100a.
+//
+// On a lattice of a few thousand sites (the 2D Ising L = 64 parity run) a
+// launch per cluster, per colour and per measurement costs more than the
+// work, and a breadth-first cluster pays a CTA barrier per level of its
+// depth.  Here one CTA loads a lattice's state once and runs a whole chunk of
+// EMCS (EMCS<H,L>::move, src/libmarqov/emcs.h:69-109: ncluster Wolff
+// clusters, then nmetro sweeps, then the measurement) before writing it back:
+//   * each cluster by connected-component labelling in shared memory: the
+//     seed and its new state from the WOLFF_SEED substream (the breadth-first
+//     kernel's draws), every bond between two sites in the seed's old state
+//     tested once on its keyed draw (lower id, cluster serial, upper id),
+//     union-find with compare-and-swap hooking on 16-bit parent indices, then
+//     the seed's component flipped -- the same cluster as the breadth-first
+//     growth (the cluster is the seed's component of activated bonds,
+//     whatever the order) at a cost independent of the cluster's depth;
+//   * each sweep as the per-colour kernels do it (int8_site on the same
+//     keyed words, the warps' acceptance bytes shared per block of runs);
+//   * the measurement accumulators of every EMCS, as measure_int8.
+// Results equal the per-launch path bit for bit.  A single handle runs one
+// CTA (emcs_resident); a batch runs one CTA per small member
+// (batch_resident), members being independent.
+#include <cuda_runtime.h>
+
+#include "batch.h"
+#include "int8_site.cuh"
+#include "wolff_int8.cuh"
+
+namespace mqv {
+
+constexpr int kResThreads = 512;
+constexpr int kResWarps = kResThreads / 32;
+
+struct ResidentRun {
+    ModelDev m;
+    StencilDev st;  // the lattice in its global layout (split rows or not)
+    WolffDev w;
+    Key key;
+    uint32_t replica, sweep0, cluster0;  // counters of the chunk's first EMCS
+    int n_emcs, ncluster, nmetro, D, runs;
+    const unsigned long long* cuts;
+    int8_t* state;      // global state, read at the start and written at the end
+    long long* acc;     // measurement accumulators of the first EMCS (zeroed), or NULL
+    int64_t acc_e;      // stride between EMCS (long longs)
+    int32_t* csize;     // cluster size of the first cluster
+    int64_t csize_e;    // stride between EMCS
+    int64_t csize_c;    // stride between the clusters of one EMCS
+};
+
+// shared memory: the warps' acceptance tables, 16-bit parents, candidate bits, state
+__host__ __device__ inline size_t resident_smem_bytes(int64_t n)
+{
+    const int64_t words = (n + 31) / 32;
+    return (size_t)kResWarps * kAccTab * 16 + (size_t)((2 * n + 15) & ~15ll) + (size_t)words * 4 +
+           (size_t)((n + 15) & ~15ll);
+}
+
+// union-find on 16-bit parent indices (path halving; hooks by CAS, larger root under smaller)
+__device__ __forceinline__ int rfind(volatile unsigned short* p, int x)
+{
+    while (true) {
+        const int px = p[x];
+        if (px == x) return x;
+        const int gp = p[px];
+        if (gp != px) p[x] = (unsigned short)gp;
+        x = gp;
+    }
+}
+__device__ __forceinline__ void runite(volatile unsigned short* p, int a, int b)
+{
+    while (true) {
+        a = rfind(p, a);
+        b = rfind(p, b);
+        if (a == b) return;
+        if (a < b) {
+            const int t = a;
+            a = b;
+            b = t;
+        }
+        if (atomicCAS((unsigned short*)p + a, (unsigned short)a, (unsigned short)b) == (unsigned short)a) return;
+    }
+}
+
+__device__ void resident_run(const ResidentRun& R, unsigned char* smem)
+{
+    __shared__ int s_rsite, s_val, s_newq, s_root, s_size;
+    const int64_t n = R.st.n;
+    const int64_t words = (n + 31) / 32;
+    uint4* tab = reinterpret_cast<uint4*>(smem) + (threadIdx.x >> 5) * kAccTab;
+    unsigned char* p = smem + (size_t)kResWarps * kAccTab * 16;
+    volatile unsigned short* par = reinterpret_cast<unsigned short*>(p);
+    p += (size_t)((2 * n + 15) & ~15ll);
+    uint32_t* cand = reinterpret_cast<uint32_t*>(p);
+    p += (size_t)words * 4;
+    int8_t* s = reinterpret_cast<int8_t*>(p);
+    StencilDev lst = R.st;
+    lst.split = 0;  // site order in shared memory
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int64_t i = tid; i < n; i += kResThreads) s[i] = R.state[R.st.addr(i)];
+    __syncthreads();
+    const uint32_t tgs = tag(kWolffSeed, R.replica), tgb = tag(kWolffBond, R.replica);
+    for (int e = 0; e < R.n_emcs; ++e) {
+        for (int c = 0; c < R.ncluster; ++c) {
+            const uint32_t serial = R.cluster0 + (uint32_t)(e * R.ncluster + c);
+            if (tid == 0) {
+                int val, newq;
+                s_rsite = (int)wolff_int8_seed(R.w, lst, s, R.key, serial, tgs, val, newq);
+                s_val = val;
+                s_newq = newq;
+                s_size = 0;
+            }
+            __syncthreads();
+            const int val = s_val;
+            // candidates: sites in the seed's old state, each its own root
+            for (int64_t wd = tid; wd < words; wd += kResThreads) {
+                uint32_t bits = 0;
+                for (int b = 0; b < 32; ++b) {
+                    const int64_t i = wd * 32 + b;
+                    if (i < n && s[i] == val) {
+                        bits |= 1u << b;
+                        par[i] = (unsigned short)i;
+                    }
+                }
+                cand[wd] = bits;
+            }
+            __syncthreads();
+            for (int64_t i = tid; i < n; i += kResThreads) {
+                if (!((cand[i >> 5] >> (i & 31)) & 1u)) continue;
+                for (int d = 0; d < lst.dim; ++d) {
+                    const int64_t j = lst.nbr(i, 2 * d);
+                    if (((cand[j >> 5] >> (j & 31)) & 1u) &&
+                        wolff_int8_active(R.w, (uint32_t)i, (uint32_t)j, serial, tgb, R.key))
+                        runite(par, (int)i, (int)j);
+                }
+            }
+            __syncthreads();
+            if (tid == 0) {
+                int x = s_rsite, px;
+                while ((px = par[x]) != x) x = px;
+                s_root = x;
+            }
+            __syncthreads();
+            const int root = s_root;
+            const int8_t nv = (int8_t)s_newq;
+            int cnt = 0;
+            for (int64_t i = tid; i < n; i += kResThreads) {
+                if (!((cand[i >> 5] >> (i & 31)) & 1u)) continue;
+                int x = (int)i, px;
+                while ((px = par[x]) != x) x = px;  // read-only walks
+                if (x == root) {
+                    s[i] = nv;
+                    ++cnt;
+                }
+            }
+            cnt = __reduce_add_sync(0xffffffffu, cnt);
+            if (lane == 0 && cnt) atomicAdd(&s_size, cnt);
+            __syncthreads();
+            if (tid == 0) R.csize[e * R.csize_e + c * R.csize_c] = s_size;
+        }
+        for (int j = 0; j < R.nmetro; ++j) {
+            const uint32_t sweep = R.sweep0 + (uint32_t)(e * R.nmetro + j);
+            const int64_t half = n / 2, bs = 32 * (int64_t)R.runs, nblk = (half + bs - 1) / bs;
+            for (int colour = 0; colour < 2; ++colour) {
+                for (int64_t b = warp; b < nblk; b += kResWarps) {
+                    const uint32_t run0 = (uint32_t)(b * R.runs);
+                    accept_tab_fill(tab, run0, R.key, sweep, R.replica, (uint32_t)R.runs);
+                    for (int k = 0; k < R.runs; ++k) {
+                        const int64_t t = b * bs + k * 32 + lane;
+                        const bool live = t < half;
+                        int8_site(R.m, lst, s, live ? parity_site(lst, t, colour) : 0, R.key, sweep, R.replica, R.cuts,
+                                  R.D, live, colour, tab, run0);
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        if (R.acc) measure_int8_part(R.m, lst, s, R.acc + e * R.acc_e, 0, 1);
+        __syncthreads();
+    }
+    for (int64_t i = tid; i < n; i += kResThreads) R.state[R.st.addr(i)] = s[i];
+}
+
+// acceptance blocks of `runs` 64-site runs: enough blocks per colour for every warp
+__host__ __device__ inline int resident_runs(int64_t n)
+{
+    int runs = 1;
+    while (runs < kAccRuns && (n / 2) / (32 * (int64_t)runs * 2) >= kResWarps) runs *= 2;
+    return runs;
+}
+
+__global__ void __launch_bounds__(kResThreads) emcs_resident(ResidentRun R)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    resident_run(R, smem);
+}
+
+// One CTA per member of `order` (the batch's resident members, largest
+// first): EMCS e0 .. e0 + count - 1 of the run, measurement slots slot0 ..
+__global__ void __launch_bounds__(kResThreads)
+    batch_resident(const BatchRep* __restrict__ reps, const int32_t* __restrict__ order, int nrep, uint32_t e0,
+                   int slot0, int count, int ncluster, int nmetro, long long* __restrict__ acc,
+                   int32_t* __restrict__ csize)
+{
+    extern __shared__ __align__(16) unsigned char smem[];
+    const int r = order[blockIdx.x];
+    const BatchRep& B = reps[r];
+    ResidentRun R;
+    R.m = B.md;
+    R.st = B.st;
+    R.w = B.w;
+    R.key = B.key;
+    R.replica = B.replica;
+    R.sweep0 = B.sweep0 + e0 * (uint32_t)nmetro;
+    R.cluster0 = B.cluster0 + e0 * (uint32_t)ncluster;
+    R.n_emcs = count;
+    R.ncluster = ncluster;
+    R.nmetro = nmetro;
+    R.D = B.D;
+    R.runs = resident_runs(B.st.n);
+    R.cuts = B.cuts;
+    R.state = (int8_t*)B.s;
+    R.acc = acc + ((size_t)slot0 * nrep + r) * kAccStride;
+    R.acc_e = (int64_t)nrep * kAccStride;
+    R.csize = csize + (size_t)slot0 * ncluster * nrep + r;
+    R.csize_e = (int64_t)ncluster * nrep;
+    R.csize_c = nrep;
+    resident_run(R, smem);
+}
+
+// Lattices this path takes: int8 models on hypercubic stencils of at most
+// kResidentMaxSites sites.
+bool resident_fits(const Sim* s)
+{
+    return !s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC && s->n <= kResidentMaxSites && s->n >= 2;
+}
+
+static cudaError_t resident_attr(int device)
+{
+    static bool done[64] = {};
+    if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
+    const int bytes = (int)resident_smem_bytes(kResidentMaxSites);
+    cudaError_t e = cudaFuncSetAttribute(emcs_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(batch_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess && device >= 0 && device < 64) done[device] = true;
+    return e;
+}
+
+// n_emcs EMCS (clusters, sweeps, the measurement into acc slots 0 ..
+// n_emcs - 1 when acc is given, cluster sizes into csize) in one launch;
+// advances the counters.
+cudaError_t launch_emcs_resident(Sim* s, int n_emcs, int ncluster, int nmetro, bool measure, long long* acc,
+                                 int32_t* csize)
+{
+    cudaError_t e = resident_attr(s->device);
+    if (e != cudaSuccess) return e;
+    ResidentRun R{};
+    R.m = s->md;
+    R.st = s->sten;
+    if (ncluster > 0) R.w = wolff_int8_params(s->md);
+    R.key = make_key(s->seed);
+    R.replica = s->replica;
+    R.sweep0 = (uint32_t)s->sweep;
+    R.cluster0 = (uint32_t)s->cluster;
+    R.n_emcs = n_emcs;
+    R.ncluster = ncluster;
+    R.nmetro = nmetro;
+    R.D = s->max_degree;
+    R.runs = resident_runs(s->n);
+    R.cuts = s->d_cuts;
+    R.state = (int8_t*)s->state[s->cur];
+    R.acc = measure ? acc : nullptr;
+    R.acc_e = kAccStride;
+    R.csize = csize;
+    R.csize_e = ncluster;
+    R.csize_c = 1;
+    emcs_resident<<<1, kResThreads, resident_smem_bytes(s->n), s->stream>>>(R);
+    s->launches++;
+    s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
+    s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
+    return cudaGetLastError();
+}
+
+// The batch's resident members (order: member ids, largest first; nres of
+// them, the largest with max_n sites), EMCS e0 .. e0 + count - 1.
+cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, int64_t max_n,
+                                  uint32_t e0, int slot0, int count, int ncluster, int nmetro, int device)
+{
+    if (nres <= 0 || count <= 0) return cudaSuccess;
+    cudaError_t e = resident_attr(device);
+    if (e != cudaSuccess) return e;
+    batch_resident<<<nres, kResThreads, resident_smem_bytes(max_n), st>>>(b.reps, order, b.nrep, e0, slot0, count,
+                                                                          ncluster, nmetro, b.acc, b.csize);
+    return cudaGetLastError();
+}
+
+}  // namespace mqv

@@ -19,6 +19,7 @@
 
 #include <mutex>
 
+#include "wolff_ccl.cuh"
 #include "wolff_int8.cuh"
 
 namespace mqv {
@@ -80,6 +81,86 @@ cudaError_t launch_wolff_int8(Sim* s, int slot)
         wolff_int8<<<1, 1024, 0, s->stream>>>(w, s->csr, st, s->d_visited, s->d_queue, out, key, serial,
                                               tag(kWolffSeed, s->replica), tag(kWolffBond, s->replica), s->max_degree);
     s->launches++;
+    s->cluster++;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// One cluster of one lattice by connected-component labelling (the batched
+// path's kernels, wolff_ccl.cuh, over a one-member table): a fixed number of
+// whole-lattice passes whatever the cluster's depth, where a breadth-first
+// growth pays a CTA barrier per level -- thousands of levels for a critical
+// cluster on a large lattice.  The labels are the handle's queue (n int32).
+
+__global__ void single_rep_set(BatchRep* __restrict__ d, BatchRep r, BatchCtr* __restrict__ ctr, uint32_t serial)
+{
+    *d = r;
+    ctr->e = serial;  // serial = cluster0 (0) + e * 1 + 0; slot = e - ebase = 0
+    ctr->ebase = serial;
+}
+
+static BatchRep single_rep(const Sim* s)
+{
+    BatchRep r{};
+    r.md = s->md;
+    r.st = s->sten;
+    r.csr = s->csr;
+    r.lat_kind = s->lat_kind;
+    r.order = s->d_order;
+    if (!s->is_f32) r.w = wolff_int8_params(s->md);
+    r.key = make_key(s->seed);
+    r.replica = s->replica;
+    r.sweep0 = (uint32_t)s->sweep;
+    r.cluster0 = 0;
+    r.s = s->state[s->cur];
+    r.visited = s->d_visited;
+    r.queue = s->d_queue;
+    r.cuts = s->d_cuts;
+    r.D = s->max_degree;
+    return r;
+}
+
+template <bool F32>
+static void launch_label_t(Sim* s, int32_t* csize)
+{
+    const int64_t n = s->n;
+    const unsigned gb = (unsigned)((n + kBatchMetroThreads - 1) / kBatchMetroThreads);
+    CclSeed* sd = (CclSeed*)s->d_seed1;
+    single_rep_set<<<1, 1, 0, s->stream>>>(s->d_rep1, single_rep(s), s->d_ctr1, (uint32_t)s->cluster);
+    ccl_seed<F32><<<1, 32, 0, s->stream>>>(s->d_rep1, s->d_ctr1, 1, 0, sd, csize, 1);
+    ccl_local<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1,
+                                                             1, 0);
+    ccl_hook<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1,
+                                                            1, 0);
+    ccl_compress<<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n);
+    ccl_flip<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1, 1,
+                                                            0, csize, 1);
+    s->launches += 6;
+}
+
+// The one-member tables of the labelling path, allocated on first use.
+cudaError_t ensure_label_tables(Sim* s)
+{
+    if (s->d_rep1) return cudaSuccess;
+    const int64_t n = s->n;
+    const int64_t gb = (n + kBatchMetroThreads - 1) / kBatchMetroThreads;
+    const int64_t pre[2] = {0, n};
+    cudaError_t e = cudaMalloc(&s->d_rep1, sizeof(BatchRep));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_ctr1, sizeof(BatchCtr));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_seed1, sizeof(CclSeed));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_sprefix1, sizeof(pre));
+    if (e == cudaSuccess) e = cudaMalloc(&s->d_sbrep1, sizeof(int32_t) * (size_t)gb);
+    if (e == cudaSuccess) e = cudaMemcpy(s->d_sprefix1, pre, sizeof(pre), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(s->d_sbrep1, 0, sizeof(int32_t) * (size_t)gb);
+    return e;
+}
+
+cudaError_t launch_wolff_label(Sim* s, int slot)
+{
+    const cudaError_t e = ensure_label_tables(s);
+    if (e != cudaSuccess) return e;
+    if (s->is_f32) launch_label_t<true>(s, s->d_csize + slot);
+    else launch_label_t<false>(s, s->d_csize + slot);
     s->cluster++;
     return cudaGetLastError();
 }

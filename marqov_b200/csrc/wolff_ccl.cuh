@@ -82,6 +82,7 @@ __global__ void ccl_seed(const BatchRep* __restrict__ reps, const BatchCtr* __re
     const int r = blockIdx.x * blockDim.x + threadIdx.x;
     if (r >= nrep) return;
     const BatchRep& R = reps[r];
+    if (R.resident) return;  // clusters grown by batch_resident
     const uint32_t e = ctr->e, slot = e - ctr->ebase;
     const uint32_t serial = R.cluster0 + e * (uint32_t)ncluster + (uint32_t)c;
     const uint32_t tgs = tag(kWolffSeed, R.replica);
@@ -234,7 +235,7 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
     });
 }
 
-__global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+static __global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
                              const int32_t* __restrict__ block_rep, int64_t total)
 {
     const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
