@@ -68,6 +68,42 @@ def dist_env():
     return ws, rank, local
 
 
+def weak_scaling_value(group, updates_per_rank, ms_this_rank):
+    """Whole-job rate of N ranks that each ran `updates_per_rank` site
+    updates: (updates/ns over all ranks, the slowest rank's milliseconds)."""
+    ms_max = group.max(ms_this_rank)
+    return group.world * updates_per_rank / (ms_max * 1e6), ms_max
+
+
+def _free_port():
+    import socket
+    with socket.socket() as sk:
+        sk.bind(("127.0.0.1", 0))
+        return sk.getsockname()[1]
+
+
+def _spawned_rank(rank, world, port, argv):
+    os.environ.update(RANK=str(rank), WORLD_SIZE=str(world), LOCAL_RANK=str(rank), LOCAL_WORLD_SIZE=str(world),
+                      MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    sys.argv = [sys.argv[0]] + list(argv)
+    rc = main()
+    if rc:
+        raise SystemExit(rc)
+
+
+def spawn_ranks(args):
+    """`--gpus N` (N > 1) started without a launcher: N rank processes on this
+    node, one per GPU, as torchrun would start them."""
+    import torch
+    import torch.multiprocessing as mp
+    if args.impl == "engine":
+        nvis = torch.cuda.device_count()
+        if nvis < args.gpus:
+            raise SystemExit(f"bench.py: --gpus {args.gpus} but only {nvis} CUDA device(s) are visible")
+    mp.spawn(_spawned_rank, args=(args.gpus, _free_port(), sys.argv[1:]), nprocs=args.gpus, join=True)
+    return 0
+
+
 # ---------------------------------------------------------------------------
 # clocks (NVML reads only)
 
@@ -237,62 +273,136 @@ def stream_of(core):
     return int(p.value or 0)
 
 
-def workload_potts_batch(M, torch, emcs_batched=100, emcs_plain=4, warmup=5):
-    """Config 3: the 256-replica farm, batched (one graph launch per 8 EMCS)
-    against the same members as plain handles (one mqv_emcs call each).
-    Batched and plain runs produce identical chains, so equal observable
-    error bars mean equal EMCS counts and the rates compare directly."""
+def _tau_err(x):
+    from oracle import stats as S
+    m, err, tau = S.mean_err_tau(np.asarray(x, float))
+    return {"mean": m, "err": err, "tau_int": tau}
+
+
+def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
+    """Config 3: the 256-replica farm, batched against plain per-replica runs
+    over the same EMCS window after the same thermalisation.
+
+    Batched: one Batch (resident CTAs for the members that fit shared memory,
+    graph-replayed kernels for the others), CUDA events around the window.
+    Plain: the same members as 256 independent handles, each on its own
+    stream, issued from a pool of host threads (one member at a time per
+    thread, no synchronisation between members), wall time around the
+    window.  Both arms run the identical chains (bit-exact), so the
+    tau_int-corrected error bars of E and |m| reported for a few members are
+    equal at equal EMCS counts and the rates compare directly."""
+    from concurrent.futures import ThreadPoolExecutor
     members = potts_farm(M)
     sites = sum(m[0].size() for m in members)
     with M.Batch(members, graph_steps=8) as b:
         b.init()
-        b.emcs(warmup, 1, 1)
+        b.emcs(therm, 1, 1)
         st = torch.cuda.ExternalStream(stream_of(b.member(0)))
-        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         l0 = b.launches
         torch.cuda.synchronize()
         w0 = time.perf_counter()
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         ev0.record(st)
-        obs, mc = b.emcs(emcs_batched, 1, 1)
+        obs_b, mc_b = b.emcs(emcs, 1, 1)
         ev1.record(st)
         torch.cuda.synchronize()
         wall_b = time.perf_counter() - w0
         dev_b = ev0.elapsed_time(ev1) * 1e-3
         launches_b = b.launches - l0
+        final_b = [b.member(i).state for i in (0, 1, 2)]
         # Wolff only (nmetro = 0: clusters and the measurement)
-        w1 = time.perf_counter()
-        _, mcw = b.emcs(20, 1, 0)
-        wall_w = time.perf_counter() - w1
+        res = []
+        tw = timed(torch, st, lambda: res.append(b.emcs(50, 1, 0)))
+        mcw = res[0][1]
     singles = [M.makeCore(*m) for m in members]
+    nthreads = threads or min(32, os.cpu_count() or 1)
     try:
-        for c in singles:
-            c.init()
-            c.emcs(1, 1, 1)
-        torch.cuda.synchronize()
-        w0 = time.perf_counter()
-        for c in singles:
-            c.emcs(emcs_plain, 1, 1)
-        torch.cuda.synchronize()
-        wall_p = time.perf_counter() - w0
+        with ThreadPoolExecutor(nthreads) as ex:
+            def prep(c):
+                c.init()
+                c.emcs(therm, 1, 1, measure=False)
+                c.synchronize()
+            list(ex.map(prep, singles))
+            torch.cuda.synchronize()
+            w0 = time.perf_counter()
+            outs = list(ex.map(lambda c: c.emcs(emcs, 1, 1), singles))
+            torch.cuda.synchronize()
+            wall_p = time.perf_counter() - w0
+        same = all((outs[i][0] == obs_b[:, i, :]).all() for i in range(len(singles)))
+        same = same and all((singles[i].state == final_b[i]).all() for i in range(3))
     finally:
         for c in singles:
             c.close()
-    rate_b = sites * emcs_batched / (dev_b * 1e9)
-    rate_b_wall = sites * emcs_batched / (wall_b * 1e9)
-    rate_p = sites * emcs_plain / (wall_p * 1e9)
+    rate_b = sites * emcs / (dev_b * 1e9)
+    rate_b_wall = sites * emcs / (wall_b * 1e9)
+    rate_p = sites * emcs / (wall_p * 1e9)
+    pick = [0, 1, 2, int(np.argmax([m[0].size() for m in members]))]
+    bars = {str(i): {"L": int(members[i][0].len),
+                     "batched": {"e": _tau_err(obs_b[:, i, 0]), "m": _tau_err(obs_b[:, i, 1])},
+                     "plain": {"e": _tau_err(outs[i][0][:, 0]), "m": _tau_err(outs[i][0][:, 1])}} for i in pick}
     return {
         "workload": "256 q=3 Potts replicas, L uniform in {32..512}, T uniform in [0.9,1.1] Tc; "
                     "EMCS = 1 Wolff cluster + 1 checkerboard sweep + measurement",
-        "sites": int(sites), "unit": UNIT,
-        "batched": {"value": rate_b, "value_wall": rate_b_wall, "emcs": emcs_batched, "seconds_device": dev_b,
-                    "gpu_launches": int(launches_b), "graph_emcs_per_launch": 8},
-        "plain": {"value": rate_p, "emcs": emcs_plain, "seconds_wall": wall_p,
-                  "how": "256 handles, one mqv_emcs call each (per-kernel launches, host-synchronised)"},
+        "sites": int(sites), "unit": UNIT, "emcs_window": emcs, "thermalisation": therm,
+        "batched": {"value": rate_b, "value_wall": rate_b_wall, "emcs": emcs, "seconds_device": dev_b,
+                    "seconds_wall": wall_b, "gpu_launches": int(launches_b), "graph_emcs_per_launch": 8},
+        "plain": {"value": rate_p, "emcs": emcs, "seconds_wall": wall_p,
+                  "how": f"256 handles, each on its own stream, one mqv_emcs call each from {nthreads} host "
+                         f"threads (no synchronisation between members)"},
         "batched_vs_plain": rate_b_wall / rate_p,
-        "wolff_cluster_spins_per_ns": float(mcw.sum()) / (wall_w * 1e9),
-        "mean_cluster": float(mc.mean()),
-        "equal_error_bars": "identical chains (bit-exact batched == plain), equal EMCS counts",
+        "chains_identical": bool(same),
+        "error_bars": bars,
+        "wolff_cluster_spins_per_ns": float(mcw.sum()) / (tw * 1e9),
+        "mean_cluster": float(mc_b.mean()),
     }
+
+
+def workload_wolff(M, torch, clusters=4000, big_clusters=6):
+    """Wolff cluster-spins/ns of single lattices: config 1 (2D Ising L = 64 at
+    beta_c, clusters alone and full EMCS = 1 cluster + 1 sweep) on the
+    resident path, and 2D Ising L = 16384 at beta_c (labelling clusters),
+    beside the reference's Wolff<Ising<int>> on one host core."""
+    out = {}
+    L = 64
+    st = torch.cuda.Stream()
+    with M.makeCore(M.RegularHypercubic(L, 2), M.Config(seed=5, repid=0), M.Ising(-1.0), BETA_C) as c:
+        c.set_stream(st.cuda_stream)
+        c.init()
+        c.emcs(200, ncluster=1, nmetro=1, measure=False)
+        res = []
+        t_w = timed(torch, st, lambda: res.append(c.wolff(clusters)))
+        res2 = []
+        t_e = timed(torch, st, lambda: res2.append(c.emcs(clusters, ncluster=1, nmetro=1)))
+        path = c.describe()
+    sizes = res[0]
+    out["ising2d_L64"] = {
+        "cluster_spins_per_ns": float(np.sum(sizes)) / (t_w * 1e9), "mean_cluster": float(np.mean(sizes)),
+        "us_per_cluster": 1e6 * t_w / clusters, "clusters": clusters,
+        "emcs_per_s": clusters / t_e, "emcs_updates_per_ns": L * L * clusters / (t_e * 1e9),
+        "emcs_mean_cluster": float(np.mean(res2[0][1])), "path": path,
+        "includes": "one mqv_wolff / mqv_emcs call each (cluster sizes / observables copied to the host)"}
+    try:
+        from oracle.oracle import RefHarness
+        t, tot = RefHarness().wolff_ising2d_timed(L, BETA_C, 5, 200, 20000)
+        out["ising2d_L64"]["reference_one_core"] = {
+            "cluster_spins_per_ns": tot / (t * 1e9), "mean_cluster": tot / 20000, "clusters": 20000,
+            "what": "Wolff<Ising<int>> on FixedDimRegularHypercubic<2> with RNGCache<mt19937_64>, one core"}
+    except Exception as exc:
+        out["ising2d_L64"]["reference_one_core"] = {"unavailable": str(exc)}
+    L = 16384
+    with M.makeCore(M.RegularHypercubic(L, 2), M.Config(seed=6, repid=0), M.Ising(-1.0), BETA_C) as c:
+        c.set_stream(st.cuda_stream)
+        c.init()
+        c.emcs(50, ncluster=1, nmetro=4, measure=False)
+        res = []
+        t_w = timed(torch, st, lambda: res.append(c.wolff(big_clusters)))
+        path = c.describe()
+    sizes = res[0]
+    out["ising2d_L16384"] = {
+        "cluster_spins_per_ns": float(np.sum(sizes)) / (t_w * 1e9), "mean_cluster": float(np.mean(sizes)),
+        "ms_per_cluster": 1e3 * t_w / big_clusters, "clusters": big_clusters, "path": path,
+        "note": "after 50 EMCS of 1 cluster + 4 sweeps from a random start (not yet at the critical cluster scale)"}
+    return out
 
 
 def timed(torch, stream, fn):
@@ -447,7 +557,8 @@ def workload_phi4_autograd(M, torch, n_therm=10, n_meas=40):
 
 def secondary(M, torch):
     out = {}
-    for name, fn in (("potts_batch", workload_potts_batch), ("heisenberg3d_L128", workload_heisenberg),
+    for name, fn in (("potts_batch", workload_potts_batch), ("wolff", workload_wolff),
+                     ("heisenberg3d_L128", workload_heisenberg),
                      ("phi4_autograd_64xL64", workload_phi4_autograd), ("rgg_ising_N1M", workload_rgg),
                      ("ea_3d_L32x32", workload_ea), ("tempering_ising2d_64xL128", workload_tempering)):
         try:
@@ -520,9 +631,8 @@ def run_engine(args, ws, rank, local):
     launches = core.launches - l0
     kernel_desc = core.describe()
     ms = ev0.elapsed_time(ev1)
-    ms_max = max_over_ranks(ms)
     updates = n * args.nmetro * args.steps
-    value = ws * updates / (ms_max * 1e6)
+    value, ms_max = weak_scaling_value(group, updates, ms)
 
     # ---- end to end through the public call, host buffers
     obs = torch.zeros(4, dtype=torch.float64).pin_memory()
@@ -591,7 +701,12 @@ def run_engine(args, ws, rank, local):
 
 def main():
     args = parse()
+    if args.gpus > 1 and "WORLD_SIZE" not in os.environ:
+        return spawn_ranks(args)
     ws, rank, local = dist_env()
+    if ws != args.gpus and rank == 0:
+        print(f"bench.py: WORLD_SIZE={ws} but --gpus {args.gpus}; reporting the {ws} ranks that run",
+              file=sys.stderr)
     if args.impl == "reference":
         return run_reference(args, ws, rank)
     if args.workload != "ising2d":

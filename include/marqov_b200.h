@@ -54,7 +54,8 @@ enum {
     MQV_ERR_UNSUPPORTED_TERM = 2, /* model / term shape the engine does not lower */
     MQV_ERR_BAD_DESCRIPTOR = 3,   /* inconsistent lattice or model descriptor */
     MQV_ERR_CUDA = 4,             /* CUDA runtime error (message in mqv_last_error) */
-    MQV_ERR_TIMEOUT = 5,          /* a bounded device wait gave up */
+    MQV_ERR_TIMEOUT = 5,          /* a bounded device wait gave up; the handle refuses compute
+                                     (MQV_ERR_STATE) until its state is set again */
     MQV_ERR_CHECKSUM = 6,         /* checkpoint / state checksum mismatch */
     MQV_ERR_NO_DEVICE = 7,        /* no usable CUDA device */
     MQV_ERR_OUT_OF_MEMORY = 8,    /* device allocation failed */
@@ -163,6 +164,14 @@ MQV_API mqv_status mqv_init_state(mqv_sim* sim);
  * components per site; int8 for integer models, float32 otherwise. */
 MQV_API mqv_status mqv_get_state(mqv_sim* sim, void* host, size_t bytes);
 MQV_API mqv_status mqv_set_state(mqv_sim* sim, const void* host, size_t bytes);
+/* No counterpart in the reference.  mqv_get_state / mqv_set_state with a
+ * checksum: *hash receives the FNV-1a 64-bit hash of the host bytes, and
+ * mqv_set_state_checked refuses a buffer whose hash differs with
+ * MQV_ERR_CHECKSUM (a corrupt or truncated stored state), leaving the
+ * handle's state untouched.  The dump container stores the hash beside the
+ * state (core.h:543-607 is the reference's restart-from-dump path). */
+MQV_API mqv_status mqv_get_state_checked(mqv_sim* sim, void* host, size_t bytes, uint64_t* hash);
+MQV_API mqv_status mqv_set_state_checked(mqv_sim* sim, const void* host, size_t bytes, uint64_t hash);
 /* Device pointer of the current state (valid until the next engine call).
  * Layout: the reference site order, except (a) on the fused 2D Ising path,
  * whose rows hold the even-x sites, then the odd-x sites, with the 32 bytes
@@ -311,16 +320,25 @@ MQV_API mqv_status mqv_batch_tempering(mqv_batch* batch, int32_t n_steps, int32_
                                       mqv_obs* obs, int32_t* accepted);
 MQV_API mqv_status mqv_batch_launch_count(mqv_batch* batch, uint64_t* count);
 
-/* Self test: Philox blocks for n counters (c0 = i, other words given) computed
- * on the device by the engine and by cuRAND's Philox4_32_10; out_engine and
- * out_curand receive 4n words each (host). */
 /* Self test (host only, no device needed): the closed-form acceptance cut
  * the sweep kernels use, cut[i] = the smallest word >> 11 that
  * update_accepted<pref>(dE[i], beta[i], word) rejects (2^53: none). */
 MQV_API mqv_status mqv_selftest_accept_cut(int32_t pref, int32_t n, const double* dE, const double* beta,
                                            uint64_t* cut);
+/* Self test: Philox blocks for n counters (c0 = i, other words given) computed
+ * on the device by the engine and by cuRAND's Philox4_32_10; out_engine and
+ * out_curand receive 4n words each (host). */
 MQV_API mqv_status mqv_selftest_philox(uint64_t seed, uint32_t c1, uint32_t c2, uint32_t c3,
                                        int32_t n, uint32_t* out_engine, uint32_t* out_curand);
+/* Self test of the bounded device waits: the next fused 2D Ising sweep of
+ * the handle (band kernel, L = 8192 or 16384) has CTA 0 withhold its staged
+ * row `row` (2 .. 64) and waits at most wait_ns for a row, so that the wait
+ * for the withheld row runs out.  The kernel then sets MQV_ERR_TIMEOUT,
+ * lets the copies it issued land and returns; the call that reads the
+ * device status reports MQV_ERR_TIMEOUT, and the handle refuses compute
+ * (MQV_ERR_STATE) until its state is set again.  Nothing faults or hangs:
+ * every other wait is bounded by the same limit. */
+MQV_API mqv_status mqv_selftest_inject_timeout(mqv_sim* sim, int32_t row, uint64_t wait_ns);
 
 #ifdef __cplusplus
 }

@@ -78,6 +78,9 @@ SIGNATURES = {
                                C.POINTER(_vp)]),
     "mqv_destroy": (C.c_int32, [_vp]),
     "mqv_set_wolff": (C.c_int32, [_vp, C.c_int32]),
+    "mqv_get_state_checked": (C.c_int32, [_vp, _vp, C.c_size_t, C.POINTER(C.c_uint64)]),
+    "mqv_set_state_checked": (C.c_int32, [_vp, _vp, C.c_size_t, C.c_uint64]),
+    "mqv_selftest_inject_timeout": (C.c_int32, [_vp, C.c_int32, C.c_uint64]),
     "mqv_set_stream": (C.c_int32, [_vp, _vp]),
     "mqv_get_stream": (C.c_int32, [_vp, C.POINTER(_vp)]),
     "mqv_set_beta": (C.c_int32, [_vp, C.c_double]),

@@ -16,13 +16,16 @@ package, so the same tree is kept as a directory, one file per data set:
             config/lattice.json                 the lattice's parameters
             config/hamiltonian.json             the Hamiltonian's name and parameters
             state/hamiltonianstatespace.npy     final state, reference site order
+            state/hash.json                     FNV-1a 64-bit hash of the state's bytes
             state/RNG.txt                       the generator's name
             state/rngstate.npy                  uint64: seed, replica, sweep, cluster
             observables/<name>.npy              one value per measurement
                                                 (e, m, m2, m4, clustersize)
 
 The engine's random numbers are keyed by (seed, replica, sweep, cluster),
-so those four words are the whole RNG state.
+so those four words are the whole RNG state.  A step whose state file is
+truncated or unreadable, or whose bytes do not match the stored hash, is
+refused with MarqovError(CHECKSUM) instead of being continued from.
 """
 from __future__ import annotations
 
@@ -94,8 +97,11 @@ class Step:
                     {"name": type(ham).__name__, **_params(ham)})
         return self
 
-    def write_state(self, state: np.ndarray, seed: int, replica: int, sweep: int, cluster: int) -> None:
+    def write_state(self, state: np.ndarray, seed: int, replica: int, sweep: int, cluster: int,
+                    hash_: int | None = None) -> None:
         np.save(os.path.join(self.path, "state", "hamiltonianstatespace.npy"), state)
+        if hash_ is not None:
+            _write_json(os.path.join(self.path, "state", "hash.json"), {"fnv1a64": int(hash_)})
         with open(os.path.join(self.path, "state", "RNG.txt"), "w") as fh:
             fh.write(RNG_NAME + "\n")
         np.save(os.path.join(self.path, "state", "rngstate.npy"),
@@ -106,10 +112,22 @@ class Step:
             np.save(os.path.join(self.path, "observables", f"{name}.npy"), np.asarray(values))
 
     def read_state(self):
-        """(state, (seed, replica, sweep, cluster)) of a completed step."""
-        st = np.load(os.path.join(self.path, "state", "hamiltonianstatespace.npy"))
-        rng = np.load(os.path.join(self.path, "state", "rngstate.npy"))
-        return st, tuple(int(x) for x in rng)
+        """(state, (seed, replica, sweep, cluster), hash or None) of a completed
+        step; a file that cannot be read back whole raises MarqovError(CHECKSUM)."""
+        from ._lib import ERR_CHECKSUM, MarqovError
+        try:
+            st = np.load(os.path.join(self.path, "state", "hamiltonianstatespace.npy"))
+            rng = np.load(os.path.join(self.path, "state", "rngstate.npy"))
+            if rng.shape != (4,):
+                raise ValueError(f"RNG state of shape {rng.shape}")
+        except (OSError, ValueError, EOFError) as exc:
+            raise MarqovError(ERR_CHECKSUM, f"{self.path}: unreadable state ({exc})") from exc
+        h = None
+        hp = os.path.join(self.path, "state", "hash.json")
+        if os.path.exists(hp):
+            with open(hp) as fh:
+                h = int(json.load(fh)["fnv1a64"])
+        return st, tuple(int(x) for x in rng), h
 
     def read_observables(self) -> dict:
         d = os.path.join(self.path, "observables")

@@ -111,7 +111,10 @@ class Core:
         L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
         self._seed, self._replica = seed, replica
         if restore is not None:
-            self.state = restore[0]
+            if restore[2] is None:
+                self.state = restore[0]
+            else:
+                self.set_state_checked(restore[0], restore[2])
             self.counters = restore[1][2:]
             self._restored = True
         # the step group exists only for a Core that could be set up
@@ -147,7 +150,8 @@ class Core:
             return
         self._step.write_observables(self.obs.arrays())
         sweep, cluster = self.counters
-        self._step.write_state(self.state, self._seed, self._replica, sweep, cluster)
+        st, h = self.get_state_checked()
+        self._step.write_state(st, self._seed, self._replica, sweep, cluster, h)
 
     def close(self):
         if self._h and self._owner is None:
@@ -260,6 +264,18 @@ class Core:
     def state(self, value):
         v = np.ascontiguousarray(value, self.dtype).reshape(-1)
         L.check(self._lib.mqv_set_state(self._h, v.ctypes.data, v.nbytes))
+
+    def get_state_checked(self) -> tuple[np.ndarray, int]:
+        """The state and its FNV-1a 64-bit hash (mqv_get_state_checked)."""
+        out = np.empty(self.n * self.symd, self.dtype)
+        h = C.c_uint64()
+        L.check(self._lib.mqv_get_state_checked(self._h, out.ctypes.data, out.nbytes, C.byref(h)))
+        return out, int(h.value)
+
+    def set_state_checked(self, value, hash_: int):
+        """Set the state if its hash matches (else MarqovError CHECKSUM, state untouched)."""
+        v = np.ascontiguousarray(value, self.dtype).reshape(-1)
+        L.check(self._lib.mqv_set_state_checked(self._h, v.ctypes.data, v.nbytes, int(hash_) & (2 ** 64 - 1)))
 
     def state_device_ptr(self) -> tuple[int, int]:
         p = C.c_void_p()

@@ -65,6 +65,7 @@ unsigned long long accept_cut(int pref, double dE, double beta)
 static bool is_f32_kind(int k) { return k == MQV_MODEL_HEISENBERG || k == MQV_MODEL_PHI4 || k == MQV_MODEL_XXZ; }
 
 bool ising2d_supported(int L);
+int ising2d_band_config(const Sim* s);
 const char* ising2d_config_name(Sim* s, char* buf, int len);
 cudaError_t launch_split_rows(Sim* s, const void* rowmajor, void* split);
 cudaError_t launch_merge_rows(Sim* s, const void* split, void* rowmajor);
@@ -157,8 +158,21 @@ static mqv_status check_device_status(Sim* s)
     MQV_CK(cudaStreamSynchronize(s->stream));
     if (st != 0) {
         MQV_CK(cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream));
-        return fail(st, "a device-side wait gave up (status " + std::to_string(st) + ")");
+        s->failed = true;
+        return fail(st, "a device-side wait gave up (status " + std::to_string(st) +
+                            "): the sweep in flight was abandoned and the state is incomplete; set the state "
+                            "again (mqv_set_state or mqv_init_state) before the next run");
     }
+    return MQV_OK;
+}
+
+// Compute on a handle whose last run timed out is refused until its state is set again.
+static mqv_status check_runnable(const Sim* s)
+{
+    if (s->failed)
+        return fail(MQV_ERR_STATE, "a device wait timed out in an earlier run; set the state again (mqv_set_state "
+                                   "or mqv_init_state) first");
+    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
     return MQV_OK;
 }
 
@@ -575,6 +589,7 @@ MQV_API mqv_status mqv_init_state(mqv_sim* h)
     MQV_GUARD(s);
     MQV_CK(s->is_f32 ? launch_init_f32(s) : launch_init_int8(s));
     s->initialised = true;
+    s->failed = false;
     return MQV_OK;
 }
 
@@ -590,6 +605,7 @@ MQV_API mqv_status mqv_get_state(mqv_sim* h, void* host, size_t bytes)
 {
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
+    if (s->failed) return check_runnable(s);
     if (!host || bytes != s->state_bytes)
         return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
     if (s->fused_ising2d) {
@@ -630,6 +646,7 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
         MQV_CK(launch_split_rows(s, s->state[s->cur ^ 1], s->state[s->cur]));
         MQV_CK(cudaStreamSynchronize(s->stream));
         s->initialised = true;
+        s->failed = false;
         return MQV_OK;
     }
     if (!s->is_f32) {
@@ -653,11 +670,13 @@ MQV_API mqv_status mqv_set_state(mqv_sim* h, const void* host, size_t bytes)
         MQV_CK(cudaMemcpyAsync(s->state[s->cur], soa.data(), bytes, cudaMemcpyHostToDevice, s->stream));
         MQV_CK(cudaStreamSynchronize(s->stream));
         s->initialised = true;
+        s->failed = false;
         return MQV_OK;
     }
     MQV_CK(cudaMemcpyAsync(s->state[s->cur], host, bytes, cudaMemcpyHostToDevice, s->stream));
     MQV_CK(cudaStreamSynchronize(s->stream));
     s->initialised = true;
+        s->failed = false;
     return MQV_OK;
 }
 
@@ -693,7 +712,10 @@ MQV_API mqv_status mqv_metropolis(mqv_sim* h, int32_t nsweeps)
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     if (nsweeps < 0) return fail(MQV_ERR_INVALID_ARG, "nsweeps < 0");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     for (int t = 0; t < nsweeps; ++t) {
         mqv_status st = launch_sweep(s, -1);
         if (st) return st;
@@ -706,7 +728,10 @@ MQV_API mqv_status mqv_wolff(mqv_sim* h, int32_t nclusters, int32_t* sizes)
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     if (nclusters < 0) return fail(MQV_ERR_INVALID_ARG, "nclusters < 0");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     mqv_status st = check_wolff_supported(s);
     if (st) return st;
     int done = 0;
@@ -738,7 +763,10 @@ MQV_API mqv_status mqv_wolff_noalloc(mqv_sim* h, int32_t nclusters, int32_t* siz
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     if (nclusters < 0) return fail(MQV_ERR_INVALID_ARG, "nclusters < 0");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     mqv_status st = check_wolff_supported(s);
     if (st) return st;
     if (s->is_f32)
@@ -769,7 +797,10 @@ MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     if (ncluster > 0) {
         mqv_status st = check_wolff_supported(s);
         if (st) return st;
@@ -834,7 +865,10 @@ MQV_API mqv_status mqv_emcs_samples(mqv_sim* h, int32_t n_emcs, int32_t ncluster
     MQV_GUARD(s);
     if (n_emcs < 0 || ncluster < 0 || nmetro < 0) return fail(MQV_ERR_INVALID_ARG, "negative count");
     if (n_emcs > 0 && !d_samples) return fail(MQV_ERR_INVALID_ARG, "null sample buffer");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     if (ncluster > 0) {
         mqv_status st = check_wolff_supported(s);
         if (st) return st;
@@ -893,7 +927,10 @@ MQV_API mqv_status mqv_measure(mqv_sim* h, mqv_obs* out)
     Sim* s = reinterpret_cast<Sim*>(h);
     MQV_GUARD(s);
     if (!out) return fail(MQV_ERR_INVALID_ARG, "null output");
-    if (!s->initialised) return fail(MQV_ERR_STATE, "state not initialised");
+    {
+        const mqv_status rs = check_runnable(s);
+        if (rs) return rs;
+    }
     MQV_CK(cudaMemsetAsync(s->d_acc, 0, sizeof(long long) * kAccStride, s->stream));
     mqv_status st = launch_measure(s, 0);
     if (st) return st;
@@ -924,6 +961,40 @@ MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
                                   : (s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8")),
                   cfg[0] ? " kernel=" : "", cfg,
                   use_resident(s) ? "label-smem" : (cluster_by_label(s) ? "label" : "bfs"));
+    return MQV_OK;
+}
+
+static uint64_t state_hash(const void* p, size_t bytes) { return fnv1a(p, bytes); }
+
+MQV_API mqv_status mqv_get_state_checked(mqv_sim* h, void* host, size_t bytes, uint64_t* hash)
+{
+    if (!hash) return fail(MQV_ERR_INVALID_ARG, "null hash");
+    const mqv_status st = mqv_get_state(h, host, bytes);
+    if (st) return st;
+    *hash = state_hash(host, bytes);
+    return MQV_OK;
+}
+
+MQV_API mqv_status mqv_set_state_checked(mqv_sim* h, const void* host, size_t bytes, uint64_t hash)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s || !host) return fail(MQV_ERR_INVALID_ARG, "null argument");
+    if (bytes != s->state_bytes)
+        return fail(MQV_ERR_INVALID_ARG, "state buffer size mismatch (expected " + std::to_string(s->state_bytes) + ")");
+    if (state_hash(host, bytes) != hash)
+        return fail(MQV_ERR_CHECKSUM, "state checksum mismatch: the stored state is corrupt");
+    return mqv_set_state(h, host, bytes);
+}
+
+MQV_API mqv_status mqv_selftest_inject_timeout(mqv_sim* h, int32_t row, uint64_t wait_ns)
+{
+    Sim* s = reinterpret_cast<Sim*>(h);
+    if (!s) return fail(MQV_ERR_INVALID_ARG, "null handle");
+    if (!s->fused_ising2d || ising2d_band_config(s) < 0)
+        return fail(MQV_ERR_UNSUPPORTED_TERM, "timeout injection needs the fused 2D Ising band path (L = 8192 or 16384)");
+    if (row < 2 || row > 64) return fail(MQV_ERR_INVALID_ARG, "withheld row must be in [2, 64]");
+    s->inject_row = row;
+    s->inject_wait_ns = wait_ns;
     return MQV_OK;
 }
 
@@ -1130,6 +1201,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
     if (ncluster > 64 || nmetro > 64) return fail(MQV_ERR_INVALID_ARG, "at most 64 clusters and 64 sweeps per EMCS");
     for (Sim* s : b->sims) {
         if (!s->initialised) return fail(MQV_ERR_STATE, "state of a batch member not initialised");
+        if (s->failed) return check_runnable(s);
         if (!b->f32) MQV_CK(ensure_cuts(s));
         if (ncluster > 0) {
             mqv_status st = check_wolff_supported(s);

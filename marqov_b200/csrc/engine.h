@@ -194,6 +194,11 @@ struct Sim {
     unsigned long long thr_cut[5] = {};
     int sweep_cfg = -1;  // autotuned fused-sweep configuration (-1: not chosen yet)
     uint32_t flags = 0;  // MQV_FLAG_* of the run parameters
+    // a device wait gave up: compute is refused until the state is set again
+    bool failed = false;
+    // one-shot injected timeout of the next fused band sweep (tests)
+    int inject_row = -1;
+    unsigned long long inject_wait_ns = 0;
     // int8 models: u53 cut of every possible dE (int8_cut_table), on the device
     unsigned long long* d_cuts = nullptr;
     int n_cuts = 0;

@@ -64,6 +64,11 @@ struct Ising2DArgs {
     int* status;
     int* counter;  // next tile (zeroed before the launch)
     uint32_t rk0[10], rk1[10];  // Philox round keys of `key`
+    // bounded waits: a wait gives up after wait_ns and sets MQV_ERR_TIMEOUT.
+    // withhold >= 0 (tests of that path, band kernel only): CTA 0 never
+    // issues its staged row `withhold`, so the wait for it runs out.
+    unsigned long long wait_ns;
+    int withhold;
 };
 
 // Philox4x32-10 with the round keys taken from the launch arguments (the
@@ -377,7 +382,7 @@ __global__ void __launch_bounds__(NWARP * 32) ising2d_sweep(const __grid_constan
                     for (uint32_t k = 1;; ++k) {
                         __nanosleep(64);
                         if (mbar_try_wait(bar, par)) break;
-                        if ((k & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
+                        if ((k & 63u) == 0 && global_timer_ns() - t0 > a.wait_ns) {
                             timed_out = 1;
                             break;
                         }
@@ -568,6 +573,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     __syncthreads();
     // staged row r -> slot r % NSB (thread 0)
     auto issue = [&](int r) {
+        if (blockIdx.x == 0 && r == a.withhold) return;  // injected: the row's wait runs out
         const int y = wrapi(y0 - 2 + r, L);
         const uint32_t bar = smem_addr(&bars[r % NSB]);
         mbar_expect_tx(bar, (uint32_t)L);
@@ -651,7 +657,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
                 for (uint32_t i = 1;; ++i) {
                     __nanosleep(64);
                     if (mbar_try_wait(bar, par)) break;
-                    if ((i & 63u) == 0 && global_timer_ns() - t0 > 2000000000ull) {
+                    if ((i & 63u) == 0 && global_timer_ns() - t0 > a.wait_ns) {
                         timed_out = 1;
                         break;
                     }
@@ -751,6 +757,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
             const uint64_t t0 = global_timer_ns();
             const int issued = k == 0 ? NSB : k - 1 + NSB;  // rows issued before the stop
             for (int r = k; r < NR && r < issued; ++r) {
+                if (blockIdx.x == 0 && r == a.withhold) continue;  // never issued
                 const uint32_t bar = smem_addr(&bars[r % NSB]);
                 const uint32_t par = (uint32_t)(r / NSB) & 1u;
                 while (!mbar_try_wait(bar, par) && global_timer_ns() - t0 < 1000000000ull) __nanosleep(1000);
@@ -1005,6 +1012,8 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
     a.acc = acc;
     a.status = s->d_status;
     a.counter = s->d_counter;
+    a.wait_ns = 2000000000ull;  // 2 s
+    a.withhold = -1;
 }
 
 // Time every fitting candidate on this lattice (sweeps into the scratch
@@ -1074,8 +1083,17 @@ static int pick_config(Sim* s)
     return best;
 }
 
+// A band configuration that fits the lattice (-1: none), for the injected timeout.
+int ising2d_band_config(const Sim* s)
+{
+    for (int k = 0; k < kNumConfigs; ++k)
+        if (kConfigs[k].band && config_fits(kConfigs[k], s->len)) return k;
+    return -1;
+}
+
 cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
 {
+    if (s->inject_row >= 0) s->sweep_cfg = ising2d_band_config(s);
     if (s->sweep_cfg < 0) {
         s->sweep_cfg = pick_config(s);
         if (s->sweep_cfg < 0) return cudaErrorInvalidValue;
@@ -1083,6 +1101,11 @@ cudaError_t launch_ising2d_sweep(Sim* s, long long* acc)
     const SweepConfig& c = kConfigs[s->sweep_cfg];
     Ising2DArgs a{};
     fill_args(s, c, acc, a);
+    if (s->inject_row >= 0) {  // one sweep only
+        a.withhold = s->inject_row;
+        a.wait_ns = s->inject_wait_ns;
+        s->inject_row = -1;
+    }
     if (!c.band) {  // tiles are taken from a counter; bands are fixed per CTA
         const cudaError_t e = cudaMemsetAsync(s->d_counter, 0, sizeof(int), s->stream);
         if (e != cudaSuccess) return e;

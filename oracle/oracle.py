@@ -246,6 +246,8 @@ class RefHarness:
         lib.ref_emcs_generic.restype = C.c_int
         lib.ref_emcs_generic.argtypes = [C.c_int, C.c_int, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double,
                                          C.c_double, C.c_uint64, C.c_int, C.c_int, C.c_int, C.c_int, _f64p, _f64p]
+        lib.ref_wolff_ising2d.restype = C.c_int
+        lib.ref_wolff_ising2d.argtypes = [C.c_int, C.c_double, C.c_uint64, C.c_int, C.c_int, _f64p, _f64p]
         lib.ref_calc_mh_ratio.restype = C.c_double
         lib.ref_calc_mh_ratio.argtypes = [C.c_double]
         lib.ref_pt_calcprob.restype = C.c_int
@@ -381,6 +383,14 @@ class RefHarness:
         assert self.lib.ref_emcs_generic(kind, L, dim, J, p0, p1, p2, beta, seed, ncluster, nmetro, ntherm, nmeas,
                                          obs, mc) == 0
         return obs.reshape(nmeas, 2), mc
+
+    def wolff_ising2d_timed(self, L, beta, seed, ntherm, nclusters):
+        """The reference's Wolff<Ising<int>> on one core: (seconds, summed
+        cluster size) of nclusters clusters after ntherm EMCS."""
+        t = np.zeros(1)
+        tot = np.zeros(1)
+        assert self.lib.ref_wolff_ising2d(L, beta, seed, ntherm, nclusters, t, tot) == 0
+        return float(t[0]), float(tot[0])
 
     def farm(self, length, beta, nthreads, seed=12345):
         return RefFarm(self.lib, length, beta, nthreads, seed)

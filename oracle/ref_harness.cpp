@@ -806,3 +806,31 @@ extern "C" int ref_emcs_generic(int kind, int len, int dim, double J, double p0,
     }
     return 0;
 }
+
+// The reference's Wolff<Ising<int>> (src/hamiltonian/Ising.h:122-169) on
+// FixedDimRegularHypercubic<2>(len) with RNGCache<mt19937_64>: ntherm EMCS of
+// one cluster + one random-site sweep from initstatespace, then nclusters
+// clusters alone, timed.  Writes the seconds and the summed cluster size.
+extern "C" int ref_wolff_ising2d(int len, double beta, uint64_t seed, int ntherm, int nclusters, double* seconds,
+                                 double* total)
+{
+    typedef FixedDimRegularHypercubic<2> G;
+    G grid(len);
+    Ising<int> ham(-1.0);
+    MARQOV::Space<std::array<int, 1>, G> ss(grid.size());
+    RNGCache<std::mt19937_64> rng(seed);
+    ham.initstatespace(ss, grid, rng);
+    MARQOV::Wolff<Ising<int>, G> wolff;
+    const int N = (int)grid.size();
+    for (int t = 0; t < ntherm; ++t) {
+        wolff.move(ham, grid, ss, rng, beta, rng.integer(N));
+        for (int i = 0; i < N; ++i) MARQOV::Metropolis<Ising<int>, G>::move(ham, grid, ss, rng, beta, rng.integer(N));
+    }
+    double tot = 0;
+    const auto t0 = std::chrono::steady_clock::now();
+    for (int c = 0; c < nclusters; ++c) tot += wolff.move(ham, grid, ss, rng, beta, rng.integer(N));
+    const auto t1 = std::chrono::steady_clock::now();
+    *seconds = std::chrono::duration<double>(t1 - t0).count();
+    *total = tot;
+    return 0;
+}
