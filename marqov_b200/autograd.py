@@ -119,3 +119,52 @@ def phi4_observables(beta: torch.Tensor, lam: torch.Tensor, ens: Phi4Ensemble) -
     """<E>, <|m|>, U4 per (beta, lambda) pair, [R, 3]; differentiable in beta
     and lambda through the fluctuation-dissipation kernel."""
     return _Phi4Observables.apply(beta, lam, ens)
+
+
+# ---------------------------------------------------------------------------
+# Uses of the gradients: coupling fitting and critical-point location.
+
+def _scalar_obs(beta: float, lam: float, ens: Phi4Ensemble):
+    """(observables [3], d obs / d beta [3]) of one chain at (beta, lam)."""
+    b = torch.tensor([beta], dtype=torch.float64)
+    lm = torch.tensor([lam], dtype=torch.float64)
+    s = ens.samples(b, lm)
+    obs, jac, _ = phi4_fdt(s, b, lm, ens)
+    return obs[0].cpu(), jac[0, :, 0].cpu()
+
+
+def fit_beta(target: float, lam: float, ens: Phi4Ensemble, beta0: float, which: int = 0, steps: int = 6,
+             max_step: float = 0.01):
+    """The beta at which observable `which` (0: <E>, 1: <|m|>, 2: U4) of the
+    phi^4 ensemble equals `target`: Newton steps beta <- beta - (O - target) /
+    (dO/dbeta) with the derivative from the fluctuation-dissipation kernel,
+    each step capped at max_step.  Returns (beta, [(beta, O, dO/dbeta), ...]).
+    Each step runs fresh chains with the ensemble's seed plus the step."""
+    beta, hist = float(beta0), []
+    for k in range(steps):
+        e = Phi4Ensemble(**{**ens.__dict__, "seed": ens.seed + k})
+        obs, d = _scalar_obs(beta, lam, e)
+        o, do = float(obs[which]), float(d[which])
+        hist.append((beta, o, do))
+        step = -(o - target) / do if do != 0 else 0.0
+        beta += max(-max_step, min(max_step, step))
+    return beta, hist
+
+
+def binder_crossing(lam: float, ens_a: Phi4Ensemble, ens_b: Phi4Ensemble, beta0: float, steps: int = 5,
+                    max_step: float = 0.005):
+    """The beta at which the Binder cumulants U4 of two lattice sizes cross
+    (the finite-size estimate of the critical coupling): Newton steps on
+    f(beta) = U4_a - U4_b with f' = dU4_a/dbeta - dU4_b/dbeta from the
+    fluctuation-dissipation kernel.  Returns (beta, [(beta, f, f'), ...])."""
+    beta, hist = float(beta0), []
+    for k in range(steps):
+        ea = Phi4Ensemble(**{**ens_a.__dict__, "seed": ens_a.seed + k})
+        eb = Phi4Ensemble(**{**ens_b.__dict__, "seed": ens_b.seed + k})
+        oa, da = _scalar_obs(beta, lam, ea)
+        ob, db = _scalar_obs(beta, lam, eb)
+        f, fp = float(oa[2] - ob[2]), float(da[2] - db[2])
+        hist.append((beta, f, fp))
+        step = -f / fp if fp != 0 else 0.0
+        beta += max(-max_step, min(max_step, step))
+    return beta, hist

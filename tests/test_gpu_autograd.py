@@ -54,31 +54,65 @@ def test_kernel_matches_histogram_reweighting():
 
 
 def test_fdt_agrees_with_finite_differences_common_randoms():
-    """FDT gradients at beta = 0.37, lambda = 1.1 within 2 sigma of central
-    differences (the FD runs reuse the chains' random numbers)."""
-    n = 20000
-    e = ens(n_meas=n, n_therm=500, common_random_numbers=True)
-    b0, l0, db, dl = 0.37, LAM, 0.01, 0.02
-    bs = torch.tensor([b0, b0 + db, b0 - db, b0, b0], dtype=torch.float64)
-    ls = torch.tensor([l0, l0, l0, l0 + dl, l0 - dl], dtype=torch.float64)
+    """FDT gradients of <E>, <|m|> and U4 with respect to beta and lambda, at
+    beta = 0.37, lambda = 1.1 on 3D L = 16, all six within 2 sigma of central
+    differences with step 1e-3 whose chains reuse the central chain's random
+    numbers.  Sigmas: batch means over 20 common batches, the FD one from the
+    per-batch differences (so it keeps the correlation of the paired chains)."""
+    n, nb, h = 40000, 20, 1e-3
+    e = ens(L=16, n_meas=n, n_therm=1000, common_random_numbers=True)
+    b0, l0 = 0.37, LAM
+    bs = torch.tensor([b0, b0 + h, b0 - h, b0, b0], dtype=torch.float64)
+    ls = torch.tensor([l0, l0, l0, l0 + h, l0 - h], dtype=torch.float64)
     s = e.samples(bs, ls).cpu().numpy()
     N = e.sites
     _, jac = FDT.fdt(s[0], N, b0, l0, e.mass)
-    obs, jc, _ = A.phi4_fdt(torch.from_numpy(s[:1]).cuda(), bs[:1], ls[:1], e)
+    _, jc, _ = A.phi4_fdt(torch.from_numpy(s[:1]).cuda(), bs[:1], ls[:1], e)
     np.testing.assert_allclose(jc[0].cpu().numpy(), jac, rtol=1e-8, atol=1e-10)
-    per = [FDT.per_sample(s[k], N, float(bs[k]), float(ls[k]), e.mass) for k in range(5)]
-    # sigma of the FDT estimate from batch means of the per-batch FDT values
-    nb = 20
-    fd_batches = np.stack([FDT.fdt(x, N, b0, l0, e.mass)[1] for x in np.array_split(s[0], nb)])
-    sig_fdt = fd_batches.std(0, ddof=1) / np.sqrt(nb)
-    z = []
-    for t, (i_up, i_dn, h) in enumerate(((1, 2, db), (3, 4, dl))):
-        for j, key in enumerate(("E", "am")):
-            diff = (per[i_up][key] - per[i_dn][key]) / (2 * h)
-            fd, sig_fd = diff.mean(), FDT.batch_sigma(diff, nb)
-            z.append(abs(fd - jac[j, t]) / np.hypot(sig_fd, sig_fdt[j, t]))
-    z = np.array(z)
-    assert (z < 2.0).mean() >= 0.75 and (z < 4.0).all(), f"z-scores {z}"
+    split = [np.array_split(s[k], nb) for k in range(5)]
+    jac_b = np.stack([FDT.fdt(x, N, b0, l0, e.mass)[1] for x in split[0]])
+    sig_fdt = jac_b.std(0, ddof=1) / np.sqrt(nb)
+    obs_b = [np.stack([FDT.observables(x, N, float(bs[k]), float(ls[k]), e.mass) for x in split[k]])
+             for k in range(5)]
+    obs_all = [FDT.observables(s[k], N, float(bs[k]), float(ls[k]), e.mass) for k in range(5)]
+    z = np.zeros((3, 2))
+    for t, (up, dn) in enumerate(((1, 2), (3, 4))):
+        fd = (obs_all[up] - obs_all[dn]) / (2 * h)
+        fd_b = (obs_b[up] - obs_b[dn]) / (2 * h)
+        sig_fd = fd_b.std(0, ddof=1) / np.sqrt(nb)
+        z[:, t] = np.abs(fd - jac[:, t]) / np.hypot(sig_fd, sig_fdt[:, t])
+    assert (z < 2.0).all(), f"z-scores (rows E, |m|, U4; columns beta, lambda):\n{z}"
+
+
+def test_fit_beta_recovers_a_known_coupling():
+    """Coupling fitting with the FDT derivative: the beta whose <E> equals the
+    <E> measured at beta* = 0.372, found by Newton steps from beta = 0.36."""
+    e = ens(L=8, n_meas=20000, n_therm=500, seed=5)
+    target = float(A._scalar_obs(0.372, LAM, A.Phi4Ensemble(**{**e.__dict__, "seed": 999}))[0][0])
+    beta, hist = A.fit_beta(target, LAM, e, 0.36, which=0, steps=5)
+    assert abs(beta - 0.372) < 0.002, (beta, hist)
+    assert all(h[2] < 0 for h in hist)  # <E> falls with beta
+
+
+def test_binder_crossing_locates_the_transition():
+    """Critical-point location with the FDT derivative: the crossing of the
+    Binder cumulants of L = 6 and L = 10 by Newton steps on U4_6 - U4_10,
+    starting at 0.365; it must settle inside the window the configuration
+    scans (0.36 .. 0.38) with a residual within 2 sigma of zero."""
+    ea = ens(L=6, n_meas=30000, n_therm=1000, seed=21)
+    eb = ens(L=10, n_meas=30000, n_therm=1000, seed=41)
+    beta, hist = A.binder_crossing(LAM, ea, eb, 0.365, steps=5)
+    assert 0.36 < beta < 0.385, (beta, hist)
+    # the residual at the final beta, with its batch-means error
+    b = torch.tensor([beta], dtype=torch.float64)
+    lm = torch.tensor([LAM], dtype=torch.float64)
+    u = []
+    for e in (A.Phi4Ensemble(**{**ea.__dict__, "seed": 7}), A.Phi4Ensemble(**{**eb.__dict__, "seed": 8})):
+        sm = e.samples(b, lm).cpu().numpy()[0]
+        ub = np.array([FDT.observables(x, e.sites, beta, LAM, e.mass)[2] for x in np.array_split(sm, 20)])
+        u.append((FDT.observables(sm, e.sites, beta, LAM, e.mass)[2], ub.std(ddof=1) / np.sqrt(20)))
+    f, sf = u[0][0] - u[1][0], np.hypot(u[0][1], u[1][1])
+    assert abs(f) < 2 * sf + 1e-3, (beta, f, sf, hist)
 
 
 def test_autograd_backward_is_vjp_of_the_kernel_jacobian():
