@@ -49,9 +49,219 @@ inline void check(mqv_status s)
     throw Error(s, std::string("[marqov_b200] ") + m);
 }
 
-// Hamiltonian -> model descriptor; specialise lower(const H&, double beta).
+// ---- generic lowering of a Hamiltonian by its term objects -----------------
+//
+// A Hamiltonian written against MARQOV's term API (interactions / onsite /
+// multisite containers of term objects with get(), J, h, k;
+// src/hamiltonian/util/hamparts.h:27-104) is lowered without a
+// specialisation: the containers are found with the reference's detection
+// rules (HasInteractions / HasOnsite / HasFlexTerms,
+// src/libmarqov/metropolishelpers.h:203-288), and each term is recognised by
+// probing its get() -- a linear interaction diagonal in the components
+// (weights (1, ..., 1): the standard interaction; (Delta, Delta, 1): XXZ),
+// onsite terms s^2, (s^2 - 1)^2, s_z or s_z^2.  A term of any other shape
+// gives kind 0, which mqv_create refuses with MQV_ERR_UNSUPPORTED_TERM (no CPU
+// fallback).  The Metropolis proposal is the model's Initializer<H>
+// (ProposalOf<H>; the default of its state type unless specialised).
+namespace detail {
+template <class T, class = int>
+struct has_interactions : std::false_type {};
+template <class T>
+struct has_interactions<T, decltype((void)T::interactions, 0)> : std::true_type {};
+template <class T, class = int>
+struct has_onsite : std::false_type {};
+template <class T>
+struct has_onsite<T, decltype((void)T::onsite, 0)> : std::true_type {};
+template <class T, class = int>
+struct has_multisite : std::false_type {};
+template <class T>
+struct has_multisite<T, decltype((void)T::multisite, 0)> : std::true_type {};
+template <class T, class = int>
+struct has_q : std::false_type {};
+template <class T>
+struct has_q<T, decltype((void)T::q, 0)> : std::true_type {};
+
+template <class SV>
+SV unit(int c, double v)
+{
+    SV x{};
+    x[c] = (typename SV::value_type)v;
+    return x;
+}
+
+// weights of an interaction term whose get() is linear and diagonal in the
+// components; false for any other shape
+template <class SV, class T>
+bool diagonal_weights(T* t, double* w)
+{
+    constexpr int D = (int)std::tuple_size<SV>::value;
+    for (int c = 0; c < D; ++c) {
+        const SV g1 = t->get(unit<SV>(c, 1.0)), g2 = t->get(unit<SV>(c, 2.0));
+        for (int d = 0; d < D; ++d)
+            if (d != c && ((double)g1[d] != 0.0 || (double)g2[d] != 0.0)) return false;
+        w[c] = (double)g1[c];
+        if ((double)g2[c] != 2.0 * w[c]) return false;
+    }
+    return true;
+}
+
+enum OnsiteShape { kOnsiteOther = 0, kOnsiteSq, kOnsiteQuartic, kOnsiteZ, kOnsiteZ2 };
+
+// shape of an onsite term from its values at a few states
+template <class SV, class T>
+int onsite_shape(T* t)
+{
+    constexpr int D = (int)std::tuple_size<SV>::value;
+    auto f = [&](const SV& v) { return (double)t->get(v); };
+    if (D == 1) {
+        const double a = f(unit<SV>(0, 0.0)), b = f(unit<SV>(0, 1.0)), c = f(unit<SV>(0, -1.0)), d = f(unit<SV>(0, 2.0));
+        if (a == 0 && b == 1 && c == 1 && d == 4) return kOnsiteSq;
+        if (a == 1 && b == 0 && c == 0 && d == 9) return kOnsiteQuartic;
+        return kOnsiteOther;
+    }
+    if (D == 3) {
+        const double x = f(unit<SV>(0, 1.0)), y = f(unit<SV>(1, 1.0)), z = f(unit<SV>(2, 1.0)), z2 = f(unit<SV>(2, 2.0)),
+                     zm = f(unit<SV>(2, -1.0)), o = f(SV{});
+        if (o == 0 && x == 0 && y == 0 && z == 1 && z2 == 2 && zm == -1) return kOnsiteZ;
+        if (o == 0 && x == 0 && y == 0 && z == 1 && z2 == 4 && zm == 1) return kOnsiteZ2;
+    }
+    return kOnsiteOther;
+}
+
+template <class C>
+std::size_t size_of(const C& c)
+{
+    return c.size();
+}
+}  // namespace detail
+
+// The Metropolis proposal of Initializer<H>: specialise value for models
+// whose Initializer is not the default of their state type
+// (marqov_b200_marqov.hpp does so from the reference's initializer classes).
+enum { kProposalDefault = 0, kProposalSpin1 = 1, kProposalPottsQ = 2, kProposalShift = 3 };
 template <class H, class Enable = void>
-struct ModelLowering;
+struct ProposalOf {
+    static constexpr int value = kProposalDefault;
+};
+
+template <class H>
+void lower_inter(const H& h, double& J, double* w, int& n, bool& ok, std::true_type)
+{
+    typedef typename H::StateVector SV;
+    n = (int)detail::size_of(h.interactions);
+    if (n >= 1) {
+        J = (double)h.interactions[0]->J;
+        ok = detail::diagonal_weights<SV>(h.interactions[0], w);
+    }
+}
+template <class H>
+void lower_inter(const H&, double&, double*, int& n, bool&, std::false_type)
+{
+    n = 0;
+}
+template <class H>
+bool lower_onsite(const H& h, int* shapes, double* coef, int& n, std::true_type)
+{
+    typedef typename H::StateVector SV;
+    n = (int)detail::size_of(h.onsite);
+    if (n > 2) return false;
+    for (int k = 0; k < n; ++k) {
+        shapes[k] = detail::onsite_shape<SV>(h.onsite[k]);
+        coef[k] = (double)h.onsite[k]->h;
+        if (shapes[k] == detail::kOnsiteOther) return false;
+    }
+    return true;
+}
+template <class H>
+bool lower_onsite(const H&, int*, double*, int& n, std::false_type)
+{
+    n = 0;
+    return true;
+}
+template <class H>
+void lower_potts(const H& h, mqv_model_desc& d, std::true_type)
+{
+    if (detail::size_of(h.multisite) != 1 || ProposalOf<H>::value != kProposalPottsQ) return;
+    d.kind = MQV_MODEL_POTTS;
+    d.q = H::q;
+    d.k = (double)h.multisite[0]->k;
+}
+template <class H>
+void lower_potts(const H&, mqv_model_desc&, std::false_type)
+{
+}
+
+template <class H>
+mqv_model_desc lower_by_terms(const H& h)
+{
+    typedef typename H::StateVector SV;
+    typedef typename SV::value_type T;
+    constexpr int D = (int)std::tuple_size<SV>::value;
+    mqv_model_desc d{};
+    d.kind = 0;  // unsupported unless recognised below
+    double J = 0, w[3] = {1, 1, 1};
+    int ninter = 0;
+    bool inter_ok = true;
+    lower_inter(h, J, w, ninter, inter_ok, detail::has_interactions<H>{});
+    if (!inter_ok || ninter > 1) return d;
+    int shapes[2] = {0, 0};
+    double coef[2] = {0, 0};
+    int nons = 0;
+    if (!lower_onsite(h, shapes, coef, nons, detail::has_onsite<H>{})) return d;
+    const bool flex = detail::has_multisite<H>::value;
+    if (std::is_integral<T>::value && D == 1) {
+        if (flex) {
+            lower_potts(h, d, std::integral_constant<bool, detail::has_q<H>::value && detail::has_multisite<H>::value>{});
+            return d;
+        }
+        if (ninter != 1 || w[0] != 1.0) return d;
+        d.J = J;
+        if (nons == 0 && ProposalOf<H>::value == kProposalDefault) {
+            d.kind = MQV_MODEL_ISING_EMBED;  // the generic Wolff + Embedder of a user Ising
+            return d;
+        }
+        if (ProposalOf<H>::value == kProposalSpin1 && nons >= 1 && shapes[0] == detail::kOnsiteSq &&
+            (nons == 1 || shapes[1] == detail::kOnsiteSq)) {
+            d.kind = MQV_MODEL_BLUME_CAPEL;
+            d.h = coef[0];
+            d.h2 = nons > 1 ? coef[1] : 0.0;
+        }
+        return d;
+    }
+    if (!std::is_floating_point<T>::value || flex || ninter != 1) return d;
+    d.J = J;
+    if (D == 3 && ProposalOf<H>::value == kProposalDefault && w[0] == w[1] && w[2] == 1.0) {
+        bool ok = true;
+        for (int k = 0; k < nons; ++k) ok = ok && shapes[k] == (k == 0 ? detail::kOnsiteZ : detail::kOnsiteZ2);
+        if (!ok) return d;
+        if (nons == 0 && w[0] == 1.0) {
+            d.kind = MQV_MODEL_HEISENBERG;
+            return d;
+        }
+        d.kind = MQV_MODEL_XXZ;
+        d.delta = w[0];
+        d.h = nons > 0 ? coef[0] : 0.0;
+        d.h2 = nons > 1 ? coef[1] : 0.0;
+        return d;
+    }
+    if (D == 1 && w[0] == 1.0 && ProposalOf<H>::value == kProposalShift) {
+        for (int k = 0; k < nons; ++k)
+            if (shapes[k] != (k == 0 ? detail::kOnsiteSq : detail::kOnsiteQuartic)) return d;
+        d.kind = MQV_MODEL_PHI4;
+        d.h = nons > 0 ? coef[0] : 0.0;
+        d.h2 = nons > 1 ? coef[1] : 0.0;
+        d.cap = 0.5;  // Phi4_Initializer_Cartesian's amplitude (src/hamiltonian/Phi4.h:47)
+    }
+    return d;
+}
+
+// Hamiltonian -> model descriptor.  The primary template lowers by term
+// probing (lower_by_terms); specialise lower(const H&, double beta) for a
+// model whose terms are not of the recognised shapes.
+template <class H, class Enable = void>
+struct ModelLowering {
+    static mqv_model_desc lower(const H& h, double) { return lower_by_terms(h); }
+};
 
 // Hypercubic lattices: specialise get() to return true with (dim, len).
 template <class L, class Enable = void>

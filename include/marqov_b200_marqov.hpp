@@ -15,9 +15,12 @@
  *   RegularHypercubic, FixedDimRegularHypercubic<d>: stencil  src/lattice/regular_hypercubic.h
  *   SimpleBipartite: stencil + termselector by sublattice     src/lattice/simple_bipartite.h:8-58
  * Other lattices (RegularRandomBond, GraphFromCSV, ...) are lowered to CSR
- * from nbrs() / bnds() by LatticeLowering.  MARQOV's Phi4 is a three-
- * component field; the engine's phi^4 is the scalar form and has no
- * lowering from that class.
+ * from nbrs() / bnds() by LatticeLowering.  Hamiltonians without a block
+ * here -- user classes written with MARQOV's term API -- are lowered by
+ * probing their terms (lower_by_terms in marqov_b200_core.hpp); the
+ * ProposalOf blocks below tell it their Initializer.  MARQOV's Phi4 is a
+ * three-component field; the engine's phi^4 is the scalar form, and a
+ * three-component Phi4 comes out of the term probe as unsupported.
  */
 #ifndef MARQOV_B200_MARQOV_HPP
 #define MARQOV_B200_MARQOV_HPP
@@ -159,6 +162,23 @@ struct HypercubicShape<FixedDimRegularHypercubic<D>> {
         len = g.len;
         return true;
     }
+};
+#endif
+
+// Proposals of the generic lowering, from the reference's initializer
+// classes (src/hamiltonian/util/initializers.h:87-119, src/hamiltonian/Phi4.h:37-58)
+#ifdef INITIALIZERS_H
+template <class H>
+struct ProposalOf<H, typename std::enable_if<std::is_base_of<Spin1_Initializer<typename H::StateVector>,
+                                                             Initializer<H>>::value>::type> {
+    static constexpr int value = kProposalSpin1;
+};
+#endif
+#ifdef PHI4_H
+template <class H>
+struct ProposalOf<H, typename std::enable_if<std::is_base_of<Phi4_Initializer_Cartesian<typename H::StateVector>,
+                                                             Initializer<H>>::value>::type> {
+    static constexpr int value = kProposalShift;
 };
 #endif
 

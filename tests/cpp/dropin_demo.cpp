@@ -53,6 +53,49 @@ struct Space {
 
 #include "marqov_b200_marqov.hpp"
 
+// User Hamiltonians written against MARQOV's term API (hamparts.h), with no
+// lowering of their own: the C++ layer recognises their terms.
+struct MyIsing {
+    static constexpr int SymD = 1;
+    typedef std::array<int, 1> StateVector;
+    Standard_Interaction<StateVector> inter;
+    std::array<Standard_Interaction<StateVector>*, 1> interactions{{&inter}};
+    explicit MyIsing(double J) : inter(J) {}
+};
+template <class SV>
+struct MyXXZInteraction : public Interaction<SV> {
+    double delta;
+    MyXXZInteraction(double J, double d) : Interaction<SV>(J), delta(d) {}
+    SV get(const SV& p) override { return {{delta * p[0], delta * p[1], p[2]}}; }
+};
+template <class SV>
+struct MyFieldZ : public OnSite<SV, double> {
+    explicit MyFieldZ(double h) : OnSite<SV, double>(h) {}
+    double get(const SV& p) override { return p[2]; }
+};
+struct MyXXZ {
+    static constexpr int SymD = 3;
+    typedef std::array<double, 3> StateVector;
+    MyXXZInteraction<StateVector> inter;
+    MyFieldZ<StateVector> field;
+    std::array<Interaction<StateVector>*, 1> interactions{{&inter}};
+    std::array<OnSite<StateVector, double>*, 1> onsite{{&field}};
+    MyXXZ(double delta, double h) : inter(1.0, delta), field(h) {}
+};
+// a term the engine does not lower: an interaction that mixes components
+template <class SV>
+struct SwapXY : public Interaction<SV> {
+    explicit SwapXY(double J) : Interaction<SV>(J) {}
+    SV get(const SV& p) override { return {{p[1], p[0], p[2]}}; }
+};
+struct MyOdd {
+    static constexpr int SymD = 3;
+    typedef std::array<double, 3> StateVector;
+    SwapXY<StateVector> inter{-1.0};
+    std::array<Interaction<StateVector>*, 1> interactions{{&inter}};
+    explicit MyOdd(double) {}
+};
+
 // MARQOV::Config's fields (src/libmarqov/core.h:74-192); core.h itself needs HDF5
 struct Config {
     std::string outpath;
@@ -144,6 +187,41 @@ int main()
         xxz->wrmploop();
         xxz->gameloop();
         for (const auto& o : xxz->observables()) std::printf("xxz %.17g %.17g\n", o.e, o.m);
+
+        // user term-API Hamiltonians, lowered by their terms
+        RegularHypercubic lu(16, 2);
+        Config cu("out");
+        cu.seed = 44;
+        cu.ncluster = 1;
+        cu.nmetro = 1;
+        cu.warmupsteps = 5;
+        cu.gameloopsteps = 4;
+        auto mi = marqov_b200::makeGPUCore<RegularHypercubic, MyIsing>(
+            std::make_tuple(std::ref(lu), cu, std::make_tuple(0.44, -1.0)));
+        mi->init();
+        mi->wrmploop();
+        mi->gameloop();
+        for (const auto& o : mi->observables()) std::printf("myising %.17g %.17g\n", o.e, o.m);
+        RegularHypercubic lx(6, 3);
+        Config cxx("out");
+        cxx.seed = 45;
+        cxx.ncluster = 0;
+        cxx.nmetro = 1;
+        cxx.warmupsteps = 3;
+        cxx.gameloopsteps = 3;
+        auto mx = marqov_b200::makeGPUCore<RegularHypercubic, MyXXZ>(
+            std::make_tuple(std::ref(lx), cxx, std::make_tuple(0.7, 0.6, 0.25)));
+        mx->init();
+        mx->wrmploop();
+        mx->gameloop();
+        for (const auto& o : mx->observables()) std::printf("myxxz %.17g %.17g\n", o.e, o.m);
+        try {
+            auto bad = marqov_b200::makeGPUCore<RegularHypercubic, MyOdd>(
+                std::make_tuple(std::ref(lx), cxx, std::make_tuple(0.7, 1.0)));
+            std::printf("unsupported none\n");
+        } catch (const marqov_b200::Error& e) {
+            std::printf("unsupported %d\n", (int)e.status);
+        }
     } catch (const marqov_b200::Error& e) {
         if (e.status == MQV_ERR_NO_DEVICE) {
             std::printf("no device: %s\n", e.what());

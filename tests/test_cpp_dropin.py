@@ -79,3 +79,20 @@ def test_dropin_equals_python_api():
         c.emcs(4, ncluster=0, nmetro=1, measure=False)
         xo, _ = c.emcs(3, ncluster=0, nmetro=1)
     np.testing.assert_array_equal(xxz, xo[:, :2])
+    # user term-API classes: MyIsing lowers to the generic-Wolff Ising, MyXXZ
+    # to XXZ (Delta = 0.6, H = 0.25), a component-mixing interaction is refused
+    mi = np.array([[float(a), float(b)] for t, a, b in (l for l in lines if l[0] == "myising")])
+    cfg = M.Config(seed=44, repid=0, ncluster=1, nmetro=1)
+    with M.makeCore(M.RegularHypercubic(16, 2), cfg, M.Ising(-1.0, "int8"), 0.44) as c:
+        c.init()
+        c.emcs(5, measure=False)
+        o, _ = c.emcs(4)
+    np.testing.assert_array_equal(mi, o[:, :2])
+    mx = np.array([[float(a), float(b)] for t, a, b in (l for l in lines if l[0] == "myxxz")])
+    cfg = M.Config(seed=45, repid=0, ncluster=0, nmetro=1)
+    with M.makeCore(M.RegularHypercubic(6, 3), cfg, M.XXZAntiferro(0.6, 0.25), 0.7) as c:
+        c.init()
+        c.emcs(3, ncluster=0, nmetro=1, measure=False)
+        o, _ = c.emcs(3, ncluster=0, nmetro=1)
+    np.testing.assert_array_equal(mx, o[:, :2])
+    assert [l for l in lines if l[0] == "unsupported"] == [["unsupported", str(M._lib.ERR_UNSUPPORTED_TERM)]]
