@@ -215,6 +215,23 @@ def run_reference(args, ws, rank):
         t += farm.step(nup)
     farm.close()
     value = cores * nup * args.steps / (t * 1e9)
+    # the parity mode: the reference's Metropolis in the engine's colour order
+    # on the keyed Philox stream (one core, one sweep of a smaller lattice)
+    colour = None
+    try:
+        from oracle.oracle import Oracle
+        orc = Oracle()
+        Lc = 1024
+        g = orc.hypercubic(2, Lc)
+        sp = np.where(np.random.default_rng(3).random(Lc * Lc) > 0.5, 1, -1).astype(np.int8)
+        t0 = time.perf_counter()
+        ref.sweeps_int(1, g, sp, -1.0, 0.0, BETA_C, 2024, 0, 0, 1, want_obs=False)
+        tc = time.perf_counter() - t0
+        colour = {"value": Lc * Lc / (tc * 1e9), "unit": UNIT, "cores": 1,
+                  "sample": f"one colour-order sweep of 2D Ising L={Lc} through MARQOV::Metropolis<Ising<int>> "
+                            f"with the keyed Philox RNGCache (the parity mode), {tc:.2f} s"}
+    except Exception as exc:
+        colour = {"unavailable": str(exc)}
     line = {
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * t / args.steps,
@@ -224,7 +241,11 @@ def run_reference(args, ws, rank):
                    "beta": BETA_C, "replicas": cores, "updates_per_replica_per_step": nup},
         "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "reference",
                          "sample": f"{cores} replicas x {nup} random-site updates per step on L={L}, "
-                                   f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>"},
+                                   f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>",
+                         "host_nproc": os.cpu_count(),
+                         "build": "g++ -O3 -march=x86-64-v3 from the reference's own headers (oracle/build.py): "
+                                  "built where the reference source is, run on this host, so not -march=native"},
+        "colour_order_parity_mode": colour,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line))
@@ -244,7 +265,8 @@ def cpu_baseline(L):
     farm.close()
     return {"value": nup / (t * 1e9), "unit": UNIT, "cores": 1, "kind": "reference",
             "sample": f"{nup} random-site updates (half a sweep) of one L={L} replica, "
-                      f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>, {t:.1f} s"}
+                      f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>, {t:.1f} s",
+            "host_nproc": os.cpu_count()}
 
 
 # ---------------------------------------------------------------------------

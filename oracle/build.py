@@ -3,8 +3,10 @@
 * ``oracle/liboracle.so``        -- the C restatement (oracle.c), always built.
 * ``oracle/_ref/libmarqov_ref.so`` -- ref_harness.cpp compiled against the
   reference's own headers, built only where the reference source tree exists
-  (``MARQOV_REF_SRC`` or /root/reference/src).  The output stays out of git but
+  (``MARQOV_REF_SRC`` or ``reference/src`` beside the checkout).  The output stays out of git but
   travels with the working tree, so machines without the source can still load it.
+  (The reference tree is ``MARQOV_REF_SRC``, else ``../reference/src`` beside
+  this checkout.)
 
 Both use a conservative ``-march=x86-64-v3`` so the binaries run on any AVX2
 host, not only the build machine, and ``-ffp-contract=off`` so every FP64
@@ -18,7 +20,8 @@ import subprocess
 import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-REF_SRC_DEFAULT = "/root/reference/src"
+# the reference's source tree: MARQOV_REF_SRC, else a checkout of it beside this one
+REF_SRC_DEFAULT = os.path.join(os.path.dirname(HERE), "..", "reference", "src")
 ARCH = ["-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-shared"]
 
 

@@ -1,7 +1,7 @@
 """Build recipe of the C++ drop-in test program (tests/cpp/dropin_demo.cpp).
 
 Compiles against the reference's own headers where the reference source tree
-is present (MARQOV_REF_SRC or /root/reference/src) and links the engine
+is present (MARQOV_REF_SRC, else reference/src beside this checkout) and links the engine
 library; the binary (tests/cpp/_build/dropin_demo, git-ignored) finds the
 library through its rpath.  Returns None where the reference is absent.
 """
@@ -13,7 +13,8 @@ import sys
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(os.path.dirname(HERE))
-REF_SRC_DEFAULT = "/root/reference/src"
+# the reference's source tree: MARQOV_REF_SRC, else a checkout of it beside this one
+REF_SRC_DEFAULT = os.path.join(ROOT, "..", "reference", "src")
 OUT = os.path.join(HERE, "_build", "dropin_demo")
 
 
