@@ -211,10 +211,13 @@ MQV_API mqv_status mqv_wolff(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
  * no cudaMalloc/cudaFree stalls allowed between their streams).  Same
  * clusters, sizes and counters as mqv_wolff.  The bitmap starts at zero
  * (module load) and every cluster leaves it zero.  The array is shared by
- * all handles on a device: calls whose kernels may overlap race on it and
- * must be serialised by the caller.  The first call on a device looks up the
- * array's address and may load the module, so it must come before any
- * stream capture. */
+ * all handles on a device: calls whose kernels may overlap race on it, so
+ * the caller orders them on the GPU (one stream, or an event or a
+ * synchronisation between streams); host calls one after the other are not
+ * enough when sizes is NULL, since the call then returns while its kernels
+ * run.  The first call on a device looks up the array's address, keeps it
+ * and may load the module, so it must come before any stream capture, and
+ * the handle must not be used across a reset of its CUDA context. */
 MQV_API mqv_status mqv_wolff_noalloc(mqv_sim* sim, int32_t nclusters, int32_t* sizes);
 /* n_emcs elementary MC steps (ncluster clusters then nmetro sweeps each),
  * measuring after every step.  obs (host, may be NULL) receives n_emcs
