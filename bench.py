@@ -307,12 +307,16 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
 
     Batched: one Batch (resident CTAs for the members that fit shared memory,
     graph-replayed kernels for the others), CUDA events around the window.
-    Plain: the same members as 256 independent handles, each on its own
-    stream, issued from a pool of host threads (one member at a time per
-    thread, no synchronisation between members), wall time around the
-    window.  Both arms run the identical chains (bit-exact), so the
-    tau_int-corrected error bars of E and |m| reported for a few members are
-    equal at equal EMCS counts and the rates compare directly."""
+    Plain per-replica launches: the same members as 256 independent handles
+    on the launch-per-step path (a launch per cluster, per colour and per
+    measurement; MQV_FLAG_NO_RESIDENT), each on its own stream, issued from a
+    pool of host threads (no synchronisation between members), wall time
+    around the window.  The same handles on the resident path (small members
+    keep their state in one CTA's shared memory for a whole call) are timed
+    as a second plain variant.  All arms run the identical chains
+    (bit-exact), so the tau_int-corrected error bars of E and |m| reported
+    for a few members are equal at equal EMCS counts and the rates compare
+    directly."""
     from concurrent.futures import ThreadPoolExecutor
     members = potts_farm(M)
     sites = sum(m[0].size() for m in members)
@@ -336,28 +340,39 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
         res = []
         tw = timed(torch, st, lambda: res.append(b.emcs(50, 1, 0)))
         mcw = res[0][1]
-    singles = [M.makeCore(*m) for m in members]
     nthreads = threads or min(32, os.cpu_count() or 1)
-    try:
-        with ThreadPoolExecutor(nthreads) as ex:
-            def prep(c):
-                c.init()
-                c.emcs(therm, 1, 1, measure=False)
-                c.synchronize()
-            list(ex.map(prep, singles))
-            torch.cuda.synchronize()
-            w0 = time.perf_counter()
-            outs = list(ex.map(lambda c: c.emcs(emcs, 1, 1), singles))
-            torch.cuda.synchronize()
-            wall_p = time.perf_counter() - w0
-        same = all((outs[i][0] == obs_b[:, i, :]).all() for i in range(len(singles)))
-        same = same and all((singles[i].state == final_b[i]).all() for i in range(3))
-    finally:
-        for c in singles:
-            c.close()
+
+    def plain(resident):
+        singles = []
+        for lat, cfg, ham, beta in members:
+            c1 = M.Config(seed=cfg.seed, repid=cfg.repid, resident=resident)
+            singles.append(M.makeCore(lat, c1, ham, beta))
+        try:
+            with ThreadPoolExecutor(nthreads) as ex:
+                def prep(c):
+                    c.init()
+                    c.emcs(therm, 1, 1, measure=False)
+                    c.synchronize()
+                list(ex.map(prep, singles))
+                torch.cuda.synchronize()
+                w0 = time.perf_counter()
+                outs = list(ex.map(lambda c: c.emcs(emcs, 1, 1), singles))
+                torch.cuda.synchronize()
+                wall = time.perf_counter() - w0
+            same = all((outs[i][0] == obs_b[:, i, :]).all() for i in range(len(singles)))
+            same = same and all((singles[i].state == final_b[i]).all() for i in range(3))
+        finally:
+            for c in singles:
+                c.close()
+        return wall, outs, same
+
+    wall_p, outs, same = plain(False)
+    wall_pr, _, same_r = plain(True)
+    same = same and same_r
     rate_b = sites * emcs / (dev_b * 1e9)
     rate_b_wall = sites * emcs / (wall_b * 1e9)
     rate_p = sites * emcs / (wall_p * 1e9)
+    rate_pr = sites * emcs / (wall_pr * 1e9)
     pick = [0, 1, 2, int(np.argmax([m[0].size() for m in members]))]
     bars = {str(i): {"L": int(members[i][0].len),
                      "batched": {"e": _tau_err(obs_b[:, i, 0]), "m": _tau_err(obs_b[:, i, 1])},
@@ -369,9 +384,13 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
         "batched": {"value": rate_b, "value_wall": rate_b_wall, "emcs": emcs, "seconds_device": dev_b,
                     "seconds_wall": wall_b, "gpu_launches": int(launches_b), "graph_emcs_per_launch": 8},
         "plain": {"value": rate_p, "emcs": emcs, "seconds_wall": wall_p,
-                  "how": f"256 handles, each on its own stream, one mqv_emcs call each from {nthreads} host "
-                         f"threads (no synchronisation between members)"},
+                  "how": f"256 handles on the launch-per-step path, each on its own stream, one mqv_emcs call "
+                         f"each from {nthreads} host threads (no synchronisation between members)"},
+        "plain_resident": {"value": rate_pr, "emcs": emcs, "seconds_wall": wall_pr,
+                           "how": "the same handles on the resident path (members of <= 65536 sites in one CTA's "
+                                  "shared memory per call)"},
         "batched_vs_plain": rate_b_wall / rate_p,
+        "batched_vs_plain_resident": rate_b_wall / rate_pr,
         "chains_identical": bool(same),
         "error_bars": bars,
         "wolff_cluster_spins_per_ns": float(mcw.sum()) / (tw * 1e9),
