@@ -78,6 +78,11 @@ cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluste
 // largest with max_n sites), measurement slots from slot0 (smem_emcs.cu)
 cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, int64_t max_n,
                                   uint32_t e0, int slot0, int count, int ncluster, int nmetro, int device);
+// the same for members held by clusters of `ctas` CTAs (cluster_emcs.cu)
+cudaError_t batch_launch_cluster(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nmem, int ctas,
+                                 uint32_t e0, int slot0, int count, int ncluster, int nmetro);
+int cluster_ctas(int64_t n);
+bool cluster_launchable(int ctas);
 cudaError_t batch_launch_chunk_start(const BatchLaunch& b, cudaStream_t st, uint32_t e);
 cudaError_t batch_launch_finalize(const BatchLaunch& b, cudaStream_t st, int nslots, double* out);
 // raw sums of the chunk's slots -> samples[r][e0 + slot][4] (n_total EMCS per member)

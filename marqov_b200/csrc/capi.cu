@@ -40,6 +40,7 @@ cudaError_t wolff_noalloc_scratch(int device, uint32_t** out);
 cudaError_t launch_wolff_int8_noalloc(Sim* s, uint32_t* scratch, int slot);
 const int32_t* wolff_noalloc_sizes(const uint32_t* scratch);
 bool resident_fits(const Sim* s);
+cudaError_t launch_emcs_cluster(Sim* s, int n_emcs, int ncluster, int nmetro, long long* acc, int32_t* csize);
 cudaError_t launch_emcs_resident(Sim* s, int n_emcs, int ncluster, int nmetro, bool measure, long long* acc,
                                  int32_t* csize);
 cudaError_t launch_acc_to_samples(const long long* acc, int is_f32, int nslots, double* out, cudaStream_t st);
@@ -402,6 +403,17 @@ static mqv_status check_wolff_supported(Sim* s)
 
 // EMCS of this handle run on the resident path (smem_emcs.cu)?
 static bool use_resident(const Sim* s) { return !(s->flags & MQV_FLAG_NO_RESIDENT) && resident_fits(s); }
+// ... or on a thread-block cluster (cluster_emcs.cu), for int8 stencils of
+// 65,537 .. 262,144 sites the device can co-schedule
+static bool use_cluster(Sim* s)
+{
+    if ((s->flags & MQV_FLAG_NO_RESIDENT) || s->is_f32 || s->lat_kind != MQV_LATTICE_HYPERCUBIC || resident_fits(s))
+        return false;
+    const int c = cluster_ctas(s->n);
+    if (c < 2) return false;
+    if (s->cluster_ok < 0) s->cluster_ok = cluster_launchable(c) ? 1 : 0;
+    return s->cluster_ok == 1;
+}
 
 }  // namespace mqv
 
@@ -741,6 +753,8 @@ MQV_API mqv_status mqv_wolff(mqv_sim* h, int32_t nclusters, int32_t* sizes)
         if (st) return st;
         if (use_resident(s)) {
             MQV_CK(launch_emcs_resident(s, chunk, 1, 0, false, nullptr, s->d_csize));
+        } else if (use_cluster(s)) {
+            MQV_CK(launch_emcs_cluster(s, chunk, 1, 0, nullptr, s->d_csize));
         } else {
             for (int c = 0; c < chunk; ++c) {
                 st = launch_cluster(s, c);
@@ -820,6 +834,9 @@ MQV_API mqv_status mqv_emcs(mqv_sim* h, int32_t n_emcs, int32_t ncluster, int32_
         if (use_resident(s)) {
             MQV_CK(ensure_cuts(s));
             MQV_CK(launch_emcs_resident(s, ch, ncluster, nmetro, true, s->d_acc, s->d_csize));
+        } else if (use_cluster(s)) {
+            MQV_CK(ensure_cuts(s));
+            MQV_CK(launch_emcs_cluster(s, ch, ncluster, nmetro, s->d_acc, s->d_csize));
         } else {
             for (int e = 0; e < ch; ++e) {
                 for (int c = 0; c < ncluster; ++c) {
@@ -887,6 +904,9 @@ MQV_API mqv_status mqv_emcs_samples(mqv_sim* h, int32_t n_emcs, int32_t ncluster
         if (use_resident(s)) {
             MQV_CK(ensure_cuts(s));
             MQV_CK(launch_emcs_resident(s, ch, ncluster, nmetro, true, s->d_acc, s->d_csize));
+        } else if (use_cluster(s)) {
+            MQV_CK(ensure_cuts(s));
+            MQV_CK(launch_emcs_cluster(s, ch, ncluster, nmetro, s->d_acc, s->d_csize));
         } else {
             for (int e = 0; e < ch; ++e) {
                 for (int c = 0; c < ncluster; ++c) {
@@ -952,15 +972,17 @@ MQV_API mqv_status mqv_synchronize(mqv_sim* h)
 MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
 {
     Sim* s = reinterpret_cast<Sim*>(h);
+    MQV_GUARD(s);
     if (!s || !buf || len == 0) return fail(MQV_ERR_INVALID_ARG, "bad arguments");
     char cfg[96] = "";
     if (s->fused_ising2d) ising2d_config_name(s, cfg, sizeof(cfg));
     std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s clusters=%s", s->md.kind,
                   s->lat_kind == MQV_LATTICE_HYPERCUBIC ? (s->termsel ? "bipartite" : "hypercubic") : "csr", (long long)s->n,
                   use_resident(s) ? "resident-smem"
-                                  : (s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8")),
+                  : use_cluster(s) ? "resident-cluster"
+                                   : (s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8")),
                   cfg[0] ? " kernel=" : "", cfg,
-                  use_resident(s) ? "label-smem" : (cluster_by_label(s) ? "label" : "bfs"));
+                  use_resident(s) ? "label-smem" : use_cluster(s) ? "label-dsmem" : (cluster_by_label(s) ? "label" : "bfs"));
     return MQV_OK;
 }
 
@@ -1072,6 +1094,10 @@ struct Batch {
     int32_t* d_res_order = nullptr;
     int nres[2] = {0, 0};
     int64_t res_maxn[2] = {0, 0};
+    // members held by thread-block clusters of c CTAs (c = 2 .. 8): ncl[c]
+    // of them at d_res_order + cl_off[c]
+    int ncl[9] = {};
+    int cl_off[9] = {};
     int64_t* d_site_prefix = nullptr;
     int32_t* d_site_block_rep = nullptr;
     int32_t* d_meas_prefix = nullptr;
@@ -1230,7 +1256,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         r.queue = s->d_queue;
         r.cuts = s->d_cuts;
         r.D = s->max_degree;
-        r.resident = b->resident[(size_t)i];
+        r.resident = b->resident[(size_t)i] ? 1 : 0;
     }
     MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
                            b->stream));
@@ -1292,6 +1318,12 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
             MQV_CK(batch_launch_resident(b->L, b->stream, b->d_res_order + (cls ? b->nres[0] : 0), b->nres[cls],
                                          b->res_maxn[cls], (uint32_t)(done_run + k0), k0, count, ncluster, nmetro,
                                          b->device));
+            b->launches++;
+        }
+        for (int c = 2; c <= 8; ++c) {
+            if (!b->ncl[c]) continue;
+            MQV_CK(batch_launch_cluster(b->L, b->stream, b->d_res_order + b->cl_off[c], b->ncl[c], c,
+                                        (uint32_t)(done_run + k0), k0, count, ncluster, nmetro));
             b->launches++;
         }
         int j = 0;
@@ -1489,12 +1521,21 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     // resident members: int8 stencil lattices that fit one CTA's shared
     // memory, unless their spec asks for the launch path
     b->resident.assign((size_t)n, 0);
-    std::vector<int32_t> res_order[2];
+    std::vector<int32_t> res_order[2], cl_order[9];
+    bool cl_ok[9] = {};
+    for (int c = 2; c <= 8; ++c) cl_ok[c] = cluster_launchable(c);
     for (int r = 0; r < n; ++r) {
         const Sim* s = b->sims[(size_t)r];
-        if (!(specs[r].params.flags & MQV_FLAG_NO_RESIDENT) && resident_fits(s)) {
+        if (specs[r].params.flags & MQV_FLAG_NO_RESIDENT) continue;
+        if (resident_fits(s)) {
             b->resident[(size_t)r] = 1;
             res_order[s->n > kResSmall ? 1 : 0].push_back(r);
+        } else if (!s->is_f32 && s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
+            const int c = cluster_ctas(s->n);
+            if (c >= 2 && cl_ok[c]) {
+                b->resident[(size_t)r] = 2;
+                cl_order[c].push_back(r);
+            }
         }
     }
     for (int k = 0; k < 2; ++k) {
@@ -1505,6 +1546,11 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     }
     std::vector<int32_t> res_all(res_order[0]);
     res_all.insert(res_all.end(), res_order[1].begin(), res_order[1].end());
+    for (int c = 2; c <= 8; ++c) {
+        b->cl_off[c] = (int)res_all.size();
+        b->ncl[c] = (int)cl_order[c].size();
+        res_all.insert(res_all.end(), cl_order[c].begin(), cl_order[c].end());
+    }
     // per-colour work: colour c concatenates every graph member's colour-c
     // sites (resident members contribute none), each member's count padded
     // to whole warp blocks of kAccSites, so that a warp's block lies in one

@@ -146,6 +146,9 @@ constexpr int64_t kResidentMaxSites = 65536;
 constexpr int64_t kResSmall = 16384;
 struct Sim;
 bool resident_fits(const Sim* s);
+// lattices of up to 8 x 32768 sites on a thread-block cluster (cluster_emcs.cu)
+int cluster_ctas(int64_t n);
+bool cluster_launchable(int ctas);
 
 struct Sim;
 // Smallest u53 rejected by update_accepted<pref>(dE, beta, .) (2^53: all accepted).
@@ -196,6 +199,7 @@ struct Sim {
     uint32_t flags = 0;  // MQV_FLAG_* of the run parameters
     // a device wait gave up: compute is refused until the state is set again
     bool failed = false;
+    int cluster_ok = -1;  // the device co-schedules this lattice's thread-block cluster (-1: not asked yet)
     // one-shot injected timeout of the next fused band sweep (tests)
     int inject_row = -1;
     unsigned long long inject_wait_ns = 0;

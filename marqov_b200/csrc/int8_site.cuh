@@ -15,8 +15,8 @@ namespace mqv {
 // update_accepted<1>(dE, beta, word) on the site's acceptance word.  `sub`:
 // the site's sublattice (checkerboard colour) where the lattice has a
 // termselector.  Lanes with live == false touch no memory.
-template <class Lat>
-__device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, int8_t* __restrict__ s, int64_t i,
+template <class Lat, class SP>
+__device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, SP s, int64_t i,
                                           Key key, uint32_t sweep, uint32_t replica,
                                           const unsigned long long* __restrict__ cuts, int D, bool live, int sub = 0,
                                           const uint4* tab = nullptr, uint32_t run0 = 0)
@@ -114,6 +114,16 @@ __device__ __forceinline__ int int8_bond_sum(const ModelDev& m, const Lat& lat, 
         loc *= si;
     }
     return loc;
+}
+template <class SP>
+__device__ __forceinline__ int int8_bond_sum_stencil(const StencilDev& st, SP s, int64_t i, int si, bool potts)
+{
+    int loc = 0;
+    for (int d = 0; d < st.dim; ++d) {
+        const int v = s[st.addr(st.nbr(i, 2 * d))];
+        loc += potts ? (v == si) : st.bond(i, 2 * d) * v;
+    }
+    return 2 * (potts ? loc : loc * si);
 }
 __device__ __forceinline__ int int8_bond_sum(const ModelDev&, const StencilDev& st, const int8_t* __restrict__ s,
                                              int64_t i, int si, bool potts)

@@ -155,6 +155,27 @@ cudaError_t ensure_label_tables(Sim* s)
     return e;
 }
 
+// n_emcs EMCS of a mid-size int8 lattice on a thread-block cluster
+// (cluster_emcs.cu) through the one-member table; acc NULL: no measurement.
+cudaError_t launch_emcs_cluster(Sim* s, int n_emcs, int ncluster, int nmetro, long long* acc, int32_t* csize)
+{
+    cudaError_t e = ensure_label_tables(s);
+    if (e != cudaSuccess) return e;
+    BatchRep r = single_rep(s);
+    r.cluster0 = (uint32_t)s->cluster;
+    single_rep_set<<<1, 1, 0, s->stream>>>(s->d_rep1, r, s->d_ctr1, 0u);
+    BatchLaunch b{};
+    b.reps = s->d_rep1;
+    b.nrep = 1;
+    b.acc = acc;
+    b.csize = csize;
+    e = batch_launch_cluster(b, s->stream, s->d_sbrep1, 1, cluster_ctas(s->n), 0u, 0, n_emcs, ncluster, nmetro);
+    s->launches += 2;
+    s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
+    s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
+    return e;
+}
+
 cudaError_t launch_wolff_label(Sim* s, int slot)
 {
     const cudaError_t e = ensure_label_tables(s);

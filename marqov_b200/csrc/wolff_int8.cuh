@@ -11,9 +11,9 @@ namespace mqv {
 // Seed site, its state and the cluster's new state from the WOLFF_SEED
 // substream (Ising: the flipped spin; Potts: Embedder<Potts<Q>>::draw, a new
 // state different from the old one).
-template <class Lat>
-__device__ __forceinline__ int64_t wolff_int8_seed(const WolffDev& w, const Lat& lat, const int8_t* __restrict__ s,
-                                                   Key key, uint32_t serial, uint32_t tg_seed, int& val, int& newq)
+template <class Lat, class SP>
+__device__ __forceinline__ int64_t wolff_int8_seed(const WolffDev& w, const Lat& lat, SP s, Key key, uint32_t serial,
+                                                   uint32_t tg_seed, int& val, int& newq)
 {
     SubStream rng(key, 0u, serial, tg_seed);
     const int64_t rsite = (int64_t)(rng.next() % (uint64_t)lat.n);

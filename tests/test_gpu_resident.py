@@ -30,6 +30,11 @@ CASES = [
     ("potts2d_L48", lambda M: (M.RegularHypercubic(48, 2), M.Potts(3, -1.0), 1.0050525)),
     ("potts3d_L8_q5", lambda M: (M.RegularHypercubic(8, 3), M.Potts(5, -1.0), 0.9)),
     ("potts2d_L256", lambda M: (M.RegularHypercubic(256, 2), M.Potts(3, -1.0), 1.0050525)),
+    # thread-block clusters (distributed shared memory): 2 .. 8 CTAs
+    ("ising2d_L384_cluster", lambda M: (M.RegularHypercubic(384, 2), M.Ising(-1.0), 0.44068679)),
+    ("potts2d_L512_cluster", lambda M: (M.RegularHypercubic(512, 2), M.Potts(3, -1.0), 1.0050525)),
+    ("ising3d_L48_cluster", lambda M: (M.RegularHypercubic(48, 3), M.Ising(-1.0, "int8"), 0.2216544)),
+    ("ising2d_L320_cluster", lambda M: (M.RegularHypercubic(320, 2), M.Ising(-1.0), 0.5)),
 ]
 
 
@@ -40,6 +45,7 @@ def test_resident_equals_launch_path(name, make, ncluster, nmetro):
     lat, ham, beta = make(M)
     a = run(M, lat, ham, beta, 77, True, 25, ncluster, nmetro)
     b = run(M, lat, ham, beta, 77, False, 25, ncluster, nmetro)
+    assert "resident" in a[3] and "resident" not in b[3], (a[3], b[3])
     assert (a[0] == b[0]).all(), "observables"
     assert (a[1] == b[1]).all(), "cluster sizes"
     assert (a[2] == b[2]).all(), "state"
@@ -103,7 +109,7 @@ def test_batch_resident_members_equal_launch_path():
     (too large, or asked for the launch path) equals the members run one by
     one on the launch path, bit for bit, with and without replica exchange."""
     import marqov_b200 as M
-    sizes = [32, 48, 64, 128, 192, 256, 384, 96]
+    sizes = [32, 48, 64, 128, 192, 256, 384, 512, 96]
     ms = [(M.RegularHypercubic(L, 2), M.Config(seed=40 + i, repid=i), M.Potts(3, -1.0), 1.0 + 0.01 * i)
           for i, L in enumerate(sizes)]
     solo = []
