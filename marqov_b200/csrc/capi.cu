@@ -264,12 +264,12 @@ static mqv_status lower_csr(Sim* s, const mqv_lattice_desc* L)
     MQV_CK(cudaMalloc(&s->d_rp, sizeof(int32_t) * (size_t)(n + 1)));
     MQV_CK(cudaMalloc(&s->d_ci, sizeof(int32_t) * (size_t)std::max<int64_t>(nnz, 1)));
     MQV_CK(cudaMalloc(&s->d_order, sizeof(int32_t) * (size_t)n));
-    MQV_CK(cudaMemcpy(s->d_rp, rp, sizeof(int32_t) * (size_t)(n + 1), cudaMemcpyHostToDevice));
-    if (nnz) MQV_CK(cudaMemcpy(s->d_ci, ci, sizeof(int32_t) * (size_t)nnz, cudaMemcpyHostToDevice));
-    MQV_CK(cudaMemcpy(s->d_order, order.data(), sizeof(int32_t) * (size_t)n, cudaMemcpyHostToDevice));
+    MQV_CK(upload_sync(s->stream, s->d_rp, rp, sizeof(int32_t) * (size_t)(n + 1)));
+    MQV_CK(upload_sync(s->stream, s->d_ci, ci, sizeof(int32_t) * (size_t)nnz));
+    MQV_CK(upload_sync(s->stream, s->d_order, order.data(), sizeof(int32_t) * (size_t)n));
     if (L->bonds) {
         MQV_CK(cudaMalloc(&s->d_bonds, (size_t)std::max<int64_t>(nnz, 1)));
-        if (nnz) MQV_CK(cudaMemcpy(s->d_bonds, L->bonds, (size_t)nnz, cudaMemcpyHostToDevice));
+        MQV_CK(upload_sync(s->stream, s->d_bonds, L->bonds, (size_t)nnz));
     }
     s->n = n;
     s->max_degree = maxdeg;
@@ -312,7 +312,7 @@ static mqv_status lower_stencil_bonds(Sim* s, const int8_t* bonds)
             fb[(size_t)d * n + i] = w;
         }
     MQV_CK(cudaMalloc(&s->d_bonds, fb.size()));
-    MQV_CK(cudaMemcpy(s->d_bonds, fb.data(), fb.size(), cudaMemcpyHostToDevice));
+    MQV_CK(upload_sync(s->stream, s->d_bonds, fb.data(), fb.size()));
     s->sten.fb = s->d_bonds;
     s->lat_hash = fnv1a(fb.data(), fb.size());
     return MQV_OK;
@@ -521,7 +521,7 @@ MQV_API mqv_status mqv_create(const mqv_model_desc* model, const mqv_lattice_des
                        (s->md.kind == MQV_MODEL_ISING || s->md.kind == MQV_MODEL_ISING_EMBED);
     s->sten.split = s->fused_ising2d ? 1 : 0;
     cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, s->device);
-    if (cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess || cudaMemset(s->d_status, 0, sizeof(int)) != cudaSuccess ||
+    if (cudaMalloc(&s->d_status, sizeof(int)) != cudaSuccess || cudaMemsetAsync(s->d_status, 0, sizeof(int), s->stream) != cudaSuccess ||
         cudaMalloc(&s->d_counter, sizeof(int)) != cudaSuccess) {
         cudaGetLastError();
         set_error("device allocation of the status word failed");
@@ -976,13 +976,14 @@ MQV_API mqv_status mqv_describe(mqv_sim* h, char* buf, size_t len)
     if (!s || !buf || len == 0) return fail(MQV_ERR_INVALID_ARG, "bad arguments");
     char cfg[96] = "";
     if (s->fused_ising2d) ising2d_config_name(s, cfg, sizeof(cfg));
-    std::snprintf(buf, len, "model=%d lattice=%s n=%lld path=%s%s%s clusters=%s", s->md.kind,
+    // the sweep kernel's name, when there is one, ends the line
+    std::snprintf(buf, len, "model=%d lattice=%s n=%lld clusters=%s path=%s%s%s", s->md.kind,
                   s->lat_kind == MQV_LATTICE_HYPERCUBIC ? (s->termsel ? "bipartite" : "hypercubic") : "csr", (long long)s->n,
+                  use_resident(s) ? "label-smem" : use_cluster(s) ? "label-dsmem" : (cluster_by_label(s) ? "label" : "bfs"),
                   use_resident(s) ? "resident-smem"
                   : use_cluster(s) ? "resident-cluster"
                                    : (s->fused_ising2d ? "fused-2d-bitsliced" : (s->is_f32 ? "per-colour-f32" : "per-colour-int8")),
-                  cfg[0] ? " kernel=" : "", cfg,
-                  use_resident(s) ? "label-smem" : use_cluster(s) ? "label-dsmem" : (cluster_by_label(s) ? "label" : "bfs"));
+                  cfg[0] ? " kernel=" : "", cfg);
     return MQV_OK;
 }
 
@@ -1600,7 +1601,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     }
     auto dcopy = [&](void** dst, const void* src, size_t bytes) -> mqv_status {
         MQV_CK(cudaMalloc(dst, bytes));
-        MQV_CK(cudaMemcpy(*dst, src, bytes, cudaMemcpyHostToDevice));
+        MQV_CK(upload_sync(b->stream, *dst, src, bytes));
         return MQV_OK;
     };
     // measurement CTAs: about 4096 sites each, at least one per member
@@ -1784,9 +1785,8 @@ MQV_API mqv_status mqv_batch_tempering(mqv_batch* h, int32_t n_steps, int32_t em
         return fail(MQV_ERR_OUT_OF_MEMORY, "device allocation of the exchange plan failed");
     }
     cudaError_t ce = cudaSuccess;
-    if (nflags) ce = cudaMemcpy(d_plan, plan, sizeof(int32_t) * 2 * nflags, cudaMemcpyHostToDevice);
-    if (ce == cudaSuccess)
-        ce = cudaMemcpy(d_perm, ident.data(), sizeof(int32_t) * ident.size(), cudaMemcpyHostToDevice);
+    if (nflags) ce = upload_sync(b->stream, d_plan, plan, sizeof(int32_t) * 2 * nflags);
+    if (ce == cudaSuccess) ce = upload_sync(b->stream, d_perm, ident.data(), sizeof(int32_t) * ident.size());
     if (ce != cudaSuccess) {
         release();
         return fail(MQV_ERR_CUDA, std::string("upload of the exchange plan failed: ") + cudaGetErrorString(ce));

@@ -229,4 +229,16 @@ struct Sim {
 
 void set_error(const std::string& msg);
 
+// Host -> device copy ordered on `st` and complete on return.  The handles'
+// streams are created non-blocking, so a cudaMemcpy / cudaMemset on the
+// legacy stream is NOT ordered before their kernels (a pageable cudaMemcpy may
+// return before its DMA lands, and cudaMemset of device memory is
+// asynchronous): every upload a handle's kernels read goes through here.
+inline cudaError_t upload_sync(cudaStream_t st, void* dst, const void* src, size_t bytes)
+{
+    if (bytes == 0) return cudaSuccess;
+    const cudaError_t e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, st);
+    return e != cudaSuccess ? e : cudaStreamSynchronize(st);  // the host buffer may go out of scope
+}
+
 }  // namespace mqv

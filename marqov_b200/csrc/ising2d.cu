@@ -34,6 +34,7 @@
 // block.  The result equals update_accepted<1>(dE, beta, word) bit for bit.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cstdlib>
 #include <cstring>
 
@@ -900,8 +901,8 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
     using G = TileGeom<TX, TY, NWARP>;
     auto kern = ising2d_sweep<TX, TY, NWARP, MEAS>;
-    static int cps = 0;  // resident CTAs per SM for this instantiation
-    if (cps == 0) {
+    static std::atomic<int> cps{0};  // resident CTAs per SM for this instantiation (host threads share it)
+    if (cps.load() == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         if (e != cudaSuccess) return e;
         int c = 0;
@@ -921,8 +922,8 @@ static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t strea
 {
     using G = BandGeom<NT, S, NSB, W>;
     auto kern = ising2d_band<NT, S, NSB, MEAS, W>;
-    static int cps = 0;  // resident CTAs per SM for this instantiation
-    if (cps == 0) {
+    static std::atomic<int> cps{0};  // resident CTAs per SM for this instantiation (host threads share it)
+    if (cps.load() == 0) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
         if (e != cudaSuccess) return e;
         int c = 0;

@@ -23,6 +23,8 @@
 // (batch_resident), members being independent.
 #include <cuda_runtime.h>
 
+#include <atomic>
+
 #include "batch.h"
 #include "int8_site.cuh"
 #include "wolff_int8.cuh"
@@ -237,7 +239,7 @@ bool resident_fits(const Sim* s)
 
 static cudaError_t resident_attr(int device)
 {
-    static bool done[64] = {};
+    static std::atomic<bool> done[64] = {};  // host threads share it
     if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
     const int bytes = (int)resident_smem_bytes(kResidentMaxSites);
     cudaError_t e = cudaFuncSetAttribute(emcs_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);

@@ -141,17 +141,22 @@ static void launch_label_t(Sim* s, int32_t* csize)
 // The one-member tables of the labelling path, allocated on first use.
 cudaError_t ensure_label_tables(Sim* s)
 {
-    if (s->d_rep1) return cudaSuccess;
+    if (s->d_sbrep1) return cudaSuccess;  // allocated last: all tables present
     const int64_t n = s->n;
     const int64_t gb = (n + kBatchMetroThreads - 1) / kBatchMetroThreads;
     const int64_t pre[2] = {0, n};
-    cudaError_t e = cudaMalloc(&s->d_rep1, sizeof(BatchRep));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_ctr1, sizeof(BatchCtr));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_seed1, sizeof(CclSeed));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_sprefix1, sizeof(pre));
-    if (e == cudaSuccess) e = cudaMalloc(&s->d_sbrep1, sizeof(int32_t) * (size_t)gb);
-    if (e == cudaSuccess) e = cudaMemcpy(s->d_sprefix1, pre, sizeof(pre), cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaMemset(s->d_sbrep1, 0, sizeof(int32_t) * (size_t)gb);
+    cudaError_t e = cudaSuccess;
+    if (!s->d_rep1) e = cudaMalloc(&s->d_rep1, sizeof(BatchRep));
+    if (e == cudaSuccess && !s->d_ctr1) e = cudaMalloc(&s->d_ctr1, sizeof(BatchCtr));
+    if (e == cudaSuccess && !s->d_seed1) e = cudaMalloc(&s->d_seed1, sizeof(CclSeed));
+    if (e == cudaSuccess && !s->d_sprefix1) e = cudaMalloc(&s->d_sprefix1, sizeof(pre));
+    // on the handle's stream, before the kernels that read them
+    if (e == cudaSuccess) e = upload_sync(s->stream, s->d_sprefix1, pre, sizeof(pre));
+    int32_t* brep = nullptr;
+    if (e == cudaSuccess) e = cudaMalloc(&brep, sizeof(int32_t) * (size_t)gb);
+    if (e == cudaSuccess) e = cudaMemsetAsync(brep, 0, sizeof(int32_t) * (size_t)gb, s->stream);
+    if (e == cudaSuccess) s->d_sbrep1 = brep;
+    else if (brep) cudaFree(brep);
     return e;
 }
 

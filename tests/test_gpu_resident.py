@@ -84,14 +84,16 @@ def test_resident_wolff_only_equals_oracle(orc):
                                   lambda M: (M.RegularHypercubic(32, 3), M.Heisenberg(-1.0, "smallcap", 0.5), 0.693, 3),
                                   lambda M: (M.RegularHypercubic(32, 3), M.Phi4(0.37, 1.1, 1.0), 0.37, 1)])
 def test_labelling_equals_breadth_first(make):
-    """One large lattice: clusters by whole-lattice labelling equal the
-    breadth-first ones (the same draws), states and sizes bit for bit (float
-    states: the same arithmetic, so equal too)."""
+    """One large lattice on the launch-per-step path: clusters by
+    whole-lattice labelling equal the breadth-first ones (the same draws),
+    states and sizes bit for bit (float states: the same arithmetic, so equal
+    too).  Float observables are sums of FP64 atomics, whose order differs
+    between runs: they agree to rounding."""
     import marqov_b200 as M
     lat, ham, beta, symd = make(M)
     out = []
     for algo in ("label", "bfs"):
-        cfg = M.Config(seed=12, repid=1, ncluster=1, nmetro=1)
+        cfg = M.Config(seed=12, repid=1, ncluster=1, nmetro=1, resident=False)
         with M.makeCore(lat, cfg, ham, beta) as c:
             c.set_wolff(algo)
             assert ("clusters=" + algo) in c.describe()
@@ -100,7 +102,10 @@ def test_labelling_equals_breadth_first(make):
             sizes = c.wolff(5)
             out.append((obs, mc, sizes, c.state))
     assert (out[0][1] == out[1][1]).all() and (out[0][2] == out[1][2]).all()
-    assert (out[0][0] == out[1][0]).all()
+    if symd == 0:
+        assert (out[0][0] == out[1][0]).all()
+    else:
+        assert np.allclose(out[0][0], out[1][0], rtol=1e-12, atol=1e-12)
     assert (out[0][3] == out[1][3]).all()
 
 
