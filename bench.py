@@ -192,7 +192,7 @@ def run_reference(args, ws, rank):
     if rank != 0:
         return 0
     from oracle.build import build_ref
-    from oracle.oracle import RefHarness
+    from oracle.oracle import RefHarness, ref_march
     if build_ref() is None and not os.path.exists(os.path.join(ROOT, "oracle", "_ref", "libmarqov_ref.so")):
         print(json.dumps({"impl": "reference", "unavailable": "reference harness oracle/_ref not built"}))
         return 0
@@ -243,8 +243,9 @@ def run_reference(args, ws, rank):
                          "sample": f"{cores} replicas x {nup} random-site updates per step on L={L}, "
                                    f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>",
                          "host_nproc": os.cpu_count(),
-                         "build": "g++ -O3 -march=x86-64-v3 from the reference's own headers (oracle/build.py): "
-                                  "built where the reference source is, run on this host, so not -march=native"},
+                         "build": f"g++ -O3 -march={ref_march()} from the reference's own headers "
+                                  "(oracle/build.py; the AVX-512 build where this host's CPU has it)",
+                         "cpu_model": cpu_model()},
         "colour_order_parity_mode": colour,
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
@@ -255,8 +256,19 @@ def run_reference(args, ws, rank):
 # ---------------------------------------------------------------------------
 # engine arm
 
+def cpu_model():
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return None
+
+
 def cpu_baseline(L):
-    from oracle.oracle import RefHarness
+    from oracle.oracle import RefHarness, ref_march
     ref = RefHarness()
     n = L * L
     nup = n // 2
@@ -266,7 +278,7 @@ def cpu_baseline(L):
     return {"value": nup / (t * 1e9), "unit": UNIT, "cores": 1, "kind": "reference",
             "sample": f"{nup} random-site updates (half a sweep) of one L={L} replica, "
                       f"MARQOV::Metropolis<Ising<int8_t>> + RNGCache<mt19937_64>, {t:.1f} s",
-            "host_nproc": os.cpu_count()}
+            "host_nproc": os.cpu_count(), "build": f"g++ -O3 -march={ref_march()}", "cpu_model": cpu_model()}
 
 
 # ---------------------------------------------------------------------------

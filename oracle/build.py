@@ -8,10 +8,15 @@
   (The reference tree is ``MARQOV_REF_SRC``, else ``../reference/src`` beside
   this checkout.)
 
-Both use a conservative ``-march=x86-64-v3`` so the binaries run on any AVX2
-host, not only the build machine, and ``-ffp-contract=off`` so every FP64
-operation of the acceptance rule is rounded as written (the engine does the
-same on host and device).
+Both use ``-march=x86-64-v3`` so the binaries run on any AVX2 host, not only
+the build machine, and ``-ffp-contract=off`` so every FP64 operation of the
+acceptance rule is rounded as written (the engine does the same on host and
+device).  The reference harness is also built for ``-march=x86-64-v4``
+(AVX-512) as ``libmarqov_ref_v4.so``; ``oracle.oracle.ref_path`` loads that
+one on hosts whose CPU has the AVX-512 subsets of x86-64-v4, which is the
+closest a binary built on one machine gets to ``-march=native`` on another.
+Neither flag changes a result: without contraction or fast-math every FP
+operation is the same IEEE operation in either build.
 """
 from __future__ import annotations
 
@@ -50,13 +55,14 @@ def build_ref(force: bool = False) -> str | None:
     os.makedirs(out_dir, exist_ok=True)
     srcs = [os.path.join(HERE, "ref_harness.cpp"), os.path.join(HERE, "oracle.c"),
             os.path.join(HERE, "ref_scheduler.cpp"), os.path.join(HERE, "ref_io.cpp")]
-    if force or not _newer(out, srcs):
-        obj = os.path.join(out_dir, "oracle_c.o")
-        subprocess.check_call(["gcc", "-std=gnu11", "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fPIC", "-c",
-                               "-o", obj, srcs[1]])
-        cmd = ["g++", "-std=gnu++14", *ARCH, "-w", "-I", src_root, "-o", out, srcs[0], srcs[2], srcs[3], obj,
-               "-lm", "-lpthread"]
-        subprocess.check_call(cmd)
+    for march, lib in (("x86-64-v3", out), ("x86-64-v4", os.path.join(out_dir, "libmarqov_ref_v4.so"))):
+        if force or not _newer(lib, srcs):
+            obj = os.path.join(out_dir, f"oracle_c_{march}.o")
+            subprocess.check_call(["gcc", "-std=gnu11", "-O3", f"-march={march}", "-ffp-contract=off", "-fPIC", "-c",
+                                   "-o", obj, srcs[1]])
+            cmd = ["g++", "-std=gnu++14", "-O3", f"-march={march}", "-ffp-contract=off", "-fPIC", "-shared", "-w",
+                   "-I", src_root, "-o", lib, srcs[0], srcs[2], srcs[3], obj, "-lm", "-lpthread"]
+            subprocess.check_call(cmd)
     return out
 
 

@@ -198,8 +198,32 @@ class Oracle:
         return int(acc), dec
 
 
+# the AVX-512 subsets that -march=x86-64-v4 may use
+_V4_FLAGS = {"avx512f", "avx512bw", "avx512cd", "avx512dq", "avx512vl"}
+
+
+def host_has_v4() -> bool:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("flags"):
+                    return _V4_FLAGS <= set(line.split(":", 1)[1].split())
+    except OSError:
+        pass
+    return False
+
+
 def ref_path() -> str:
+    """The reference harness for this host: the x86-64-v4 (AVX-512) build
+    where the CPU has it, else the x86-64-v3 one."""
+    v4 = os.path.join(HERE, "_ref", "libmarqov_ref_v4.so")
+    if host_has_v4() and os.path.exists(v4):
+        return v4
     return os.path.join(HERE, "_ref", "libmarqov_ref.so")
+
+
+def ref_march(path: str | None = None) -> str:
+    return "x86-64-v4" if (path or ref_path()).endswith("_v4.so") else "x86-64-v3"
 
 
 class RefHarness:
