@@ -1125,6 +1125,13 @@ struct Batch {
     int graph_steps = 8;  // EMCS per graph launch
     uint64_t launches = 0;
     uint32_t temper_steps = 0;  // replica-exchange steps done (part of their draws' counters)
+    // Members are independent, so the resident classes and the cluster sizes
+    // run on side streams beside the graph members on `stream`: forked from
+    // it by fork_ev, joined back by join_ev[i] before anything that reads
+    // every member (exchanges, the chunk's reductions and copies).
+    static constexpr int kSide = 9;  // 2 resident classes + cluster sizes 2 .. 8
+    cudaStream_t side[kSide] = {};
+    cudaEvent_t fork_ev = nullptr, join_ev[kSide] = {};
 };
 
 static void free_graphs(Batch* b)
@@ -1145,6 +1152,12 @@ static void free_batch(Batch* b)
     free_graphs(b);
     for (cudaEvent_t e : b->ev)
         if (e) cudaEventDestroy(e);
+    for (int i = 0; i < Batch::kSide; ++i) {
+        if (b->side[i]) cudaStreamSynchronize(b->side[i]);
+        if (b->side[i]) cudaStreamDestroy(b->side[i]);
+        if (b->join_ev[i]) cudaEventDestroy(b->join_ev[i]);
+    }
+    if (b->fork_ev) cudaEventDestroy(b->fork_ev);
     for (Sim* s : b->sims) free_sim(s);
     for (void* p : {(void*)b->d_reps, (void*)b->d_prefix, (void*)b->d_block_rep, (void*)b->d_cbegin,
                     (void*)b->d_ccount, (void*)b->d_res_order, (void*)b->d_ctr,
@@ -1311,20 +1324,49 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         l.wolff_ccl = w;
         per_emcs[w] = batch_launches_per_emcs(l, ncluster, nmetro);
     }
-    // `count` EMCS with the graphs of algorithm w, after the same EMCS of the
-    // resident members (chunk positions from k0; members are independent)
+    // side streams of the resident classes and cluster sizes (created once)
+    int nside_needed = (b->nres[0] ? 1 : 0) + (b->nres[1] ? 1 : 0);
+    for (int c = 2; c <= 8; ++c) nside_needed += b->ncl[c] ? 1 : 0;
+    if (nside_needed && !b->fork_ev) {
+        MQV_CK(cudaEventCreateWithFlags(&b->fork_ev, cudaEventDisableTiming));
+        for (int i = 0; i < Batch::kSide; ++i) {
+            MQV_CK(cudaStreamCreateWithFlags(&b->side[i], cudaStreamNonBlocking));
+            MQV_CK(cudaEventCreateWithFlags(&b->join_ev[i], cudaEventDisableTiming));
+        }
+    }
+    // `count` EMCS of every member from chunk position k0: the resident
+    // classes and each cluster size on their own side stream, the graph
+    // members (algorithm w) on the batch stream, joined at the end
     auto launch_emcs = [&](int w, int count, int k0) -> mqv_status {
+        int nside = 0;
+        if (nside_needed) MQV_CK(cudaEventRecord(b->fork_ev, b->stream));
+        // the next side stream, ordered after the fork
+        auto side_stream = [&](cudaStream_t& st2) -> cudaError_t {
+            st2 = b->side[nside];
+            return cudaStreamWaitEvent(st2, b->fork_ev, 0);
+        };
+        auto side_done = [&](cudaStream_t st2) -> cudaError_t {
+            const cudaError_t e = cudaEventRecord(b->join_ev[nside], st2);
+            ++nside;
+            return e;
+        };
         for (int cls = 0; cls < 2; ++cls) {
             if (!b->nres[cls]) continue;
-            MQV_CK(batch_launch_resident(b->L, b->stream, b->d_res_order + (cls ? b->nres[0] : 0), b->nres[cls],
+            cudaStream_t st2 = nullptr;
+            MQV_CK(side_stream(st2));
+            MQV_CK(batch_launch_resident(b->L, st2, b->d_res_order + (cls ? b->nres[0] : 0), b->nres[cls],
                                          b->res_maxn[cls], (uint32_t)(done_run + k0), k0, count, ncluster, nmetro,
                                          b->device));
+            MQV_CK(side_done(st2));
             b->launches++;
         }
         for (int c = 2; c <= 8; ++c) {
             if (!b->ncl[c]) continue;
-            MQV_CK(batch_launch_cluster(b->L, b->stream, b->d_res_order + b->cl_off[c], b->ncl[c], c,
+            cudaStream_t st2 = nullptr;
+            MQV_CK(side_stream(st2));
+            MQV_CK(batch_launch_cluster(b->L, st2, b->d_res_order + b->cl_off[c], b->ncl[c], c,
                                         (uint32_t)(done_run + k0), k0, count, ncluster, nmetro));
+            MQV_CK(side_done(st2));
             b->launches++;
         }
         int j = 0;
@@ -1332,6 +1374,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
             for (; j + K <= count; j += K) MQV_CK(cudaGraphLaunch(b->g_many[w], b->stream));
         for (; j < count; ++j) MQV_CK(cudaGraphLaunch(b->g_one[w], b->stream));
         b->launches += per_emcs[w] * (uint64_t)count;
+        for (int i = 0; i < nside; ++i) MQV_CK(cudaStreamWaitEvent(b->stream, b->join_ev[i], 0));
         return MQV_OK;
     };
     // the exchange step that ends after EMCS `e` of the run, if any
@@ -1348,7 +1391,6 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
     int done = 0;
     while (done < n_emcs) {
         const int ch = std::min(n_emcs - done, CH);
-        done_run = done;
         done_run = done;
         MQV_CK(cudaMemsetAsync(b->d_acc, 0, sizeof(long long) * kAccStride * (size_t)ch * b->nrep, b->stream));
         MQV_CK(batch_launch_chunk_start(b->L, b->stream, (uint32_t)done));
