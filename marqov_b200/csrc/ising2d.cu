@@ -536,6 +536,7 @@ struct BandGeom {
     static constexpr int TIECAP = 32 + 64 * W;   // tie entries per warp: a step adds at most 64 W
     static constexpr int TIES = NW * TIECAP * 16;
     static constexpr int SMEM = STAGE + BITS + TIES + NSB * 8;
+    static constexpr int SMEM_RS = BITS + TIES;  // register-staged rows: no staging ring
     static_assert(NT % 32 == 0 && S >= 1 && W >= 1, "band shape");
 };
 
@@ -546,16 +547,24 @@ struct BandTie {
     int32_t y;     // lattice row
 };
 
-template <int NT, int S, int NSB_, bool MEAS, int W = 1>
-__global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising2DArgs a)
+// RS (register staging): instead of the bulk-copy ring, every thread loads
+// its own columns of staged row k + 1 into registers (two 16-byte loads per
+// column and half, a warp's loads one contiguous kilobyte) right after packing
+// row k, so the loads are in flight during the step's updates and are packed
+// after the next barrier.  Without the staging ring a CTA needs a third of the
+// shared memory, and more CTAs share an SM; no wait can hang (plain loads).
+// MINB: CTAs per SM the register allocation must allow (0: no bound).
+template <int NT, int S, int NSB_, bool MEAS, int W = 1, bool RS = false, int MINB = 0>
+__global__ void __launch_bounds__(NT, MINB) ising2d_band(const __grid_constant__ Ising2DArgs a)
 {
     using G = BandGeom<NT, S, NSB_, W>;
     constexpr int RB = G::RB, NSB = G::NSB, L = G::L, Lh = L / 2, NC = G::NC;
+    constexpr int STAGE = RS ? 0 : G::STAGE;
     extern __shared__ __align__(128) uint8_t smem[];
     uint8_t* stage = smem;
-    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + G::STAGE);
-    BandTie* ties = reinterpret_cast<BandTie*>(smem + G::STAGE + G::BITS);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + G::STAGE + G::BITS + G::TIES);
+    uint32_t* bits = reinterpret_cast<uint32_t*>(smem + STAGE);
+    BandTie* ties = reinterpret_cast<BandTie*>(smem + STAGE + G::BITS);
+    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + STAGE + G::BITS + G::TIES);
     const int t = threadIdx.x, lane = t & 31, warp = t >> 5;
     const int y0 = (int)(((long long)blockIdx.x * L) / gridDim.x);
     const int y1 = (int)(((long long)(blockIdx.x + 1) * L) / gridDim.x);
@@ -567,7 +576,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     auto coll = [&](int c) { return c == 0 ? NC - 1 : c - 1; };
     auto colr = [&](int c) { return c == NC - 1 ? 0 : c + 1; };
 
-    if (t == 0) {
+    if (!RS && t == 0) {
         for (int k = 0; k < NSB; ++k) mbar_init(smem_addr(&bars[k]), 1);
         mbar_fence_init();
     }
@@ -580,8 +589,22 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
         mbar_expect_tx(bar, (uint32_t)L);
         bulk_g2s(smem_addr(stage + (r % NSB) * L), a.src + (size_t)y * L, (uint32_t)L, bar);
     };
-    if (t == 0)
+    if (!RS && t == 0)
         for (int r = 0; r < NSB && r < NR; ++r) issue(r);
+    // RS: this thread's bytes of the next staged row, [column][half][16-byte part]
+    uint4 pre[RS ? W : 1][2][2];
+    auto load_row = [&](int r) {
+        const int8_t* rowp = a.src + (size_t)wrapi(y0 - 2 + r, L) * L;
+#pragma unroll
+        for (int j = 0; j < W; ++j)
+#pragma unroll
+            for (int h = 0; h < 2; ++h) {
+                const uint4* q = reinterpret_cast<const uint4*>(rowp + h * Lh + 32 * col(j));
+                pre[RS ? j : 0][h][0] = __ldg(q);
+                pre[RS ? j : 0][h][1] = __ldg(q + 1);
+            }
+    };
+    if (RS) load_row(0);
 
     BandTie* tl = ties + warp * G::TIECAP;
     int ntie = 0;
@@ -649,7 +672,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     bool stop = false;
     for (; k < NR + 2 * S; ++k, sk = sk + 1 == RB ? 0 : sk + 1) {
         int timed_out = 0;
-        if (k < NR) {
+        if (!RS && k < NR) {
             // every thread waits for row k (bounded: a stuck copy sets an error status)
             const uint32_t bar = smem_addr(&bars[k % NSB]);
             const uint32_t par = (uint32_t)(k / NSB) & 1u;
@@ -671,20 +694,28 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
             stop = true;
             break;
         }
-        if (t == 0 && k >= 1 && k - 1 + NSB < NR) {
+        if (!RS && t == 0 && k >= 1 && k - 1 + NSB < NR) {
             fence_proxy_async_smem();
             issue(k - 1 + NSB);
         }
         if (k < NR) {
-            const uint8_t* row = stage + (k % NSB) * L;
             uint32_t* brow = bits + sk * 2 * NC;
+            if (RS) {
 #pragma unroll
-            for (int j = 0; j < W; ++j) {
-                const int c = col(j);
+                for (int j = 0; j < W; ++j)
 #pragma unroll
-                for (int h = 0; h < 2; ++h) {
-                    const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * c);
-                    brow[h * NC + c] = pack_word(q[0], q[1]);
+                    for (int h = 0; h < 2; ++h) brow[h * NC + col(j)] = pack_word(pre[RS ? j : 0][h][0], pre[RS ? j : 0][h][1]);
+                if (k + 1 < NR) load_row(k + 1);
+            } else {
+                const uint8_t* row = stage + (k % NSB) * L;
+#pragma unroll
+                for (int j = 0; j < W; ++j) {
+                    const int c = col(j);
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint4* q = reinterpret_cast<const uint4*>(row + h * Lh + 32 * c);
+                        brow[h * NC + c] = pack_word(q[0], q[1]);
+                    }
                 }
             }
         }
@@ -753,7 +784,7 @@ __global__ void __launch_bounds__(NT) ising2d_band(const __grid_constant__ Ising
     }
     if (stop) {
         // wait (bounded) for the copies still in flight before the CTA leaves
-        if (t == 0) {
+        if (!RS && t == 0) {
             atomicExch(a.status, MQV_ERR_TIMEOUT);
             const uint64_t t0 = global_timer_ns();
             const int issued = k == 0 ? NSB : k - 1 + NSB;  // rows issued before the stop
@@ -917,24 +948,28 @@ static cudaError_t launch_t(const Ising2DArgs& a, int nsm, cudaStream_t stream)
     return cudaGetLastError();
 }
 
-template <int NT, int S, int NSB, bool MEAS, int W = 1>
+// RS / MINB: see ising2d_band; with MINB > 0 the grid has at most MINB CTAs
+// per SM (longer bands re-read fewer halo rows).
+template <int NT, int S, int NSB, bool MEAS, int W = 1, bool RS = false, int MINB = 0>
 static cudaError_t launch_band(const Ising2DArgs& a, int nsm, cudaStream_t stream)
 {
     using G = BandGeom<NT, S, NSB, W>;
-    auto kern = ising2d_band<NT, S, NSB, MEAS, W>;
+    constexpr int SMEM = RS ? G::SMEM_RS : G::SMEM;
+    auto kern = ising2d_band<NT, S, NSB, MEAS, W, RS, MINB>;
     static std::atomic<int> cps{0};  // resident CTAs per SM for this instantiation (host threads share it)
     if (cps.load() == 0) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, G::SMEM);
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, SMEM);
         if (e != cudaSuccess) return e;
         int c = 0;
-        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NT, G::SMEM);
+        e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&c, kern, NT, SMEM);
         if (e != cudaSuccess) return e;
+        if (MINB > 0 && c > MINB) c = MINB;
         cps = c < 1 ? 1 : c;
     }
     // one band per CTA, at least 8 rows each
     long long grid = (long long)nsm * cps;
     if (grid > G::L / 8) grid = G::L / 8;
-    kern<<<(int)grid, NT, G::SMEM, stream>>>(a);
+    kern<<<(int)grid, NT, SMEM, stream>>>(a);
     return cudaGetLastError();
 }
 
@@ -948,6 +983,7 @@ struct SweepConfig {
     int nsb;            // band: staged row slots
     SweepLauncher plain, meas;
     int w;              // band: word columns per thread
+    int rs = 0;         // band: rows staged in registers, at most rs CTAs per SM (0: bulk-copy ring)
 };
 
 #define MQV_CFG(TX, TY, NW) \
@@ -960,6 +996,10 @@ struct SweepConfig {
                 NSB,         launch_band<NT, S, NSB, false, W>,                                          \
                 launch_band<NT, S, NSB, true, W>, W}
 
+#define MQV_BANDRS(NT, S, W, MINB)                                                                        \
+    SweepConfig{64 * NT * W, S, NT / 32, true, 0, launch_band<NT, S, 2, false, W, true, MINB>,             \
+                launch_band<NT, S, 2, true, W, true, MINB>, W, MINB}
+
 static const SweepConfig kConfigs[] = {
     MQV_CFG(512, 32, 4), MQV_CFG(256, 32, 4), MQV_CFG(512, 32, 2), MQV_CFG(256, 32, 8),
     MQV_CFG(1024, 32, 2), MQV_CFG(128, 32, 4), MQV_CFG(64, 32, 4),
@@ -967,6 +1007,8 @@ static const SweepConfig kConfigs[] = {
     MQV_BAND(128, 4, 2), MQV_BAND(128, 4, 4),
     MQV_BANDW(128, 4, 2, 2), MQV_BANDW(128, 2, 2, 2), MQV_BANDW(128, 1, 2, 2), MQV_BANDW(128, 3, 2, 2),
     MQV_BANDW(64, 4, 2, 2),
+    MQV_BANDRS(128, 1, 2, 5), MQV_BANDRS(128, 1, 2, 6), MQV_BANDRS(128, 2, 2, 5),
+    MQV_BANDRS(256, 1, 1, 3), MQV_BANDRS(256, 1, 1, 4),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 
@@ -1022,7 +1064,8 @@ static void fill_args(Sim* s, const SweepConfig& c, long long* acc, Ising2DArgs&
 // lattices take the first fitting candidate.
 static void config_name(const SweepConfig& c, char* buf, int len)
 {
-    if (c.band && c.w > 1) snprintf(buf, len, "ising2d_band<%d,%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb, c.w);
+    if (c.band && c.rs) snprintf(buf, len, "ising2d_band_rs<%d,%d,%d,%d>", c.nwarp * 32, c.ty, c.w, c.rs);
+    else if (c.band && c.w > 1) snprintf(buf, len, "ising2d_band<%d,%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb, c.w);
     else if (c.band) snprintf(buf, len, "ising2d_band<%d,%d,%d>", c.nwarp * 32, c.ty, c.nsb);
     else snprintf(buf, len, "ising2d_sweep<%d,%d,%d>", c.tx, c.ty, c.nwarp);
 }
@@ -1084,11 +1127,12 @@ static int pick_config(Sim* s)
     return best;
 }
 
-// A band configuration that fits the lattice (-1: none), for the injected timeout.
+// A band configuration with the bulk-copy ring (and its bounded waits) that
+// fits the lattice (-1: none), for the injected timeout.
 int ising2d_band_config(const Sim* s)
 {
     for (int k = 0; k < kNumConfigs; ++k)
-        if (kConfigs[k].band && config_fits(kConfigs[k], s->len)) return k;
+        if (kConfigs[k].band && !kConfigs[k].rs && config_fits(kConfigs[k], s->len)) return k;
     return -1;
 }
 

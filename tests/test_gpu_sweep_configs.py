@@ -22,6 +22,11 @@ CONFIGS = [
     ("ising2d_band<128,1,2,2>", 16384),
     ("ising2d_band<128,3,2,2>", 16384),
     ("ising2d_band<64,4,2,2>", 8192),
+    ("ising2d_band_rs<128,1,2,5>", 16384),
+    ("ising2d_band_rs<128,1,2,6>", 16384),
+    ("ising2d_band_rs<128,2,2,5>", 16384),
+    ("ising2d_band_rs<256,1,1,3>", 16384),
+    ("ising2d_band_rs<256,1,1,4>", 16384),
     ("ising2d_sweep<512,32,4>", 8192),
     ("ising2d_sweep<256,32,4>", 8192),
     ("ising2d_sweep<512,32,2>", 8192),
