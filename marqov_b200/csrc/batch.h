@@ -97,7 +97,7 @@ inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int 
 {
     int live = 0;
     for (int c = 0; c < b.ncol; ++c) live += b.total[c] > 0;
-    const uint64_t ccl = b.site_blocks > 0 ? 5ull : 1ull;
+    const uint64_t ccl = b.site_blocks > 0 ? 6ull : 0ull;  // seed, local, hook, halve, compress, flip
     return (uint64_t)ncluster * (b.wolff_ccl ? ccl : 1ull) + (uint64_t)nmetro * (uint64_t)live +
            (b.meas_blocks > 0 ? 2ull : 1ull);
 }

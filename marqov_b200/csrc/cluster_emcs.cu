@@ -156,11 +156,12 @@ __global__ void __launch_bounds__(kClThreads)
                 }
             }
             cl.sync();
-            if (me == 0 && tid == 0) {
-                int x = rsite, px;
-                while ((px = *(volatile int*)dp.ptr(x)) != x) x = px;
-                s_root = x;
-            }
+            // every candidate's path halved once, all side by side (the
+            // one-CTA kernel's compression pass): the walks after it are short
+            for (int64_t i = lo + tid; i < hi; i += kClThreads)
+                if ((cand[(i - lo) >> 5] >> (i & 31)) & 1u) dfind(dp, (int)i);
+            cl.sync();
+            if (me == 0 && tid == 0) s_root = dfind(dp, rsite);
             cl.sync();
             const int root = *cl.map_shared_rank(&s_root, 0);
             int cnt = 0;

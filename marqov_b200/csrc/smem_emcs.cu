@@ -137,11 +137,16 @@ __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
                 }
             }
             __syncthreads();
-            if (tid == 0) {
-                int x = s_rsite, px;
-                while ((px = par[x]) != x) x = px;
-                s_root = x;
-            }
+            // Hooks made side by side chain up (a warp hooks 32 consecutive
+            // sites one under the next), so the trees can be as deep as a
+            // row.  Every candidate's path is halved once, all at the same
+            // time (a write only ever points a site to an ancestor, so the
+            // forest stays valid while other walks read it); the walks after
+            // this are short.
+            for (int64_t i = tid; i < n; i += kResThreads)
+                if ((cand[i >> 5] >> (i & 31)) & 1u) rfind(par, (int)i);
+            __syncthreads();
+            if (tid == 0) s_root = rfind(par, s_rsite);
             __syncthreads();
             const int root = s_root;
             const int8_t nv = (int8_t)s_newq;

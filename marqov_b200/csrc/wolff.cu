@@ -132,10 +132,11 @@ static void launch_label_t(Sim* s, int32_t* csize)
                                                              1, 0);
     ccl_hook<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1,
                                                             1, 0);
+    ccl_halve<<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n);
     ccl_compress<<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n);
     ccl_flip<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1, 1,
                                                             0, csize, 1);
-    s->launches += 6;
+    s->launches += 7;
 }
 
 // The one-member tables of the labelling path, allocated on first use.

@@ -16,6 +16,8 @@
 //                 sites are united in shared memory first; each candidate's
 //                 label becomes its local root, non-candidates get -1;
 //   ccl_hook      the other activated bonds between candidates are united;
+//   ccl_halve     every candidate's path to its root halved (hooks made side
+//                 by side chain up, so the trees can be deep);
 //   ccl_compress  label = root (read-only walks: only roots are written);
 //   ccl_flip      members of the seed's component are flipped / reflected and
 //                 counted into the cluster size.
@@ -201,6 +203,8 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
         });
     }
     __syncthreads();
+    if (cand) ccl_lfind(slab, (int)threadIdx.x);  // paths halved side by side first
+    __syncthreads();
     if (g < total) {
         int lab = -1;
         if (cand) {
@@ -233,6 +237,22 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
         if (ccl_same_block(g, off + j) || __ldcg(lab + j) < 0) return;
         if (ccl_active<F32>(R, sd, serial, i, j)) ccl_unite(lab, (int)i, (int)j);
     });
+}
+
+// Hooks made side by side chain up, so trees can be deep and read-only walks
+// long: first every candidate's path is halved (all side by side; a write
+// only ever points a site to an ancestor, so the forest stays valid), then
+// ccl_compress walks the short paths that remain.
+static __global__ void ccl_halve(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
+                                 const int32_t* __restrict__ block_rep, int64_t total)
+{
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= total) return;
+    int64_t i;
+    const int r = ccl_member(g, prefix, block_rep, i);
+    int* lab = reps[r].queue;
+    if (__ldcg(lab + i) < 0) return;
+    ccl_find(lab, (int)i);
 }
 
 static __global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
