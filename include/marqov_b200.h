@@ -121,9 +121,13 @@ typedef struct mqv_lattice_desc {
 /* Run flags. */
 enum {
     MQV_FLAG_PER_COLOUR = 1,  /* always use one launch per colour class (no fused two-colour tiles) */
-    MQV_FLAG_NO_RESIDENT = 2  /* never run a small int8 lattice (<= 32768 sites) as one resident CTA that
+    MQV_FLAG_NO_RESIDENT = 2, /* never run an int8 stencil lattice on the resident path -- one CTA
+                                 (<= 65536 sites) or one thread-block cluster (<= 262144 sites) that
                                  keeps the state in shared memory for a whole chunk of EMCS; launch
                                  per cluster, colour and measurement instead (same results) */
+    MQV_FLAG_RESIDENT = 4     /* take the resident path wherever the lattice fits it, also where the
+                                 default choice would not (a batch whose resident CTAs would fill
+                                 less than half the SMs runs every other member on the graph path) */
 };
 
 typedef struct mqv_run_params {
@@ -197,7 +201,8 @@ enum { MQV_WOLFF_AUTO = 0, MQV_WOLFF_BFS = 1, MQV_WOLFF_LABEL = 2 };
 /* No counterpart in the reference.  The cluster algorithm of a handle:
  * MQV_WOLFF_AUTO (default) labels int8 lattices of at least 2^18 sites and
  * grows the others breadth first; lattices on the resident path
- * (MQV_FLAG_NO_RESIDENT unset, int8, <= 32768 sites) label in shared memory. */
+ * (MQV_FLAG_NO_RESIDENT unset, int8 stencils of <= 262144 sites) label in
+ * (distributed) shared memory. */
 MQV_API mqv_status mqv_set_wolff(mqv_sim* sim, int32_t algorithm);
 /* nclusters Wolff clusters; sizes (host, may be NULL) receives each size
  * (synchronises when sizes != NULL). */

@@ -33,6 +33,7 @@ PROPOSAL_DEFAULT, PROPOSAL_SMALL_CAP = 0, 1
 LATTICE_HYPERCUBIC, LATTICE_CSR, LATTICE_BIPARTITE = 1, 2, 3
 FLAG_PER_COLOUR = 1
 FLAG_NO_RESIDENT = 2
+FLAG_RESIDENT = 4
 WOLFF_AUTO, WOLFF_BFS, WOLFF_LABEL = 0, 1, 2
 
 

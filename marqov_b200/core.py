@@ -18,6 +18,13 @@ from .hamiltonians import Hamiltonian
 from .lattices import Lattice
 
 
+def _resident_flag(config) -> int:
+    """Run flags of Config.resident: None (engine's choice), True, False."""
+    if config.resident is None:
+        return 0
+    return L.FLAG_RESIDENT if config.resident else L.FLAG_NO_RESIDENT
+
+
 @dataclass
 class Config:
     """``MARQOV::Config`` (core.h:74-192): method parameters."""
@@ -34,9 +41,12 @@ class Config:
     device: int = 0
     # force one launch per colour class (no fused two-colour tiles)
     per_colour: bool = False
-    # small int8 lattices (<= 32768 sites) run whole chunks of EMCS in one
-    # CTA's shared memory; False forces the launch-per-step path (same results)
-    resident: bool = True
+    # int8 stencil lattices of <= 65536 sites (one CTA) or <= 262144 sites (a
+    # thread-block cluster) run whole chunks of EMCS in shared memory.  None:
+    # the engine decides (in a batch, only while the resident CTAs fill half
+    # the SMs); True: wherever the lattice fits; False: never (launch per
+    # step).  The results are the same.
+    resident: bool | None = None
 
     def setid(self, i):
         self.id = i
@@ -106,8 +116,7 @@ class Core:
         md = ham.desc(self.beta)
         ld = lattice.desc()
         rp = L.RunParams(beta=self.beta, seed=seed & (2 ** 64 - 1), replica=replica, device=int(config.device),
-                         flags=(L.FLAG_PER_COLOUR if config.per_colour else 0) |
-                         (0 if config.resident else L.FLAG_NO_RESIDENT))
+                         flags=(L.FLAG_PER_COLOUR if config.per_colour else 0) | _resident_flag(config))
         L.check(lib.mqv_create(C.byref(md), C.byref(ld), C.byref(rp), C.byref(self._h)))
         self._seed, self._replica = seed, replica
         if restore is not None:
@@ -332,7 +341,7 @@ class Batch:
             specs[i].lattice = lat.desc()
             specs[i].params = L.RunParams(beta=float(beta), seed=int(cfg.seed) & (2 ** 64 - 1),
                                           replica=int(cfg.repid), device=int(cfg.device),
-                                          flags=0 if cfg.resident else L.FLAG_NO_RESIDENT)
+                                          flags=_resident_flag(cfg))
         L.check(lib.mqv_batch_create(specs, len(members), C.byref(self._h)))
         L.check(lib.mqv_batch_set_graph_steps(self._h, int(graph_steps)))
         self.n = len(members)

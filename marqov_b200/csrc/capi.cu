@@ -1581,6 +1581,24 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
             }
         }
     }
+    // A resident member runs on one CTA (or one cluster) for a whole chunk of
+    // EMCS, so residency pays only while the resident CTAs fill the device:
+    // with fewer CTAs than half the SMs (a handful of realisations) the
+    // graph path, whose launches spread every member over all SMs, is
+    // faster, and every member takes it.
+    {
+        int sms = 148;
+        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+        int64_t ctas = (int64_t)res_order[0].size() + (int64_t)res_order[1].size();
+        for (int c = 2; c <= 8; ++c) ctas += (int64_t)c * (int64_t)cl_order[c].size();
+        if (ctas > 0 && 2 * ctas < sms) {
+            auto keep = [&](int32_t r) { return (specs[r].params.flags & MQV_FLAG_RESIDENT) != 0; };
+            for (int r = 0; r < n; ++r)
+                if (!keep(r)) b->resident[(size_t)r] = 0;
+            for (auto& v : res_order) v.erase(std::remove_if(v.begin(), v.end(), [&](int32_t r) { return !keep(r); }), v.end());
+            for (auto& v : cl_order) v.erase(std::remove_if(v.begin(), v.end(), [&](int32_t r) { return !keep(r); }), v.end());
+        }
+    }
     for (int k = 0; k < 2; ++k) {
         std::stable_sort(res_order[k].begin(), res_order[k].end(),
                          [&](int32_t x, int32_t y) { return b->sims[(size_t)x]->n > b->sims[(size_t)y]->n; });

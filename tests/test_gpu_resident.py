@@ -115,8 +115,9 @@ def test_batch_resident_members_equal_launch_path():
     one on the launch path, bit for bit, with and without replica exchange."""
     import marqov_b200 as M
     sizes = [32, 48, 64, 128, 192, 256, 384, 512, 96]
-    ms = [(M.RegularHypercubic(L, 2), M.Config(seed=40 + i, repid=i), M.Potts(3, -1.0), 1.0 + 0.01 * i)
-          for i, L in enumerate(sizes)]
+    # resident=True: nine members fill too few SMs for the default choice
+    ms = [(M.RegularHypercubic(L, 2), M.Config(seed=40 + i, repid=i, resident=True), M.Potts(3, -1.0),
+           1.0 + 0.01 * i) for i, L in enumerate(sizes)]
     solo = []
     try:
         for lat, cfg, ham, beta in ms:
