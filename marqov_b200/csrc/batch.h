@@ -76,7 +76,7 @@ struct BatchLaunch {
 cudaError_t batch_launch_emcs(const BatchLaunch& b, cudaStream_t st, int ncluster, int nmetro);
 // EMCS e0 .. e0 + count - 1 of the resident members order[0 .. nres) (the
 // largest with max_n sites), measurement slots from slot0 (smem_emcs.cu)
-cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, int64_t max_n,
+cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, size_t smem,
                                   uint32_t e0, int slot0, int count, int ncluster, int nmetro, int device);
 // the same for members held by clusters of `ctas` CTAs (cluster_emcs.cu)
 cudaError_t batch_launch_cluster(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nmem, int ctas,

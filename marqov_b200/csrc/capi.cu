@@ -1094,7 +1094,7 @@ struct Batch {
     std::vector<char> resident;
     int32_t* d_res_order = nullptr;
     int nres[2] = {0, 0};
-    int64_t res_maxn[2] = {0, 0};
+    size_t res_smem[2] = {0, 0};  // dynamic shared memory of each class (its largest layout)
     // members held by thread-block clusters of c CTAs (c = 2 .. 8): ncl[c]
     // of them at d_res_order + cl_off[c]
     int ncl[9] = {};
@@ -1355,7 +1355,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
             cudaStream_t st2 = nullptr;
             MQV_CK(side_stream(st2));
             MQV_CK(batch_launch_resident(b->L, st2, b->d_res_order + (cls ? b->nres[0] : 0), b->nres[cls],
-                                         b->res_maxn[cls], (uint32_t)(done_run + k0), k0, count, ncluster, nmetro,
+                                         b->res_smem[cls], (uint32_t)(done_run + k0), k0, count, ncluster, nmetro,
                                          b->device));
             MQV_CK(side_done(st2));
             b->launches++;
@@ -1603,7 +1603,8 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         std::stable_sort(res_order[k].begin(), res_order[k].end(),
                          [&](int32_t x, int32_t y) { return b->sims[(size_t)x]->n > b->sims[(size_t)y]->n; });
         b->nres[k] = (int)res_order[k].size();
-        b->res_maxn[k] = res_order[k].empty() ? 0 : b->sims[(size_t)res_order[k][0]]->n;
+        b->res_smem[k] = 0;
+        for (int32_t r : res_order[k]) b->res_smem[k] = std::max(b->res_smem[k], resident_smem_for(b->sims[(size_t)r]->sten));
     }
     std::vector<int32_t> res_all(res_order[0]);
     res_all.insert(res_all.end(), res_order[1].begin(), res_order[1].end());

@@ -146,6 +146,8 @@ constexpr int64_t kResidentMaxSites = 65536;
 constexpr int64_t kResSmall = 16384;
 struct Sim;
 bool resident_fits(const Sim* s);
+// dynamic shared memory of the resident kernels for one lattice (smem_emcs.cu)
+size_t resident_smem_for(const StencilDev& st);
 // lattices of up to 8 x 32768 sites on a thread-block cluster (cluster_emcs.cu)
 int cluster_ctas(int64_t n);
 bool cluster_launchable(int ctas);

@@ -7,14 +7,18 @@
 // depth.  Here one CTA loads a lattice's state once and runs a whole chunk of
 // EMCS (EMCS<H,L>::move, src/libmarqov/emcs.h:69-109: ncluster Wolff
 // clusters, then nmetro sweeps, then the measurement) before writing it back:
-//   * each cluster by connected-component labelling in shared memory: the
-//     seed and its new state from the WOLFF_SEED substream (the breadth-first
+//   * each cluster as the seed's component of the activated bonds: the seed
+//     and its new state from the WOLFF_SEED substream (the breadth-first
 //     kernel's draws), every bond between two sites in the seed's old state
-//     tested once on its keyed draw (lower id, cluster serial, upper id),
-//     union-find with compare-and-swap hooking on 16-bit parent indices, then
-//     the seed's component flipped -- the same cluster as the breadth-first
-//     growth (the cluster is the seed's component of activated bonds,
-//     whatever the order) at a cost independent of the cluster's depth;
+//     tested once on its keyed draw (lower id, cluster serial, upper id) --
+//     the same cluster as the breadth-first growth, whatever the order.  On
+//     lattices of two or more dimensions the component is found by a
+//     bit-parallel flood fill (resident_cluster_bits): candidate and
+//     active-bond bit planes from warp ballots, then rows closed along x by
+//     prefix scans on 32-site words and joined across rows by prefix scans
+//     over a warp's lanes, repeated until nothing changes -- no atomics, and
+//     a cost of a few passes over n / 32 words.  One-dimensional chains
+//     take union-find on 16-bit parent indices instead;
 //   * each sweep as the per-colour kernels do it (int8_site on the same
 //     keyed words, the warps' acceptance bytes shared per block of runs);
 //   * the measurement accumulators of every EMCS, as measure_int8.
@@ -50,13 +54,34 @@ struct ResidentRun {
     int64_t csize_c;    // stride between the clusters of one EMCS
 };
 
-// shared memory: the warps' acceptance tables, 16-bit parents, candidate bits, state
-__host__ __device__ inline size_t resident_smem_bytes(int64_t n)
+// Bit planes of the flood-fill cluster: rows are the x-lines of the lattice
+// (n / len of them), each padded to kRowWords(len) 32-site words.
+__host__ __device__ inline int res_row_words(int len) { return (len + 31) / 32; }
+// the flood fill applies to lattices of >= 2 dimensions with rows of <= 8 words
+__host__ __device__ inline bool res_bits_ok(int dim, int len) { return dim >= 2 && res_row_words(len) <= 8; }
+// planes: candidates, flood, x bonds, one per other dimension
+__host__ __device__ inline size_t res_bits_bytes(int64_t n, int dim, int len)
 {
-    const int64_t words = (n + 31) / 32;
-    return (size_t)kResWarps * kAccTab * 16 + (size_t)((2 * n + 15) & ~15ll) + (size_t)words * 4 +
-           (size_t)((n + 15) & ~15ll);
+    return (size_t)(2 + dim) * (size_t)(n / len) * (size_t)res_row_words(len) * 4;
 }
+// union-find layout: 16-bit parents, candidate bits
+__host__ __device__ inline size_t res_uf_bytes(int64_t n)
+{
+    return (size_t)((2 * n + 15) & ~15ll) + (size_t)((n + 31) / 32) * 4;
+}
+// shared memory: the warps' acceptance tables, the cluster's work area (bit
+// planes or union-find arrays), the state
+__host__ __device__ inline size_t resident_smem_bytes(int64_t n, int dim, int len)
+{
+    const size_t work = res_bits_ok(dim, len) ? res_bits_bytes(n, dim, len) : res_uf_bytes(n);
+    return (size_t)kResWarps * kAccTab * 16 + ((work + 15) & ~(size_t)15) + (size_t)((n + 15) & ~15ll);
+}
+// the largest of any lattice on this path
+__host__ __device__ inline size_t resident_smem_max()
+{
+    return (size_t)kResWarps * kAccTab * 16 + res_uf_bytes(kResidentMaxSites) + (size_t)kResidentMaxSites;
+}
+size_t resident_smem_for(const StencilDev& st) { return resident_smem_bytes(st.n, st.dim, st.len); }
 
 // union-find on 16-bit parent indices (path halving; hooks by CAS, larger root under smaller)
 __device__ __forceinline__ int rfind(volatile unsigned short* p, int x)
@@ -84,18 +109,197 @@ __device__ __forceinline__ void runite(volatile unsigned short* p, int a, int b)
     }
 }
 
+// rows (x-lines) of a stencil: the row of site index i = r len, and the row
+// one step up / down in dimension d >= 1, periodic
+__device__ __forceinline__ uint32_t res_row_of(const StencilDev& st, uint32_t i)
+{
+    return st.lg >= 0 ? i >> st.lg : st.divlen(i);
+}
+__device__ __forceinline__ uint32_t res_row_step(const StencilDev& st, uint32_t r, int d, int dir)
+{
+    return res_row_of(st, (uint32_t)st.nbr((int64_t)r * st.len, 2 * d + (dir < 0 ? 1 : 0)));
+}
+
+// The seed's component of the activated bonds as the bit plane F, by flood
+// fill (every thread of the CTA calls it).  Planes of NW = rows x WR words:
+// C candidates (sites in the seed's old state), Bx the +x bond of each site
+// (periodic; bit len-1 of a row is the bond to its site 0), Bd + (d-1) NW the
+// +d bond of each site for d = 1 .. dim-1; a bond is set when both ends are
+// candidates and its keyed draw activates it (wolff_int8_active, the other
+// paths' rule).  The fill repeats, until no word changes: every row takes the
+// flood of its neighbouring rows through their bonds (every dimension >= 1),
+// spreads it over the rows a warp holds along dimension 1 (prefix scans over
+// the lanes, down and up), and closes it along its own x-line (prefix scans
+// over the bits of its words, forward and backward, with the periodic carry).
+// Every step only adds sites joined to the flood by an active bond, and the
+// fill stops when the flood is closed: F is the component.
+__device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, const int8_t* s, int val,
+                                      uint32_t rsite, uint32_t serial, uint32_t tgb, Key key, uint32_t* C,
+                                      uint32_t* F, uint32_t* Bx, uint32_t* Bd)
+{
+    const int len = lst.len, WR = res_row_words(len), D = lst.dim;
+    const uint32_t R = (uint32_t)(lst.n / len), NW = R * (uint32_t)WR;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    // candidates; the flood cleared
+    for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
+        const uint32_t r = wi / (uint32_t)WR;
+        const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
+        const bool c = x < len && s[(int64_t)r * len + x] == val;
+        const uint32_t b = __ballot_sync(0xffffffffu, c);
+        if (lane == 0) {
+            C[wi] = b;
+            F[wi] = 0u;
+        }
+    }
+    __syncthreads();
+    // active bonds
+    for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
+        const uint32_t r = wi / (uint32_t)WR;
+        const int wx = (int)(wi - r * (uint32_t)WR);
+        const int x = wx * 32 + lane;  // C bits of x >= len are clear
+        const bool ci = ((C[wi] >> lane) & 1u) != 0;
+        const uint32_t i = r * (uint32_t)len + (uint32_t)x;
+        {
+            const int xj = x + 1 == len ? 0 : x + 1;
+            const bool cj = ci && ((C[r * WR + (xj >> 5)] >> (xj & 31)) & 1u);
+            const bool act = cj && wolff_int8_active(w, i, r * (uint32_t)len + (uint32_t)xj, serial, tgb, key);
+            const uint32_t b = __ballot_sync(0xffffffffu, act);
+            if (lane == 0) Bx[wi] = b;
+        }
+        for (int d = 1; d < D; ++d) {
+            const uint32_t rp = res_row_step(lst, r, d, +1);
+            const bool cj = ci && ((C[rp * WR + wx] >> lane) & 1u);
+            const bool act = cj && wolff_int8_active(w, i, rp * (uint32_t)len + (uint32_t)x, serial, tgb, key);
+            const uint32_t b = __ballot_sync(0xffffffffu, act);
+            if (lane == 0) Bd[(size_t)(d - 1) * NW + wi] = b;
+        }
+    }
+    if (tid == 0) {
+        const uint32_t rr = res_row_of(lst, rsite), xx = rsite - rr * (uint32_t)len;
+        F[rr * WR + (xx >> 5)] = 1u << (xx & 31);
+    }
+    __syncthreads();
+    const int lb = (len - 1) & 31, lw = WR - 1;
+    const uint32_t rounds = (R + kResThreads - 1) / kResThreads;
+    for (uint32_t it = 0; it <= NW * 32u; ++it) {  // each pass adds a site or ends the fill
+        int changed = 0;
+        for (uint32_t k = 0; k < rounds; ++k) {
+            const uint32_t r = k * kResThreads + (uint32_t)tid;  // a warp's lanes: consecutive rows
+            const bool live = r < R;
+            uint32_t G[8], old[8];
+#pragma unroll
+            for (int q = 0; q < 8; ++q) old[q] = G[q] = (live && q < WR) ? F[r * WR + q] : 0u;
+            int y = 0;
+            if (live) {
+                y = lst.coord((int64_t)r * len, 1);
+                for (int d = 1; d < D; ++d) {
+                    const uint32_t rp = res_row_step(lst, r, d, +1), rm = res_row_step(lst, r, d, -1);
+                    const uint32_t* B = Bd + (size_t)(d - 1) * NW;
+#pragma unroll
+                    for (int q = 0; q < 8; ++q)
+                        if (q < WR) G[q] |= (F[rp * WR + q] & B[r * WR + q]) | (F[rm * WR + q] & B[rm * WR + q]);
+                }
+            }
+            // along dimension 1 over the warp's lanes (rows r - 1, r + 1 when
+            // they are this row's neighbours without the periodic wrap)
+            const bool hasprev = live && y != 0, hasnext = live && y != len - 1;
+#pragma unroll
+            for (int q = 0; q < 8; ++q) {
+                if (q >= WR) break;
+                uint32_t X = G[q];
+                uint32_t P = hasprev ? Bd[(r - 1) * WR + q] : 0u;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t Xo = __shfl_up_sync(0xffffffffu, X, o), Po = __shfl_up_sync(0xffffffffu, P, o);
+                    if (lane >= o) {
+                        X |= P & Xo;
+                        P &= Po;
+                    }
+                }
+                uint32_t Q = hasnext ? Bd[r * WR + q] : 0u;
+#pragma unroll
+                for (int o = 1; o < 32; o <<= 1) {
+                    const uint32_t Xo = __shfl_down_sync(0xffffffffu, X, o), Qo = __shfl_down_sync(0xffffffffu, Q, o);
+                    if (lane + o < 32) {
+                        X |= Q & Xo;
+                        Q &= Qo;
+                    }
+                }
+                G[q] = X;
+            }
+            if (live) {
+                // along the row's x-line: the bond bits without the periodic
+                // one (bit lb of the last word), which is carried explicitly
+                uint32_t bx[8];
+#pragma unroll
+                for (int q = 0; q < 8; ++q) bx[q] = q < WR ? Bx[r * WR + q] : 0u;
+                const uint32_t wrap = (bx[lw] >> lb) & 1u;
+                bx[lw] &= ~(1u << lb);
+                uint32_t cin = (G[lw] >> lb) & wrap;  // site len-1 -> site 0
+#pragma unroll
+                for (int q = 0; q < 8; ++q) {
+                    if (q >= WR) break;
+                    uint32_t X = G[q] | cin, p = bx[q] << 1;
+                    X |= (X << 1) & p;
+                    p &= p << 1;
+                    X |= (X << 2) & p;
+                    p &= p << 2;
+                    X |= (X << 4) & p;
+                    p &= p << 4;
+                    X |= (X << 8) & p;
+                    p &= p << 8;
+                    X |= (X << 16) & p;
+                    G[q] = X;
+                    cin = (X >> 31) & (bx[q] >> 31);
+                }
+                cin = G[0] & 1u & wrap;  // site 0 -> site len-1
+#pragma unroll
+                for (int q = 7; q >= 0; --q) {
+                    if (q > lw) continue;
+                    uint32_t X = G[q] | (cin << (q == lw ? lb : 31)), p = bx[q];
+                    X |= (X >> 1) & p;
+                    p &= p >> 1;
+                    X |= (X >> 2) & p;
+                    p &= p >> 2;
+                    X |= (X >> 4) & p;
+                    p &= p >> 4;
+                    X |= (X >> 8) & p;
+                    p &= p >> 8;
+                    X |= (X >> 16) & p;
+                    G[q] = X;
+                    cin = q > 0 ? (X & 1u) & (bx[q - 1] >> 31) : 0u;
+                }
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (q < WR && G[q] != old[q]) {
+                        F[r * WR + q] = G[q];
+                        changed = 1;
+                    }
+            }
+        }
+        if (!__syncthreads_or(changed)) break;
+    }
+}
+
 __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
 {
     __shared__ int s_rsite, s_val, s_newq, s_root, s_size;
     const int64_t n = R.st.n;
     const int64_t words = (n + 31) / 32;
     uint4* tab = reinterpret_cast<uint4*>(smem) + (threadIdx.x >> 5) * kAccTab;
-    unsigned char* p = smem + (size_t)kResWarps * kAccTab * 16;
-    volatile unsigned short* par = reinterpret_cast<unsigned short*>(p);
-    p += (size_t)((2 * n + 15) & ~15ll);
-    uint32_t* cand = reinterpret_cast<uint32_t*>(p);
-    p += (size_t)words * 4;
-    int8_t* s = reinterpret_cast<int8_t*>(p);
+    // the cluster's work area (bit planes, or union-find parents and
+    // candidate bits on one-dimensional chains), then the state
+    const bool bits_mode = res_bits_ok(R.st.dim, R.st.len);
+    const size_t work = bits_mode ? res_bits_bytes(n, R.st.dim, R.st.len) : res_uf_bytes(n);
+    unsigned char* wk = smem + (size_t)kResWarps * kAccTab * 16;
+    volatile unsigned short* par = reinterpret_cast<unsigned short*>(wk);
+    uint32_t* cand = reinterpret_cast<uint32_t*>(wk + (size_t)((2 * n + 15) & ~15ll));
+    const uint32_t NW = (uint32_t)(n / R.st.len) * (uint32_t)res_row_words(R.st.len);
+    uint32_t* bC = reinterpret_cast<uint32_t*>(wk);
+    uint32_t* bF = bC + NW;
+    uint32_t* bX = bF + NW;
+    uint32_t* bD = bX + NW;
+    int8_t* s = reinterpret_cast<int8_t*>(wk + ((work + 15) & ~(size_t)15));
     StencilDev lst = R.st;
     lst.split = 0;  // site order in shared memory
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -114,6 +318,26 @@ __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
             }
             __syncthreads();
             const int val = s_val;
+            if (bits_mode) {
+                resident_cluster_bits(lst, R.w, s, val, (uint32_t)s_rsite, serial, tgb, R.key, bC, bF, bX, bD);
+                // flip the component and count it
+                const int8_t nv = (int8_t)s_newq;
+                const int len = lst.len, WR = res_row_words(len);
+                int cnt = 0;
+                for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
+                    const uint32_t b = bF[wi];
+                    if (b) {
+                        const uint32_t r = wi / (uint32_t)WR;
+                        const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
+                        if ((b >> lane) & 1u) s[(int64_t)r * len + x] = nv;
+                        if (lane == 0) cnt += __popc(b);
+                    }
+                }
+                if (lane == 0 && cnt) atomicAdd(&s_size, cnt);
+                __syncthreads();
+                if (tid == 0) R.csize[e * R.csize_e + c * R.csize_c] = s_size;
+                continue;
+            }
             // candidates: sites in the seed's old state, each its own root
             for (int64_t wd = tid; wd < words; wd += kResThreads) {
                 uint32_t bits = 0;
@@ -246,7 +470,7 @@ static cudaError_t resident_attr(int device)
 {
     static std::atomic<bool> done[64] = {};  // host threads share it
     if (device >= 0 && device < 64 && done[device]) return cudaSuccess;
-    const int bytes = (int)resident_smem_bytes(kResidentMaxSites);
+    const int bytes = (int)resident_smem_max();
     cudaError_t e = cudaFuncSetAttribute(emcs_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(batch_resident, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -282,7 +506,7 @@ cudaError_t launch_emcs_resident(Sim* s, int n_emcs, int ncluster, int nmetro, b
     R.csize = csize;
     R.csize_e = ncluster;
     R.csize_c = 1;
-    emcs_resident<<<1, kResThreads, resident_smem_bytes(s->n), s->stream>>>(R);
+    emcs_resident<<<1, kResThreads, resident_smem_for(s->sten), s->stream>>>(R);
     s->launches++;
     s->sweep += (uint64_t)n_emcs * (uint64_t)nmetro;
     s->cluster += (uint64_t)n_emcs * (uint64_t)ncluster;
@@ -290,14 +514,14 @@ cudaError_t launch_emcs_resident(Sim* s, int n_emcs, int ncluster, int nmetro, b
 }
 
 // The batch's resident members (order: member ids, largest first; nres of
-// them, the largest with max_n sites), EMCS e0 .. e0 + count - 1.
-cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, int64_t max_n,
+// them, smem: the largest shared-memory layout among them), EMCS e0 .. e0 + count - 1.
+cudaError_t batch_launch_resident(const BatchLaunch& b, cudaStream_t st, const int32_t* order, int nres, size_t smem,
                                   uint32_t e0, int slot0, int count, int ncluster, int nmetro, int device)
 {
     if (nres <= 0 || count <= 0) return cudaSuccess;
     cudaError_t e = resident_attr(device);
     if (e != cudaSuccess) return e;
-    batch_resident<<<nres, kResThreads, resident_smem_bytes(max_n), st>>>(b.reps, order, b.nrep, e0, slot0, count,
+    batch_resident<<<nres, kResThreads, smem, st>>>(b.reps, order, b.nrep, e0, slot0, count,
                                                                           ncluster, nmetro, b.acc, b.csize);
     return cudaGetLastError();
 }
