@@ -88,7 +88,7 @@ __device__ __forceinline__ bool dcand(const Dist<uint32_t>& c, int64_t j)
 
 // One cluster per member of `order`: EMCS e0 .. e0 + count - 1 of the run,
 // measurement slots from slot0.  The cluster has ceil(n / kClSlab) CTAs.
-__global__ void __launch_bounds__(kClThreads)
+__global__ void __launch_bounds__(kClThreads, 1)
     batch_resident_cluster(const BatchRep* __restrict__ reps, const int32_t* __restrict__ order, int nrep,
                            uint32_t e0, int slot0, int count, int ncluster, int nmetro, long long* __restrict__ acc,
                            int32_t* __restrict__ csize)

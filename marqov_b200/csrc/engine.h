@@ -84,10 +84,13 @@ struct StencilDev {
         return split_addr(coord(i, 1), coord(i, 0), len);  // split layouts are 2D
     }
     MQV_HD int degree(int64_t) const { return 2 * dim; }
+    // pows[j] by selects: no dynamic index, so that a copy of the stencil in
+    // a kernel stays in registers instead of local memory
+    MQV_HD int64_t pow_of(int j) const { return j == 0 ? pows[0] : j == 1 ? pows[1] : j == 2 ? pows[2] : pows[3]; }
     MQV_HD int64_t nbr(int64_t i, int slot) const
     {
         const int j = slot >> 1;
-        const int64_t p = pows[j];
+        const int64_t p = pow_of(j);
         const int x = coord(i, j);
         if ((slot & 1) == 0) return x == len - 1 ? i - (int64_t)(len - 1) * p : i + p;
         return x == 0 ? i + (int64_t)(len - 1) * p : i - p;

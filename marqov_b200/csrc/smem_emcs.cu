@@ -230,12 +230,17 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
             if (live) {
                 // along the row's x-line: the bond bits without the periodic
                 // one (bit lb of the last word), which is carried explicitly
-                uint32_t bx[8];
+                uint32_t bx[8], wrap = 0u, glast = 0u;
 #pragma unroll
-                for (int q = 0; q < 8; ++q) bx[q] = q < WR ? Bx[r * WR + q] : 0u;
-                const uint32_t wrap = (bx[lw] >> lb) & 1u;
-                bx[lw] &= ~(1u << lb);
-                uint32_t cin = (G[lw] >> lb) & wrap;  // site len-1 -> site 0
+                for (int q = 0; q < 8; ++q) {
+                    bx[q] = q < WR ? Bx[r * WR + q] : 0u;
+                    if (q == lw) {  // constant indices only: the arrays stay in registers
+                        wrap = (bx[q] >> lb) & 1u;
+                        bx[q] &= ~(1u << lb);
+                        glast = G[q];
+                    }
+                }
+                uint32_t cin = (glast >> lb) & wrap;  // site len-1 -> site 0
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
                     if (q >= WR) break;
@@ -420,7 +425,7 @@ __host__ __device__ inline int resident_runs(int64_t n)
     return runs;
 }
 
-__global__ void __launch_bounds__(kResThreads) emcs_resident(ResidentRun R)
+__global__ void __launch_bounds__(kResThreads, 1) emcs_resident(ResidentRun R)
 {
     extern __shared__ __align__(16) unsigned char smem[];
     resident_run(R, smem);
@@ -428,7 +433,7 @@ __global__ void __launch_bounds__(kResThreads) emcs_resident(ResidentRun R)
 
 // One CTA per member of `order` (the batch's resident members, largest
 // first): EMCS e0 .. e0 + count - 1 of the run, measurement slots slot0 ..
-__global__ void __launch_bounds__(kResThreads)
+__global__ void __launch_bounds__(kResThreads, 1)
     batch_resident(const BatchRep* __restrict__ reps, const int32_t* __restrict__ order, int nrep, uint32_t e0,
                    int slot0, int count, int ncluster, int nmetro, long long* __restrict__ acc,
                    int32_t* __restrict__ csize)
