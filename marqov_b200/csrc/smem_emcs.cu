@@ -127,12 +127,14 @@ __device__ __forceinline__ uint32_t res_row_step(const StencilDev& st, uint32_t 
 // +d bond of each site for d = 1 .. dim-1; a bond is set when both ends are
 // candidates and its keyed draw activates it (wolff_int8_active, the other
 // paths' rule).  The fill repeats, until no word changes: every row takes the
-// flood of its neighbouring rows through their bonds (every dimension >= 1),
-// spreads it over the rows a warp holds along dimension 1 (prefix scans over
-// the lanes, down and up), and closes it along its own x-line (prefix scans
-// over the bits of its words, forward and backward, with the periodic carry).
-// Every step only adds sites joined to the flood by an active bond, and the
-// fill stops when the flood is closed: F is the component.
+// flood of its neighbouring rows through their bonds (every dimension >= 1);
+// then each warp, whose lanes hold consecutive rows, alternates spreading
+// the flood along dimension 1 over its lanes (prefix scans over the lanes,
+// down and up) with closing it along each row's x-line (prefix scans over the
+// bits of the row's words, forward and backward, with the periodic carry)
+// until neither adds a site.  Every step only adds sites joined to the flood
+// by an active bond, and the fill stops when the flood is closed: F is the
+// component.
 __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, const int8_t* s, int val,
                                       uint32_t rsite, uint32_t serial, uint32_t tgb, Key key, uint32_t* C,
                                       uint32_t* F, uint32_t* Bx, uint32_t* Bd)
@@ -184,6 +186,7 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
     for (uint32_t it = 0; it <= NW * 32u; ++it) {  // each pass adds a site or ends the fill
         int changed = 0;
         for (uint32_t k = 0; k < rounds; ++k) {
+            if (k * kResThreads + (uint32_t)warp * 32u >= R) break;  // this warp holds no rows (uniform)
             const uint32_t r = k * kResThreads + (uint32_t)tid;  // a warp's lanes: consecutive rows
             const bool live = r < R;
             uint32_t G[8], old[8];
@@ -200,46 +203,55 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
                         if (q < WR) G[q] |= (F[rp * WR + q] & B[r * WR + q]) | (F[rm * WR + q] & B[rm * WR + q]);
                 }
             }
-            // along dimension 1 over the warp's lanes (rows r - 1, r + 1 when
-            // they are this row's neighbours without the periodic wrap)
+            // Warp-local fixpoint: alternate the spread along dimension 1
+            // over the warp's lanes (rows r - 1, r + 1 when they are this
+            // row's neighbours without the periodic wrap) with the closure
+            // along each row's x-line, until no lane changes; the other
+            // warps' rows and the periodic wraps come in through the
+            // neighbour rows at the next pass.
             const bool hasprev = live && y != 0, hasnext = live && y != len - 1;
+            uint32_t bx[8], pb[8], qb[8], wrap = 0u;
 #pragma unroll
             for (int q = 0; q < 8; ++q) {
-                if (q >= WR) break;
-                uint32_t X = G[q];
-                uint32_t P = hasprev ? Bd[(r - 1) * WR + q] : 0u;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t Xo = __shfl_up_sync(0xffffffffu, X, o), Po = __shfl_up_sync(0xffffffffu, P, o);
-                    if (lane >= o) {
-                        X |= P & Xo;
-                        P &= Po;
-                    }
+                bx[q] = (live && q < WR) ? Bx[r * WR + q] : 0u;
+                pb[q] = (hasprev && q < WR) ? Bd[(r - 1) * WR + q] : 0u;
+                qb[q] = (hasnext && q < WR) ? Bd[r * WR + q] : 0u;
+                if (q == lw) {  // constant indices only: the arrays stay in registers
+                    wrap = (bx[q] >> lb) & 1u;
+                    bx[q] &= ~(1u << lb);
                 }
-                uint32_t Q = hasnext ? Bd[r * WR + q] : 0u;
-#pragma unroll
-                for (int o = 1; o < 32; o <<= 1) {
-                    const uint32_t Xo = __shfl_down_sync(0xffffffffu, X, o), Qo = __shfl_down_sync(0xffffffffu, Q, o);
-                    if (lane + o < 32) {
-                        X |= Q & Xo;
-                        Q &= Qo;
-                    }
-                }
-                G[q] = X;
             }
-            if (live) {
-                // along the row's x-line: the bond bits without the periodic
-                // one (bit lb of the last word), which is carried explicitly
-                uint32_t bx[8], wrap = 0u, glast = 0u;
+            for (;;) {
+                uint32_t moved = 0u;
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
-                    bx[q] = q < WR ? Bx[r * WR + q] : 0u;
-                    if (q == lw) {  // constant indices only: the arrays stay in registers
-                        wrap = (bx[q] >> lb) & 1u;
-                        bx[q] &= ~(1u << lb);
-                        glast = G[q];
+                    if (q >= WR) break;
+                    uint32_t X = G[q], P = pb[q], Q = qb[q];
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t Xo = __shfl_up_sync(0xffffffffu, X, o), Po = __shfl_up_sync(0xffffffffu, P, o);
+                        if (lane >= o) {
+                            X |= P & Xo;
+                            P &= Po;
+                        }
                     }
+#pragma unroll
+                    for (int o = 1; o < 32; o <<= 1) {
+                        const uint32_t Xo = __shfl_down_sync(0xffffffffu, X, o), Qo = __shfl_down_sync(0xffffffffu, Q, o);
+                        if (lane + o < 32) {
+                            X |= Q & Xo;
+                            Q &= Qo;
+                        }
+                    }
+                    moved |= X ^ G[q];
+                    G[q] = X;
                 }
+                // along the row's x-line (the periodic bond, bit lb of the
+                // last word, carried explicitly)
+                uint32_t glast = 0u;
+#pragma unroll
+                for (int q = 0; q < 8; ++q)
+                    if (q == lw) glast = G[q];
                 uint32_t cin = (glast >> lb) & wrap;  // site len-1 -> site 0
 #pragma unroll
                 for (int q = 0; q < 8; ++q) {
@@ -254,6 +266,7 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
                     X |= (X << 8) & p;
                     p &= p << 8;
                     X |= (X << 16) & p;
+                    moved |= X ^ G[q];
                     G[q] = X;
                     cin = (X >> 31) & (bx[q] >> 31);
                 }
@@ -271,9 +284,13 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
                     X |= (X >> 8) & p;
                     p &= p >> 8;
                     X |= (X >> 16) & p;
+                    moved |= X ^ G[q];
                     G[q] = X;
                     cin = q > 0 ? (X & 1u) & (bx[q - 1] >> 31) : 0u;
                 }
+                if (!__any_sync(0xffffffffu, moved != 0u)) break;
+            }
+            if (live) {
 #pragma unroll
                 for (int q = 0; q < 8; ++q)
                     if (q < WR && G[q] != old[q]) {
