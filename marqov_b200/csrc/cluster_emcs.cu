@@ -69,7 +69,7 @@ __device__ __forceinline__ void dunite(const Dist<int>& p, int a, int b)
         a = dfind(p, a);
         b = dfind(p, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_prio((uint32_t)a) > uf_prio((uint32_t)b)) {  // the root of lower priority hangs below
             const int t = a;
             a = b;
             b = t;

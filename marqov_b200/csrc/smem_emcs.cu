@@ -83,7 +83,7 @@ __host__ __device__ inline size_t resident_smem_max()
 }
 size_t resident_smem_for(const StencilDev& st) { return resident_smem_bytes(st.n, st.dim, st.len); }
 
-// union-find on 16-bit parent indices (path halving; hooks by CAS, larger root under smaller)
+// union-find on 16-bit parent indices (path halving; hooks by CAS, linking by uf_prio16)
 __device__ __forceinline__ int rfind(volatile unsigned short* p, int x)
 {
     while (true) {
@@ -100,7 +100,7 @@ __device__ __forceinline__ void runite(volatile unsigned short* p, int a, int b)
         a = rfind(p, a);
         b = rfind(p, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_prio16((uint32_t)a) > uf_prio16((uint32_t)b)) {  // the root of lower priority hangs below
             const int t = a;
             a = b;
             b = t;

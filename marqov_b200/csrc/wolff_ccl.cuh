@@ -6,7 +6,8 @@
 // one CTA needs one step per level of the cluster; this variant labels every
 // component of the activated-bond graph of every member in a fixed number of
 // whole-lattice passes -- lock-free union-find: each undirected bond once,
-// roots hooked by compare-and-swap, paths halved on the way -- and flips the
+// roots hooked by compare-and-swap in a fixed pseudo-random order (uf_prio),
+// paths halved on the way -- and flips the
 // seed's component:
 //   ccl_seed      one thread per member: seed site, old/new state or the
 //                 reflection vector (the same substream draws as the BFS);
@@ -63,12 +64,12 @@ __device__ __forceinline__ void ccl_unite(int* __restrict__ p, int a, int b)
         a = ccl_find(p, a);
         b = ccl_find(p, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_prio((uint32_t)a) > uf_prio((uint32_t)b)) {  // the root of lower priority hangs below
             const int t = a;
             a = b;
             b = t;
         }
-        if (atomicCAS(p + a, a, b) == a) return;  // the larger root hangs below the smaller
+        if (atomicCAS(p + a, a, b) == a) return;
     }
 }
 
@@ -151,7 +152,7 @@ __device__ __forceinline__ void ccl_lunite(volatile int* p, int a, int b)
         a = ccl_lfind(p, a);
         b = ccl_lfind(p, b);
         if (a == b) return;
-        if (a < b) {
+        if (uf_prio((uint32_t)a) > uf_prio((uint32_t)b)) {  // the root of lower priority hangs below
             const int t = a;
             a = b;
             b = t;

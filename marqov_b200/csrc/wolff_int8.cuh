@@ -29,6 +29,15 @@ __device__ __forceinline__ int64_t wolff_int8_seed(const WolffDev& w, const Lat&
     return rsite;
 }
 
+// Union-find linking order of the labelling kernels: of two roots, the one
+// of lower priority hangs below the other.  Priorities are a fixed
+// pseudo-random permutation of the site index (multiplication by an odd
+// constant is a bijection modulo 2^32 and modulo 2^16), so the trees stay
+// O(log n) deep in expectation whatever order the bonds are united in --
+// hooking by index chains up sites that are united side by side.
+__device__ __forceinline__ uint32_t uf_prio(uint32_t i) { return i * 0x9E3779B1u; }
+__device__ __forceinline__ uint32_t uf_prio16(uint32_t i) { return (i * 0x9E37u) & 0xFFFFu; }
+
 // Bond activation of the int8 rules on the bond's keyed word
 __device__ __forceinline__ bool wolff_int8_active(const WolffDev& w, uint32_t a, uint32_t b, uint32_t serial,
                                                   uint32_t tg_bond, Key key)
