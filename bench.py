@@ -317,8 +317,10 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
     """Config 3: the 256-replica farm, batched against plain per-replica runs
     over the same EMCS window after the same thermalisation.
 
-    Batched: one Batch (resident CTAs for the members that fit shared memory,
-    graph-replayed kernels for the others), CUDA events around the window.
+    Batched: one Batch on its graph path (every member's sites in the same
+    launches, replayed from CUDA graphs), CUDA events around the window; the
+    same farm with every member resident is timed as a second batched
+    variant.
     Plain per-replica launches: the same members as 256 independent handles
     on the launch-per-step path (a launch per cluster, per colour and per
     measurement; MQV_FLAG_NO_RESIDENT), each on its own stream, issued from a
@@ -332,6 +334,21 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
     from concurrent.futures import ThreadPoolExecutor
     members = potts_farm(M)
     sites = sum(m[0].size() for m in members)
+
+    def batched_resident():
+        """The same farm with every member resident (MQV_FLAG_RESIDENT): one
+        CTA, or one thread-block cluster, per member for whole chunks."""
+        ms = [(lat, M.Config(seed=cfg.seed, repid=cfg.repid, resident=True), ham, beta)
+              for lat, cfg, ham, beta in members]
+        with M.Batch(ms, graph_steps=8) as br:
+            br.init()
+            br.emcs(therm, 1, 1)
+            st2 = torch.cuda.ExternalStream(stream_of(br.member(0)))
+            res = []
+            t = timed(torch, st2, lambda: res.append(br.emcs(emcs, 1, 1)))
+            final = [br.member(i).state for i in (0, 1, 2)]
+        return t, res[0][0], final
+
     with M.Batch(members, graph_steps=8) as b:
         b.init()
         b.emcs(therm, 1, 1)
@@ -380,7 +397,8 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
 
     wall_p, outs, same = plain(False)
     wall_pr, _, same_r = plain(True)
-    same = same and same_r
+    dev_br, obs_br, final_br = batched_resident()
+    same = same and same_r and bool((obs_br == obs_b).all()) and all((final_br[i] == final_b[i]).all() for i in range(3))
     rate_b = sites * emcs / (dev_b * 1e9)
     rate_b_wall = sites * emcs / (wall_b * 1e9)
     rate_p = sites * emcs / (wall_p * 1e9)
@@ -394,7 +412,12 @@ def workload_potts_batch(M, torch, emcs=1000, therm=200, threads=None):
                     "EMCS = 1 Wolff cluster + 1 checkerboard sweep + measurement",
         "sites": int(sites), "unit": UNIT, "emcs_window": emcs, "thermalisation": therm,
         "batched": {"value": rate_b, "value_wall": rate_b_wall, "emcs": emcs, "seconds_device": dev_b,
-                    "seconds_wall": wall_b, "gpu_launches": int(launches_b), "graph_emcs_per_launch": 8},
+                    "seconds_wall": wall_b, "gpu_launches": int(launches_b), "graph_emcs_per_launch": 8,
+                    "how": "graph path: every member's sites in one launch per colour, one labelling pass set per "
+                           "cluster and one measurement launch per EMCS, replayed from CUDA graphs"},
+        "batched_resident": {"value": sites * emcs / (dev_br * 1e9), "seconds_device": dev_br,
+                             "how": "every member resident (one CTA per member of <= 65536 sites, a thread-block "
+                                    "cluster for the larger ones) for whole chunks of EMCS"},
         "plain": {"value": rate_p, "emcs": emcs, "seconds_wall": wall_p,
                   "how": f"256 handles on the launch-per-step path, each on its own stream, one mqv_emcs call "
                          f"each from {nthreads} host threads (no synchronisation between members)"},

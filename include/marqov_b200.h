@@ -125,9 +125,9 @@ enum {
                                  (<= 65536 sites) or one thread-block cluster (<= 262144 sites) that
                                  keeps the state in shared memory for a whole chunk of EMCS; launch
                                  per cluster, colour and measurement instead (same results) */
-    MQV_FLAG_RESIDENT = 4     /* take the resident path wherever the lattice fits it, also where the
-                                 default choice would not (a batch whose resident CTAs would fill
-                                 less than half the SMs runs every other member on the graph path) */
+    MQV_FLAG_RESIDENT = 4     /* take the resident path wherever the lattice fits it.  Default (neither
+                                 flag): a single handle is resident up to 16384 sites; batch members
+                                 run on the batch's graph path */
 };
 
 typedef struct mqv_run_params {

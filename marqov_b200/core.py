@@ -42,10 +42,10 @@ class Config:
     # force one launch per colour class (no fused two-colour tiles)
     per_colour: bool = False
     # int8 stencil lattices of <= 65536 sites (one CTA) or <= 262144 sites (a
-    # thread-block cluster) run whole chunks of EMCS in shared memory.  None:
-    # the engine decides (in a batch, only while the resident CTAs fill half
-    # the SMs); True: wherever the lattice fits; False: never (launch per
-    # step).  The results are the same.
+    # thread-block cluster) can run whole chunks of EMCS in shared memory.
+    # None: the engine decides (single handles up to 16384 sites; batch
+    # members take the batch's graph path); True: wherever the lattice fits;
+    # False: never (launch per step).  The results are the same.
     resident: bool | None = None
 
     def setid(self, i):

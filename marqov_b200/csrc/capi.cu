@@ -401,13 +401,22 @@ static mqv_status check_wolff_supported(Sim* s)
     return MQV_OK;
 }
 
+// A single handle takes the resident path by default up to this many sites:
+// one SM then beats a launch per cluster, colour and measurement (2D Ising
+// at L = 128: 176 against 335 us per EMCS); above it the launches, which
+// spread a sweep over every SM, win (L = 256: 678 against 646 us).
+constexpr int64_t kResidentAutoSites = 16384;
 // EMCS of this handle run on the resident path (smem_emcs.cu)?
-static bool use_resident(const Sim* s) { return !(s->flags & MQV_FLAG_NO_RESIDENT) && resident_fits(s); }
+static bool use_resident(const Sim* s)
+{
+    if ((s->flags & MQV_FLAG_NO_RESIDENT) || !resident_fits(s)) return false;
+    return (s->flags & MQV_FLAG_RESIDENT) || s->n <= kResidentAutoSites;
+}
 // ... or on a thread-block cluster (cluster_emcs.cu), for int8 stencils of
-// 65,537 .. 262,144 sites the device can co-schedule
+// 65,537 .. 262,144 sites the device can co-schedule (when asked for)
 static bool use_cluster(Sim* s)
 {
-    if ((s->flags & MQV_FLAG_NO_RESIDENT) || s->is_f32 || s->lat_kind != MQV_LATTICE_HYPERCUBIC || resident_fits(s))
+    if (!(s->flags & MQV_FLAG_RESIDENT) || s->is_f32 || s->lat_kind != MQV_LATTICE_HYPERCUBIC || resident_fits(s))
         return false;
     const int c = cluster_ctas(s->n);
     if (c < 2) return false;
@@ -1562,14 +1571,19 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         if (st) return bail(st);
     }
     // resident members: int8 stencil lattices that fit one CTA's shared
-    // memory, unless their spec asks for the launch path
+    // memory (or a thread-block cluster's) and whose spec asks for it
     b->resident.assign((size_t)n, 0);
     std::vector<int32_t> res_order[2], cl_order[9];
     bool cl_ok[9] = {};
     for (int c = 2; c <= 8; ++c) cl_ok[c] = cluster_launchable(c);
     for (int r = 0; r < n; ++r) {
         const Sim* s = b->sims[(size_t)r];
-        if (specs[r].params.flags & MQV_FLAG_NO_RESIDENT) continue;
+        // A resident member runs on one CTA (or one cluster) for a whole chunk
+        // of EMCS, which leaves it at the speed of one SM (or a few): the
+        // graph path, whose launches spread every member over all SMs, is the
+        // default (the 256-replica Potts farm: 1.8 against 3.4 ms per EMCS);
+        // members that ask for it (MQV_FLAG_RESIDENT) stay resident.
+        if (!(specs[r].params.flags & MQV_FLAG_RESIDENT)) continue;
         if (resident_fits(s)) {
             b->resident[(size_t)r] = 1;
             res_order[s->n > kResSmall ? 1 : 0].push_back(r);
@@ -1581,24 +1595,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
             }
         }
     }
-    // A resident member runs on one CTA (or one cluster) for a whole chunk of
-    // EMCS, so residency pays only while the resident CTAs fill the device:
-    // with fewer CTAs than half the SMs (a handful of realisations) the
-    // graph path, whose launches spread every member over all SMs, is
-    // faster, and every member takes it.
-    {
-        int sms = 148;
-        cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-        int64_t ctas = (int64_t)res_order[0].size() + (int64_t)res_order[1].size();
-        for (int c = 2; c <= 8; ++c) ctas += (int64_t)c * (int64_t)cl_order[c].size();
-        if (ctas > 0 && 2 * ctas < sms) {
-            auto keep = [&](int32_t r) { return (specs[r].params.flags & MQV_FLAG_RESIDENT) != 0; };
-            for (int r = 0; r < n; ++r)
-                if (!keep(r)) b->resident[(size_t)r] = 0;
-            for (auto& v : res_order) v.erase(std::remove_if(v.begin(), v.end(), [&](int32_t r) { return !keep(r); }), v.end());
-            for (auto& v : cl_order) v.erase(std::remove_if(v.begin(), v.end(), [&](int32_t r) { return !keep(r); }), v.end());
-        }
-    }
+
     for (int k = 0; k < 2; ++k) {
         std::stable_sort(res_order[k].begin(), res_order[k].end(),
                          [&](int32_t x, int32_t y) { return b->sims[(size_t)x]->n > b->sims[(size_t)y]->n; });
