@@ -248,7 +248,6 @@ static void launch_emcs_t(const BatchLaunch& b, cudaStream_t st, int ncluster, i
             ccl_hook<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
                                                              sd, b.ctr, ncluster, c);
             ccl_halve<<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites);
-            ccl_compress<<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites);
             ccl_flip<F32><<<gb, kBatchMetroThreads, 0, st>>>(b.reps, b.site_prefix, b.site_block_rep, b.total_sites,
                                                              sd, b.ctr, ncluster, c, b.csize, b.nrep);
         } else {

@@ -21,7 +21,19 @@ struct BatchRep {
     const unsigned long long* cuts;  // int8: the member's Metropolis cut table
     int D;                           // int8: its maximum degree
     int resident;                    // runs in one CTA's shared memory (batch_resident), not in the graphs
+    int tile;                        // labelling order (ccl_site): 0 site order, 2 16x16 tiles, 3 8x8x4 tiles
 };
+
+// Labelling order of a lattice: 2D stencils with len % 16 == 0 in 16 x 16
+// tiles, 3D stencils with len % 8 == 0 in 8 x 8 x 4 tiles (256 sites, one
+// CTA block of the labelling kernels each), others in site order.
+inline int ccl_tile_kind(int lat_kind, int dim, int len)
+{
+    if (lat_kind != MQV_LATTICE_HYPERCUBIC) return 0;
+    if (dim == 2 && len % 16 == 0) return 2;
+    if (dim == 3 && len % 8 == 0) return 3;
+    return 0;
+}
 
 // Sites of a member's lattice.
 __host__ __device__ __forceinline__ int64_t rep_sites(const BatchRep& R)
@@ -97,7 +109,7 @@ inline uint64_t batch_launches_per_emcs(const BatchLaunch& b, int ncluster, int 
 {
     int live = 0;
     for (int c = 0; c < b.ncol; ++c) live += b.total[c] > 0;
-    const uint64_t ccl = b.site_blocks > 0 ? 6ull : 0ull;  // seed, local, hook, halve, compress, flip
+    const uint64_t ccl = b.site_blocks > 0 ? 5ull : 0ull;  // seed, local, hook, halve, flip
     return (uint64_t)ncluster * (b.wolff_ccl ? ccl : 1ull) + (uint64_t)nmetro * (uint64_t)live +
            (b.meas_blocks > 0 ? 2ull : 1ull);
 }

@@ -1280,6 +1280,7 @@ static mqv_status batch_run(Batch* b, int n_emcs, int ncluster, int nmetro, mqv_
         r.cuts = s->d_cuts;
         r.D = s->max_degree;
         r.resident = b->resident[(size_t)i] ? 1 : 0;
+        r.tile = ccl_tile_kind(s->lat_kind, s->dim, s->len);
     }
     MQV_CK(cudaMemcpyAsync(b->d_reps, b->reps.data(), sizeof(BatchRep) * b->reps.size(), cudaMemcpyHostToDevice,
                            b->stream));

@@ -117,6 +117,7 @@ static BatchRep single_rep(const Sim* s)
     r.queue = s->d_queue;
     r.cuts = s->d_cuts;
     r.D = s->max_degree;
+    r.tile = ccl_tile_kind(s->lat_kind, s->dim, s->len);
     return r;
 }
 
@@ -133,10 +134,9 @@ static void launch_label_t(Sim* s, int32_t* csize)
     ccl_hook<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1,
                                                             1, 0);
     ccl_halve<<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n);
-    ccl_compress<<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n);
     ccl_flip<F32><<<gb, kBatchMetroThreads, 0, s->stream>>>(s->d_rep1, s->d_sprefix1, s->d_sbrep1, n, sd, s->d_ctr1, 1,
                                                             0, csize, 1);
-    s->launches += 7;
+    s->launches += 6;
 }
 
 // The one-member tables of the labelling path, allocated on first use.

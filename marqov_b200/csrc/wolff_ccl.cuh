@@ -17,11 +17,10 @@
 //                 sites are united in shared memory first; each candidate's
 //                 label becomes its local root, non-candidates get -1;
 //   ccl_hook      the other activated bonds between candidates are united;
-//   ccl_halve     every candidate's path to its root halved (hooks made side
-//                 by side chain up, so the trees can be deep);
-//   ccl_compress  label = root (read-only walks: only roots are written);
-//   ccl_flip      members of the seed's component are flipped / reflected and
-//                 counted into the cluster size.
+//   ccl_halve     every candidate's path to its root halved;
+//   ccl_flip      members of the seed's component (read-only walks to the
+//                 roots) are flipped / reflected and counted into the cluster
+//                 size.
 // The label array is the member's BFS queue (n int32); the visited bitmap is
 // not touched.
 #pragma once
@@ -45,6 +44,35 @@ __device__ __forceinline__ int ccl_member(int64_t g, const int64_t* __restrict__
     while (g >= prefix[r + 1]) ++r;
     i = g - prefix[r];
     return r;
+}
+
+// Position <-> site of a member in its labelling order (BatchRep::tile): the
+// labelling kernels give CTA block b the positions [256 b, 256 b + 256) of
+// the concatenated members, so that with tiles a block holds a 16 x 16 (2D)
+// or 8 x 8 x 4 (3D) tile and most bonds join two sites of one block.
+__device__ __forceinline__ int64_t ccl_site(const BatchRep& R, int64_t pos)
+{
+    if (R.tile == 0) return pos;
+    const uint32_t L = (uint32_t)R.st.len, t = (uint32_t)(pos >> 8), o = (uint32_t)pos & 255u;
+    if (R.tile == 2) {
+        const uint32_t nx = L >> 4, ty = t / nx, tx = t - ty * nx;
+        return (int64_t)((ty << 4) + (o >> 4)) * L + (tx << 4) + (o & 15u);
+    }
+    const uint32_t nx = L >> 3, ny = L >> 3, tyz = t / nx, tx = t - tyz * nx, tz = tyz / ny, ty = tyz - tz * ny;
+    const uint32_t x = (tx << 3) + (o & 7u), y = (ty << 3) + ((o >> 3) & 7u), z = (tz << 2) + (o >> 6);
+    return ((int64_t)z * L + y) * L + x;
+}
+__device__ __forceinline__ int64_t ccl_pos(const BatchRep& R, int64_t site)
+{
+    if (R.tile == 0) return site;
+    const uint32_t L = (uint32_t)R.st.len, u = (uint32_t)site;
+    if (R.tile == 2) {
+        const uint32_t y = u / L, x = u - y * L;
+        return (int64_t)(((y >> 4) * (L >> 4) + (x >> 4)) << 8) + ((y & 15u) << 4) + (x & 15u);
+    }
+    const uint32_t yz = u / L, x = u - yz * L, z = yz / L, y = yz - z * L;
+    const uint32_t t = ((z >> 2) * (L >> 3) + (y >> 3)) * (L >> 3) + (x >> 3);
+    return (int64_t)(t << 8) + ((z & 3u) << 6) + ((y & 7u) << 3) + (x & 7u);
 }
 
 __device__ __forceinline__ int ccl_find(int* __restrict__ p, int x)
@@ -177,11 +205,12 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
     const int64_t base = (int64_t)blockIdx.x * kBatchMetroThreads;
     const int64_t g = base + threadIdx.x;
     int r = 0;
-    int64_t i = 0;
+    int64_t i = 0;  // this thread's site (position g in the labelling order)
     bool cand = false;
     if (g < total) {
         r = ccl_member(g, prefix, block_rep, i);
         const BatchRep& R = reps[r];
+        i = ccl_site(R, i);
         cand = true;
         if (!F32) {
             const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
@@ -197,7 +226,7 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
         const int64_t off = prefix[r];
         volatile int* vl = slab;
         ccl_forward_bonds(R, i, [&](int64_t j) {
-            const int64_t gj = off + j;
+            const int64_t gj = off + ccl_pos(R, j);
             if (!ccl_same_block(g, gj)) return;
             const int k = (int)(gj - base);
             if (vl[k] >= 0 && ccl_active<F32>(R, sd, serial, i, j)) ccl_lunite(vl, (int)threadIdx.x, k);
@@ -212,7 +241,7 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
             // read-only walk to the local root (same member: bonds join only its sites)
             int x = (int)threadIdx.x, px;
             while ((px = ((volatile int*)slab)[x]) != x) x = px;
-            lab = (int)(base + x - prefix[r]);
+            lab = (int)ccl_site(reps[r], base + x - prefix[r]);
         }
         reps[r].queue[i] = lab;
     }
@@ -228,6 +257,7 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
     int64_t i;
     const int r = ccl_member(g, prefix, block_rep, i);
     const BatchRep& R = reps[r];
+    i = ccl_site(R, i);
     int* lab = R.queue;
     if (__ldcg(lab + i) < 0) return;
     const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
@@ -235,15 +265,14 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
     const int64_t off = prefix[r];
     // bonds within the CTA block were united by ccl_local
     ccl_forward_bonds(R, i, [&](int64_t j) {
-        if (ccl_same_block(g, off + j) || __ldcg(lab + j) < 0) return;
+        if (ccl_same_block(g, off + ccl_pos(R, j)) || __ldcg(lab + j) < 0) return;
         if (ccl_active<F32>(R, sd, serial, i, j)) ccl_unite(lab, (int)i, (int)j);
     });
 }
 
-// Hooks made side by side chain up, so trees can be deep and read-only walks
-// long: first every candidate's path is halved (all side by side; a write
-// only ever points a site to an ancestor, so the forest stays valid), then
-// ccl_compress walks the short paths that remain.
+// Every candidate's path halved, all side by side (a write only ever points
+// a site to an ancestor, so the forest stays valid while others walk it), so
+// that ccl_flip's walks are short.
 static __global__ void ccl_halve(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
                                  const int32_t* __restrict__ block_rep, int64_t total)
 {
@@ -254,22 +283,6 @@ static __global__ void ccl_halve(const BatchRep* __restrict__ reps, const int64_
     int* lab = reps[r].queue;
     if (__ldcg(lab + i) < 0) return;
     ccl_find(lab, (int)i);
-}
-
-static __global__ void ccl_compress(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
-                             const int32_t* __restrict__ block_rep, int64_t total)
-{
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
-    int64_t i;
-    const int r = ccl_member(g, prefix, block_rep, i);
-    int* lab = reps[r].queue;
-    if (__ldcg(lab + i) < 0) return;
-    // read-only walk to the root: a halving write here could replace a label
-    // that another thread has just set to its root by a non-root ancestor
-    int x = (int)i, px;
-    while ((px = __ldcg(lab + x)) != x) x = px;
-    lab[i] = x;
 }
 
 template <bool F32>
@@ -285,8 +298,15 @@ __global__ void ccl_flip(const BatchRep* __restrict__ reps, const int64_t* __res
         r = ccl_member(g, prefix, block_rep, i);
         const BatchRep& R = reps[r];
         const CclSeed& sd = seeds[r];
-        const int root = R.queue[sd.rsite];
-        in = root >= 0 && R.queue[i] == root;
+        // read-only walks to the roots (short after ccl_halve)
+        const int* lab = R.queue;
+        int root = __ldcg(lab + sd.rsite), x = __ldcg(lab + i);
+        if (root >= 0 && x >= 0) {
+            int p;
+            while ((p = __ldcg(lab + root)) != root) root = p;
+            while ((p = __ldcg(lab + x)) != x) x = p;
+            in = x == root;
+        }
         if (in) {
             if (F32) {
                 embed_reflect(R.md.symd, (float*)R.s, rep_sites(R), i, sd.r[0], sd.r[1], sd.r[2]);
