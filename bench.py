@@ -54,8 +54,11 @@ def parse():
     p.add_argument("--L", type=int, default=16384)
     p.add_argument("--nmetro", type=int, default=20, help="sweeps per step (one EMCS)")
     p.add_argument("--no-cpu-baseline", action="store_true")
-    p.add_argument("--workload", choices=["ising2d", "potts-batch", "secondary"], default="ising2d",
-                   help="ising2d: the headline line; potts-batch / secondary: those lines alone")
+    p.add_argument("--workload", choices=["ising2d", "potts-batch", "secondary", "profile"], default="ising2d",
+                   help="ising2d: the headline line; potts-batch / secondary: those lines alone; profile: a "
+                        "short run of one secondary case (--case) for ncu launch lists and captures")
+    p.add_argument("--case", choices=list(PROFILE_CASES), default="heisenberg",
+                   help="the case of --workload profile")
     p.add_argument("--no-secondary", action="store_true",
                    help="leave the secondary workloads out of the headline line")
     return p.parse_args()
@@ -654,6 +657,59 @@ def secondary(M, torch):
     return out
 
 
+# ---------------------------------------------------------------------------
+# short runs of the secondary workloads' kernels, for ncu (few launches, a few
+# hundred MB on the device at most)
+
+def _profile_heisenberg(M, steps):
+    """3D Heisenberg L=128, small-cap Metropolis sweeps and plane-reflection clusters."""
+    with M.makeCore(M.RegularHypercubic(128, 3), M.Config(seed=31, repid=0),
+                    M.Heisenberg(-1.0, "smallcap", -0.9697), 0.693) as c:
+        c.init()
+        c.metropolis(steps)
+        c.wolff(steps)
+        c.synchronize()
+
+
+def _profile_ea(M, steps):
+    """32 EA realisations on 3D L=32 as one batch, EMCS = 1 sweep + measurement."""
+    members = [(M.RegularRandomBond(32, 3, 0.5, seed=100 + r), M.Config(seed=500 + r, repid=r),
+                M.EdwardsAndersonIsing(-1.0), 0.9) for r in range(32)]
+    with M.Batch(members, graph_steps=4) as b:
+        b.init()
+        b.emcs(steps, ncluster=0, nmetro=1)
+
+
+def _profile_phi4(M, steps):
+    """64 phi^4 chains on 3D L=64 as one batch, EMCS = 1 cluster + 1 sweep."""
+    members = [(M.RegularHypercubic(64, 3), M.Config(seed=600 + r, repid=r),
+                M.Phi4(0.36 + 0.02 * r / 64, 1.1, 1.0, 1.0), 0.36 + 0.02 * r / 64) for r in range(64)]
+    with M.Batch(members, graph_steps=4) as b:
+        b.init()
+        b.emcs(steps, 1, 1)
+
+
+def _profile_potts(M, steps):
+    """The 256-replica q=3 Potts farm on its graph path, EMCS = 1 cluster + 1 sweep."""
+    with M.Batch(potts_farm(M), graph_steps=4) as b:
+        b.init()
+        b.emcs(steps, 1, 1)
+
+
+def _profile_wolff64(M, steps):
+    """Config 1 on the resident path: 2D Ising L=64, clusters alone, then EMCS."""
+    with M.makeCore(M.RegularHypercubic(64, 2), M.Config(seed=5, repid=0), M.Ising(-1.0), BETA_C) as c:
+        c.init()
+        c.emcs(steps, ncluster=1, nmetro=1, measure=False)
+        c.wolff(steps)
+        c.emcs(steps, 1, 1)
+        c.synchronize()
+
+
+PROFILE_CASES = {"heisenberg": _profile_heisenberg, "ea": _profile_ea, "phi4": _profile_phi4,
+                 "potts": _profile_potts, "wolff64": _profile_wolff64}
+
+
 def run_workload(args, ws, rank, local):
     import torch
 
@@ -662,6 +718,11 @@ def run_workload(args, ws, rank, local):
     if args.workload == "secondary":
         if rank == 0:
             print(json.dumps({"secondary": secondary(M, torch)}))
+        return 0
+    if args.workload == "profile":
+        if rank == 0:
+            PROFILE_CASES[args.case](M, args.steps)
+            print(json.dumps({"profile": args.case, "steps": args.steps}))
         return 0
     res = workload_potts_batch(M, torch)
     line = {"metric": METRIC, "value": res["batched"]["value"], "unit": UNIT, "n_gpus": 1,

@@ -55,7 +55,11 @@ enum {
     MQV_ERR_BAD_DESCRIPTOR = 3,   /* inconsistent lattice or model descriptor */
     MQV_ERR_CUDA = 4,             /* CUDA runtime error (message in mqv_last_error) */
     MQV_ERR_TIMEOUT = 5,          /* a bounded device wait gave up; the handle refuses compute
-                                     (MQV_ERR_STATE) until its state is set again */
+                                     (MQV_ERR_STATE) until its state is set again.  Outside
+                                     the injected test case treat it as fatal for the
+                                     context: a bulk copy still in flight when the block
+                                     left may land in reassigned shared memory, so destroy
+                                     the device's handles and reset its context */
     MQV_ERR_CHECKSUM = 6,         /* checkpoint / state checksum mismatch */
     MQV_ERR_NO_DEVICE = 7,        /* no usable CUDA device */
     MQV_ERR_OUT_OF_MEMORY = 8,    /* device allocation failed */

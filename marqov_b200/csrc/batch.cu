@@ -36,12 +36,13 @@ __device__ __forceinline__ void batch_site(const BatchRep& R, const Lat& lat, in
     else int8_site(R.md, lat, (int8_t*)R.s, i, R.key, sweep, R.replica, R.cuts, R.D, live, sub, tab, run0);
 }
 
-// One colour of a sweep over every member.  Each warp takes one block of
-// kAccSites consecutive positions of one member's colour-c sites (member
-// counts are padded to whole blocks, positions past a member's count are
-// idle lanes): on hypercubic members the block's sites fill kAccRuns
-// aligned 64-site runs, whose acceptance bytes the warp draws once
-// (accept_tab_fill); CSR members draw per site.
+// One colour of a sweep over every member.  Each CTA takes one block of
+// kAccSites consecutive positions of one member's colour-c sites, one
+// position per thread (member counts are padded to whole blocks, positions
+// past a member's count are idle threads): on hypercubic members the block's
+// sites fill kAccRuns aligned 64-site runs, whose acceptance bytes the first
+// warp draws once (accept_tab_fill) for the whole CTA; CSR members draw per
+// site.
 template <bool F32>
 __global__ void __launch_bounds__(kBatchMetroThreads)
     batch_metro(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
@@ -49,33 +50,28 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
                 const int32_t* __restrict__ ccount, int ncol, int64_t total, int colour,
                 const BatchCtr* __restrict__ ctr, int nmetro, int j)
 {
-    __shared__ uint4 tabs[kBatchMetroThreads / 32][kAccTab];
-    uint4* tab = tabs[threadIdx.x >> 5];
-    const int64_t g0 = ((int64_t)blockIdx.x * (kBatchMetroThreads / 32) + (threadIdx.x >> 5)) * kAccSites;
-    if (g0 >= total) return;  // whole warps
-    int r = block_rep[blockIdx.x];
-    while (g0 >= prefix[r + 1]) ++r;
+    static_assert(kBatchMetroThreads == kAccSites, "one position per thread");
+    __shared__ uint4 tab[kAccTab];
+    const int64_t g0 = (int64_t)blockIdx.x * kAccSites;
+    if (g0 >= total) return;  // whole CTAs
+    const int r = block_rep[blockIdx.x];
     const BatchRep& R = reps[r];
     const int64_t t0 = g0 - prefix[r];
     const int64_t cnt = ccount[(size_t)r * ncol + colour];
     const uint32_t sweep = R.sweep0 + ctr->e * (uint32_t)nmetro + (uint32_t)j;
-    const unsigned lane = threadIdx.x & 31u;
+    const int64_t t = t0 + threadIdx.x;
+    const bool live = t < cnt;
     if (R.lat_kind == MQV_LATTICE_HYPERCUBIC) {
         const uint32_t run0 = (uint32_t)(t0 / 32);  // sites [2 t0, 2 t0 + 2 kAccSites)
-        accept_tab_fill(tab, run0, R.key, sweep, R.replica);
-        for (int k = 0; k < kAccRuns; ++k) {
-            const int64_t t = t0 + k * 32 + lane;
-            const bool live = t < cnt;
-            batch_site<F32>(R, R.st, F32 ? parity_site_f(R.st, t, colour) : parity_site(R.st, t, colour), sweep,
-                            live, colour, tab, run0);
-        }
+        if (threadIdx.x < 32) accept_tab_fill(tab, run0, R.key, sweep, R.replica);
+        __syncthreads();
+        with_dim(R.st, [&](const auto& lt) {
+            batch_site<F32>(R, lt, F32 ? parity_site_f(lt, t, colour) : parity_site(lt, t, colour), sweep, live,
+                            colour, tab, run0);
+        });
     } else {
         const int32_t* ord = R.order + cbegin[(size_t)r * ncol + colour];
-        for (int k = 0; k < kAccRuns; ++k) {
-            const int64_t t = t0 + k * 32 + lane;
-            const bool live = t < cnt;
-            batch_site<F32>(R, R.csr, live ? (int64_t)ord[t] : 0, sweep, live, 0, nullptr, 0u);
-        }
+        batch_site<F32>(R, R.csr, live ? (int64_t)ord[t] : 0, sweep, live, 0, nullptr, 0u);
     }
 }
 
@@ -122,12 +118,12 @@ __global__ void batch_measure(const BatchRep* __restrict__ reps, const BatchCtr*
     long long* a = acc + ((size_t)slot * nrep + r) * kAccStride;
     if (F32) {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            measure_f32_part(R.md, R.st, (const float*)R.s, (double*)a, part, nparts);
+            with_dim(R.st, [&](const auto& lt) { measure_f32_part(R.md, lt, (const float*)R.s, (double*)a, part, nparts); });
         else
             measure_f32_part(R.md, R.csr, (const float*)R.s, (double*)a, part, nparts);
     } else {
         if (R.lat_kind == MQV_LATTICE_HYPERCUBIC)
-            measure_int8_part(R.md, R.st, (const int8_t*)R.s, a, part, nparts);
+            with_dim(R.st, [&](const auto& lt) { measure_int8_part(R.md, lt, (const int8_t*)R.s, a, part, nparts); });
         else
             measure_int8_part(R.md, R.csr, (const int8_t*)R.s, a, part, nparts);
     }

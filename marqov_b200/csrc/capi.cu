@@ -1613,8 +1613,8 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     }
     // per-colour work: colour c concatenates every graph member's colour-c
     // sites (resident members contribute none), each member's count padded
-    // to whole warp blocks of kAccSites, so that a warp's block lies in one
-    // member (batch_metro)
+    // to whole blocks of kAccSites, so that a CTA's block lies in one member
+    // (batch_metro)
     int ncol = 0;
     for (Sim* s : b->sims) ncol = std::max(ncol, (int)s->colour_ptr.size() - 1);
     std::vector<int64_t> prefix((size_t)ncol * (n + 1), 0);
@@ -1622,7 +1622,7 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
     b->block_off.assign((size_t)ncol, 0);
     b->blocks.assign((size_t)ncol, 0);
     b->total.assign((size_t)ncol, 0);
-    const int64_t per_cta = (int64_t)kBatchMetroThreads / 32 * kAccSites;  // padded positions per CTA
+    const int64_t per_cta = kAccSites;  // padded positions per CTA: one block
     for (int c = 0; c < ncol; ++c) {
         int64_t* pf = prefix.data() + (size_t)c * (n + 1);
         for (int r = 0; r < n; ++r) {
@@ -1663,11 +1663,13 @@ MQV_API mqv_status mqv_batch_create(const mqv_sim_spec* specs, int32_t n, mqv_ba
         MQV_CK(upload_sync(b->stream, *dst, src, bytes));
         return MQV_OK;
     };
-    // measurement CTAs: about 4096 sites each, at least one per member
+    // measurement CTAs: about 1024 sites each (four per thread: enough CTAs
+    // to fill the SMs on farms of small members, few enough that the CTAs'
+    // atomic adds and reductions stay a small part), at least one per member
     std::vector<int32_t> mprefix((size_t)n + 1, 0), mrep;
     for (int r = 0; r < n; ++r) {
         const int64_t parts =
-            b->resident[(size_t)r] ? 0 : std::max<int64_t>(1, (b->sims[(size_t)r]->n + 4095) / 4096);
+            b->resident[(size_t)r] ? 0 : std::max<int64_t>(1, (b->sims[(size_t)r]->n + 1023) / 1024);
         if (mprefix[(size_t)r] + parts >= (int64_t)1 << 31) return bail(fail(MQV_ERR_INVALID_ARG, "batch too large"));
         mprefix[(size_t)r + 1] = mprefix[(size_t)r] + (int32_t)parts;
         for (int64_t k = 0; k < parts; ++k) mrep.push_back(r);

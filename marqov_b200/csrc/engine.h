@@ -103,6 +103,68 @@ struct StencilDev {
     }
 };
 
+// The same stencil with its dimension, whether its side is a power of two
+// and whether its state is stored in split rows fixed at compile time, for
+// the per-site kernels: neighbour loops unroll (degree 2 D), each coordinate
+// is computed once per site and shared by its two neighbours, the last
+// coordinate needs no remainder, and index arithmetic stays in 32 bits
+// (n < 2^31).  The neighbour order and the sites are those of StencilDev.
+template <int D, bool P2, bool SPLIT = false>
+struct StencilDim : StencilDev {
+    MQV_HD explicit StencilDim(const StencilDev& s) : StencilDev(s) {}
+    MQV_HD int degree(int64_t) const { return 2 * D; }
+    MQV_HD int coord(int64_t i, int j) const
+    {
+        uint32_t u = (uint32_t)i;
+        if (P2) return j == D - 1 ? (int)(u >> (lg * j)) : (int)((u >> (lg * j)) & (uint32_t)(len - 1));
+        if (j >= 1) u = divlen(u);
+        if (j >= 2) u = divlen(u);
+        if (j == D - 1) return (int)u;  // u < len already
+        return (int)(u - divlen(u) * (uint32_t)len);
+    }
+    MQV_HD int64_t addr(int64_t i) const
+    {
+        if (!SPLIT) return i;
+        return split_addr(coord(i, 1), coord(i, 0), len);
+    }
+    MQV_HD int64_t nbr(int64_t i, int slot) const
+    {
+        const int j = slot >> 1;
+        const uint32_t p = (uint32_t)pow_of(j), u = (uint32_t)i, w = (uint32_t)(len - 1) * p;
+        const int x = coord(i, j);
+        if ((slot & 1) == 0) return (int64_t)(x == len - 1 ? u - w : u + p);
+        return (int64_t)(x == 0 ? u + w : u - p);
+    }
+    MQV_HD int bond(int64_t i, int slot) const
+    {
+        if (!fb) return 1;
+        const int64_t j = (slot & 1) ? nbr(i, slot) : i;
+        return fb[(int64_t)(slot >> 1) * n + j];
+    }
+};
+
+// Call f(lat) with the stencil's dimension (2 or 3), power-of-two side and
+// split-row storage fixed where possible (StencilDev otherwise).
+template <class F>
+__device__ __forceinline__ void with_dim(const StencilDev& st, F&& f)
+{
+    const bool p2 = st.lg >= 0;
+    if (st.dim == 2) {
+        if (st.split) {
+            if (p2) f(StencilDim<2, true, true>(st));
+            else f(StencilDim<2, false, true>(st));
+        } else {
+            if (p2) f(StencilDim<2, true>(st));
+            else f(StencilDim<2, false>(st));
+        }
+    } else if (st.dim == 3 && !st.split) {
+        if (p2) f(StencilDim<3, true>(st));
+        else f(StencilDim<3, false>(st));
+    } else {
+        f(st);
+    }
+}
+
 struct CSRDev {
     int64_t n;
     const int32_t* rp;

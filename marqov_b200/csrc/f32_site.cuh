@@ -140,11 +140,12 @@ __device__ __forceinline__ void f32_site(const ModelDev& m, const Lat& lat, floa
     }
 }
 
-__device__ __forceinline__ int64_t parity_site_f(const StencilDev& st, int64_t t, int colour)
+template <class ST>
+__device__ __forceinline__ int64_t parity_site_f(const ST& st, int64_t t, int colour)
 {
     const int64_t i0 = 2 * t;
     int par = 0;
-    for (int j = 1; j < st.dim; ++j) par += st.coord(i0, j);
+    for (int j = 1; j < st.degree(0) / 2; ++j) par += st.coord(i0, j);
     return i0 + (((par & 1) != colour) ? 1 : 0);
 }
 

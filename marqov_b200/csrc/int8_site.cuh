@@ -77,11 +77,12 @@ __device__ __forceinline__ void int8_site(const ModelDev& m, const Lat& lat, SP 
 // Site of colour `colour` in pair t of a parity-coloured hypercubic lattice
 // with even side: sites 2t and 2t+1 differ only in x, so they have opposite
 // colours.
-__device__ __forceinline__ int64_t parity_site(const StencilDev& st, int64_t t, int colour)
+template <class ST>
+__device__ __forceinline__ int64_t parity_site(const ST& st, int64_t t, int colour)
 {
     const int64_t i0 = 2 * t;
     int par = 0;
-    for (int j = 1; j < st.dim; ++j) par += st.coord(i0, j);
+    for (int j = 1; j < st.degree(0) / 2; ++j) par += st.coord(i0, j);
     return i0 + (((par & 1) != colour) ? 1 : 0);
 }
 
@@ -115,11 +116,11 @@ __device__ __forceinline__ int int8_bond_sum(const ModelDev& m, const Lat& lat, 
     }
     return loc;
 }
-template <class SP>
-__device__ __forceinline__ int int8_bond_sum_stencil(const StencilDev& st, SP s, int64_t i, int si, bool potts)
+template <class ST, class SP>
+__device__ __forceinline__ int int8_bond_sum_stencil(const ST& st, SP s, int64_t i, int si, bool potts)
 {
     int loc = 0;
-    for (int d = 0; d < st.dim; ++d) {
+    for (int d = 0; d < st.degree(i) / 2; ++d) {
         const int v = s[st.addr(st.nbr(i, 2 * d))];
         loc += potts ? (v == si) : st.bond(i, 2 * d) * v;
     }
@@ -128,12 +129,13 @@ __device__ __forceinline__ int int8_bond_sum_stencil(const StencilDev& st, SP s,
 __device__ __forceinline__ int int8_bond_sum(const ModelDev&, const StencilDev& st, const int8_t* __restrict__ s,
                                              int64_t i, int si, bool potts)
 {
-    int loc = 0;
-    for (int d = 0; d < st.dim; ++d) {
-        const int v = s[st.addr(st.nbr(i, 2 * d))];
-        loc += potts ? (v == si) : st.bond(i, 2 * d) * v;
-    }
-    return 2 * (potts ? loc : loc * si);
+    return int8_bond_sum_stencil(st, s, i, si, potts);
+}
+template <int D, bool P2, bool SPLIT>
+__device__ __forceinline__ int int8_bond_sum(const ModelDev&, const StencilDim<D, P2, SPLIT>& st, const int8_t* __restrict__ s,
+                                             int64_t i, int si, bool potts)
+{
+    return int8_bond_sum_stencil(st, s, i, si, potts);
 }
 
 // Part `part` of `nparts` of the accumulation (a grid-stride share per CTA;

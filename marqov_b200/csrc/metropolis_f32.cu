@@ -14,26 +14,28 @@ namespace mqv {
 
 unsigned long long accept_cut(int pref, double dE, double beta);
 
-// One colour of a stencil sweep.  Warps take aligned blocks of kAccSites
-// sites of the colour (kAccRuns runs of 64 lattice sites): the warp draws the
-// block's acceptance bytes once (accept_tab_fill), then its lanes update
-// kAccRuns sites each, 32 neighbouring sites per step.
-constexpr int kMetroThreads = 256;
+// One colour of a stencil sweep.  A CTA takes one aligned block of kAccSites
+// sites of the colour (kAccRuns runs of 64 lattice sites), one site per
+// thread: its first warp draws the block's acceptance bytes (accept_tab_fill,
+// one Philox block per lane), a CTA barrier publishes them, and every thread
+// updates its site.  One site per thread keeps enough warps in flight to
+// cover the FP64 latency of the proposal and the acceptance.
+constexpr int kMetroThreads = kAccSites;
 __global__ void __launch_bounds__(kMetroThreads) metro_f32_stencil(ModelDev m, StencilDev st, float* __restrict__ s,
                                                                    int colour, Key key, uint32_t sweep, uint32_t replica)
 {
-    __shared__ uint4 tabs[kMetroThreads / 32][kAccTab];
-    uint4* tab = tabs[threadIdx.x >> 5];
+    __shared__ uint4 tab[kAccTab];
     const int64_t half = st.n / 2, nblk = (half + kAccSites - 1) / kAccSites;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += nw) {
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
         const uint32_t run0 = (uint32_t)(b * kAccRuns);
-        accept_tab_fill(tab, run0, key, sweep, replica);
-        for (int j = 0; j < kAccRuns; ++j) {
-            const int64_t t = b * kAccSites + j * 32 + (threadIdx.x & 31u);
-            const bool live = t < half;
-            f32_site(m, st, s, live ? parity_site_f(st, t, colour) : 0, key, sweep, replica, live, colour, tab, run0);
-        }
+        if (threadIdx.x < 32) accept_tab_fill(tab, run0, key, sweep, replica);
+        __syncthreads();
+        const int64_t t = b * kAccSites + threadIdx.x;
+        const bool live = t < half;
+        with_dim(st, [&](const auto& lt) {
+            f32_site(m, lt, s, live ? parity_site_f(lt, t, colour) : 0, key, sweep, replica, live, colour, tab, run0);
+        });
+        __syncthreads();  // every thread has read the table before the next block's draw
     }
 }
 
@@ -52,6 +54,11 @@ template <class Lat>
 __global__ void measure_f32(ModelDev m, Lat lat, const float* __restrict__ s, double* __restrict__ acc)
 {
     measure_f32_part(m, lat, s, acc, blockIdx.x, gridDim.x);
+}
+template <>
+__global__ void measure_f32(ModelDev m, StencilDev st, const float* __restrict__ s, double* __restrict__ acc)
+{
+    with_dim(st, [&](const auto& lt) { measure_f32_part(m, lt, s, acc, blockIdx.x, gridDim.x); });
 }
 
 __global__ void finalize_f32(ModelDev m, int64_t n, const double* __restrict__ acc, int nslots, double* __restrict__ out)
@@ -134,8 +141,8 @@ cudaError_t launch_metropolis_f32(Sim* s, int slot)
     const Key key = make_key(s->seed);
     float* st = (float*)s->state[s->cur];
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
-        // one warp per block of kAccSites sites of a colour, up to 16 CTAs per SM
-        const int g = grid_for_f((s->n / 2 + kAccSites - 1) / kAccSites * 32, kMetroThreads);
+        // one CTA per block of kAccSites sites of a colour
+        const int g = grid_for_f((s->n / 2 + kAccSites - 1) / kAccSites * kMetroThreads, kMetroThreads);
         for (int c = 0; c < 2; ++c) {
             metro_f32_stencil<<<g, kMetroThreads, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep,
                                                                   s->replica);

@@ -18,29 +18,30 @@
 
 namespace mqv {
 
-// One colour of a stencil sweep.  Warps take aligned blocks of kAccSites
-// sites of the colour (kAccRuns runs of 64 lattice sites): the warp draws the
-// block's acceptance bytes once (accept_tab_fill), then its lanes update
-// kAccRuns sites each, 32 neighbouring sites per step.
-constexpr int kMetroThreads = 256;
+// One colour of a stencil sweep.  A CTA takes one aligned block of kAccSites
+// sites of the colour (kAccRuns runs of 64 lattice sites), one site per
+// thread: its first warp draws the block's acceptance bytes (accept_tab_fill,
+// one Philox block per lane), a CTA barrier publishes them, and every thread
+// updates its site.
+constexpr int kMetroThreads = kAccSites;
 __global__ void __launch_bounds__(kMetroThreads) metro_int8_stencil(ModelDev m, StencilDev st, int8_t* __restrict__ s,
                                                                     int colour, Key key, uint32_t sweep,
                                                                     uint32_t replica,
                                                                     const unsigned long long* __restrict__ cuts, int D)
 {
-    __shared__ uint4 tabs[kMetroThreads / 32][kAccTab];
-    uint4* tab = tabs[threadIdx.x >> 5];
+    __shared__ uint4 tab[kAccTab];
     const int64_t half = st.n / 2, nblk = (half + kAccSites - 1) / kAccSites;
-    const int64_t nw = ((int64_t)gridDim.x * blockDim.x) >> 5;
-    for (int64_t b = ((int64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; b < nblk; b += nw) {
+    for (int64_t b = blockIdx.x; b < nblk; b += gridDim.x) {
         const uint32_t run0 = (uint32_t)(b * kAccRuns);
-        accept_tab_fill(tab, run0, key, sweep, replica);
-        for (int j = 0; j < kAccRuns; ++j) {
-            const int64_t t = b * kAccSites + j * 32 + (threadIdx.x & 31u);
-            const bool live = t < half;
-            int8_site(m, st, s, live ? parity_site(st, t, colour) : 0, key, sweep, replica, cuts, D, live, colour, tab,
+        if (threadIdx.x < 32) accept_tab_fill(tab, run0, key, sweep, replica);
+        __syncthreads();
+        const int64_t t = b * kAccSites + threadIdx.x;
+        const bool live = t < half;
+        with_dim(st, [&](const auto& lt) {
+            int8_site(m, lt, s, live ? parity_site(lt, t, colour) : 0, key, sweep, replica, cuts, D, live, colour, tab,
                       run0);
-        }
+        });
+        __syncthreads();  // every thread has read the table before the next block's draw
     }
 }
 
@@ -115,6 +116,11 @@ template <class Lat>
 __global__ void measure_int8(ModelDev m, Lat lat, const int8_t* __restrict__ s, long long* __restrict__ acc)
 {
     measure_int8_part(m, lat, s, acc, blockIdx.x, gridDim.x);
+}
+template <>
+__global__ void measure_int8(ModelDev m, StencilDev st, const int8_t* __restrict__ s, long long* __restrict__ acc)
+{
+    with_dim(st, [&](const auto& lt) { measure_int8_part(m, lt, s, acc, blockIdx.x, gridDim.x); });
 }
 
 __global__ void finalize_int8(ModelDev m, int64_t n, const long long* __restrict__ acc, int nslots,
@@ -207,8 +213,8 @@ cudaError_t launch_metropolis_int8(Sim* s, int slot)
     err = ensure_cuts(s);
     if (err != cudaSuccess) return err;
     if (s->lat_kind == MQV_LATTICE_HYPERCUBIC) {
-        // one warp per block of kAccSites sites of a colour, up to 16 CTAs per SM
-        const int g = grid_for((s->n / 2 + kAccSites - 1) / kAccSites * 32, kMetroThreads);
+        // one CTA per block of kAccSites sites of a colour
+        const int g = grid_for((s->n / 2 + kAccSites - 1) / kAccSites * kMetroThreads, kMetroThreads);
         for (int c = 0; c < 2; ++c) {
             metro_int8_stencil<<<g, kMetroThreads, 0, s->stream>>>(s->md, s->sten, st, c, key, (uint32_t)s->sweep,
                                                                    s->replica, s->d_cuts, s->max_degree);

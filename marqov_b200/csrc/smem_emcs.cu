@@ -361,16 +361,12 @@ __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
                 continue;
             }
             // candidates: sites in the seed's old state, each its own root
-            for (int64_t wd = tid; wd < words; wd += kResThreads) {
-                uint32_t bits = 0;
-                for (int b = 0; b < 32; ++b) {
-                    const int64_t i = wd * 32 + b;
-                    if (i < n && s[i] == val) {
-                        bits |= 1u << b;
-                        par[i] = (unsigned short)i;
-                    }
-                }
-                cand[wd] = bits;
+            for (int64_t wd = warp; wd < words; wd += kResWarps) {
+                const int64_t i = wd * 32 + lane;
+                const bool c = i < n && s[i] == val;
+                const uint32_t bits = __ballot_sync(0xffffffffu, c);
+                if (c) par[i] = (unsigned short)i;
+                if (lane == 0) cand[wd] = bits;
             }
             __syncthreads();
             for (int64_t i = tid; i < n; i += kResThreads) {

@@ -12,8 +12,9 @@
 //   ccl_seed      one thread per member: seed site, old/new state or the
 //                 reflection vector (the same substream draws as the BFS);
 //   ccl_local     per CTA of 256 consecutive sites: candidates (int8: state
-//                 equal to the seed's old state; float: every site) get
-//                 labels, and activated bonds with both ends in the CTA's
+//                 equal to the seed's old state; float: every site, whose
+//                 projections on the reflection vector go to shared memory)
+//                 get labels, and activated bonds with both ends in the CTA's
 //                 sites are united in shared memory first; each candidate's
 //                 label becomes its local root, non-candidates get -1;
 //   ccl_hook      the other activated bonds between candidates are united;
@@ -195,6 +196,98 @@ __device__ __forceinline__ bool ccl_same_block(int64_t g, int64_t g2)
     return g / kBatchMetroThreads == g2 / kBatchMetroThreads;
 }
 
+// Lattice coordinates of position `pos` of a tiled member (BatchRep::tile 2:
+// 16 x 16 tiles, 3: 8 x 8 x 4 tiles, tile t = pos >> 8, offset o = pos & 255),
+// by shifts where the side is a power of two.
+struct TileSite {
+    uint32_t x, y, z;
+};
+__device__ __forceinline__ TileSite ccl_tile_coords(const BatchRep& R, uint32_t pos)
+{
+    const uint32_t L = (uint32_t)R.st.len, t = pos >> 8, o = pos & 255u;
+    const int lg = R.st.lg;
+    TileSite c;
+    if (R.tile == 2) {
+        uint32_t ty, tx;
+        if (lg >= 0) {
+            ty = t >> (lg - 4);
+            tx = t & ((L >> 4) - 1u);
+        } else {
+            ty = t / (L >> 4);
+            tx = t - ty * (L >> 4);
+        }
+        c.x = (tx << 4) + (o & 15u);
+        c.y = (ty << 4) + (o >> 4);
+        c.z = 0;
+    } else {
+        uint32_t tz, ty, tx;
+        if (lg >= 0) {
+            tx = t & ((L >> 3) - 1u);
+            ty = (t >> (lg - 3)) & ((L >> 3) - 1u);
+            tz = t >> (2 * (lg - 3));
+        } else {
+            const uint32_t tyz = t / (L >> 3);
+            tx = t - tyz * (L >> 3);
+            tz = tyz / (L >> 3);
+            ty = tyz - tz * (L >> 3);
+        }
+        c.x = (tx << 3) + (o & 7u);
+        c.y = (ty << 3) + ((o >> 3) & 7u);
+        c.z = (tz << 2) + (o >> 6);
+    }
+    return c;
+}
+__device__ __forceinline__ int64_t ccl_tile_index(const BatchRep& R, const TileSite& c)
+{
+    const int64_t L = R.st.len;
+    return (R.tile == 2 ? 0 : (int64_t)c.z * L * L) + (int64_t)c.y * L + c.x;
+}
+// The forward neighbour in dimension d (+x, +y, +z, periodic) of a tiled
+// member's site: its coordinates, whether it lies in the same tile (the same
+// CTA block), and then its offset in the tile.
+__device__ __forceinline__ TileSite ccl_tile_fwd(const BatchRep& R, TileSite c, int d, bool& same, int& k)
+{
+    const uint32_t L = (uint32_t)R.st.len;
+    if (R.tile == 2) {
+        if (d == 0) {
+            const uint32_t xn = c.x + 1u == L ? 0u : c.x + 1u;
+            same = (xn >> 4) == (c.x >> 4);
+            c.x = xn;
+        } else {
+            const uint32_t yn = c.y + 1u == L ? 0u : c.y + 1u;
+            same = (yn >> 4) == (c.y >> 4);
+            c.y = yn;
+        }
+        k = (int)(((c.y & 15u) << 4) | (c.x & 15u));
+    } else {
+        if (d == 0) {
+            const uint32_t xn = c.x + 1u == L ? 0u : c.x + 1u;
+            same = (xn >> 3) == (c.x >> 3);
+            c.x = xn;
+        } else if (d == 1) {
+            const uint32_t yn = c.y + 1u == L ? 0u : c.y + 1u;
+            same = (yn >> 3) == (c.y >> 3);
+            c.y = yn;
+        } else {
+            const uint32_t zn = c.z + 1u == L ? 0u : c.z + 1u;
+            same = (zn >> 2) == (c.z >> 2);
+            c.z = zn;
+        }
+        k = (int)(((c.z & 3u) << 6) | ((c.y & 7u) << 3) | (c.x & 7u));
+    }
+    return c;
+}
+
+// activation of the bond (lo, hi) of a float member given both ends'
+// projections on the reflection vector (ccl_active's rule and order)
+__device__ __forceinline__ bool ccl_active_f32(const BatchRep& R, uint32_t serial, int64_t lo, int64_t hi, double alo,
+                                               double ahi)
+{
+    const double cpl = embed_cpl(R.md.J, alo, ahi);
+    return cpl > 0 && !update_accepted(2, cpl, R.md.beta,
+                                       lo64(philox((uint32_t)lo, serial, (uint32_t)hi, tag(kWolffBond, R.replica), R.key)));
+}
+
 template <bool F32>
 __global__ void __launch_bounds__(kBatchMetroThreads)
     ccl_local(const BatchRep* __restrict__ reps, const int64_t* __restrict__ prefix,
@@ -202,35 +295,68 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
               const BatchCtr* __restrict__ ctr, int ncluster, int c)
 {
     __shared__ int slab[kBatchMetroThreads];
+    __shared__ double sproj[F32 ? kBatchMetroThreads : 1];
     const int64_t base = (int64_t)blockIdx.x * kBatchMetroThreads;
     const int64_t g = base + threadIdx.x;
     int r = 0;
     int64_t i = 0;  // this thread's site (position g in the labelling order)
     bool cand = false;
+    TileSite tc{0, 0, 0};
+    double ai = 0.0;  // float: the site's projection on the reflection vector
+    bool tiled = false;  // the CTA block is one tile of the member
     if (g < total) {
         r = ccl_member(g, prefix, block_rep, i);
         const BatchRep& R = reps[r];
-        i = ccl_site(R, i);
+        tiled = R.tile && (prefix[r] & 255) == 0;
+        if (tiled) {
+            tc = ccl_tile_coords(R, (uint32_t)i);
+            i = ccl_tile_index(R, tc);
+        } else {
+            i = ccl_site(R, i);
+        }
         cand = true;
-        if (!F32) {
+        if (F32) {
+            const CclSeed& sd = seeds[r];
+            ai = embed_proj(R.md.symd, (const float*)R.s, rep_sites(R), i, sd.r[0], sd.r[1], sd.r[2]);
+        } else {
             const int64_t a = R.lat_kind == MQV_LATTICE_HYPERCUBIC ? R.st.addr(i) : i;
             cand = ((const int8_t*)R.s)[a] == seeds[r].val;
         }
     }
     slab[threadIdx.x] = cand ? (int)threadIdx.x : -1;
+    if (F32) sproj[threadIdx.x] = ai;
     __syncthreads();
     if (cand) {
         const BatchRep& R = reps[r];
         const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
         const CclSeed sd = seeds[r];
-        const int64_t off = prefix[r];
         volatile int* vl = slab;
-        ccl_forward_bonds(R, i, [&](int64_t j) {
-            const int64_t gj = off + ccl_pos(R, j);
-            if (!ccl_same_block(g, gj)) return;
-            const int k = (int)(gj - base);
-            if (vl[k] >= 0 && ccl_active<F32>(R, sd, serial, i, j)) ccl_lunite(vl, (int)threadIdx.x, k);
-        });
+        if (tiled) {
+            // neighbours in the same tile, their offsets from the coordinates
+            for (int d = 0; d < R.st.dim; ++d) {
+                bool same;
+                int k;
+                const TileSite nc = ccl_tile_fwd(R, tc, d, same, k);
+                if (!same || vl[k] < 0) continue;
+                const int64_t j = ccl_tile_index(R, nc);
+                bool act;
+                if (F32) {
+                    const double aj = sproj[k];
+                    act = i < j ? ccl_active_f32(R, serial, i, j, ai, aj) : ccl_active_f32(R, serial, j, i, aj, ai);
+                } else {
+                    act = ccl_active<false>(R, sd, serial, i, j);
+                }
+                if (act) ccl_lunite(vl, (int)threadIdx.x, k);
+            }
+        } else {
+            const int64_t off = prefix[r];
+            ccl_forward_bonds(R, i, [&](int64_t j) {
+                const int64_t gj = off + ccl_pos(R, j);
+                if (!ccl_same_block(g, gj)) return;
+                const int k = (int)(gj - base);
+                if (vl[k] >= 0 && ccl_active<F32>(R, sd, serial, i, j)) ccl_lunite(vl, (int)threadIdx.x, k);
+            });
+        }
     }
     __syncthreads();
     if (cand) ccl_lfind(slab, (int)threadIdx.x);  // paths halved side by side first
@@ -241,7 +367,9 @@ __global__ void __launch_bounds__(kBatchMetroThreads)
             // read-only walk to the local root (same member: bonds join only its sites)
             int x = (int)threadIdx.x, px;
             while ((px = ((volatile int*)slab)[x]) != x) x = px;
-            lab = (int)ccl_site(reps[r], base + x - prefix[r]);
+            const BatchRep& R = reps[r];
+            const int64_t rpos = base + x - prefix[r];
+            lab = (int)(tiled ? ccl_tile_index(R, ccl_tile_coords(R, (uint32_t)rpos)) : ccl_site(R, rpos));
         }
         reps[r].queue[i] = lab;
     }
@@ -257,8 +385,42 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
     int64_t i;
     const int r = ccl_member(g, prefix, block_rep, i);
     const BatchRep& R = reps[r];
-    i = ccl_site(R, i);
     int* lab = R.queue;
+    if (R.tile && (prefix[r] & 255) == 0) {
+        // CTA blocks are the member's tiles: only bonds that leave the tile
+        // remain, decided from the coordinates
+        const TileSite tc = ccl_tile_coords(R, (uint32_t)i);
+        i = ccl_tile_index(R, tc);
+        if (__ldcg(lab + i) < 0) return;
+        const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
+        double ai = 0.0;
+        bool have_ai = false;
+        for (int d = 0; d < R.st.dim; ++d) {
+            bool same;
+            int k;
+            const TileSite nc = ccl_tile_fwd(R, tc, d, same, k);
+            if (same) continue;
+            const int64_t j = ccl_tile_index(R, nc);
+            if (__ldcg(lab + j) < 0) continue;
+            bool act;
+            if (F32) {
+                const CclSeed& sd = seeds[r];
+                const float* s = (const float*)R.s;
+                const int64_t n = rep_sites(R);
+                if (!have_ai) {
+                    ai = embed_proj(R.md.symd, s, n, i, sd.r[0], sd.r[1], sd.r[2]);
+                    have_ai = true;
+                }
+                const double aj = embed_proj(R.md.symd, s, n, j, sd.r[0], sd.r[1], sd.r[2]);
+                act = i < j ? ccl_active_f32(R, serial, i, j, ai, aj) : ccl_active_f32(R, serial, j, i, aj, ai);
+            } else {
+                act = ccl_active<false>(R, seeds[r], serial, i, j);
+            }
+            if (act) ccl_unite(lab, (int)i, (int)j);
+        }
+        return;
+    }
+    i = ccl_site(R, i);
     if (__ldcg(lab + i) < 0) return;
     const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
     const CclSeed sd = seeds[r];
