@@ -120,6 +120,169 @@ __device__ __forceinline__ uint32_t res_row_step(const StencilDev& st, uint32_t 
     return res_row_of(st, (uint32_t)st.nbr((int64_t)r * st.len, 2 * d + (dir < 0 ? 1 : 0)));
 }
 
+// One warp closes the flood of a 2D lattice of at most 64 rows of at most 64
+// sites on its own (two rows per lane: rows 2 lane and 2 lane + 1), so the
+// fill needs no CTA barrier and no shared-memory round trip until it is
+// closed.  Planes as resident_cluster_bits: F (in: the seed, out: the
+// component), Bx the +x bonds, By the +y bonds (row r to row r + 1, periodic).
+// Each pass: along y by prefix scans over the lanes, upwards and downwards
+// (a lane block passes the flood from its lower to its upper row through its
+// inner bond), the periodic bond of row R - 1 to row 0, then along each row's
+// x-line by prefix scans on the bits (the periodic bond carried explicitly);
+// until a pass adds no site.
+template <int WR>  // words per row (1 or 2), fixed so that both words' scans run side by side
+__device__ void resident_fill_warp2(uint32_t* F, const uint32_t* Bx, const uint32_t* By, int R, int len)
+{
+    const unsigned lane = threadIdx.x & 31u;
+    const int lb = (len - 1) & 31;
+    constexpr int lw = WR - 1;
+    const int ra = (R - 1) >> 1, ka = (R - 1) & 1;  // lane and slot of the last row
+    uint32_t G[2][2], bx[2][2], up[2][2], wrap[2], wb[2];
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int r = 2 * (int)lane + k;
+        const bool live = r < R;
+#pragma unroll
+        for (int q = 0; q < 2; ++q) {
+            const bool w = live && q < WR;
+            G[k][q] = w ? F[r * WR + q] : 0u;
+            bx[k][q] = w ? Bx[r * WR + q] : 0u;
+            // the +y bond of the row, except the periodic one of the last row
+            up[k][q] = (w && r < R - 1) ? By[r * WR + q] : 0u;
+        }
+        wrap[k] = 0u;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (q == lw) {  // constant indices only: the arrays stay in registers
+                wrap[k] = (bx[k][q] >> lb) & 1u;
+                bx[k][q] &= ~(1u << lb);
+            }
+    }
+    // the periodic y bond (row R - 1 to row 0), on every lane
+#pragma unroll
+    for (int q = 0; q < 2; ++q) {
+        const uint32_t own = (2 * (int)lane + ka == R - 1 && q < WR) ? By[(R - 1) * WR + q] : 0u;
+        wb[q] = __shfl_sync(0xffffffffu, own, ra);
+    }
+    // The bonds do not change during the fill: the bond from the lane below
+    // into each lane's row 0 (pin) and the propagate masks of every step of
+    // the lane scans (upwards: into row 0, on through the lane's inner bond;
+    // downwards: into row 1 through b1n, on through the inner bond) are
+    // computed once, so that a scan step is one shuffle and one logic op.
+    uint32_t pin[2], Pu[2][5], Pd[2][5];
+#pragma unroll
+    for (int q = 0; q < WR; ++q) {
+        pin[q] = __shfl_up_sync(0xffffffffu, up[1][q], 1);
+        if (lane == 0) pin[q] = 0u;
+        uint32_t P = pin[q] & up[0][q];
+#pragma unroll
+        for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
+            Pu[q][s] = P;
+            const uint32_t Po = __shfl_up_sync(0xffffffffu, P, o);
+            if ((int)lane >= o) P &= Po;
+        }
+        P = up[1][q] & up[0][q];
+#pragma unroll
+        for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
+            Pd[q][s] = P;
+            const uint32_t Po = __shfl_down_sync(0xffffffffu, P, o);
+            if ((int)lane + o < 32) P &= Po;
+        }
+    }
+    for (;;) {
+        uint32_t moved = 0u;
+#pragma unroll
+        for (int q = 0; q < WR; ++q) {
+            const uint32_t g0 = G[0][q], g1 = G[1][q], b01 = up[0][q], b1n = up[1][q];
+            // within the lane first
+            uint32_t x0 = g0 | (g1 & b01), x1 = g1 | (g0 & b01);
+            // upwards: the flood at each lane block's top row
+            uint32_t X = x1;
+#pragma unroll
+            for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
+                const uint32_t Xo = __shfl_up_sync(0xffffffffu, X, o);
+                if ((int)lane >= o) X |= Pu[q][s] & Xo;
+            }
+            uint32_t below = __shfl_up_sync(0xffffffffu, X, 1);
+            if (lane == 0) below = 0u;
+            x0 |= below & pin[q];
+            x1 |= x0 & b01;
+            // downwards: the flood at each lane block's bottom row
+            X = x0;
+#pragma unroll
+            for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
+                const uint32_t Xo = __shfl_down_sync(0xffffffffu, X, o);
+                if ((int)lane + o < 32) X |= Pd[q][s] & Xo;
+            }
+            uint32_t above = __shfl_down_sync(0xffffffffu, X, 1);
+            if (lane == 31) above = 0u;
+            x1 |= above & b1n;
+            x0 |= x1 & b01;
+            // the periodic bond between row R - 1 and row 0
+            const uint32_t last = __shfl_sync(0xffffffffu, ka ? x1 : x0, ra), first = __shfl_sync(0xffffffffu, x0, 0);
+            if (lane == 0) x0 |= last & wb[q];
+            if ((int)lane == ra) {
+                if (ka) x1 |= first & wb[q];
+                else x0 |= first & wb[q];
+            }
+            moved |= (x0 ^ g0) | (x1 ^ g1);
+            G[0][q] = x0;
+            G[1][q] = x1;
+        }
+        // along each row's x-line (the periodic bond, bit lb of the last
+        // word, carried explicitly)
+#pragma unroll
+        for (int k = 0; k < 2; ++k) {
+            uint32_t glast = 0u;
+#pragma unroll
+            for (int q = 0; q < 2; ++q)
+                if (q == lw) glast = G[k][q];
+            uint32_t cin = (glast >> lb) & wrap[k];  // site len-1 -> site 0
+#pragma unroll
+            for (int q = 0; q < WR; ++q) {
+                uint32_t X = G[k][q] | cin, p = bx[k][q] << 1;
+                X |= (X << 1) & p;
+                p &= p << 1;
+                X |= (X << 2) & p;
+                p &= p << 2;
+                X |= (X << 4) & p;
+                p &= p << 4;
+                X |= (X << 8) & p;
+                p &= p << 8;
+                X |= (X << 16) & p;
+                moved |= X ^ G[k][q];
+                G[k][q] = X;
+                cin = (X >> 31) & (bx[k][q] >> 31);
+            }
+            cin = G[k][0] & 1u & wrap[k];  // site 0 -> site len-1
+#pragma unroll
+            for (int q = WR - 1; q >= 0; --q) {
+                uint32_t X = G[k][q] | (cin << (q == lw ? lb : 31)), p = bx[k][q];
+                X |= (X >> 1) & p;
+                p &= p >> 1;
+                X |= (X >> 2) & p;
+                p &= p >> 2;
+                X |= (X >> 4) & p;
+                p &= p >> 4;
+                X |= (X >> 8) & p;
+                p &= p >> 8;
+                X |= (X >> 16) & p;
+                moved |= X ^ G[k][q];
+                G[k][q] = X;
+                cin = q > 0 ? (X & 1u) & (bx[k][q - 1] >> 31) : 0u;
+            }
+        }
+        if (!__any_sync(0xffffffffu, moved != 0u)) break;
+    }
+#pragma unroll
+    for (int k = 0; k < 2; ++k) {
+        const int r = 2 * (int)lane + k;
+#pragma unroll
+        for (int q = 0; q < 2; ++q)
+            if (r < R && q < WR) F[r * WR + q] = G[k][q];
+    }
+}
+
 // The seed's component of the activated bonds as the bit plane F, by flood
 // fill (every thread of the CTA calls it).  Planes of NW = rows x WR words:
 // C candidates (sites in the seed's old state), Bx the +x bond of each site
@@ -154,7 +317,8 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
         }
     }
     __syncthreads();
-    // active bonds
+    // active bonds (two words side by side: their draws are independent)
+#pragma unroll 2
     for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
         const uint32_t r = wi / (uint32_t)WR;
         const int wx = (int)(wi - r * (uint32_t)WR);
@@ -181,6 +345,14 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
         F[rr * WR + (xx >> 5)] = 1u << (xx & 31);
     }
     __syncthreads();
+    if (D == 2 && R <= 64 && WR <= 2) {  // one warp holds the whole lattice
+        if (warp == 0) {
+            if (WR == 1) resident_fill_warp2<1>(F, Bx, Bd, (int)R, len);
+            else resident_fill_warp2<2>(F, Bx, Bd, (int)R, len);
+        }
+        __syncthreads();
+        return;
+    }
     const int lb = (len - 1) & 31, lw = WR - 1;
     const uint32_t rounds = (R + kResThreads - 1) / kResThreads;
     for (uint32_t it = 0; it <= NW * 32u; ++it) {  // each pass adds a site or ends the fill
@@ -417,14 +589,16 @@ __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
                     for (int k = 0; k < R.runs; ++k) {
                         const int64_t t = b * bs + k * 32 + lane;
                         const bool live = t < half;
-                        int8_site(R.m, lst, s, live ? parity_site(lst, t, colour) : 0, R.key, sweep, R.replica, R.cuts,
-                                  R.D, live, colour, tab, run0);
+                        with_dim(lst, [&](const auto& lt) {
+                            int8_site(R.m, lt, s, live ? parity_site(lt, t, colour) : 0, R.key, sweep, R.replica,
+                                      R.cuts, R.D, live, colour, tab, run0);
+                        });
                     }
                 }
                 __syncthreads();
             }
         }
-        if (R.acc) measure_int8_part(R.m, lst, s, R.acc + e * R.acc_e, 0, 1);
+        if (R.acc) with_dim(lst, [&](const auto& lt) { measure_int8_part(R.m, lt, s, R.acc + e * R.acc_e, 0, 1); });
         __syncthreads();
     }
     for (int64_t i = tid; i < n; i += kResThreads) R.state[R.st.addr(i)] = s[i];
