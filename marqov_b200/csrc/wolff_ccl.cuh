@@ -380,46 +380,64 @@ __global__ void ccl_hook(const BatchRep* __restrict__ reps, const int64_t* __res
                          const int32_t* __restrict__ block_rep, int64_t total, const CclSeed* __restrict__ seeds,
                          const BatchCtr* __restrict__ ctr, int ncluster, int c)
 {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= total) return;
-    int64_t i;
-    const int r = ccl_member(g, prefix, block_rep, i);
-    const BatchRep& R = reps[r];
-    int* lab = R.queue;
-    if (R.tile && (prefix[r] & 255) == 0) {
-        // CTA blocks are the member's tiles: only bonds that leave the tile
-        // remain, decided from the coordinates
-        const TileSite tc = ccl_tile_coords(R, (uint32_t)i);
-        i = ccl_tile_index(R, tc);
-        if (__ldcg(lab + i) < 0) return;
-        const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
-        double ai = 0.0;
-        bool have_ai = false;
-        for (int d = 0; d < R.st.dim; ++d) {
+    const int64_t base = (int64_t)blockIdx.x * blockDim.x, g = base + threadIdx.x;
+    if (base >= total) return;
+    {
+        // A CTA block that is one tile of a member: its threads take the
+        // bonds that leave the tile, one each (2D 16 x 16 tiles: the +x and +y
+        // faces, 32 bonds; 3D 8 x 8 x 4 tiles: the +x, +y and +z faces, 128
+        // bonds) -- the bonds inside the tile were united by ccl_local.
+        int64_t p0;
+        const int r = ccl_member(base, prefix, block_rep, p0);
+        const BatchRep& R = reps[r];
+        if (R.tile && (prefix[r] & 255) == 0) {  // the same member and test for the whole CTA
+            const uint32_t t = threadIdx.x;
+            if (t >= (R.tile == 2 ? 32u : 128u)) return;
+            uint32_t o;
+            int d;
+            if (R.tile == 2) {
+                d = t < 16u ? 0 : 1;
+                o = d == 0 ? (t << 4) | 15u : (15u << 4) | (t - 16u);
+            } else if (t < 32u) {
+                d = 0;
+                o = ((t >> 3) << 6) | ((t & 7u) << 3) | 7u;  // x = 7: (y, z) = (t & 7, t >> 3)
+            } else if (t < 64u) {
+                d = 1;
+                o = (((t >> 3) & 3u) << 6) | (7u << 3) | (t & 7u);  // y = 7: (x, z) = (t & 7, (t >> 3) & 3)
+            } else {
+                d = 2;
+                o = (3u << 6) | (((t >> 3) & 7u) << 3) | (t & 7u);  // z = 3: (x, y) = (t & 7, (t >> 3) & 7)
+            }
+            const TileSite tc = ccl_tile_coords(R, (uint32_t)p0 + o);
             bool same;
             int k;
             const TileSite nc = ccl_tile_fwd(R, tc, d, same, k);
-            if (same) continue;
-            const int64_t j = ccl_tile_index(R, nc);
-            if (__ldcg(lab + j) < 0) continue;
+            if (same) return;  // the periodic neighbour is in the same tile (side = tile width)
+            int* lab = R.queue;
+            const int64_t i = ccl_tile_index(R, tc), j = ccl_tile_index(R, nc);
+            if (__ldcg(lab + i) < 0 || __ldcg(lab + j) < 0) return;
+            const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
             bool act;
             if (F32) {
                 const CclSeed& sd = seeds[r];
                 const float* s = (const float*)R.s;
                 const int64_t n = rep_sites(R);
-                if (!have_ai) {
-                    ai = embed_proj(R.md.symd, s, n, i, sd.r[0], sd.r[1], sd.r[2]);
-                    have_ai = true;
-                }
+                const double ai = embed_proj(R.md.symd, s, n, i, sd.r[0], sd.r[1], sd.r[2]);
                 const double aj = embed_proj(R.md.symd, s, n, j, sd.r[0], sd.r[1], sd.r[2]);
                 act = i < j ? ccl_active_f32(R, serial, i, j, ai, aj) : ccl_active_f32(R, serial, j, i, aj, ai);
             } else {
                 act = ccl_active<false>(R, seeds[r], serial, i, j);
             }
             if (act) ccl_unite(lab, (int)i, (int)j);
+            return;
         }
-        return;
     }
+    if (g >= total) return;
+    int64_t i;
+    const int r = ccl_member(g, prefix, block_rep, i);
+    const BatchRep& R = reps[r];
+    int* lab = R.queue;
+    if (R.tile && (prefix[r] & 255) == 0) return;  // taken by its tile's face threads
     i = ccl_site(R, i);
     if (__ldcg(lab + i) < 0) return;
     const uint32_t serial = R.cluster0 + ctr->e * (uint32_t)ncluster + (uint32_t)c;
