@@ -28,6 +28,7 @@
 #include <cuda_runtime.h>
 
 #include <atomic>
+#include <type_traits>
 
 #include "batch.h"
 #include "int8_site.cuh"
@@ -120,45 +121,77 @@ __device__ __forceinline__ uint32_t res_row_step(const StencilDev& st, uint32_t 
     return res_row_of(st, (uint32_t)st.nbr((int64_t)r * st.len, 2 * d + (dir < 0 ? 1 : 0)));
 }
 
+// Rows of up to 64 sites as one integer (bit x = site x): the closure of a
+// set S along a line through the bonds A (bit x set: site x joined to site
+// x - 1) towards higher x, by one addition -- an entry bit just above a
+// flooded site ripples its carry through the run of joined sites above it
+// ((A + E) ^ A marks the bits it passes); an entry bit that the carry of a
+// lower one reaches keeps its value, so the entries are added back.  Towards
+// lower x: the same on the bit-reversed row.
+template <class T>
+__device__ __forceinline__ T row_brev(T x);
+template <>
+__device__ __forceinline__ uint32_t row_brev<uint32_t>(uint32_t x) { return __brev(x); }
+template <>
+__device__ __forceinline__ unsigned long long row_brev<unsigned long long>(unsigned long long x) { return __brevll(x); }
+template <class T>
+__device__ __forceinline__ T row_close_up(T S, T A)
+{
+    const T E = (S << 1) & A;
+    return S | E | (((A + E) ^ A) & A);
+}
+template <class T>
+__device__ __forceinline__ T row_close(T S, T Aup, T Adn)
+{
+    return row_brev(row_close_up(row_brev(row_close_up(S, Aup)), Adn));
+}
+__device__ __forceinline__ uint32_t fold32(uint32_t x) { return x; }
+__device__ __forceinline__ uint32_t fold32(unsigned long long x) { return (uint32_t)x | (uint32_t)(x >> 32); }
+
 // One warp closes the flood of a 2D lattice of at most 64 rows of at most 64
 // sites on its own (two rows per lane: rows 2 lane and 2 lane + 1), so the
 // fill needs no CTA barrier and no shared-memory round trip until it is
 // closed.  Planes as resident_cluster_bits: F (in: the seed, out: the
 // component), Bx the +x bonds, By the +y bonds (row r to row r + 1, periodic).
-// Each pass: along y by prefix scans over the lanes, upwards and downwards
-// (a lane block passes the flood from its lower to its upper row through its
-// inner bond), the periodic bond of row R - 1 to row 0, then along each row's
-// x-line by prefix scans on the bits (the periodic bond carried explicitly);
-// until a pass adds no site.
-template <int WR>  // words per row (1 or 2), fixed so that both words' scans run side by side
+// Each pass: along y, prefix scans over the lanes upwards and downwards side
+// by side from the same start (a column's vertical closure is what reaches up
+// plus what reaches down; a lane block passes the flood between its rows
+// through its inner bond), then the periodic bond of row R - 1 to row 0;
+// along x, each row closed as a line by additions, joined through its
+// periodic bond, closed again.  Until a pass adds no site.
+template <int WR>  // words per row (1 or 2)
 __device__ void resident_fill_warp2(uint32_t* F, const uint32_t* Bx, const uint32_t* By, int R, int len)
 {
+    using T = typename std::conditional<WR == 1, uint32_t, unsigned long long>::type;
     const unsigned lane = threadIdx.x & 31u;
-    const int lb = (len - 1) & 31;
-    constexpr int lw = WR - 1;
     const int ra = (R - 1) >> 1, ka = (R - 1) & 1;  // lane and slot of the last row
-    uint32_t G[2][2], bx[2][2], up[2][2], wrap[2], wb[2];
+    const T top = (T)1 << (len - 1), ends = top | (T)1;
+    T G[2], Aup[2], Adn[2];
+    uint32_t up[2][2];
+    bool wrap[2];
 #pragma unroll
     for (int k = 0; k < 2; ++k) {
         const int r = 2 * (int)lane + k;
         const bool live = r < R;
+        T g = 0, b = 0;
 #pragma unroll
-        for (int q = 0; q < 2; ++q) {
-            const bool w = live && q < WR;
-            G[k][q] = w ? F[r * WR + q] : 0u;
-            bx[k][q] = w ? Bx[r * WR + q] : 0u;
-            // the +y bond of the row, except the periodic one of the last row
-            up[k][q] = (w && r < R - 1) ? By[r * WR + q] : 0u;
-        }
-        wrap[k] = 0u;
+        for (int q = 0; q < WR; ++q)
+            if (live) {
+                g |= (T)F[r * WR + q] << (32 * q);
+                b |= (T)Bx[r * WR + q] << (32 * q);
+            }
+        wrap[k] = (b & top) != 0;  // the periodic x bond of the row, carried apart
+        b &= ~top;
+        G[k] = g;
+        Aup[k] = b << 1;
+        Adn[k] = row_brev(b);
 #pragma unroll
         for (int q = 0; q < 2; ++q)
-            if (q == lw) {  // constant indices only: the arrays stay in registers
-                wrap[k] = (bx[k][q] >> lb) & 1u;
-                bx[k][q] &= ~(1u << lb);
-            }
+            // the +y bond of the row, except the periodic one of the last row
+            up[k][q] = (live && q < WR && r < R - 1) ? By[r * WR + q] : 0u;
     }
     // the periodic y bond (row R - 1 to row 0), on every lane
+    uint32_t wb[2];
 #pragma unroll
     for (int q = 0; q < 2; ++q) {
         const uint32_t own = (2 * (int)lane + ka == R - 1 && q < WR) ? By[(R - 1) * WR + q] : 0u;
@@ -191,86 +224,45 @@ __device__ void resident_fill_warp2(uint32_t* F, const uint32_t* Bx, const uint3
     }
     for (;;) {
         uint32_t moved = 0u;
+        T Y[2] = {0, 0};
 #pragma unroll
         for (int q = 0; q < WR; ++q) {
-            const uint32_t g0 = G[0][q], g1 = G[1][q], b01 = up[0][q], b1n = up[1][q];
+            const uint32_t g0 = (uint32_t)(G[0] >> (32 * q)), g1 = (uint32_t)(G[1] >> (32 * q));
+            const uint32_t b01 = up[0][q], b1n = up[1][q];
             // within the lane first
-            uint32_t x0 = g0 | (g1 & b01), x1 = g1 | (g0 & b01);
-            // upwards: the flood at each lane block's top row
-            uint32_t X = x1;
+            const uint32_t x0 = g0 | (g1 & b01), x1 = g1 | (g0 & b01);
+            // upwards from each lane block's top row, downwards from its bottom row
+            uint32_t Xu = x1, Xd = x0;
 #pragma unroll
             for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
-                const uint32_t Xo = __shfl_up_sync(0xffffffffu, X, o);
-                if ((int)lane >= o) X |= Pu[q][s] & Xo;
+                const uint32_t Uo = __shfl_up_sync(0xffffffffu, Xu, o), Do = __shfl_down_sync(0xffffffffu, Xd, o);
+                if ((int)lane >= o) Xu |= Pu[q][s] & Uo;
+                if ((int)lane + o < 32) Xd |= Pd[q][s] & Do;
             }
-            uint32_t below = __shfl_up_sync(0xffffffffu, X, 1);
+            uint32_t below = __shfl_up_sync(0xffffffffu, Xu, 1), above = __shfl_down_sync(0xffffffffu, Xd, 1);
             if (lane == 0) below = 0u;
-            x0 |= below & pin[q];
-            x1 |= x0 & b01;
-            // downwards: the flood at each lane block's bottom row
-            X = x0;
-#pragma unroll
-            for (int s = 0, o = 1; s < 5; ++s, o <<= 1) {
-                const uint32_t Xo = __shfl_down_sync(0xffffffffu, X, o);
-                if ((int)lane + o < 32) X |= Pd[q][s] & Xo;
-            }
-            uint32_t above = __shfl_down_sync(0xffffffffu, X, 1);
             if (lane == 31) above = 0u;
-            x1 |= above & b1n;
-            x0 |= x1 & b01;
+            const uint32_t n0 = x0 | (below & pin[q]), n1 = x1 | (above & b1n);
+            uint32_t y0 = n0 | (n1 & b01), y1 = n1 | (n0 & b01);
             // the periodic bond between row R - 1 and row 0
-            const uint32_t last = __shfl_sync(0xffffffffu, ka ? x1 : x0, ra), first = __shfl_sync(0xffffffffu, x0, 0);
-            if (lane == 0) x0 |= last & wb[q];
+            const uint32_t last = __shfl_sync(0xffffffffu, ka ? y1 : y0, ra), first = __shfl_sync(0xffffffffu, y0, 0);
+            if (lane == 0) y0 |= last & wb[q];
             if ((int)lane == ra) {
-                if (ka) x1 |= first & wb[q];
-                else x0 |= first & wb[q];
+                if (ka) y1 |= first & wb[q];
+                else y0 |= first & wb[q];
             }
-            moved |= (x0 ^ g0) | (x1 ^ g1);
-            G[0][q] = x0;
-            G[1][q] = x1;
+            moved |= (y0 ^ g0) | (y1 ^ g1);
+            Y[0] |= (T)y0 << (32 * q);
+            Y[1] |= (T)y1 << (32 * q);
         }
-        // along each row's x-line (the periodic bond, bit lb of the last
-        // word, carried explicitly)
+        // along x: each row as a line, then through its periodic bond
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            uint32_t glast = 0u;
-#pragma unroll
-            for (int q = 0; q < 2; ++q)
-                if (q == lw) glast = G[k][q];
-            uint32_t cin = (glast >> lb) & wrap[k];  // site len-1 -> site 0
-#pragma unroll
-            for (int q = 0; q < WR; ++q) {
-                uint32_t X = G[k][q] | cin, p = bx[k][q] << 1;
-                X |= (X << 1) & p;
-                p &= p << 1;
-                X |= (X << 2) & p;
-                p &= p << 2;
-                X |= (X << 4) & p;
-                p &= p << 4;
-                X |= (X << 8) & p;
-                p &= p << 8;
-                X |= (X << 16) & p;
-                moved |= X ^ G[k][q];
-                G[k][q] = X;
-                cin = (X >> 31) & (bx[k][q] >> 31);
-            }
-            cin = G[k][0] & 1u & wrap[k];  // site 0 -> site len-1
-#pragma unroll
-            for (int q = WR - 1; q >= 0; --q) {
-                uint32_t X = G[k][q] | (cin << (q == lw ? lb : 31)), p = bx[k][q];
-                X |= (X >> 1) & p;
-                p &= p >> 1;
-                X |= (X >> 2) & p;
-                p &= p >> 2;
-                X |= (X >> 4) & p;
-                p &= p >> 4;
-                X |= (X >> 8) & p;
-                p &= p >> 8;
-                X |= (X >> 16) & p;
-                moved |= X ^ G[k][q];
-                G[k][q] = X;
-                cin = q > 0 ? (X & 1u) & (bx[k][q - 1] >> 31) : 0u;
-            }
+            T X = row_close(Y[k], Aup[k], Adn[k]);
+            if (wrap[k] && (X & ends)) X |= ends;
+            X = row_close(X, Aup[k], Adn[k]);
+            moved |= fold32(X ^ Y[k]);
+            G[k] = X;
         }
         if (!__any_sync(0xffffffffu, moved != 0u)) break;
     }
@@ -278,8 +270,8 @@ __device__ void resident_fill_warp2(uint32_t* F, const uint32_t* Bx, const uint3
     for (int k = 0; k < 2; ++k) {
         const int r = 2 * (int)lane + k;
 #pragma unroll
-        for (int q = 0; q < 2; ++q)
-            if (r < R && q < WR) F[r * WR + q] = G[k][q];
+        for (int q = 0; q < WR; ++q)
+            if (r < R) F[r * WR + q] = (uint32_t)(G[k] >> (32 * q));
     }
 }
 
