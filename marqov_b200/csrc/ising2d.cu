@@ -1009,7 +1009,8 @@ static const SweepConfig kConfigs[] = {
     MQV_BANDW(64, 4, 2, 2),
     MQV_BANDRS(128, 1, 2, 5), MQV_BANDRS(128, 1, 2, 6), MQV_BANDRS(128, 2, 2, 5),
     MQV_BANDRS(256, 1, 1, 3), MQV_BANDRS(256, 1, 1, 4),
-    MQV_BANDRS(64, 2, 4, 4), MQV_BANDRS(64, 2, 4, 6),
+    MQV_BANDRS(64, 2, 4, 4), MQV_BANDRS(64, 2, 4, 6), MQV_BANDRS(64, 2, 4, 8),
+    MQV_BANDRS(64, 1, 4, 6), MQV_BANDRS(64, 1, 4, 8),
 };
 constexpr int kNumConfigs = (int)(sizeof(kConfigs) / sizeof(kConfigs[0]));
 

@@ -29,6 +29,9 @@ CONFIGS = [
     ("ising2d_band_rs<256,1,1,4>", 16384),
     ("ising2d_band_rs<64,2,4,4>", 16384),
     ("ising2d_band_rs<64,2,4,6>", 16384),
+    ("ising2d_band_rs<64,2,4,8>", 16384),
+    ("ising2d_band_rs<64,1,4,6>", 16384),
+    ("ising2d_band_rs<64,1,4,8>", 16384),
     ("ising2d_sweep<512,32,4>", 8192),
     ("ising2d_sweep<256,32,4>", 8192),
     ("ising2d_sweep<512,32,2>", 8192),
