@@ -38,6 +38,7 @@ namespace mqv {
 
 constexpr int kResThreads = 512;
 constexpr int kResWarps = kResThreads / 32;
+constexpr int kResBatch = 4;  // plane words a warp handles side by side
 
 struct ResidentRun {
     ModelDev m;
@@ -297,40 +298,73 @@ __device__ void resident_cluster_bits(const StencilDev& lst, const WolffDev& w, 
     const int len = lst.len, WR = res_row_words(len), D = lst.dim;
     const uint32_t R = (uint32_t)(lst.n / len), NW = R * (uint32_t)WR;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    // candidates; the flood cleared
-    for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
-        const uint32_t r = wi / (uint32_t)WR;
-        const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
-        const bool c = x < len && s[(int64_t)r * len + x] == val;
-        const uint32_t b = __ballot_sync(0xffffffffu, c);
-        if (lane == 0) {
-            C[wi] = b;
-            F[wi] = 0u;
+    // row of word wi: a shift when the words per row are a power of two
+    const int wsh = (WR & (WR - 1)) == 0 ? __ffs(WR) - 1 : -1;
+    auto row_of_word = [&](uint32_t wi) { return wsh >= 0 ? wi >> wsh : wi / (uint32_t)WR; };
+    // Candidates, the flood cleared; then the active bonds.  A warp takes
+    // kResBatch words at a time and computes all of them before it stores
+    // any (a store to a plane would order the next word's loads behind it),
+    // so its loads and its bond draws run side by side.
+    for (uint32_t w0 = warp; w0 < NW; w0 += kResBatch * kResWarps) {
+        uint32_t cb[kResBatch];
+#pragma unroll
+        for (int k = 0; k < kResBatch; ++k) {
+            const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+            const uint32_t r = row_of_word(wi);
+            const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
+            const bool c = wi < NW && x < len && s[(int64_t)r * len + x] == val;
+            cb[k] = __ballot_sync(0xffffffffu, c);
         }
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < kResBatch; ++k) {
+                const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+                if (wi < NW) {
+                    C[wi] = cb[k];
+                    F[wi] = 0u;
+                }
+            }
     }
     __syncthreads();
-    // active bonds (two words side by side: their draws are independent)
-#pragma unroll 2
-    for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
-        const uint32_t r = wi / (uint32_t)WR;
-        const int wx = (int)(wi - r * (uint32_t)WR);
-        const int x = wx * 32 + lane;  // C bits of x >= len are clear
-        const bool ci = ((C[wi] >> lane) & 1u) != 0;
-        const uint32_t i = r * (uint32_t)len + (uint32_t)x;
-        {
+    // a bond is tested when both ends are candidates; its draw is made on
+    // every lane (the lanes of a warp issue it once either way), so the
+    // draws of a batch form straight-line code
+    for (uint32_t w0 = warp; w0 < NW; w0 += kResBatch * kResWarps) {
+        uint32_t ax[kResBatch], ad[2][kResBatch];
+#pragma unroll
+        for (int k = 0; k < kResBatch; ++k) {
+            const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+            const bool inw = wi < NW;  // uniform over the warp
+            const uint32_t r = row_of_word(wi);
+            const int wx = (int)(wi - r * (uint32_t)WR);
+            const int x = wx * 32 + lane;  // C bits of x >= len are clear
+            const bool ci = inw && ((C[inw ? wi : 0] >> lane) & 1u) != 0;
+            const uint32_t i = r * (uint32_t)len + (uint32_t)x;
             const int xj = x + 1 == len ? 0 : x + 1;
-            const bool cj = ci && ((C[r * WR + (xj >> 5)] >> (xj & 31)) & 1u);
-            const bool act = cj && wolff_int8_active(w, i, r * (uint32_t)len + (uint32_t)xj, serial, tgb, key);
-            const uint32_t b = __ballot_sync(0xffffffffu, act);
-            if (lane == 0) Bx[wi] = b;
+            const bool cx = ci && ((C[r * WR + (xj >> 5)] >> (xj & 31)) & 1u);
+            const bool dx = wolff_int8_active(w, i, r * (uint32_t)len + (uint32_t)xj, serial, tgb, key);
+            ax[k] = __ballot_sync(0xffffffffu, cx & dx);
+#pragma unroll
+            for (int d = 1; d < 3; ++d) {
+                ad[d - 1][k] = 0u;
+                if (d < D) {
+                    const uint32_t rp = res_row_step(lst, inw ? r : 0u, d, +1);
+                    const bool cj = ci && ((C[rp * WR + wx] >> lane) & 1u);
+                    const bool dj = wolff_int8_active(w, i, rp * (uint32_t)len + (uint32_t)x, serial, tgb, key);
+                    ad[d - 1][k] = __ballot_sync(0xffffffffu, cj & dj);
+                }
+            }
         }
-        for (int d = 1; d < D; ++d) {
-            const uint32_t rp = res_row_step(lst, r, d, +1);
-            const bool cj = ci && ((C[rp * WR + wx] >> lane) & 1u);
-            const bool act = cj && wolff_int8_active(w, i, rp * (uint32_t)len + (uint32_t)x, serial, tgb, key);
-            const uint32_t b = __ballot_sync(0xffffffffu, act);
-            if (lane == 0) Bd[(size_t)(d - 1) * NW + wi] = b;
-        }
+        if (lane == 0)
+#pragma unroll
+            for (int k = 0; k < kResBatch; ++k) {
+                const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+                if (wi < NW) {
+                    Bx[wi] = ax[k];
+                    if (D > 1) Bd[wi] = ad[0][k];
+                    if (D > 2) Bd[(size_t)NW + wi] = ad[1][k];
+                }
+            }
     }
     if (tid == 0) {
         const uint32_t rr = res_row_of(lst, rsite), xx = rsite - rr * (uint32_t)len;
@@ -510,13 +544,23 @@ __device__ void resident_run(const ResidentRun& R, unsigned char* smem)
                 const int8_t nv = (int8_t)s_newq;
                 const int len = lst.len, WR = res_row_words(len);
                 int cnt = 0;
-                for (uint32_t wi = warp; wi < NW; wi += kResWarps) {
-                    const uint32_t b = bF[wi];
-                    if (b) {
-                        const uint32_t r = wi / (uint32_t)WR;
-                        const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
-                        if ((b >> lane) & 1u) s[(int64_t)r * len + x] = nv;
-                        if (lane == 0) cnt += __popc(b);
+                for (uint32_t w0 = warp; w0 < NW; w0 += kResBatch * kResWarps) {
+                    uint32_t fb[kResBatch];
+#pragma unroll
+                    for (int k = 0; k < kResBatch; ++k) {
+                        const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+                        fb[k] = wi < NW ? bF[wi] : 0u;
+                    }
+#pragma unroll
+                    for (int k = 0; k < kResBatch; ++k) {
+                        const uint32_t b = fb[k];
+                        if (b) {
+                            const uint32_t wi = w0 + (uint32_t)(k * kResWarps);
+                            const uint32_t r = wi / (uint32_t)WR;
+                            const int x = (int)(wi - r * (uint32_t)WR) * 32 + lane;
+                            if ((b >> lane) & 1u) s[(int64_t)r * len + x] = nv;
+                            if (lane == 0) cnt += __popc(b);
+                        }
                     }
                 }
                 if (lane == 0 && cnt) atomicAdd(&s_size, cnt);
